@@ -1,0 +1,132 @@
+/*
+ * tenex_sm100.h — C ABI of libtenex_sm100.so, the sm_100a (B200) kernels behind
+ * the pairwise transfer-entropy (TE) path of TENEX.
+ *
+ * Every entry point:
+ *   - takes plain device pointers, sizes and an explicit cudaStream_t (passed
+ *     as void*; NULL means the legacy default stream),
+ *   - is asynchronous with respect to the host unless stated otherwise,
+ *   - returns a tenex_status (0 = OK); tenex_last_error() gives the text of the
+ *     last failure on the calling thread.
+ *
+ * Bin layout used by all TE entry points ("padded rows"):
+ *   bins[g * ld + i], g in [0, n_vars), i in [0, row_len), uint8, with
+ *   ld * 1 byte a multiple of 16 and the base pointer 16-byte aligned.
+ *   A reference tensor bin_arrs of shape (n, T, K) maps to row_len = T*K and
+ *   lag = tau*K: sample s in [0, N), N = row_len - lag, has
+ *   x_{t+tau} = row[s + lag], x_t = row[s], y_t = src_row[s]
+ *   (reference: tenex/kernels/scatter_add.py:63-79, the (t, k) samples of one
+ *   pair flattened in row-major order).
+ *
+ * Pair-free ids (reference: tenex/csrc/full_smem.cu:190-195):
+ *   p = tgt * (n_vars - 1) + src_local, src = src_local + (src_local >= tgt).
+ */
+#ifndef TENEX_SM100_H
+#define TENEX_SM100_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+enum {
+  TENEX_OK = 0,
+  TENEX_ERR_BADARG = 1,      /* invalid argument (shape, alignment, pointer) */
+  TENEX_ERR_UNSUPPORTED = 2, /* configuration this build cannot run */
+  TENEX_ERR_OOM = 3,         /* workspace too small / allocation failed */
+  TENEX_ERR_LAUNCH = 4,      /* CUDA launch or runtime error */
+  TENEX_ERR_TIMEOUT = 5,     /* a bounded device-side wait expired */
+  TENEX_ERR_BADDATA = 6      /* bin value >= n_per_var[g] or n_per_var out of range */
+};
+
+/* Output layouts of the TE entry points. */
+enum {
+  TENEX_OUT_PAIRFREE = 0, /* out[p - pair_offset], float32                         */
+  TENEX_OUT_MATRIX = 1    /* out[src * out_ld + tgt] = TE(src -> tgt), float32     */
+};
+
+typedef struct {
+  int sm_count;
+  int smem_optin;         /* cudaDevAttrMaxSharedMemoryPerBlockOptin */
+  int smem_per_sm;        /* cudaDevAttrMaxSharedMemoryPerMultiprocessor */
+  int l2_bytes;
+  int cc_major, cc_minor;
+  int max_threads_per_sm;
+} tenex_dev_info;
+
+/* Launch shape of the persistent histogram kernels (0 fields = defaults). */
+typedef struct {
+  int threads;      /* threads per CTA: 128, 256, 512 or 1024          */
+  int ctas_per_sm;  /* resident CTAs per SM (grid = sm_count * this)    */
+  int src_chunk;    /* sources per work item (one target per item)     */
+  int smem_bytes;   /* dynamic shared memory per CTA (0 = fill the SM)  */
+} tenex_te_config;
+
+int tenex_abi_version(void);
+/* Copies the last error text of this thread into buf (NUL-terminated). */
+int tenex_last_error(char* buf, size_t len);
+/* Replaces get_smem_optin (tenex/csrc/full_smem.cu:150-155) and the
+ * query_smem_optin helper (tenex/kernels/__init__.py:44-71). */
+int tenex_device_query(int device, tenex_dev_info* info);
+
+/* Bytes of device workspace the TE / surrogate entry points need. */
+size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len);
+
+/* Reads back the data-validation word a previous TE call left in the
+ * workspace (synchronises `stream`). Returns TENEX_ERR_BADDATA if any bin value
+ * was >= its gene's n_per_var, else TENEX_OK. */
+int tenex_workspace_status(const void* workspace, void* stream);
+
+/* Multi-bin TE over a contiguous pair-free id range, exact integer counts in
+ * shared memory, fused count -> marginal -> TE reduction.
+ * Replaces te_smem_launch_pairfree (tenex/csrc/full_smem.cu:350-381) and
+ * te_adaptive_smem_kernel_pairfree's launcher (tenex/kernels/adaptive_smem.py:1029-1107):
+ * one kernel covers both Full-SMEM (uniform b) and Adaptive-SMEM (per-gene b).
+ * b_max = max(n_per_var) (the reference's B argument), 1..255; every
+ * n_per_var[g] must lie in [1, b_max] and every bin of gene g below n_per_var[g]
+ * (checked on the device; see tenex_workspace_status). */
+int tenex_te_pairfree(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                      int b_max, int n_vars, int64_t row_len, int64_t lag,
+                      int64_t pair_offset, int64_t n_pairs,
+                      float* out, int out_mode, int64_t out_ld,
+                      void* workspace, size_t workspace_bytes,
+                      const tenex_te_config* cfg, void* stream);
+
+/* Same kernel, additionally exporting the raw int32 joint counts of every pair
+ * for parity checks: counts[(p - pair_offset) * counts_stride + xt1*bt*bs + xt*bs + yt]
+ * (the index of tenex/csrc/adaptive_smem.cu:77). */
+int tenex_te_pairfree_counts(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                             int b_max, int n_vars, int64_t row_len, int64_t lag,
+                             int64_t pair_offset, int64_t n_pairs,
+                             float* out, int32_t* counts, int64_t counts_stride,
+                             void* workspace, size_t workspace_bytes,
+                             const tenex_te_config* cfg, void* stream);
+
+/* Surrogate accumulation: TE of already-shuffled bins for the pair range, then
+ * sum[s*n+t] += te, sumsq[s*n+t] += te^2 (te rounded to float32 first, then
+ * widened), count_ge[s*n+t] += (te >= observed[s*n+t]).
+ * Replaces the per-surrogate accumulator update of
+ * tenex/inference/surrogate_test.py:389-406. */
+int tenex_surrogate_accumulate(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                               int b_max, int n_vars, int64_t row_len, int64_t lag,
+                               int64_t pair_offset, int64_t n_pairs,
+                               const float* observed, double* sum, double* sumsq,
+                               int32_t* count_ge,
+                               void* workspace, size_t workspace_bytes,
+                               const tenex_te_config* cfg, void* stream);
+
+/* Block shuffle of every gene's time axis (tenex/inference/surrogate_test.py:107-162):
+ * out[g, t*K + k] = in[g, (perm[g, t/bl]*bl + t%bl)*K + k] for t < n_blocks*bl,
+ * tail t >= n_blocks*bl unchanged. bl = 1 with n_blocks = T is the random shuffle.
+ * perm is int32 (n_vars, n_blocks) for one surrogate. */
+int tenex_block_shuffle(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T, int K,
+                        const int32_t* perm, int n_blocks, int block_length,
+                        uint8_t* out, int64_t out_ld, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TENEX_SM100_H */

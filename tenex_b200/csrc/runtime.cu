@@ -1,0 +1,152 @@
+// runtime.cu — status/error text, device attributes, and the small data-movement
+// kernels of the C ABI (block shuffle).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "common.cuh"
+
+namespace tenex {
+
+static thread_local char g_last_error[1024] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return TENEX_OK;
+  return fail(TENEX_ERR_LAUNCH, "%s: %s (%s)", what, cudaGetErrorString(e),
+              cudaGetErrorName(e));
+}
+
+int check_launch(const char* what) { return check_cuda(cudaGetLastError(), what); }
+
+int current_device_attr(DevAttr* out) {
+  static std::mutex mu;
+  static DevAttr cache[64];
+  static bool have[64] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return check_cuda(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail(TENEX_ERR_UNSUPPORTED, "device index %d", dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (!have[dev]) {
+    DevAttr a{};
+    e = cudaDeviceGetAttribute(&a.sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+      e = cudaDeviceGetAttribute(&a.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess)
+      e = cudaDeviceGetAttribute(&a.smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
+                                 dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&a.l2_bytes, cudaDevAttrL2CacheSize, dev);
+    if (e == cudaSuccess)
+      e = cudaDeviceGetAttribute(&a.max_threads_per_sm,
+                                 cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    if (e != cudaSuccess) return check_cuda(e, "cudaDeviceGetAttribute");
+    cache[dev] = a;
+    have[dev] = true;
+  }
+  *out = cache[dev];
+  return TENEX_OK;
+}
+
+// out[g, t*K+k] = in[g, (perm[g, t/bl]*bl + t%bl)*K + k] for t < n_blocks*bl; tail copied.
+// Grid: (ceil(T*K / 256 / 4), n_vars); each thread moves 4 consecutive bytes.
+__global__ void block_shuffle_kernel(const uint8_t* __restrict__ in, int64_t in_ld, int n,
+                                     int64_t T, int K, const int32_t* __restrict__ perm,
+                                     int n_blocks, int bl, uint8_t* __restrict__ out,
+                                     int64_t out_ld) {
+  const int g = blockIdx.y;
+  const int64_t row = T * K;
+  const int64_t head = (int64_t)n_blocks * bl * K;
+  const uint8_t* src = in + (int64_t)g * in_ld;
+  uint8_t* dst = out + (int64_t)g * out_ld;
+  const int32_t* pg = perm + (int64_t)g * n_blocks;
+  const int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int64_t i = i0 + u;
+    if (i >= row) break;
+    int64_t j = i;
+    if (i < head) {
+      const int64_t t = i / K, k = i - t * K;
+      const int64_t b = t / bl, off = t - b * bl;
+      int pb = pg[b];
+      if ((unsigned)pb >= (unsigned)n_blocks) pb = (int)b;  // out-of-range entry: identity
+      j = ((int64_t)pb * bl + off) * K + k;
+    }
+    dst[i] = src[j];
+  }
+}
+
+}  // namespace tenex
+
+using namespace tenex;
+
+extern "C" int tenex_abi_version(void) { return 1; }
+
+extern "C" int tenex_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return TENEX_ERR_BADARG;
+  strncpy(buf, g_last_error, len - 1);
+  buf[len - 1] = '\0';
+  return TENEX_OK;
+}
+
+extern "C" int tenex_device_query(int device, tenex_dev_info* info) {
+  if (!info) return fail(TENEX_ERR_BADARG, "info is NULL");
+  int prev = 0;
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e != cudaSuccess) return check_cuda(e, "cudaGetDevice");
+  if (device != prev) {
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return check_cuda(e, "cudaSetDevice");
+  }
+  DevAttr a;
+  int st = current_device_attr(&a);
+  int major = 0, minor = 0;
+  if (st == TENEX_OK) {
+    e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device);
+    if (e != cudaSuccess) st = check_cuda(e, "cudaDeviceGetAttribute");
+  }
+  if (device != prev) cudaSetDevice(prev);
+  if (st) return st;
+  info->sm_count = a.sm_count;
+  info->smem_optin = a.smem_optin;
+  info->smem_per_sm = a.smem_per_sm;
+  info->l2_bytes = a.l2_bytes;
+  info->cc_major = major;
+  info->cc_minor = minor;
+  info->max_threads_per_sm = a.max_threads_per_sm;
+  return TENEX_OK;
+}
+
+extern "C" int tenex_block_shuffle(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T, int K,
+                                   const int32_t* perm, int n_blocks, int block_length,
+                                   uint8_t* out, int64_t out_ld, void* stream) {
+  if (!in || !out || !perm) return fail(TENEX_ERR_BADARG, "in, out and perm must be non-NULL");
+  if (n_vars < 1 || T < 1 || K < 1) return fail(TENEX_ERR_BADARG, "empty bins");
+  if (block_length < 1 || n_blocks < 1 || (int64_t)n_blocks * block_length > T)
+    return fail(TENEX_ERR_BADARG, "need n_blocks*block_length <= T (n_blocks=%d, bl=%d, T=%lld)",
+                n_blocks, block_length, (long long)T);
+  if (in_ld < T * K || out_ld < T * K)
+    return fail(TENEX_ERR_BADARG, "row strides must be >= T*K");
+  if (in == out) return fail(TENEX_ERR_BADARG, "block shuffle cannot run in place");
+  const int64_t row = T * K;
+  const int64_t gx = (row + 1023) / 1024;
+  if (gx > 0x7fffffff || n_vars > 65535)
+    return fail(TENEX_ERR_UNSUPPORTED, "grid too large (row=%lld, n_vars=%d)", (long long)row,
+                n_vars);
+  dim3 grid((unsigned)gx, (unsigned)n_vars);
+  block_shuffle_kernel<<<grid, 256, 0, as_stream(stream)>>>(in, in_ld, n_vars, T, K, perm,
+                                                             n_blocks, block_length, out, out_ld);
+  return check_launch("block_shuffle_kernel");
+}

@@ -1,0 +1,603 @@
+// te_pair.cu — persistent pair-tile transfer-entropy kernel for multi-bin data.
+//
+// What it computes (reference: tenex/csrc/full_smem.cu:166-276 and
+// tenex/csrc/adaptive_smem.cu:158-273): for every ordered pair (source y ->
+// target x) in a pair-free id range, the joint counts
+//   c3[xt1, xt, yt] = #{s < N : x[s+lag] = xt1, x[s] = xt, y[s] = yt}
+// (exact int), the marginals c1[xt], c2a[xt1,xt], c2b[xt,yt], and
+//   TE = (1/N) * sum_{c3>0} c3 * log2(c3*c1 / (c2a*c2b)).
+//
+// How (B200 design, not the reference's one-CTA-per-pair layout):
+//   * Work item = one target and a chunk of W sources. The CTA stages the
+//     target's joint state z[s] = x[s+lag]*b_t + x[s] into shared memory ONCE
+//     per item (u8 when b_t <= 16, else u16) together with the target-only
+//     marginals c2a and c1, so sources never re-read the target.
+//   * Shared memory left after the target block is cut into histogram slots
+//     sized for this item (b_t^2 * b_s cells). A slot belongs to a group of G
+//     warps (G = 1 for the common small-b pairs: warp-private histograms, no
+//     cross-warp contention; G > 1 only for heavy pairs that need a large
+//     slot). Counters are 16-bit halves of 32-bit words when N < 65536, so a
+//     38x38x38 histogram needs 110 KB instead of 220 KB.
+//   * The source row is streamed from L2/HBM with 16-byte non-temporal loads;
+//     each sample is one shared-memory atomic add.
+//   * The entropy pass reads each slot column once to form c2b, once more to
+//     form the terms, and clears the slot for the next source (no separate
+//     zeroing pass).
+//   * Items are handed out by an atomic ticket in chunk-major order, so the
+//     CTAs resident at one moment share a small set of source rows in L2.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace tenex {
+
+enum { kOutPairfree = 0, kOutMatrix = 1, kOutStats = 2 };
+
+struct TeParams {
+  const uint8_t* bins;
+  int64_t ld;
+  const int32_t* npv;
+  int n;
+  int N;          // samples per pair (row_len - lag), < 2^31
+  int lag;
+  int64_t p0, p1;  // pair-free id range [p0, p1)
+  int t_first;
+  int n_targets;
+  int W;          // sources per item
+  int n_chunks;   // items per target
+  int64_t n_items;
+  int zbytes;     // bytes per z entry reserved (1 or 2)
+  int bmax;       // max n_per_var over the genes (sizes the c2a/c1 region)
+  int smem_bytes;
+  int out_mode;
+  float* out;
+  int64_t out_ld;
+  const float* obs;
+  double* sum;
+  double* sumsq;
+  int32_t* cnt_ge;
+  int32_t* counts_dbg;
+  int64_t counts_stride;
+  WsHeader* ws;
+};
+
+namespace {
+
+constexpr int kMaxWarps = 32;
+
+struct SmemLayout {
+  int z_off, c2a_off, c1_off, red_off, misc_off, slot_off;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int N, int zbytes, int bmax) {
+  SmemLayout L;
+  int off = 0;
+  L.misc_off = off;  off += 64;                               // int misc[16]
+  L.red_off = off;   off += kMaxWarps * 8;                    // double red[32]
+  L.c1_off = off;    off += (int)round_up((int64_t)bmax * 4, 16);
+  L.c2a_off = off;   off += (int)round_up((int64_t)bmax * bmax * 4, 16);
+  L.z_off = off;     off += (int)round_up((int64_t)N * zbytes, 16);
+  L.slot_off = off;
+  return L;
+}
+
+// One 16-sample step of the histogram: 16 source bins (yv) and 16 target
+// states. PACK16: 16-bit counters, word = z*hb + (y>>1), half = y&1.
+template <bool PACK16>
+__device__ __forceinline__ void hist_add(uint32_t* slot, uint32_t z, uint32_t y, uint32_t bs,
+                                         uint32_t hb) {
+  if (PACK16) {
+    atomicAdd(slot + (z * hb + (y >> 1)), 1u << ((y & 1u) << 4));
+  } else {
+    atomicAdd(slot + (z * bs + y), 1u);
+  }
+}
+
+template <bool PACK16>
+__device__ __forceinline__ void hist16_z8(uint32_t* slot, uint4 yv, uint4 zv, uint32_t bs,
+                                          uint32_t hb) {
+  const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
+  const uint32_t zs[4] = {zv.x, zv.y, zv.z, zv.w};
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
+      uint32_t z = __byte_perm(zs[w], 0, 0x4440 + b);
+      hist_add<PACK16>(slot, z, y, bs, hb);
+    }
+  }
+}
+
+template <bool PACK16>
+__device__ __forceinline__ void hist16_z16(uint32_t* slot, uint4 yv, uint4 za, uint4 zb,
+                                           uint32_t bs, uint32_t hb) {
+  const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
+  const uint32_t zs[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
+      uint32_t zw = zs[(w * 4 + b) >> 1];
+      uint32_t z = (b & 1) ? (zw >> 16) : (zw & 0xffffu);
+      hist_add<PACK16>(slot, z, y, bs, hb);
+    }
+  }
+}
+
+__device__ __forceinline__ float te_term(float c3, float c1, float c2a, float c2b) {
+  // Same expression as the reference's per-cell term (full_smem.cu:124-127):
+  // c3 * log2((c3*c1) / (c2a*c2b)), with IEEE division and an accurate log2.
+  return c3 * log2f(__fdiv_rn(c3 * c1, c2a * c2b));
+}
+
+}  // namespace
+
+template <bool PACK16>
+__global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const SmemLayout SL = smem_layout(P.N, P.zbytes, P.bmax);
+  int* misc = reinterpret_cast<int*>(smem + SL.misc_off);
+  double* red = reinterpret_cast<double*>(smem + SL.red_off);
+  float* c1s = reinterpret_cast<float*>(smem + SL.c1_off);
+  float* c2as = reinterpret_cast<float*>(smem + SL.c2a_off);
+  int* c2a_cnt = reinterpret_cast<int*>(smem + SL.c2a_off);
+  unsigned char* zsm = smem + SL.z_off;
+  uint32_t* slots = reinterpret_cast<uint32_t*>(smem + SL.slot_off);
+  const int slot_region = P.smem_bytes - SL.slot_off;
+
+  const int tid = threadIdx.x;
+  const int nthreads = blockDim.x;
+  const int warp = tid >> 5;
+  const int n_warps = nthreads >> 5;
+  const int nm1 = P.n - 1;
+  const int N = P.N;
+
+  if (*(volatile int*)&P.ws->bad_data != 0) return;  // validation failed: do nothing
+
+  for (;;) {
+    if (tid == 0) misc[0] = (int)atomicAdd(&P.ws->ticket, 1u);
+    __syncthreads();
+    const int64_t q = (int64_t)misc[0];
+    if (q >= P.n_items) break;
+    const int chunk = (int)(q / P.n_targets);
+    const int tgt = P.t_first + (int)(q % P.n_targets);
+    const int64_t base = (int64_t)tgt * nm1;
+    int64_t lo = base + (int64_t)chunk * P.W;
+    int64_t hi = base + min((int64_t)(chunk + 1) * P.W, (int64_t)nm1);
+    lo = max(lo, P.p0);
+    hi = min(hi, P.p1);
+    if (lo >= hi) {
+      __syncthreads();
+      continue;
+    }
+    const int n_src = (int)(hi - lo);
+    const int bt = P.npv[tgt];
+
+    // ---- max b_s over the item's sources --------------------------------
+    unsigned my_max = 1;
+    for (int r = tid; r < n_src; r += nthreads) {
+      int sl = (int)(lo + r - base);
+      int src = sl + (sl >= tgt);
+      my_max = max(my_max, (unsigned)P.npv[src]);
+    }
+    my_max = dev::warp_max(my_max);
+    if ((tid & 31) == 0) reinterpret_cast<unsigned*>(red)[warp] = my_max;
+    for (int i = tid; i < bt * bt; i += nthreads) c2a_cnt[i] = 0;
+    __syncthreads();
+    if (tid < 32) {
+      unsigned v = tid < n_warps ? reinterpret_cast<unsigned*>(red)[tid] : 1u;
+      v = dev::warp_max(v);
+      if (tid == 0) misc[1] = (int)v;
+    }
+
+    // ---- stage the target: z[s] = x[s+lag]*bt + x[s], and c2a counts ------
+    const uint8_t* trow = P.bins + (int64_t)tgt * P.ld;
+    const bool z8 = bt <= 16;
+    if (z8) {
+      for (int s = tid; s < N; s += nthreads) {
+        uint32_t z = (uint32_t)trow[s + P.lag] * bt + trow[s];
+        zsm[s] = (unsigned char)z;
+        atomicAdd(&c2a_cnt[z], 1);
+      }
+    } else {
+      uint16_t* z16 = reinterpret_cast<uint16_t*>(zsm);
+      for (int s = tid; s < N; s += nthreads) {
+        uint32_t z = (uint32_t)trow[s + P.lag] * bt + trow[s];
+        z16[s] = (uint16_t)z;
+        atomicAdd(&c2a_cnt[z], 1);
+      }
+    }
+    __syncthreads();
+    const int bsmax = misc[1];
+    for (int i = tid; i < bt * bt; i += nthreads) c2as[i] = (float)c2a_cnt[i];
+    __syncthreads();
+    for (int j = tid; j < bt; j += nthreads) {
+      float s = 0.f;
+      for (int i = 0; i < bt; ++i) s += c2as[i * bt + j];
+      c1s[j] = s;
+    }
+
+    // ---- carve slots ----------------------------------------------------
+    const int hbmax = PACK16 ? (bsmax + 1) >> 1 : bsmax;
+    const int slot_words = (int)round_up((int64_t)bt * bt * hbmax, 4);
+    const int fit = slot_region / (slot_words * 4);
+    if (fit < 1) {
+      if (tid == 0) atomicExch(&P.ws->bad_item, 1);
+      __syncthreads();
+      continue;
+    }
+    int G = 1;
+    while (n_warps / G > fit) G <<= 1;
+    while (G > 1 && G < n_warps && n_warps / G > 15) G <<= 1;
+    const int n_groups = n_warps / G;
+    const int g = warp / G;
+    const int gthreads = G * 32;
+    const int lane_g = tid - g * gthreads;
+    uint32_t* slot = slots + (int64_t)g * slot_words;
+    // slots start zeroed: clear every slot word once per item (later sources
+    // are cleared by the entropy pass).
+    for (int i = tid; i < n_groups * slot_words; i += nthreads) slots[i] = 0u;
+    __syncthreads();
+
+    const int nvec = N >> 4;
+
+    for (int r = g; r < n_src; r += n_groups) {
+      const int64_t p = lo + r;
+      const int sl = (int)(p - base);
+      const int src = sl + (sl >= tgt);
+      const uint32_t bs = (uint32_t)P.npv[src];
+      const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
+      const uint8_t* srow = P.bins + (int64_t)src * P.ld;
+      const uint4* yv = reinterpret_cast<const uint4*>(srow);
+
+      // -- histogram ------------------------------------------------------
+      if (z8) {
+        const uint4* zv = reinterpret_cast<const uint4*>(zsm);
+        int v = lane_g;
+        if (v < nvec) {
+          uint4 ycur = dev::ldg_nc_v4(yv + v);
+          for (; v < nvec; v += gthreads) {
+            const int vn = v + gthreads;
+            uint4 ynext = ycur;
+            if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
+            hist16_z8<PACK16>(slot, ycur, zv[v], bs, hb);
+            ycur = ynext;
+          }
+        }
+        for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
+          hist_add<PACK16>(slot, zsm[s], srow[s], bs, hb);
+      } else {
+        const uint4* zv = reinterpret_cast<const uint4*>(zsm);
+        const uint16_t* z16 = reinterpret_cast<const uint16_t*>(zsm);
+        int v = lane_g;
+        if (v < nvec) {
+          uint4 ycur = dev::ldg_nc_v4(yv + v);
+          for (; v < nvec; v += gthreads) {
+            const int vn = v + gthreads;
+            uint4 ynext = ycur;
+            if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
+            hist16_z16<PACK16>(slot, ycur, zv[2 * v], zv[2 * v + 1], bs, hb);
+            ycur = ynext;
+          }
+        }
+        for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
+          hist_add<PACK16>(slot, z16[s], srow[s], bs, hb);
+      }
+      if (G == 1) __syncwarp(); else dev::named_bar(1 + g, gthreads);
+
+      // -- optional raw-count export (parity checks only) ------------------
+      if (P.counts_dbg != nullptr) {
+        int32_t* cd = P.counts_dbg + (p - P.p0) * P.counts_stride;
+        const int ncell = bt * bt * (int)bs;
+        for (int c = lane_g; c < ncell; c += gthreads) {
+          const int z = c / (int)bs, y = c - z * (int)bs;
+          uint32_t v;
+          if (PACK16) {
+            uint32_t w = slot[z * hb + (y >> 1)];
+            v = (y & 1) ? (w >> 16) : (w & 0xffffu);
+          } else {
+            v = slot[z * bs + y];
+          }
+          cd[c] = (int32_t)v;
+        }
+        if (G == 1) __syncwarp(); else dev::named_bar(1 + g, gthreads);
+      }
+
+      // -- entropy pass: column (xt=j, word wk) over xt1=i ----------------
+      float acc = 0.f;
+      const int ncols = bt * (int)hb;
+      for (int col = lane_g; col < ncols; col += gthreads) {
+        const int j = col / (int)hb;
+        const int wk = col - j * (int)hb;
+        uint32_t s = 0;
+        for (int i = 0; i < bt; ++i) s += slot[(i * bt + j) * hb + wk];
+        const float c1j = c1s[j];
+        if (PACK16) {
+          const float c2b_lo = (float)(s & 0xffffu), c2b_hi = (float)(s >> 16);
+          for (int i = 0; i < bt; ++i) {
+            const int idx = (i * bt + j) * hb + wk;
+            const uint32_t w = slot[idx];
+            slot[idx] = 0u;
+            if (w != 0u) {
+              const float c2a = c2as[i * bt + j];
+              const uint32_t clo = w & 0xffffu, chi = w >> 16;
+              if (clo) acc += te_term((float)clo, c1j, c2a, c2b_lo);
+              if (chi) acc += te_term((float)chi, c1j, c2a, c2b_hi);
+            }
+          }
+        } else {
+          const float c2b = (float)s;
+          for (int i = 0; i < bt; ++i) {
+            const int idx = (i * bt + j) * hb + wk;
+            const uint32_t w = slot[idx];
+            slot[idx] = 0u;
+            if (w != 0u) acc += te_term((float)w, c1j, c2as[i * bt + j], c2b);
+          }
+        }
+      }
+      double tot = dev::warp_sum((double)acc);
+      if (G > 1) {
+        if ((tid & 31) == 0) red[warp] = tot;
+        dev::named_bar(1 + g, gthreads);
+        if (lane_g == 0) {
+          tot = 0.0;
+          for (int w = 0; w < G; ++w) tot += red[g * G + w];
+        }
+      }
+      if (lane_g == 0) {
+        const float te = (float)(tot / (double)N);
+        if (P.out_mode == kOutPairfree) {
+          P.out[p - P.p0] = te;
+        } else if (P.out_mode == kOutMatrix) {
+          P.out[(int64_t)src * P.out_ld + tgt] = te;
+        } else {
+          const int64_t m = (int64_t)src * P.n + tgt;
+          const double td = (double)te;
+          P.sum[m] += td;
+          P.sumsq[m] += td * td;
+          P.cnt_ge[m] += (te >= P.obs[m]) ? 1 : 0;
+        }
+      }
+      if (G == 1) __syncwarp(); else dev::named_bar(1 + g, gthreads);
+    }
+    __syncthreads();
+  }
+}
+
+// Validation: every bin of gene g in [0, row_len) must be < n_per_var[g], and
+// n_per_var[g] in [1, b_max]. Sets ws->bad_data otherwise. One CTA per gene.
+__global__ void validate_bins_kernel(const uint8_t* bins, int64_t ld, const int32_t* npv,
+                                     int b_max, int n, int64_t row_len, WsHeader* ws) {
+  const int g = blockIdx.x;
+  if (g >= n) return;
+  const int b = npv[g];
+  if (b < 1 || b > b_max) {
+    if (threadIdx.x == 0) atomicExch(&ws->bad_data, 1);
+    return;
+  }
+  const uint8_t* row = bins + (int64_t)g * ld;
+  const int64_t nvec = row_len >> 4;
+  bool bad = false;
+  const uint4* rv = reinterpret_cast<const uint4*>(row);
+  for (int64_t v = threadIdx.x; v < nvec; v += blockDim.x) {
+    uint4 q = __ldg(rv + v);
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+      for (int bb = 0; bb < 4; ++bb) bad |= ((w[k] >> (8 * bb)) & 0xffu) >= (uint32_t)b;
+    }
+  }
+  for (int64_t i = (nvec << 4) + threadIdx.x; i < row_len; i += blockDim.x) bad |= row[i] >= b;
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(&ws->bad_data, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+struct TeLaunch {
+  int threads, grid, smem;
+  bool pack16;
+};
+
+static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const DevAttr& A,
+                          TeLaunch* L, int* zbytes_out, int max_slot_bytes) {
+  int threads = (cfg && cfg->threads) ? cfg->threads : 512;
+  int cps = (cfg && cfg->ctas_per_sm) ? cfg->ctas_per_sm : 1;
+  if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
+    return fail(TENEX_ERR_BADARG, "threads must be 128, 256, 512 or 1024 (got %d)", threads);
+  if (cps < 1 || cps * threads > A.max_threads_per_sm)
+    return fail(TENEX_ERR_BADARG, "ctas_per_sm=%d x threads=%d exceeds %d threads/SM", cps,
+                threads, A.max_threads_per_sm);
+  int smem = (cfg && cfg->smem_bytes) ? cfg->smem_bytes : 0;
+  if (smem == 0) {
+    // fill the SM: per-SM shared memory minus the 1 KB the driver reserves per CTA
+    smem = (A.smem_per_sm / cps) - 1024;
+    if (smem > A.smem_optin) smem = A.smem_optin;
+  }
+  if (smem > A.smem_optin)
+    return fail(TENEX_ERR_BADARG, "smem_bytes=%d exceeds the device opt-in %d", smem,
+                A.smem_optin);
+  smem = smem / 16 * 16;
+  SmemLayout SL = smem_layout(P.N, *zbytes_out, P.bmax);
+  if (SL.slot_off + max_slot_bytes > smem)
+    return fail(TENEX_ERR_UNSUPPORTED,
+                "histogram of the largest pair (%d B) plus the staged target (%d B) does not "
+                "fit %d B of shared memory; coarsen bins or shorten the series",
+                max_slot_bytes, SL.slot_off, smem);
+  L->threads = threads;
+  L->smem = smem;
+  L->grid = A.sm_count * cps;
+  return TENEX_OK;
+}
+
+}  // namespace tenex
+
+using namespace tenex;
+
+extern "C" size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len) {
+  (void)n_vars;
+  (void)row_len;
+  return sizeof(WsHeader);
+}
+
+extern "C" int tenex_workspace_status(const void* workspace, void* stream) {
+  if (!workspace) return fail(TENEX_ERR_BADARG, "workspace is NULL");
+  WsHeader h;
+  cudaError_t e = cudaMemcpyAsync(&h, workspace, sizeof(h), cudaMemcpyDeviceToHost,
+                                  as_stream(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+  if (e != cudaSuccess) return check_cuda(e, "tenex_workspace_status");
+  if (h.bad_data) return fail(TENEX_ERR_BADDATA,
+                              "a bin value was >= its gene's n_per_var, or n_per_var was "
+                              "outside [1, 255]; no TE was computed");
+  if (h.bad_item) return fail(TENEX_ERR_UNSUPPORTED,
+                              "a work item's histogram did not fit shared memory");
+  return TENEX_OK;
+}
+
+// Common driver of the three TE entry points.
+static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max, int n,
+                  int64_t row_len, int64_t lag, int64_t p0, int64_t n_pairs, int out_mode,
+                  float* out, int64_t out_ld, const float* obs, double* sum, double* sumsq,
+                  int32_t* cnt, int32_t* counts, int64_t counts_stride, void* workspace,
+                  size_t ws_bytes, const tenex_te_config* cfg, void* stream_) {
+  cudaStream_t stream = as_stream(stream_);
+  if (!bins || !npv) return fail(TENEX_ERR_BADARG, "bins and n_per_var must be non-NULL");
+  if (n < 2) return fail(TENEX_ERR_BADARG, "n_vars must be >= 2 (got %d)", n);
+  if (b_max < 1 || b_max > 255)
+    return fail(TENEX_ERR_UNSUPPORTED, "b_max=%d: the shared-memory kernel handles 1..255",
+                b_max);
+  if (lag < 1 || row_len <= lag)
+    return fail(TENEX_ERR_BADARG, "need 1 <= lag < row_len (lag=%lld, row_len=%lld)",
+                (long long)lag, (long long)row_len);
+  if (row_len - lag >= ((int64_t)1 << 24))
+    return fail(TENEX_ERR_UNSUPPORTED,
+                "N=%lld samples: float32 marginals are exact only below 2^24",
+                (long long)(row_len - lag));
+  if (ld < row_len || (ld % 16) != 0 || (reinterpret_cast<uintptr_t>(bins) % 16) != 0)
+    return fail(TENEX_ERR_BADARG,
+                "bins rows must be 16-byte aligned with ld %% 16 == 0 and ld >= row_len "
+                "(ld=%lld, row_len=%lld)",
+                (long long)ld, (long long)row_len);
+  const int64_t total = (int64_t)n * (n - 1);
+  if (p0 < 0 || n_pairs < 0 || p0 + n_pairs > total)
+    return fail(TENEX_ERR_BADARG, "pair range [%lld, %lld) outside [0, %lld)", (long long)p0,
+                (long long)(p0 + n_pairs), (long long)total);
+  if (out_mode != kOutStats && !out)
+    return fail(TENEX_ERR_BADARG, "out must be non-NULL");
+  if (out_mode == kOutMatrix && out_ld < n)
+    return fail(TENEX_ERR_BADARG, "out_ld (%lld) must be >= n_vars", (long long)out_ld);
+  if (out_mode == kOutStats && (!obs || !sum || !sumsq || !cnt))
+    return fail(TENEX_ERR_BADARG, "observed, sum, sumsq and count_ge must be non-NULL");
+  if (!workspace || ws_bytes < sizeof(WsHeader))
+    return fail(TENEX_ERR_OOM, "workspace must be >= %zu bytes", sizeof(WsHeader));
+  if (n_pairs == 0) return TENEX_OK;
+  DevAttr A;
+  int st = current_device_attr(&A);
+  if (st) return st;
+
+  TeParams P{};
+  P.bins = bins;
+  P.ld = ld;
+  P.npv = npv;
+  P.n = n;
+  P.N = (int)(row_len - lag);
+  P.lag = (int)lag;
+  P.p0 = p0;
+  P.p1 = p0 + n_pairs;
+  P.t_first = (int)(p0 / (n - 1));
+  const int t_last = (int)((P.p1 - 1) / (n - 1));
+  P.n_targets = t_last - P.t_first + 1;
+  P.W = (cfg && cfg->src_chunk) ? cfg->src_chunk : 128;
+  if (P.W < 1) return fail(TENEX_ERR_BADARG, "src_chunk must be >= 1");
+  P.n_chunks = (n - 1 + P.W - 1) / P.W;
+  P.n_items = (int64_t)P.n_targets * P.n_chunks;
+  P.bmax = b_max;
+  P.zbytes = b_max <= 16 ? 1 : 2;
+  P.out_mode = out_mode;
+  P.out = out;
+  P.out_ld = out_ld;
+  P.obs = obs;
+  P.sum = sum;
+  P.sumsq = sumsq;
+  P.cnt_ge = cnt;
+  P.counts_dbg = counts;
+  P.counts_stride = counts_stride;
+  P.ws = reinterpret_cast<WsHeader*>(workspace);
+
+  const bool pack16 = P.N < 65536;
+  const int64_t hb = pack16 ? (b_max + 1) / 2 : b_max;
+  const int64_t worst_slot = round_up((int64_t)b_max * b_max * hb, 4) * 4;
+  if (counts && counts_stride < (int64_t)b_max * b_max * b_max)
+    return fail(TENEX_ERR_BADARG, "counts_stride must be >= b_max^3");
+  TeLaunch L{};
+  st = plan_te_launch(P, cfg, A, &L, &P.zbytes, (int)std::min<int64_t>(worst_slot, 1 << 30));
+  if (st) return st;
+  P.smem_bytes = L.smem;
+  int64_t grid = L.grid;
+  if (grid > P.n_items) grid = P.n_items;
+
+  cudaError_t e = cudaMemsetAsync(workspace, 0, sizeof(WsHeader), stream);
+  if (e != cudaSuccess) return check_cuda(e, "workspace reset");
+  validate_bins_kernel<<<n, 256, 0, stream>>>(bins, ld, npv, b_max, n, row_len, P.ws);
+  st = check_launch("validate_bins_kernel");
+  if (st) return st;
+  if (pack16) {
+    e = cudaFuncSetAttribute(te_pair_tile_kernel<true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem);
+    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+    te_pair_tile_kernel<true><<<(int)grid, L.threads, L.smem, stream>>>(P);
+  } else {
+    e = cudaFuncSetAttribute(te_pair_tile_kernel<false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem);
+    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+    te_pair_tile_kernel<false><<<(int)grid, L.threads, L.smem, stream>>>(P);
+  }
+  return check_launch("te_pair_tile_kernel");
+}
+
+extern "C" int tenex_te_pairfree(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                                 int b_max, int n_vars, int64_t row_len, int64_t lag,
+                                 int64_t pair_offset, int64_t n_pairs, float* out,
+                                 int out_mode, int64_t out_ld, void* workspace,
+                                 size_t workspace_bytes, const tenex_te_config* cfg,
+                                 void* stream) {
+  if (out_mode != TENEX_OUT_PAIRFREE && out_mode != TENEX_OUT_MATRIX)
+    return fail(TENEX_ERR_BADARG, "out_mode must be TENEX_OUT_PAIRFREE or TENEX_OUT_MATRIX");
+  return te_run(bins, ld, n_per_var, b_max, n_vars, row_len, lag, pair_offset, n_pairs,
+                out_mode == TENEX_OUT_PAIRFREE ? kOutPairfree : kOutMatrix, out, out_ld,
+                nullptr, nullptr, nullptr, nullptr, nullptr, 0, workspace, workspace_bytes,
+                cfg, stream);
+}
+
+extern "C" int tenex_te_pairfree_counts(const uint8_t* bins, int64_t ld,
+                                        const int32_t* n_per_var, int b_max, int n_vars,
+                                        int64_t row_len, int64_t lag, int64_t pair_offset,
+                                        int64_t n_pairs, float* out, int32_t* counts,
+                                        int64_t counts_stride, void* workspace,
+                                        size_t workspace_bytes, const tenex_te_config* cfg,
+                                        void* stream) {
+  if (!counts) return fail(TENEX_ERR_BADARG, "counts must be non-NULL");
+  return te_run(bins, ld, n_per_var, b_max, n_vars, row_len, lag, pair_offset, n_pairs,
+                kOutPairfree, out, 0, nullptr, nullptr, nullptr, nullptr, counts,
+                counts_stride, workspace, workspace_bytes, cfg, stream);
+}
+
+extern "C" int tenex_surrogate_accumulate(const uint8_t* bins, int64_t ld,
+                                          const int32_t* n_per_var, int b_max, int n_vars,
+                                          int64_t row_len, int64_t lag, int64_t pair_offset,
+                                          int64_t n_pairs, const float* observed, double* sum,
+                                          double* sumsq, int32_t* count_ge, void* workspace,
+                                          size_t workspace_bytes, const tenex_te_config* cfg,
+                                          void* stream) {
+  return te_run(bins, ld, n_per_var, b_max, n_vars, row_len, lag, pair_offset, n_pairs,
+                kOutStats, nullptr, 0, observed, sum, sumsq, count_ge, nullptr, 0, workspace,
+                workspace_bytes, cfg, stream);
+}

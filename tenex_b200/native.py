@@ -1,0 +1,130 @@
+"""ctypes binding of libtenex_sm100.so (the C ABI declared in include/tenex_sm100.h).
+
+The library is built in-tree by tenex_b200.build. There is no fallback: if the
+library is missing or fails to load, every GPU entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libtenex_sm100.so")
+
+TENEX_OK = 0
+TENEX_ERR_BADARG = 1
+TENEX_ERR_UNSUPPORTED = 2
+TENEX_ERR_OOM = 3
+TENEX_ERR_LAUNCH = 4
+TENEX_ERR_TIMEOUT = 5
+TENEX_ERR_BADDATA = 6
+
+OUT_PAIRFREE = 0
+OUT_MATRIX = 1
+
+_STATUS_NAMES = {1: "BADARG", 2: "UNSUPPORTED", 3: "OOM", 4: "LAUNCH", 5: "TIMEOUT",
+                 6: "BADDATA"}
+
+
+class TenexError(RuntimeError):
+    """A C-ABI call returned a non-zero tenex_status."""
+
+    def __init__(self, status: int, where: str, msg: str):
+        self.status = status
+        super().__init__(f"{where}: TENEX_ERR_{_STATUS_NAMES.get(status, status)}: {msg}")
+
+
+class DevInfo(ctypes.Structure):
+    _fields_ = [("sm_count", ctypes.c_int), ("smem_optin", ctypes.c_int),
+                ("smem_per_sm", ctypes.c_int), ("l2_bytes", ctypes.c_int),
+                ("cc_major", ctypes.c_int), ("cc_minor", ctypes.c_int),
+                ("max_threads_per_sm", ctypes.c_int)]
+
+
+class TeConfig(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("src_chunk", ctypes.c_int), ("smem_bytes", ctypes.c_int)]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_L = ctypes.c_int64
+_S = ctypes.c_size_t
+
+# name -> argtypes (restype int unless noted)
+_SIGS = {
+    "tenex_abi_version": [],
+    "tenex_last_error": [ctypes.c_char_p, _S],
+    "tenex_device_query": [_I, ctypes.POINTER(DevInfo)],
+    "tenex_te_workspace_bytes": [_I, _L],
+    "tenex_workspace_status": [_P, _P],
+    "tenex_te_pairfree": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _I, _L, _P, _S,
+                          ctypes.POINTER(TeConfig), _P],
+    "tenex_te_pairfree_counts": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _P, _L, _P, _S,
+                                 ctypes.POINTER(TeConfig), _P],
+    "tenex_surrogate_accumulate": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _P, _P, _P, _P, _S,
+                                   ctypes.POINTER(TeConfig), _P],
+    "tenex_block_shuffle": [_P, _L, _I, _L, _I, _P, _I, _I, _P, _L, _P],
+}
+_RESTYPES = {"tenex_te_workspace_bytes": ctypes.c_size_t}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the library once (raises if it is missing: no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing; build it with `python -m tenex_b200.build`")
+            L = ctypes.CDLL(LIB_PATH)
+            for name, args in _SIGS.items():
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = _RESTYPES.get(name, ctypes.c_int)
+            _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib().tenex_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int, where: str) -> None:
+    if status != TENEX_OK:
+        raise TenexError(status, where, last_error())
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args), name)
+
+
+def stream_ptr(stream: torch.cuda.Stream | None = None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def device_info(device: int | None = None) -> DevInfo:
+    if device is None:
+        device = torch.cuda.current_device()
+    info = DevInfo()
+    call("tenex_device_query", int(device), ctypes.byref(info))
+    return info
+
+
+def te_config(threads=0, ctas_per_sm=0, src_chunk=0, smem_bytes=0) -> TeConfig:
+    return TeConfig(int(threads), int(ctas_per_sm), int(src_chunk), int(smem_bytes))

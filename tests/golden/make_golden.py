@@ -1,0 +1,138 @@
+"""Generates tests/golden/*.npz from the reference implementation itself.
+
+Run in a container that has the reference source tree (it is imported, never
+copied):  python tests/golden/make_golden.py /path/to/reference
+
+The fixtures are small (seconds to produce) and pin the oracle and the
+product to the reference's own CPU code paths:
+  discretize_cfg1.npz   tenex.preprocess.discretize(use_numpy_bins=True) and
+                        TransferEntropyEngine.compute(accelerator="cpu") on a
+                        cfg1-shaped expression matrix (n=40, T=300)
+  scatter_multibin.npz  tenex.kernels.scatter_add.compute_te_scatter_add on
+                        random multi-bin data, all ordered pairs, tau=1 and tau=2
+  scatter_k2.npz        same with K=2 samples per time step
+  remap.npz             tenex.preprocess.remap_bins on gapped int32 bins
+  coarsen.npz           tenex.preprocess.coarsen_bins (CPU path), limit 38
+  gemm_b2.npz           tenex.kernels.gemm_b2.compute_te_gemm_b2 (torch path, CPU)
+  surrogate.npz         SurrogateTestMethod.infer on CPU (scatter_add kernel, block
+                        shuffles) plus the block permutations its RNG schedule draws
+  smem_limit.npz        compute_smem_bin_limit for a few SMEM sizes
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def main(ref: str) -> None:
+    sys.path.insert(0, ref)
+    sys.path.insert(0, REPO)
+    os.environ.setdefault("TENEX_CPU_ONLY", "1")
+    import torch
+    from tenex.preprocess import discretize, remap_bins, coarsen_bins
+    from tenex.transferentropy import TransferEntropyEngine
+    from tenex.kernels.scatter_add import compute_te_scatter_add
+    from tenex.kernels.gemm_b2 import compute_te_gemm_b2
+    from tenex.kernels.adaptive_smem import compute_smem_bin_limit
+    from tenex.inference.surrogate_test import SurrogateTestMethod, _build_block_perm
+    from tenex_b200 import workloads as W
+
+    cpu = torch.device("cpu")
+
+    # 1. discretisation + full CPU compute on cfg1-shaped expression
+    x, planted = W.cfg1_expression(n=40, T=300, seed=7, n_planted=4)
+    bins, n_bins, b_max, npv = discretize(x, method="FSBW-L", kp=0.5, device=cpu,
+                                          use_numpy_bins=True)
+    names = np.array([f"g{i}" for i in range(x.shape[0])])
+    res = TransferEntropyEngine(x, names).compute(accelerator="cpu")
+    np.savez_compressed(os.path.join(HERE, "discretize_cfg1.npz"), x=x,
+                        bins=bins.numpy().astype(np.int32), n_bins=np.asarray(n_bins),
+                        b_max=b_max, n_per_var=npv.numpy(), matrix=np.asarray(res.matrix),
+                        planted=planted)
+
+    # 2. multi-bin scatter_add, tau=1 and tau=2
+    rng = np.random.default_rng(11)
+    n, T = 24, 400
+    b = rng.integers(1, 13, n)
+    xb = np.stack([rng.integers(0, bb, T) for bb in b]).astype(np.int32)
+    xb, npv_d, bmax_d = remap_bins(torch.from_numpy(xb[:, :, None].copy()))
+    t_idx, s_idx = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    msk = t_idx != s_idx
+    pairs = np.stack([t_idx[msk], s_idx[msk]], 1).astype(np.int64)
+    te1 = compute_te_scatter_add(xb, torch.from_numpy(pairs), bmax_d, tau=1)
+    te2 = compute_te_scatter_add(xb, torch.from_numpy(pairs), bmax_d, tau=2)
+    np.savez_compressed(os.path.join(HERE, "scatter_multibin.npz"),
+                        bins=xb.numpy()[:, :, 0], n_per_var=npv_d.numpy(), b_max=bmax_d,
+                        pairs=pairs, te_tau1=te1, te_tau2=te2)
+
+    # 3. K = 2
+    n, T, K = 10, 150, 2
+    xk = rng.integers(0, 5, (n, T, K)).astype(np.int32)
+    xk, npv_k, bmax_k = remap_bins(torch.from_numpy(xk))
+    t_idx, s_idx = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    msk = t_idx != s_idx
+    pk = np.stack([t_idx[msk], s_idx[msk]], 1).astype(np.int64)
+    tek = compute_te_scatter_add(xk, torch.from_numpy(pk), bmax_k, tau=1)
+    np.savez_compressed(os.path.join(HERE, "scatter_k2.npz"), bins=xk.numpy(),
+                        n_per_var=npv_k.numpy(), b_max=bmax_k, pairs=pk, te=tek)
+
+    # 4. remap on gapped bins
+    raw = (rng.integers(0, 9, (16, 200)) * rng.integers(1, 4, (16, 1))).astype(np.int32)
+    raw[3] = 5  # a constant gene
+    rem, npv_r, bmax_r = remap_bins(torch.from_numpy(raw[:, :, None].copy()))
+    np.savez_compressed(os.path.join(HERE, "remap.npz"), raw=raw, remapped=rem.numpy()[:, :, 0],
+                        n_per_var=npv_r.numpy(), b_max=bmax_r)
+
+    # 5. coarsening (CPU path of coarsen_bins)
+    nb = rng.integers(2, 80, 20).astype(np.int32)
+    cb = np.stack([rng.integers(0, v, 300) for v in nb]).astype(np.int32)
+    for g in range(20):  # make every bin value present so n_per_var is exact
+        cb[g, :nb[g]] = np.arange(nb[g])
+    c_out, c_npv, c_bmax = coarsen_bins(torch.from_numpy(cb[:, :, None].copy()),
+                                        torch.from_numpy(nb.copy()), 38)
+    np.savez_compressed(os.path.join(HERE, "coarsen.npz"), bins=cb, n_per_var=nb,
+                        limit=38, out=c_out.numpy()[:, :, 0].astype(np.int32),
+                        out_npv=c_npv.numpy(), out_bmax=c_bmax)
+
+    # 6. GEMM-B2 (torch path on CPU)
+    xbin, _ = W.cfg2_binary(n=30, T=500, seed=5, n_planted=3)
+    gm = compute_te_gemm_b2(xbin.astype(np.int32), tau=1, device=cpu, use_triton=False)
+    np.savez_compressed(os.path.join(HERE, "gemm_b2.npz"), bins=xbin, te_ij_j_to_i=gm)
+
+    # 7. surrogate test on CPU with the scatter_add kernel
+    xs, npv_s, _pl = W.cfg5_bins(n=12, T=200, seed=9, n_planted=2)
+    xs32 = xs.astype(np.int32)[:, :, None]
+    bmax_s = int(npv_s.max())
+    t_idx, s_idx = np.meshgrid(np.arange(12), np.arange(12), indexing="ij")
+    msk = t_idx != s_idx
+    ps = np.stack([t_idx[msk], s_idx[msk]], 1).astype(np.int64)
+    te_obs = compute_te_scatter_add(torch.from_numpy(xs32), torch.from_numpy(ps), bmax_s, tau=1)
+    obs = np.zeros((12, 12), np.float32)
+    obs[ps[:, 0], ps[:, 1]] = te_obs
+    obs = obs.T.copy()  # [i, j] = TE(i -> j)
+    S, bl, seed = 6, 10, 42
+    res_s = SurrogateTestMethod().infer(obs, np.array([f"g{i}" for i in range(12)]), cpu,
+                                        bin_data=xs32, n_per_var=npv_s, b_max=bmax_s,
+                                        kernel="scatter_add", tau=1, n_surrogates=S,
+                                        block_length=bl, fdr=0.05, seed=seed)
+    perm, eff_bl, n_blocks = _build_block_perm(12, 200, 199, "block", bl, 0, S, seed, cpu)
+    np.savez_compressed(os.path.join(HERE, "surrogate.npz"), bins=xs, n_per_var=npv_s,
+                        observed=obs, perm=perm.numpy(), block_length=bl, seed=seed,
+                        mean=res_s.mean_surrogate_te, std=res_s.std_surrogate_te,
+                        effective=res_s.effective_te, p_values=res_s.p_values,
+                        n_edges=len(res_s.grn))
+
+    # 8. SMEM bin limit rule
+    sizes = np.array([49152, 101376, 166912, 232448], np.int64)
+    lim = np.array([compute_smem_bin_limit(int(s), warps=32) for s in sizes])
+    np.savez_compressed(os.path.join(HERE, "smem_limit.npz"), smem=sizes, limit=lim)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

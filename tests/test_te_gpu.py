@@ -1,0 +1,123 @@
+"""CUDA multi-bin TE kernel against the oracle: counts bit-exact, TE <= 1e-6."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tenex_b200.kernels import device as D
+from tenex_b200 import native
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6  # absolute TE tolerance against the float64 oracle
+
+
+def _rand_bins(rng, n, T, b_lo, b_hi, K=1):
+    b = rng.integers(b_lo, b_hi + 1, n)
+    x = np.stack([rng.integers(0, bb, T * K) for bb in b]).astype(np.int32)
+    rem, npv, bmax = O.remap(x)
+    return rem.reshape(n, T, K), npv, bmax
+
+
+def _gpu_te(bins, npv, bmax, cuda, tau=1, **kw):
+    db = D.pack_bins(bins, cuda)
+    npv_t = torch.as_tensor(npv, dtype=torch.int32, device=cuda)
+    out = D.te_pairfree(db, npv_t, bmax, tau=tau, **kw)
+    torch.cuda.synchronize()
+    return out
+
+
+@pytest.mark.parametrize("b_lo,b_hi,T", [(1, 4, 300), (2, 12, 1000), (2, 32, 700),
+                                         (17, 38, 400)])
+def test_counts_bitexact_and_te(cuda, b_lo, b_hi, T):
+    rng = np.random.default_rng(b_hi * 100 + T)
+    n = 9
+    bins, npv, bmax = _rand_bins(rng, n, T, b_lo, b_hi)
+    P = n * (n - 1)
+    stride = bmax ** 3
+    counts = torch.full((P, stride), -1, dtype=torch.int32, device=cuda)
+    te = _gpu_te(bins, npv, bmax, cuda, counts=counts, counts_stride=stride).cpu().numpy()
+    cnt = counts.cpu().numpy()
+    for p in range(P):
+        t, sl = divmod(p, n - 1)
+        s = sl + (sl >= t)
+        ref = O.counts(bins, 1, t, s, npv).reshape(-1)
+        assert np.array_equal(cnt[p, :ref.size], ref), (p, t, s)
+    ref_te = O.te_pairfree(bins, npv)
+    assert np.max(np.abs(te - ref_te)) <= TOL
+
+
+@pytest.mark.parametrize("tau,K", [(1, 1), (2, 1), (1, 2), (3, 2)])
+def test_tau_and_k(cuda, tau, K):
+    rng = np.random.default_rng(tau * 10 + K)
+    bins, npv, bmax = _rand_bins(rng, 11, 257, 2, 9, K=K)
+    te = _gpu_te(bins, npv, bmax, cuda, tau=tau).cpu().numpy()
+    ref = O.te_pairfree(bins, npv, tau=tau)
+    assert np.max(np.abs(te - ref)) <= TOL
+
+
+def test_matrix_mode_and_golden(cuda, golden):
+    g = golden("discretize_cfg1.npz")
+    bins = g["bins"]
+    npv = g["n_per_var"]
+    db = D.pack_bins(bins, cuda)
+    m = D.te_pairfree(db, torch.as_tensor(npv, device=cuda), int(g["b_max"]),
+                      matrix=True).cpu().numpy()
+    assert np.max(np.abs(m - g["matrix"])) <= TOL  # reference CPU compute()
+    assert np.all(np.diag(m) == 0)
+
+
+def test_pair_ranges_and_launch_shapes(cuda):
+    rng = np.random.default_rng(5)
+    n = 40
+    bins, npv, bmax = _rand_bins(rng, n, 600, 2, 16)
+    ref = O.te_pairfree(bins, npv)
+    db = D.pack_bins(bins, cuda)
+    npv_t = torch.as_tensor(npv, device=cuda)
+    for cfg in (None, dict(threads=128, src_chunk=7), dict(threads=1024, ctas_per_sm=2,
+                                                           src_chunk=3),
+                dict(threads=256, smem_bytes=48 * 1024, src_chunk=64)):
+        for p0, cnt in ((0, n * (n - 1)), (5, 77), (n * (n - 1) - 13, 13), (123, 1)):
+            te = D.te_pairfree(db, npv_t, bmax, pair_offset=p0, n_pairs=cnt, cfg=cfg)
+            assert np.max(np.abs(te.cpu().numpy() - ref[p0:p0 + cnt])) <= TOL, (cfg, p0)
+
+
+def test_long_series_u32_counters(cuda):
+    rng = np.random.default_rng(77)
+    bins, npv, bmax = _rand_bins(rng, 5, 70001, 2, 16)  # N >= 65536: 32-bit counters
+    te = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
+    assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
+
+
+def test_constant_source_gives_zero(cuda):
+    rng = np.random.default_rng(3)
+    bins, npv, bmax = _rand_bins(rng, 6, 300, 2, 5)
+    bins[2] = 0
+    npv = npv.copy()
+    npv[2] = 1
+    te = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
+    for t in range(6):
+        if t == 2:
+            continue
+        sl = 2 if 2 < t else 1  # src_local of source 2 for target t
+        assert te[t * 5 + sl] == 0.0
+
+
+def test_bad_bins_raise_without_fault(cuda):
+    rng = np.random.default_rng(4)
+    bins, npv, bmax = _rand_bins(rng, 6, 300, 2, 5)
+    npv = npv.copy()
+    npv[3] = max(1, npv[3] - 1)  # a bin value now exceeds its gene's n_per_var
+    with pytest.raises(native.TenexError, match="BADDATA"):
+        _gpu_te(bins, npv, bmax, cuda)
+    # the context stays usable
+    bins2, npv2, bmax2 = _rand_bins(rng, 6, 300, 2, 5)
+    te = _gpu_te(bins2, npv2, bmax2, cuda).cpu().numpy()
+    assert np.max(np.abs(te - O.te_pairfree(bins2, npv2))) <= TOL
+
+
+def test_determinism(cuda):
+    rng = np.random.default_rng(8)
+    bins, npv, bmax = _rand_bins(rng, 30, 2000, 2, 16)
+    a = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
+    b = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
+    assert np.array_equal(a, b)
