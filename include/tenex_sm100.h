@@ -72,8 +72,10 @@ int tenex_last_error(char* buf, size_t len);
  * query_smem_optin helper (tenex/kernels/__init__.py:44-71). */
 int tenex_device_query(int device, tenex_dev_info* info);
 
-/* Bytes of device workspace the TE / surrogate entry points need. */
-size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len);
+/* Bytes of device workspace the TE / surrogate entry points need: a 256-byte
+ * header (work ticket, validation words) plus each gene's bin marginal
+ * (n_vars * b_max int32) and most frequent bin (n_vars int32). */
+size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len, int b_max);
 
 /* Reads back the data-validation word a previous TE call left in the
  * workspace (synchronises `stream`). Returns TENEX_ERR_BADDATA if any bin value
@@ -125,6 +127,12 @@ int tenex_surrogate_accumulate(const uint8_t* bins, int64_t ld, const int32_t* n
 int tenex_block_shuffle(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T, int K,
                         const int32_t* perm, int n_blocks, int block_length,
                         uint8_t* out, int64_t out_ld, void* stream);
+
+/* Roofline probe (no reference counterpart): times `iters` shared-memory
+ * atomicAdds per thread on every SM (mode 0 conflict-free int32, 1 conflict-free
+ * 16-bit halves, 2 random words, 3 the same 32 words from every warp) and returns the increment count and the
+ * milliseconds. Synchronises `stream`. */
+int tenex_probe_smem_atomics(int mode, int iters, int64_t* increments, float* ms, void* stream);
 
 #ifdef __cplusplus
 }

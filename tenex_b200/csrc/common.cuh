@@ -36,11 +36,14 @@ __host__ __device__ inline int64_t round_up(int64_t x, int64_t m) { return (x + 
 //   [0]   uint32 work ticket of the persistent kernel
 //   [4]   int32  data-validation word (nonzero = bad bin / n_per_var)
 //   [8]   int32  unsupported-item word (nonzero = an item's histogram did not fit)
+//   [64]  uint64 phase_cycles[8] (filled only by builds with TENEX_PHASE_TIMERS)
 struct WsHeader {
   unsigned int ticket;
   int bad_data;
   int bad_item;
-  int pad[61];
+  int pad[13];
+  unsigned long long phase_cycles[8];
+  int pad2[32];
 };
 static_assert(sizeof(WsHeader) == 256, "workspace header is 256 bytes");
 

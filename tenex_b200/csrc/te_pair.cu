@@ -9,20 +9,24 @@
 //
 // How (B200 design, not the reference's one-CTA-per-pair layout):
 //   * Work item = one target and a chunk of W sources. The CTA stages the
-//     target's joint state z[s] = x[s+lag]*b_t + x[s] into shared memory ONCE
-//     per item (u8 when b_t <= 16, else u16) together with the target-only
-//     marginals c2a and c1, so sources never re-read the target.
-//   * Shared memory left after the target block is cut into histogram slots
-//     sized for this item (b_t^2 * b_s cells). A slot belongs to a group of G
-//     warps (G = 1 for the common small-b pairs: warp-private histograms, no
-//     cross-warp contention; G > 1 only for heavy pairs that need a large
-//     slot). Counters are 16-bit halves of 32-bit words when N < 65536, so a
-//     38x38x38 histogram needs 110 KB instead of 220 KB.
-//   * The source row is streamed from L2/HBM with 16-byte non-temporal loads;
-//     each sample is one shared-memory atomic add.
+//     target's joint state z[s] = x[s+lag]*b_t + x[s] into shared memory once
+//     per item (u8 when b_t <= 16, else u16) with the target-only marginals
+//     c2a (= row sums of c3 over yt) and c1, so sources never re-read it.
+//   * Shared memory after the target block is cut into histogram slots sized
+//     for the item (b_t^2 * b_s cells); a slot belongs to a group of G warps
+//     (G = 1: warp-private histograms for the common small pairs). Counters are
+//     32-bit when the slots fit, else 16-bit halves of a word (N < 65536).
+//   * Shared-memory atomics serialise on bank conflicts and on lanes hitting
+//     the same word, and the hottest words are the cells of the most frequent
+//     values. The kernel therefore never counts a sample whose target state is
+//     the target's most frequent state z_dom or whose source bin is the
+//     source's most frequent value y_dom. Those cells are exact by subtraction:
+//       c3[z, y_dom]    = c2a[z] - sum_{y != y_dom} c3[z, y]        (z != z_dom)
+//       c3[z_dom, y]    = m_src[y] - sum_{z != z_dom} c3[z, y]      (all y)
+//     where m_src is the source's marginal over [0, N) (a per-gene pre-pass).
+//     On skewed bins this halves the wavefronts per atomic.
 //   * The entropy pass reads each slot column once to form c2b, once more to
-//     form the terms, and clears the slot for the next source (no separate
-//     zeroing pass).
+//     form the terms, and clears the slot for the next source.
 //   * Items are handed out by an atomic ticket in chunk-major order, so the
 //     CTAs resident at one moment share a small set of source rows in L2.
 #include <cuda_runtime.h>
@@ -41,7 +45,7 @@ struct TeParams {
   int64_t ld;
   const int32_t* npv;
   int n;
-  int N;          // samples per pair (row_len - lag), < 2^31
+  int N;          // samples per pair (row_len - lag), < 2^24
   int lag;
   int64_t p0, p1;  // pair-free id range [p0, p1)
   int t_first;
@@ -50,7 +54,7 @@ struct TeParams {
   int n_chunks;   // items per target
   int64_t n_items;
   int zbytes;     // bytes per z entry reserved (1 or 2)
-  int bmax;       // max n_per_var over the genes (sizes the c2a/c1 region)
+  int bmax;       // max n_per_var (sizes the c2a/c1 region and the marginal rows)
   int smem_bytes;
   int out_mode;
   float* out;
@@ -61,8 +65,28 @@ struct TeParams {
   int32_t* cnt_ge;
   int32_t* counts_dbg;
   int64_t counts_stride;
+  const int32_t* marg;  // (n, bmax) per-gene marginal over [0, N)
+  const int32_t* ydom;  // (n,) most frequent bin of each gene over [0, N)
   WsHeader* ws;
 };
+
+// Workspace: header | marg (n*bmax int32) | ydom (n int32), 256-byte aligned.
+__host__ __device__ inline int64_t ws_marg_off() { return (int64_t)sizeof(WsHeader); }
+__host__ __device__ inline int64_t ws_ydom_off(int n, int bmax) {
+  return round_up(ws_marg_off() + (int64_t)n * bmax * 4, 256);
+}
+__host__ __device__ inline int64_t ws_total(int n, int bmax) {
+  return round_up(ws_ydom_off(n, bmax) + (int64_t)n * 4, 256);
+}
+
+#ifdef TENEX_PHASE_TIMERS
+#define PHASE_MARK(var) const long long var = clock64()
+#define PHASE_ADD(k, a, b) \
+  if (lane_g == 0) atomicAdd(&P.ws->phase_cycles[k], (unsigned long long)((b) - (a)))
+#else
+#define PHASE_MARK(var)
+#define PHASE_ADD(k, a, b)
+#endif
 
 namespace {
 
@@ -80,64 +104,278 @@ __host__ __device__ inline SmemLayout smem_layout(int N, int zbytes, int bmax) {
   L.c1_off = off;    off += (int)round_up((int64_t)bmax * 4, 16);
   L.c2a_off = off;   off += (int)round_up((int64_t)bmax * bmax * 4, 16);
   L.z_off = off;     off += (int)round_up((int64_t)N * zbytes, 16);
-  L.slot_off = off;
+  L.slot_off = (int)round_up(off, 128);
   return L;
 }
 
-// One 16-sample step of the histogram: 16 source bins (yv) and 16 target
-// states. PACK16: 16-bit counters, word = z*hb + (y>>1), half = y&1.
+// Slot cell (z, y): PACK16 -> 16-bit half (y & 1) of word z*hb + (y >> 1),
+// else word z*bs + y.
 template <bool PACK16>
-__device__ __forceinline__ void hist_add(uint32_t* slot, uint32_t z, uint32_t y, uint32_t bs,
-                                         uint32_t hb) {
+__device__ __forceinline__ uint32_t cell_get(const uint32_t* slot, uint32_t z, uint32_t y,
+                                             uint32_t bs, uint32_t hb) {
   if (PACK16) {
-    atomicAdd(slot + (z * hb + (y >> 1)), 1u << ((y & 1u) << 4));
-  } else {
-    atomicAdd(slot + (z * bs + y), 1u);
+    const uint32_t w = slot[z * hb + (y >> 1)];
+    return (y & 1u) ? (w >> 16) : (w & 0xffffu);
   }
+  return slot[z * bs + y];
 }
 
 template <bool PACK16>
-__device__ __forceinline__ void hist16_z8(uint32_t* slot, uint4 yv, uint4 zv, uint32_t bs,
-                                          uint32_t hb) {
+__device__ __forceinline__ void cell_add(uint32_t* slot, uint32_t z, uint32_t y, uint32_t bs,
+                                         uint32_t hb, uint32_t v) {
+  if (PACK16) {
+    atomicAdd(slot + (z * hb + (y >> 1)), v << ((y & 1u) << 4));
+  } else {
+    atomicAdd(slot + (z * bs + y), v);
+  }
+}
+
+// Counts one sample unless it belongs to the derived row (z_dom) or column
+// (y_dom). The skip is a predicate on a single red.shared instruction (inline
+// PTX) so the compiler cannot turn the 16 unrolled updates into branches.
+// slot32 is the slot's 32-bit shared-window address.
+template <bool PACK16>
+__device__ __forceinline__ void hist_add(uint32_t slot32, uint32_t z, uint32_t y, uint32_t bs,
+                                         uint32_t hb, uint32_t zdom, uint32_t yd) {
+  uint32_t addr, inc;
+  if (PACK16) {
+    addr = slot32 + ((z * hb + (y >> 1)) << 2);
+    inc = (y & 1u) * 0xffffu + 1u;
+  } else {
+    addr = slot32 + ((z * bs + y) << 2);
+    inc = 1u;
+  }
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.u32 p, %2, %3;\n\t"
+      "setp.ne.and.u32 p, %4, %5, p;\n\t"
+      "@p red.shared.add.u32 [%0], %1;\n\t}"
+      ::"r"(addr), "r"(inc), "r"(z), "r"(zdom), "r"(y), "r"(yd)
+      : "memory");
+}
+
+template <bool PACK16>
+__device__ __forceinline__ void hist16_z8(uint32_t slot, uint4 yv, uint4 zv, uint32_t bs,
+                                          uint32_t hb, uint32_t zdom, uint32_t yd) {
   const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
   const uint32_t zs[4] = {zv.x, zv.y, zv.z, zv.w};
 #pragma unroll
   for (int w = 0; w < 4; ++w) {
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
-      uint32_t z = __byte_perm(zs[w], 0, 0x4440 + b);
-      hist_add<PACK16>(slot, z, y, bs, hb);
+      const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
+      const uint32_t z = __byte_perm(zs[w], 0, 0x4440 + b);
+      hist_add<PACK16>(slot, z, y, bs, hb, zdom, yd);
     }
   }
 }
 
 template <bool PACK16>
-__device__ __forceinline__ void hist16_z16(uint32_t* slot, uint4 yv, uint4 za, uint4 zb,
-                                           uint32_t bs, uint32_t hb) {
+__device__ __forceinline__ void hist16_z16(uint32_t slot, uint4 yv, uint4 za, uint4 zb,
+                                           uint32_t bs, uint32_t hb, uint32_t zdom,
+                                           uint32_t yd) {
   const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
   const uint32_t zs[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
 #pragma unroll
   for (int w = 0; w < 4; ++w) {
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
-      uint32_t zw = zs[(w * 4 + b) >> 1];
-      uint32_t z = (b & 1) ? (zw >> 16) : (zw & 0xffffu);
-      hist_add<PACK16>(slot, z, y, bs, hb);
+      const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
+      const uint32_t zw = zs[(w * 4 + b) >> 1];
+      const uint32_t z = (b & 1) ? (zw >> 16) : (zw & 0xffffu);
+      hist_add<PACK16>(slot, z, y, bs, hb, zdom, yd);
     }
   }
 }
 
 __device__ __forceinline__ float te_term(float c3, float c1, float c2a, float c2b) {
-  // Same expression as the reference's per-cell term (full_smem.cu:124-127):
+  // The reference's per-cell term (full_smem.cu:124-127),
   // c3 * log2((c3*c1) / (c2a*c2b)), with IEEE division and an accurate log2.
   return c3 * log2f(__fdiv_rn(c3 * c1, c2a * c2b));
 }
 
+__device__ __forceinline__ void group_sync(int G, int g, int gthreads) {
+  if (G == 1) __syncwarp();
+  else dev::named_bar(1 + g, gthreads);
+}
+
+// One group's pass over its sources of the current item.
+template <bool PACK16>
+__device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, int G, int g,
+                                            int n_groups, int lane_g, int tid, int warp,
+                                            int tgt, int64_t lo, int64_t base, int n_src,
+                                            int bt, uint32_t zdom, const unsigned char* zsm,
+                                            bool z8, const float* c1s, const float* c2as,
+                                            double* red) {
+  const int gthreads = G * 32;
+  const int N = P.N;
+  const int nvec = N >> 4;
+  const int bt2 = bt * bt;
+  for (int r = g; r < n_src; r += n_groups) {
+    const int64_t p = lo + r;
+    const int sl = (int)(p - base);
+    const int src = sl + (sl >= tgt);
+    const uint32_t bs = (uint32_t)P.npv[src];
+    const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
+    const uint32_t yd = (uint32_t)P.ydom[src];
+    const uint8_t* srow = P.bins + (int64_t)src * P.ld;
+    const uint4* yv = reinterpret_cast<const uint4*>(srow);
+    const uint32_t slot32 = (uint32_t)__cvta_generic_to_shared(slot);
+    PHASE_MARK(t0);
+
+    // -- histogram of the counted cells ------------------------------------
+    if (z8) {
+      const uint4* zv = reinterpret_cast<const uint4*>(zsm);
+      int v = lane_g;
+      if (v < nvec) {
+        uint4 ycur = dev::ldg_nc_v4(yv + v);
+        for (; v < nvec; v += gthreads) {
+          const int vn = v + gthreads;
+          uint4 ynext = ycur;
+          if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
+          hist16_z8<PACK16>(slot32, ycur, zv[v], bs, hb, zdom, yd);
+          ycur = ynext;
+        }
+      }
+      for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
+        hist_add<PACK16>(slot32, zsm[s], srow[s], bs, hb, zdom, yd);
+    } else {
+      const uint4* zv = reinterpret_cast<const uint4*>(zsm);
+      const uint16_t* z16 = reinterpret_cast<const uint16_t*>(zsm);
+      int v = lane_g;
+      if (v < nvec) {
+        uint4 ycur = dev::ldg_nc_v4(yv + v);
+        for (; v < nvec; v += gthreads) {
+          const int vn = v + gthreads;
+          uint4 ynext = ycur;
+          if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
+          hist16_z16<PACK16>(slot32, ycur, zv[2 * v], zv[2 * v + 1], bs, hb, zdom, yd);
+          ycur = ynext;
+        }
+      }
+      for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
+        hist_add<PACK16>(slot32, z16[s], srow[s], bs, hb, zdom, yd);
+    }
+    group_sync(G, g, gthreads);
+    PHASE_MARK(t1);
+
+    // -- derived cells: column y_dom from the row sums c2a, then row z_dom
+    //    from the source marginal ------------------------------------------
+    for (int z = lane_g; z < bt2; z += gthreads) {
+      if ((uint32_t)z == zdom) continue;
+      uint32_t rs = 0;
+      for (uint32_t y = 0; y < bs; ++y) rs += cell_get<PACK16>(slot, z, y, bs, hb);
+      cell_add<PACK16>(slot, z, yd, bs, hb, (uint32_t)c2as[z] - rs);
+    }
+    group_sync(G, g, gthreads);
+    // row z_dom: partial column sums over z != z_dom are accumulated into the
+    // (still empty) z_dom row by all lanes, then each word of the row is
+    // finalised by one lane as m_src[y] - sum.
+    const int32_t* msrc = P.marg + (int64_t)src * P.bmax;
+    const int nparts = max(1, gthreads / (int)bs);
+    for (int idx = lane_g; idx < (int)bs * nparts; idx += gthreads) {
+      const int part = idx / (int)bs;
+      const uint32_t y = (uint32_t)(idx - part * (int)bs);
+      uint32_t cs = 0;
+      for (int z = part; z < bt2; z += nparts)
+        if ((uint32_t)z != zdom) cs += cell_get<PACK16>(slot, z, y, bs, hb);
+      if (cs) cell_add<PACK16>(slot, zdom, y, bs, hb, cs);
+    }
+    group_sync(G, g, gthreads);
+    for (int w = lane_g; w < (int)hb; w += gthreads) {
+      uint32_t* wp = slot + zdom * hb + w;
+      if (PACK16) {
+        const uint32_t cur = *wp;
+        const uint32_t y0 = 2u * w, y1 = 2u * w + 1u;
+        const uint32_t lo = (uint32_t)msrc[y0] - (cur & 0xffffu);
+        const uint32_t hi = y1 < bs ? (uint32_t)msrc[y1] - (cur >> 16) : 0u;
+        *wp = lo | (hi << 16);
+      } else {
+        *wp = (uint32_t)msrc[w] - *wp;
+      }
+    }
+    group_sync(G, g, gthreads);
+    PHASE_MARK(t2);
+
+    // -- optional raw-count export (parity checks only) --------------------
+    if (P.counts_dbg != nullptr) {
+      int32_t* cd = P.counts_dbg + (p - P.p0) * P.counts_stride;
+      const int ncell = bt2 * (int)bs;
+      for (int c = lane_g; c < ncell; c += gthreads) {
+        const int z = c / (int)bs, y = c - z * (int)bs;
+        cd[c] = (int32_t)cell_get<PACK16>(slot, z, y, bs, hb);
+      }
+      group_sync(G, g, gthreads);
+    }
+
+    // -- entropy pass: column (xt=j, word wk) over xt1=i, clearing the slot --
+    float acc = 0.f;
+    const int ncols = bt * (int)hb;
+    for (int col = lane_g; col < ncols; col += gthreads) {
+      const int j = col / (int)hb;
+      const int wk = col - j * (int)hb;
+      uint32_t s = 0;
+      for (int i = 0; i < bt; ++i) s += slot[(i * bt + j) * hb + wk];
+      if (s == 0u) continue;
+      const float c1j = c1s[j];
+      if (PACK16) {
+        const float c2b_lo = (float)(s & 0xffffu), c2b_hi = (float)(s >> 16);
+        for (int i = 0; i < bt; ++i) {
+          const int idx = (i * bt + j) * hb + wk;
+          const uint32_t w = slot[idx];
+          if (w != 0u) {
+            slot[idx] = 0u;
+            const float c2a = c2as[i * bt + j];
+            const uint32_t clo = w & 0xffffu, chi = w >> 16;
+            if (clo) acc += te_term((float)clo, c1j, c2a, c2b_lo);
+            if (chi) acc += te_term((float)chi, c1j, c2a, c2b_hi);
+          }
+        }
+      } else {
+        const float c2b = (float)s;
+        for (int i = 0; i < bt; ++i) {
+          const int idx = (i * bt + j) * hb + wk;
+          const uint32_t w = slot[idx];
+          if (w != 0u) {
+            slot[idx] = 0u;
+            acc += te_term((float)w, c1j, c2as[i * bt + j], c2b);
+          }
+        }
+      }
+    }
+    double tot = dev::warp_sum((double)acc);
+    if (G > 1) {
+      if ((tid & 31) == 0) red[warp] = tot;
+      dev::named_bar(1 + g, gthreads);
+      if (lane_g == 0) {
+        tot = 0.0;
+        for (int w = 0; w < G; ++w) tot += red[g * G + w];
+      }
+    }
+    if (lane_g == 0) {
+      const float te = (float)(tot / (double)N);
+      if (P.out_mode == kOutPairfree) {
+        P.out[p - P.p0] = te;
+      } else if (P.out_mode == kOutMatrix) {
+        P.out[(int64_t)src * P.out_ld + tgt] = te;
+      } else {
+        const int64_t m = (int64_t)src * P.n + tgt;
+        const double td = (double)te;
+        P.sum[m] += td;
+        P.sumsq[m] += td * td;
+        P.cnt_ge[m] += (te >= P.obs[m]) ? 1 : 0;
+      }
+    }
+    group_sync(G, g, gthreads);
+    PHASE_MARK(t3);
+    PHASE_ADD(0, t0, t1);
+    PHASE_ADD(1, t1, t2);
+    PHASE_ADD(2, t2, t3);
+  }
+}
+
 }  // namespace
 
-template <bool PACK16>
 __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout SL = smem_layout(P.N, P.zbytes, P.bmax);
@@ -177,6 +415,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     }
     const int n_src = (int)(hi - lo);
     const int bt = P.npv[tgt];
+    const int bt2 = bt * bt;
 
     // ---- max b_s over the item's sources --------------------------------
     unsigned my_max = 1;
@@ -187,7 +426,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     }
     my_max = dev::warp_max(my_max);
     if ((tid & 31) == 0) reinterpret_cast<unsigned*>(red)[warp] = my_max;
-    for (int i = tid; i < bt * bt; i += nthreads) c2a_cnt[i] = 0;
+    for (int i = tid; i < bt2; i += nthreads) c2a_cnt[i] = 0;
     __syncthreads();
     if (tid < 32) {
       unsigned v = tid < n_warps ? reinterpret_cast<unsigned*>(red)[tid] : 1u;
@@ -213,19 +452,47 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       }
     }
     __syncthreads();
+    // z_dom = most frequent target state (ties: smallest z). Key = count<<11 | (2047 - z)
+    // (count <= N < 2^21 when packed this way; z < bt2 <= 65025 needs 16 bits, so use 64-bit)
+    unsigned long long key = 0ull;
+    for (int z = tid; z < bt2; z += nthreads) {
+      const unsigned long long k =
+          ((unsigned long long)(unsigned)c2a_cnt[z] << 32) | (0xffffffffu - (unsigned)z);
+      key = k > key ? k : key;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long w = __shfl_xor_sync(0xffffffffu, key, o);
+      key = w > key ? w : key;
+    }
+    if ((tid & 31) == 0) reinterpret_cast<unsigned long long*>(red)[warp] = key;
     const int bsmax = misc[1];
-    for (int i = tid; i < bt * bt; i += nthreads) c2as[i] = (float)c2a_cnt[i];
+    for (int i = tid; i < bt2; i += nthreads) c2as[i] = (float)c2a_cnt[i];
     __syncthreads();
+    if (tid < 32) {
+      unsigned long long v =
+          tid < n_warps ? reinterpret_cast<unsigned long long*>(red)[tid] : 0ull;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+      }
+      if (tid == 0) misc[2] = (int)(0xffffffffu - (unsigned)(v & 0xffffffffull));
+    }
     for (int j = tid; j < bt; j += nthreads) {
       float s = 0.f;
       for (int i = 0; i < bt; ++i) s += c2as[i * bt + j];
       c1s[j] = s;
     }
 
-    // ---- carve slots ----------------------------------------------------
-    const int hbmax = PACK16 ? (bsmax + 1) >> 1 : bsmax;
-    const int slot_words = (int)round_up((int64_t)bt * bt * hbmax, 4);
-    const int fit = slot_region / (slot_words * 4);
+    // ---- carve slots: 32-bit counters when groups of <= 4 warps fit --------
+    const int words32 = (int)round_up((int64_t)bt2 * bsmax, 4);
+    const int words16 = (int)round_up((int64_t)bt2 * ((bsmax + 1) >> 1), 4);
+    const int fit32 = slot_region / (words32 * 4);
+    const int fit16 = slot_region / (words16 * 4);
+    const bool pack16 = (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
+    const int fit = pack16 ? fit16 : fit32;
+    const int slot_words = pack16 ? words16 : words32;
     if (fit < 1) {
       if (tid == 0) atomicExch(&P.ws->bad_item, 1);
       __syncthreads();
@@ -236,165 +503,84 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     while (G > 1 && G < n_warps && n_warps / G > 15) G <<= 1;
     const int n_groups = n_warps / G;
     const int g = warp / G;
-    const int gthreads = G * 32;
-    const int lane_g = tid - g * gthreads;
+    const int lane_g = tid - g * G * 32;
     uint32_t* slot = slots + (int64_t)g * slot_words;
-    // slots start zeroed: clear every slot word once per item (later sources
-    // are cleared by the entropy pass).
     for (int i = tid; i < n_groups * slot_words; i += nthreads) slots[i] = 0u;
     __syncthreads();
+    const uint32_t zdom = (uint32_t)misc[2];
 
-    const int nvec = N >> 4;
-
-    for (int r = g; r < n_src; r += n_groups) {
-      const int64_t p = lo + r;
-      const int sl = (int)(p - base);
-      const int src = sl + (sl >= tgt);
-      const uint32_t bs = (uint32_t)P.npv[src];
-      const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
-      const uint8_t* srow = P.bins + (int64_t)src * P.ld;
-      const uint4* yv = reinterpret_cast<const uint4*>(srow);
-
-      // -- histogram ------------------------------------------------------
-      if (z8) {
-        const uint4* zv = reinterpret_cast<const uint4*>(zsm);
-        int v = lane_g;
-        if (v < nvec) {
-          uint4 ycur = dev::ldg_nc_v4(yv + v);
-          for (; v < nvec; v += gthreads) {
-            const int vn = v + gthreads;
-            uint4 ynext = ycur;
-            if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
-            hist16_z8<PACK16>(slot, ycur, zv[v], bs, hb);
-            ycur = ynext;
-          }
-        }
-        for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
-          hist_add<PACK16>(slot, zsm[s], srow[s], bs, hb);
-      } else {
-        const uint4* zv = reinterpret_cast<const uint4*>(zsm);
-        const uint16_t* z16 = reinterpret_cast<const uint16_t*>(zsm);
-        int v = lane_g;
-        if (v < nvec) {
-          uint4 ycur = dev::ldg_nc_v4(yv + v);
-          for (; v < nvec; v += gthreads) {
-            const int vn = v + gthreads;
-            uint4 ynext = ycur;
-            if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
-            hist16_z16<PACK16>(slot, ycur, zv[2 * v], zv[2 * v + 1], bs, hb);
-            ycur = ynext;
-          }
-        }
-        for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
-          hist_add<PACK16>(slot, z16[s], srow[s], bs, hb);
-      }
-      if (G == 1) __syncwarp(); else dev::named_bar(1 + g, gthreads);
-
-      // -- optional raw-count export (parity checks only) ------------------
-      if (P.counts_dbg != nullptr) {
-        int32_t* cd = P.counts_dbg + (p - P.p0) * P.counts_stride;
-        const int ncell = bt * bt * (int)bs;
-        for (int c = lane_g; c < ncell; c += gthreads) {
-          const int z = c / (int)bs, y = c - z * (int)bs;
-          uint32_t v;
-          if (PACK16) {
-            uint32_t w = slot[z * hb + (y >> 1)];
-            v = (y & 1) ? (w >> 16) : (w & 0xffffu);
-          } else {
-            v = slot[z * bs + y];
-          }
-          cd[c] = (int32_t)v;
-        }
-        if (G == 1) __syncwarp(); else dev::named_bar(1 + g, gthreads);
-      }
-
-      // -- entropy pass: column (xt=j, word wk) over xt1=i ----------------
-      float acc = 0.f;
-      const int ncols = bt * (int)hb;
-      for (int col = lane_g; col < ncols; col += gthreads) {
-        const int j = col / (int)hb;
-        const int wk = col - j * (int)hb;
-        uint32_t s = 0;
-        for (int i = 0; i < bt; ++i) s += slot[(i * bt + j) * hb + wk];
-        const float c1j = c1s[j];
-        if (PACK16) {
-          const float c2b_lo = (float)(s & 0xffffu), c2b_hi = (float)(s >> 16);
-          for (int i = 0; i < bt; ++i) {
-            const int idx = (i * bt + j) * hb + wk;
-            const uint32_t w = slot[idx];
-            slot[idx] = 0u;
-            if (w != 0u) {
-              const float c2a = c2as[i * bt + j];
-              const uint32_t clo = w & 0xffffu, chi = w >> 16;
-              if (clo) acc += te_term((float)clo, c1j, c2a, c2b_lo);
-              if (chi) acc += te_term((float)chi, c1j, c2a, c2b_hi);
-            }
-          }
-        } else {
-          const float c2b = (float)s;
-          for (int i = 0; i < bt; ++i) {
-            const int idx = (i * bt + j) * hb + wk;
-            const uint32_t w = slot[idx];
-            slot[idx] = 0u;
-            if (w != 0u) acc += te_term((float)w, c1j, c2as[i * bt + j], c2b);
-          }
-        }
-      }
-      double tot = dev::warp_sum((double)acc);
-      if (G > 1) {
-        if ((tid & 31) == 0) red[warp] = tot;
-        dev::named_bar(1 + g, gthreads);
-        if (lane_g == 0) {
-          tot = 0.0;
-          for (int w = 0; w < G; ++w) tot += red[g * G + w];
-        }
-      }
-      if (lane_g == 0) {
-        const float te = (float)(tot / (double)N);
-        if (P.out_mode == kOutPairfree) {
-          P.out[p - P.p0] = te;
-        } else if (P.out_mode == kOutMatrix) {
-          P.out[(int64_t)src * P.out_ld + tgt] = te;
-        } else {
-          const int64_t m = (int64_t)src * P.n + tgt;
-          const double td = (double)te;
-          P.sum[m] += td;
-          P.sumsq[m] += td * td;
-          P.cnt_ge[m] += (te >= P.obs[m]) ? 1 : 0;
-        }
-      }
-      if (G == 1) __syncwarp(); else dev::named_bar(1 + g, gthreads);
-    }
+    if (pack16)
+      run_sources<true>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src, bt,
+                        zdom, zsm, z8, c1s, c2as, red);
+    else
+      run_sources<false>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src, bt,
+                         zdom, zsm, z8, c1s, c2as, red);
     __syncthreads();
   }
 }
 
-// Validation: every bin of gene g in [0, row_len) must be < n_per_var[g], and
-// n_per_var[g] in [1, b_max]. Sets ws->bad_data otherwise. One CTA per gene.
-__global__ void validate_bins_kernel(const uint8_t* bins, int64_t ld, const int32_t* npv,
-                                     int b_max, int n, int64_t row_len, WsHeader* ws) {
+// Per-gene pre-pass: validation (every bin of gene g in [0, row_len) below
+// n_per_var[g], and 1 <= n_per_var[g] <= b_max; sets ws->bad_data otherwise),
+// the marginal m[g][y] over samples [0, N) and its most frequent bin ydom[g]
+// (ties: smallest y). One CTA per gene.
+__global__ void gene_prepass_kernel(const uint8_t* bins, int64_t ld, const int32_t* npv,
+                                    int b_max, int n, int64_t row_len, int N, int32_t* marg,
+                                    int32_t* ydom, WsHeader* ws) {
+  __shared__ int h[256];
+  __shared__ unsigned long long wkey[32];
   const int g = blockIdx.x;
   if (g >= n) return;
   const int b = npv[g];
-  if (b < 1 || b > b_max) {
-    if (threadIdx.x == 0) atomicExch(&ws->bad_data, 1);
-    return;
-  }
+  const bool bad_b = b < 1 || b > b_max;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+  __syncthreads();
   const uint8_t* row = bins + (int64_t)g * ld;
   const int64_t nvec = row_len >> 4;
-  bool bad = false;
+  bool bad = bad_b;
   const uint4* rv = reinterpret_cast<const uint4*>(row);
   for (int64_t v = threadIdx.x; v < nvec; v += blockDim.x) {
-    uint4 q = __ldg(rv + v);
+    const uint4 q = __ldg(rv + v);
     const uint32_t w[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
 #pragma unroll
-      for (int bb = 0; bb < 4; ++bb) bad |= ((w[k] >> (8 * bb)) & 0xffu) >= (uint32_t)b;
+      for (int bb = 0; bb < 4; ++bb) {
+        const uint32_t val = (w[k] >> (8 * bb)) & 0xffu;
+        bad |= val >= (uint32_t)b;
+        if (v * 16 + k * 4 + bb < N) atomicAdd(&h[val], 1);
+      }
     }
   }
-  for (int64_t i = (nvec << 4) + threadIdx.x; i < row_len; i += blockDim.x) bad |= row[i] >= b;
-  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(&ws->bad_data, 1);
+  for (int64_t i = (nvec << 4) + threadIdx.x; i < row_len; i += blockDim.x) {
+    bad |= row[i] >= b;
+    if (i < N) atomicAdd(&h[row[i]], 1);
+  }
+  if (__syncthreads_or(bad)) {
+    if (threadIdx.x == 0) atomicExch(&ws->bad_data, 1);
+    return;
+  }
+  unsigned long long key = 0ull;
+  for (int y = threadIdx.x; y < b; y += blockDim.x) {
+    marg[(int64_t)g * b_max + y] = h[y];
+    const unsigned long long k = ((unsigned long long)(unsigned)h[y] << 32) | (255u - (unsigned)y);
+    key = k > key ? k : key;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, key, o);
+    key = w > key ? w : key;
+  }
+  if ((threadIdx.x & 31) == 0) wkey[threadIdx.x >> 5] = key;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    unsigned long long v = threadIdx.x < (blockDim.x >> 5) ? wkey[threadIdx.x] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+      v = w > v ? w : v;
+    }
+    if (threadIdx.x == 0) ydom[g] = (int32_t)(255u - (unsigned)(v & 0xffull));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -403,13 +589,12 @@ __global__ void validate_bins_kernel(const uint8_t* bins, int64_t ld, const int3
 
 struct TeLaunch {
   int threads, grid, smem;
-  bool pack16;
 };
 
 static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const DevAttr& A,
-                          TeLaunch* L, int* zbytes_out, int max_slot_bytes) {
-  int threads = (cfg && cfg->threads) ? cfg->threads : 512;
-  int cps = (cfg && cfg->ctas_per_sm) ? cfg->ctas_per_sm : 1;
+                          TeLaunch* L, int64_t max_slot_bytes) {
+  const int threads = (cfg && cfg->threads) ? cfg->threads : 512;
+  const int cps = (cfg && cfg->ctas_per_sm) ? cfg->ctas_per_sm : 1;
   if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
     return fail(TENEX_ERR_BADARG, "threads must be 128, 256, 512 or 1024 (got %d)", threads);
   if (cps < 1 || cps * threads > A.max_threads_per_sm)
@@ -425,12 +610,12 @@ static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const D
     return fail(TENEX_ERR_BADARG, "smem_bytes=%d exceeds the device opt-in %d", smem,
                 A.smem_optin);
   smem = smem / 16 * 16;
-  SmemLayout SL = smem_layout(P.N, *zbytes_out, P.bmax);
-  if (SL.slot_off + max_slot_bytes > smem)
+  const SmemLayout SL = smem_layout(P.N, P.zbytes, P.bmax);
+  if ((int64_t)SL.slot_off + max_slot_bytes > smem)
     return fail(TENEX_ERR_UNSUPPORTED,
-                "histogram of the largest pair (%d B) plus the staged target (%d B) does not "
+                "histogram of the largest pair (%lld B) plus the staged target (%d B) does not "
                 "fit %d B of shared memory; coarsen bins or shorten the series",
-                max_slot_bytes, SL.slot_off, smem);
+                (long long)max_slot_bytes, SL.slot_off, smem);
   L->threads = threads;
   L->smem = smem;
   L->grid = A.sm_count * cps;
@@ -441,10 +626,10 @@ static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const D
 
 using namespace tenex;
 
-extern "C" size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len) {
-  (void)n_vars;
+extern "C" size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len, int b_max) {
   (void)row_len;
-  return sizeof(WsHeader);
+  if (n_vars < 1 || b_max < 1) return sizeof(WsHeader);
+  return (size_t)ws_total(n_vars, b_max);
 }
 
 extern "C" int tenex_workspace_status(const void* workspace, void* stream) {
@@ -454,15 +639,16 @@ extern "C" int tenex_workspace_status(const void* workspace, void* stream) {
                                   as_stream(stream));
   if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
   if (e != cudaSuccess) return check_cuda(e, "tenex_workspace_status");
-  if (h.bad_data) return fail(TENEX_ERR_BADDATA,
-                              "a bin value was >= its gene's n_per_var, or n_per_var was "
-                              "outside [1, 255]; no TE was computed");
+  if (h.bad_data)
+    return fail(TENEX_ERR_BADDATA,
+                "a bin value was >= its gene's n_per_var, or n_per_var was outside [1, b_max]; "
+                "no TE was computed");
   if (h.bad_item) return fail(TENEX_ERR_UNSUPPORTED,
                               "a work item's histogram did not fit shared memory");
   return TENEX_OK;
 }
 
-// Common driver of the three TE entry points.
+// Common driver of the TE entry points.
 static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max, int n,
                   int64_t row_len, int64_t lag, int64_t p0, int64_t n_pairs, int out_mode,
                   float* out, int64_t out_ld, const float* obs, double* sum, double* sumsq,
@@ -490,14 +676,16 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   if (p0 < 0 || n_pairs < 0 || p0 + n_pairs > total)
     return fail(TENEX_ERR_BADARG, "pair range [%lld, %lld) outside [0, %lld)", (long long)p0,
                 (long long)(p0 + n_pairs), (long long)total);
-  if (out_mode != kOutStats && !out)
-    return fail(TENEX_ERR_BADARG, "out must be non-NULL");
+  if (out_mode != kOutStats && !out) return fail(TENEX_ERR_BADARG, "out must be non-NULL");
   if (out_mode == kOutMatrix && out_ld < n)
     return fail(TENEX_ERR_BADARG, "out_ld (%lld) must be >= n_vars", (long long)out_ld);
   if (out_mode == kOutStats && (!obs || !sum || !sumsq || !cnt))
     return fail(TENEX_ERR_BADARG, "observed, sum, sumsq and count_ge must be non-NULL");
-  if (!workspace || ws_bytes < sizeof(WsHeader))
-    return fail(TENEX_ERR_OOM, "workspace must be >= %zu bytes", sizeof(WsHeader));
+  if (!workspace || (int64_t)ws_bytes < ws_total(n, b_max))
+    return fail(TENEX_ERR_OOM, "workspace must be >= %lld bytes (tenex_te_workspace_bytes)",
+                (long long)ws_total(n, b_max));
+  if (counts && counts_stride < (int64_t)b_max * b_max * b_max)
+    return fail(TENEX_ERR_BADARG, "counts_stride must be >= b_max^3");
   if (n_pairs == 0) return TENEX_OK;
   DevAttr A;
   int st = current_device_attr(&A);
@@ -519,6 +707,9 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   if (P.W < 1) return fail(TENEX_ERR_BADARG, "src_chunk must be >= 1");
   P.n_chunks = (n - 1 + P.W - 1) / P.W;
   P.n_items = (int64_t)P.n_targets * P.n_chunks;
+  if (P.n_items > 0x7fffffffLL - 65536)
+    return fail(TENEX_ERR_UNSUPPORTED, "too many work items (%lld); raise src_chunk",
+                (long long)P.n_items);
   P.bmax = b_max;
   P.zbytes = b_max <= 16 ? 1 : 2;
   P.out_mode = out_mode;
@@ -531,14 +722,17 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   P.counts_dbg = counts;
   P.counts_stride = counts_stride;
   P.ws = reinterpret_cast<WsHeader*>(workspace);
+  unsigned char* wsb = reinterpret_cast<unsigned char*>(workspace);
+  int32_t* marg = reinterpret_cast<int32_t*>(wsb + ws_marg_off());
+  int32_t* ydom = reinterpret_cast<int32_t*>(wsb + ws_ydom_off(n, b_max));
+  P.marg = marg;
+  P.ydom = ydom;
 
-  const bool pack16 = P.N < 65536;
-  const int64_t hb = pack16 ? (b_max + 1) / 2 : b_max;
+  // worst case the device can meet: 16-bit halves when N < 65536, else 32-bit
+  const int64_t hb = P.N < 65536 ? (b_max + 1) / 2 : b_max;
   const int64_t worst_slot = round_up((int64_t)b_max * b_max * hb, 4) * 4;
-  if (counts && counts_stride < (int64_t)b_max * b_max * b_max)
-    return fail(TENEX_ERR_BADARG, "counts_stride must be >= b_max^3");
   TeLaunch L{};
-  st = plan_te_launch(P, cfg, A, &L, &P.zbytes, (int)std::min<int64_t>(worst_slot, 1 << 30));
+  st = plan_te_launch(P, cfg, A, &L, worst_slot);
   if (st) return st;
   P.smem_bytes = L.smem;
   int64_t grid = L.grid;
@@ -546,20 +740,14 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
 
   cudaError_t e = cudaMemsetAsync(workspace, 0, sizeof(WsHeader), stream);
   if (e != cudaSuccess) return check_cuda(e, "workspace reset");
-  validate_bins_kernel<<<n, 256, 0, stream>>>(bins, ld, npv, b_max, n, row_len, P.ws);
-  st = check_launch("validate_bins_kernel");
+  gene_prepass_kernel<<<n, 256, 0, stream>>>(bins, ld, npv, b_max, n, row_len, P.N, marg, ydom,
+                                             P.ws);
+  st = check_launch("gene_prepass_kernel");
   if (st) return st;
-  if (pack16) {
-    e = cudaFuncSetAttribute(te_pair_tile_kernel<true>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem);
-    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
-    te_pair_tile_kernel<true><<<(int)grid, L.threads, L.smem, stream>>>(P);
-  } else {
-    e = cudaFuncSetAttribute(te_pair_tile_kernel<false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem);
-    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
-    te_pair_tile_kernel<false><<<(int)grid, L.threads, L.smem, stream>>>(P);
-  }
+  e = cudaFuncSetAttribute(te_pair_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           L.smem);
+  if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+  te_pair_tile_kernel<<<(int)grid, L.threads, L.smem, stream>>>(P);
   return check_launch("te_pair_tile_kernel");
 }
 

@@ -75,8 +75,8 @@ def _ptr(t: torch.Tensor | None) -> int | None:
     return None if t is None else int(t.data_ptr())
 
 
-def workspace(device, n: int, row_len: int) -> torch.Tensor:
-    nb = int(native.lib().tenex_te_workspace_bytes(int(n), int(row_len)))
+def workspace(device, n: int, row_len: int, b_max: int) -> torch.Tensor:
+    nb = int(native.lib().tenex_te_workspace_bytes(int(n), int(row_len), int(b_max)))
     return torch.empty(nb, dtype=torch.uint8, device=device)
 
 
@@ -107,7 +107,7 @@ def te_pairfree(db: DeviceBins, n_per_var: torch.Tensor, b_max: int, tau: int = 
     if out is None:
         out = (torch.zeros((n, n), dtype=torch.float32, device=dev) if matrix
                else torch.empty(max(n_pairs, 0), dtype=torch.float32, device=dev))
-    ws = workspace(dev, n, db.row_len)
+    ws = workspace(dev, n, db.row_len, b_max)
     s = native.stream_ptr()
     lag = tau * db.K
     if counts is not None:
@@ -135,7 +135,7 @@ def surrogate_accumulate(db: DeviceBins, n_per_var: torch.Tensor, b_max: int, ta
     if n_pairs is None:
         n_pairs = n * (n - 1) - pair_offset
     if ws is None:
-        ws = workspace(db.data.device, n, db.row_len)
+        ws = workspace(db.data.device, n, db.row_len, b_max)
     native.call("tenex_surrogate_accumulate", db.data.data_ptr(), db.ld,
                 n_per_var.data_ptr(), int(b_max), n, db.row_len, tau * db.K, int(pair_offset),
                 int(n_pairs), observed.data_ptr(), ssum.data_ptr(), ssq.data_ptr(),

@@ -59,7 +59,7 @@ _SIGS = {
     "tenex_abi_version": [],
     "tenex_last_error": [ctypes.c_char_p, _S],
     "tenex_device_query": [_I, ctypes.POINTER(DevInfo)],
-    "tenex_te_workspace_bytes": [_I, _L],
+    "tenex_te_workspace_bytes": [_I, _L, _I],
     "tenex_workspace_status": [_P, _P],
     "tenex_te_pairfree": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _I, _L, _P, _S,
                           ctypes.POINTER(TeConfig), _P],
@@ -68,6 +68,8 @@ _SIGS = {
     "tenex_surrogate_accumulate": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _P, _P, _P, _P, _S,
                                    ctypes.POINTER(TeConfig), _P],
     "tenex_block_shuffle": [_P, _L, _I, _L, _I, _P, _I, _I, _P, _L, _P],
+    "tenex_probe_smem_atomics": [_I, _I, ctypes.POINTER(ctypes.c_int64),
+                                 ctypes.POINTER(ctypes.c_float), _P],
 }
 _RESTYPES = {"tenex_te_workspace_bytes": ctypes.c_size_t}
 
@@ -128,3 +130,12 @@ def device_info(device: int | None = None) -> DevInfo:
 
 def te_config(threads=0, ctas_per_sm=0, src_chunk=0, smem_bytes=0) -> TeConfig:
     return TeConfig(int(threads), int(ctas_per_sm), int(src_chunk), int(smem_bytes))
+
+
+def probe_smem_atomics(mode: int = 0, iters: int = 4096) -> float:
+    """Measured shared-memory atomic increments per second over all SMs."""
+    inc = ctypes.c_int64()
+    ms = ctypes.c_float()
+    call("tenex_probe_smem_atomics", int(mode), int(iters), ctypes.byref(inc), ctypes.byref(ms),
+         stream_ptr())
+    return inc.value / (ms.value * 1e-3)

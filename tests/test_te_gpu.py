@@ -26,16 +26,18 @@ def _gpu_te(bins, npv, bmax, cuda, tau=1, **kw):
     return out
 
 
+@pytest.mark.parametrize("threads", [128, 512])
 @pytest.mark.parametrize("b_lo,b_hi,T", [(1, 4, 300), (2, 12, 1000), (2, 32, 700),
-                                         (17, 38, 400)])
-def test_counts_bitexact_and_te(cuda, b_lo, b_hi, T):
+                                         (17, 38, 400), (2, 16, 3000), (1, 2, 500)])
+def test_counts_bitexact_and_te(cuda, b_lo, b_hi, T, threads):
     rng = np.random.default_rng(b_hi * 100 + T)
     n = 9
     bins, npv, bmax = _rand_bins(rng, n, T, b_lo, b_hi)
     P = n * (n - 1)
     stride = bmax ** 3
     counts = torch.full((P, stride), -1, dtype=torch.int32, device=cuda)
-    te = _gpu_te(bins, npv, bmax, cuda, counts=counts, counts_stride=stride).cpu().numpy()
+    te = _gpu_te(bins, npv, bmax, cuda, counts=counts, counts_stride=stride,
+                 cfg=dict(threads=threads)).cpu().numpy()
     cnt = counts.cpu().numpy()
     for p in range(P):
         t, sl = divmod(p, n - 1)
@@ -73,18 +75,41 @@ def test_pair_ranges_and_launch_shapes(cuda):
     ref = O.te_pairfree(bins, npv)
     db = D.pack_bins(bins, cuda)
     npv_t = torch.as_tensor(npv, device=cuda)
-    for cfg in (None, dict(threads=128, src_chunk=7), dict(threads=1024, ctas_per_sm=2,
-                                                           src_chunk=3),
-                dict(threads=256, smem_bytes=48 * 1024, src_chunk=64)):
+    for cfg in (None, dict(threads=128, src_chunk=7),
+                dict(threads=1024, ctas_per_sm=2, src_chunk=3),
+                dict(threads=256, smem_bytes=48 * 1024, src_chunk=64),
+                dict(threads=256, ctas_per_sm=2, src_chunk=5),
+                dict(smem_bytes=40 * 1024, threads=1024),
+                dict(smem_bytes=24 * 1024, threads=128)):
         for p0, cnt in ((0, n * (n - 1)), (5, 77), (n * (n - 1) - 13, 13), (123, 1)):
             te = D.te_pairfree(db, npv_t, bmax, pair_offset=p0, n_pairs=cnt, cfg=cfg)
             assert np.max(np.abs(te.cpu().numpy() - ref[p0:p0 + cnt])) <= TOL, (cfg, p0)
 
 
-def test_long_series_u32_counters(cuda):
+@pytest.mark.parametrize("threads", [256, 1024])
+def test_long_series_u32_counters(cuda, threads):
     rng = np.random.default_rng(77)
     bins, npv, bmax = _rand_bins(rng, 5, 70001, 2, 16)  # N >= 65536: 32-bit counters
-    te = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
+    te = _gpu_te(bins, npv, bmax, cuda, cfg=dict(threads=threads)).cpu().numpy()
+    assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
+
+
+def test_shared_slot_counts(cuda):
+    """Small shared memory forces several warps per slot (named barriers); counts exact."""
+    rng = np.random.default_rng(12)
+    n = 6
+    bins, npv, bmax = _rand_bins(rng, n, 2500, 10, 16)
+    P = n * (n - 1)
+    stride = bmax ** 3
+    counts = torch.full((P, stride), -1, dtype=torch.int32, device=cuda)
+    te = _gpu_te(bins, npv, bmax, cuda, counts=counts, counts_stride=stride,
+                 cfg=dict(smem_bytes=24 * 1024, threads=1024)).cpu().numpy()
+    cnt = counts.cpu().numpy()
+    for p in range(P):
+        t, sl = divmod(p, n - 1)
+        s = sl + (sl >= t)
+        ref = O.counts(bins, 1, t, s, npv).reshape(-1)
+        assert np.array_equal(cnt[p, :ref.size], ref), (p, t, s)
     assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
 
 
@@ -121,3 +146,29 @@ def test_determinism(cuda):
     a = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
     b = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
     assert np.array_equal(a, b)
+
+
+def test_skewed_bins_dominant_value_derivation(cuda):
+    """Heavily skewed and constant genes exercise the derived row/column."""
+    rng = np.random.default_rng(21)
+    n, T = 12, 4000
+    x = np.zeros((n, T), np.int32)
+    for g in range(n):
+        b = int(rng.integers(2, 20))
+        p = np.ones(b)
+        p[0] = 40.0 * (g % 3)  # g % 3 == 0: no dominant value
+        p /= p.sum()
+        x[g] = rng.choice(b, T, p=p)
+    x[5] = 3  # constant gene
+    bins, npv, bmax = O.remap(x)
+    P = n * (n - 1)
+    stride = bmax ** 3
+    counts = torch.full((P, stride), -1, dtype=torch.int32, device=cuda)
+    te = _gpu_te(bins, npv, bmax, cuda, counts=counts, counts_stride=stride).cpu().numpy()
+    cnt = counts.cpu().numpy()
+    for p in range(P):
+        t, sl = divmod(p, n - 1)
+        s = sl + (sl >= t)
+        ref = O.counts(bins, 1, t, s, npv).reshape(-1)
+        assert np.array_equal(cnt[p, :ref.size], ref), (p, t, s)
+    assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
