@@ -107,6 +107,19 @@ int tenex_te_pairfree_counts(const uint8_t* bins, int64_t ld, const int32_t* n_p
                              void* workspace, size_t workspace_bytes,
                              const tenex_te_config* cfg, void* stream);
 
+/* TE for an explicit pair list (the source-filter path of the reference:
+ * te_smem_launch, tenex/csrc/full_smem.cu:319-347, and compute_single_gpu).
+ * pairs: device int64 (n_pairs, 2) = [target, source], grouped so that equal
+ * targets are consecutive; item_start: device int64 (n_items + 1) splitting the
+ * list into runs of one target (the caller chooses the run length, e.g. <= 128).
+ * out[i] = TE(pairs[i,1] -> pairs[i,0]). Malformed items (mixed targets, indices
+ * out of range) are skipped and reported by tenex_workspace_status. */
+int tenex_te_pairs(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                   int b_max, int n_vars, int64_t row_len, int64_t lag,
+                   const int64_t* pairs, int64_t n_pairs, const int64_t* item_start,
+                   int64_t n_items, float* out, void* workspace, size_t workspace_bytes,
+                   const tenex_te_config* cfg, void* stream);
+
 /* Surrogate accumulation: TE of already-shuffled bins for the pair range, then
  * sum[s*n+t] += te, sumsq[s*n+t] += te^2 (te rounded to float32 first, then
  * widened), count_ge[s*n+t] += (te >= observed[s*n+t]).
@@ -127,6 +140,43 @@ int tenex_surrogate_accumulate(const uint8_t* bins, int64_t ld, const int32_t* n
 int tenex_block_shuffle(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T, int K,
                         const int32_t* perm, int n_blocks, int block_length,
                         uint8_t* out, int64_t out_ld, void* stream);
+
+/* FSBW-L discretisation, bit-identical to the reference's numpy path
+ * (bin_fsbw_l_numpy, tenex/preprocess.py:61-88, then clamp(min=0) of :680):
+ * x float32 (n_vars, T) row stride ldx; bins int32 (n_vars, T) row stride ldb;
+ * n_bins[g] = ceil((max-min)/std). T <= 114688. */
+int tenex_fsbwl_bins(const float* x, int64_t ldx, int n_vars, int T, float kp,
+                     int32_t* bins, int64_t ldb, int32_t* n_bins, void* stream);
+
+/* Dense per-gene relabelling, replaces remap_bins (tenex/preprocess.py:401-459):
+ * out[g, i] = rank of max(raw[g, i], 0) among gene g's distinct values.
+ * in_bytes 1 (uint8), 2 (uint16) or 4 (int32); out_bytes 1 (uint8) or 2 (uint16).
+ * *err (device int, caller-zeroed) becomes 1 if a gene spans more than 8192 raw
+ * values, 2 if a gene has more distinct values than the output type holds. */
+int tenex_remap_dense(const void* raw, int in_bytes, int64_t ldr, int n_vars, int64_t row_len,
+                      void* out, int out_bytes, int64_t ldo, int32_t* n_per_var, int* err,
+                      void* stream);
+
+/* In-place coarsening of uint8 padded rows, replaces coarsen_bins / coarsen_bins_cuda
+ * (tenex/preprocess.py:462-551, tenex/csrc/adaptive_smem.cu:557-592):
+ * genes with n_per_var > limit get bin*limit/n_per_var and n_per_var = limit. */
+int tenex_coarsen(uint8_t* bins, int64_t ld, int n_vars, int64_t row_len, int32_t* n_per_var,
+                  int limit, void* stream);
+
+/* Binary (b_max = 2) TE matrix on the tensor cores; replaces compute_te_gemm_b2
+ * (tenex/kernels/gemm_b2.py:307-425) and its Triton epilogue (:65-187).
+ * bins: uint8 {0,1} padded rows; out[src * out_ld + tgt] = TE(src -> tgt)
+ * (diagonal untouched; the caller zeroes it). L = row_len - lag < 2^24.
+ * workspace: tenex_b2_workspace_bytes(), 256-byte aligned (operand copies and
+ * per-gene counts). */
+size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t lag);
+int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
+                           int64_t lag, float* out, int64_t out_ld, void* workspace,
+                           size_t workspace_bytes, void* stream);
+/* Error word of the last tenex_te_binary_matrix call on this workspace
+ * (synchronises `stream`): TENEX_ERR_TIMEOUT if a pipeline wait expired. */
+int tenex_b2_status(const void* workspace, int n_vars, int64_t row_len, int64_t lag,
+                    void* stream);
 
 /* Roofline probe (no reference counterpart): times `iters` shared-memory
  * atomicAdds per thread on every SM (mode 0 conflict-free int32, 1 conflict-free

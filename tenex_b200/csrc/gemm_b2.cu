@@ -1,0 +1,463 @@
+// gemm_b2.cu — binary (b_max = 2) TE matrix on the 5th-generation tensor cores.
+//
+// Reference: tenex/kernels/gemm_b2.py:307-425 (three FP32 cuBLAS GEMMs
+// C = fp.p^T, D = p.p^T, E = f.p^T, with f = x[:, tau:], p = x[:, :-tau],
+// fp = f*p) and the Triton epilogue :65-187 (8 joint cells from C, D, E and
+// per-gene marginals, then sum c*log2(c*c1/(c2a*c2b)) / N).
+//
+// B200 design:
+//   * pack kernel: one pass over the bins writes the three K-major int8
+//     operands F, P, FP (rows padded to a multiple of 128 bytes, zero filled)
+//     and the per-gene counts nf, np, nfp.
+//   * GEMM kernel: one CTA per 128 x 128 (target x source) output tile.
+//     TMA (cp.async.bulk.tensor.2d, no multicast) brings 16-byte x 128-row
+//     planes of FP, P, F (targets) and P (sources) into shared memory in the
+//     K-major SWIZZLE_NONE canonical layout; one thread issues, per 32-byte
+//     K step, three tcgen05.mma.kind::i8 (FP x P^T -> C, P x P^T -> D,
+//     F x P^T -> E) into int32 accumulators in TMEM (3 x 128 columns). The
+//     counts are exact integers (int32, N < 2^31).
+//   * Epilogue: four warps read their 32 TMEM lanes (one target row each) with
+//     tcgen05.ld, form the 8 cells and write TE(src -> tgt) to out[src, tgt].
+//   * Every mbarrier wait is bounded; on expiry the kernel records an error
+//     word, drains the copies it issued (bounded), frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+
+#include "common.cuh"
+
+namespace tenex {
+namespace {
+
+constexpr int kTile = 128;     // M = N = 128
+constexpr int kKt = 128;       // bytes of K per pipeline stage (4 MMA K-steps of 32)
+constexpr int kStages = 3;
+constexpr int kPlane = 16 * kTile;             // one 16-byte x 128-row plane
+constexpr int kOpBytes = kKt * kTile;          // one operand tile per stage (16 KB)
+constexpr int kStageBytes = 4 * kOpBytes;      // FP, P, F (targets) + P (sources)
+constexpr int kTmemCols = 512;
+constexpr uint32_t kSpinLimit = 1u << 22;      // bounded mbarrier polling (seconds at most)
+
+struct B2Params {
+  int n;            // genes
+  int L;            // samples per pair
+  int Lpad;         // padded K (multiple of kKt)
+  const int32_t* marg;  // (3, n): nf, np, nfp
+  float* out;       // (n, n): out[src * ld + tgt]
+  int64_t out_ld;
+  int* err;         // device error word (1 = a wait expired)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Polls the phase `parity` of an mbarrier at most kSpinLimit times; false on expiry.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, "
+      "{%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// K-major SWIZZLE_NONE shared-memory descriptor (version 1 for sm_100):
+// start >> 4 in [0,14), LBO >> 4 in [16,30), SBO >> 4 in [32,46), version 1 at [46,48).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t start, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((start >> 4) & 0x3fffu);
+  d |= (uint64_t)((lbo >> 4) & 0x3fffu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3fffu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;  // base_offset 0, lbo_mode 0, layout_type 0 (SWIZZLE_NONE)
+}
+
+// Instruction descriptor, kind::i8: D s32 (bits 4-5 = 2), A/B unsigned 8-bit (0),
+// K-major A and B, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+  return (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ float cell_term(float c, float c1, float c2a, float c2b) {
+  return c > 0.f ? c * log2f(__fdiv_rn(c * c1, c2a * c2b)) : 0.f;
+}
+
+// Pack: F[g, t] = x[g, t+lag], P[g, t] = x[g, t], FP = F & P for t < L (0 beyond),
+// plus nf, np, nfp. One CTA per gene.
+__global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L,
+                               int lag, int Lpad, uint8_t* __restrict__ ops,
+                               int32_t* __restrict__ marg) {
+  const int g = blockIdx.x;
+  const uint8_t* row = bins + (int64_t)g * ld;
+  uint8_t* Fr = ops + ((int64_t)0 * n + g) * Lpad;
+  uint8_t* Pr = ops + ((int64_t)1 * n + g) * Lpad;
+  uint8_t* FPr = ops + ((int64_t)2 * n + g) * Lpad;
+  int nf = 0, np = 0, nfp = 0;
+  for (int t = threadIdx.x; t < Lpad; t += blockDim.x) {
+    uint8_t f = 0, p = 0;
+    if (t < L) {
+      f = row[t + lag] ? 1 : 0;
+      p = row[t] ? 1 : 0;
+    }
+    Fr[t] = f;
+    Pr[t] = p;
+    FPr[t] = f & p;
+    nf += f;
+    np += p;
+    nfp += f & p;
+  }
+  __shared__ int red[3][32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    nf += __shfl_xor_sync(0xffffffffu, nf, o);
+    np += __shfl_xor_sync(0xffffffffu, np, o);
+    nfp += __shfl_xor_sync(0xffffffffu, nfp, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = nf;
+    red[1][threadIdx.x >> 5] = np;
+    red[2][threadIdx.x >> 5] = nfp;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    int s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+    marg[(int64_t)threadIdx.x * n + g] = s;
+  }
+}
+
+// Tensor maps of the three operand matrices (each n x Lpad bytes).
+struct B2Maps {
+  CUtensorMap F, P, FP;
+};
+
+__global__ void __launch_bounds__(128, 1)
+    b2_gemm_kernel(const __grid_constant__ B2Maps maps, B2Params prm) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte align the operand region
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* stage_base = smem;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* accbar = empty + kStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accbar + 1);
+  int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int m0 = blockIdx.y * kTile;  // targets
+  const int n0 = blockIdx.x * kTile;  // sources
+  const int nk = prm.Lpad / kKt;
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accbar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (tid == 0) {
+    // ---- producer: TMA loads of stage k into buffer k % kStages -----------
+    // (one thread also issues the MMAs: producer runs kStages ahead)
+    const uint32_t idesc = idesc_i8(kTile, kTile);
+    int issued = 0;
+    bool ok = true;
+    auto load_stage = [&](int k) {
+      const int s = k % kStages;
+      unsigned char* buf = stage_base + s * kStageBytes;
+      mbar_expect_tx(&full[s], kStageBytes);
+      const int x0 = k * kKt;
+      for (int c = 0; c < kKt / 16; ++c) {
+        tma_load_2d(buf + 0 * kOpBytes + c * kPlane, &maps.FP, x0 + 16 * c, m0, &full[s]);
+        tma_load_2d(buf + 1 * kOpBytes + c * kPlane, &maps.P, x0 + 16 * c, m0, &full[s]);
+        tma_load_2d(buf + 2 * kOpBytes + c * kPlane, &maps.F, x0 + 16 * c, m0, &full[s]);
+        tma_load_2d(buf + 3 * kOpBytes + c * kPlane, &maps.P, x0 + 16 * c, n0, &full[s]);
+      }
+    };
+    const int pre = nk < kStages ? nk : kStages;
+    for (int k = 0; k < pre; ++k) load_stage(k);
+    issued = pre;
+    for (int k = 0; k < nk && ok; ++k) {
+      const int s = k % kStages;
+      const uint32_t ph = (uint32_t)((k / kStages) & 1);
+      if (!mbar_wait(&full[s], ph)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      unsigned char* buf = stage_base + s * kStageBytes;
+      const uint32_t aFP = smem_u32(buf + 0 * kOpBytes);
+      const uint32_t aP = smem_u32(buf + 1 * kOpBytes);
+      const uint32_t aF = smem_u32(buf + 2 * kOpBytes);
+      const uint32_t bP = smem_u32(buf + 3 * kOpBytes);
+#pragma unroll
+      for (int kk = 0; kk < kKt / 32; ++kk) {
+        const uint32_t off = kk * 2 * kPlane;  // two 16-byte planes per 32-byte K step
+        const uint64_t bd = smem_desc(bP + off, kPlane, 128);
+        const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+        mma_i8(tmem + 0, smem_desc(aFP + off, kPlane, 128), bd, idesc, acc);
+        mma_i8(tmem + 128, smem_desc(aP + off, kPlane, 128), bd, idesc, acc);
+        mma_i8(tmem + 256, smem_desc(aF + off, kPlane, 128), bd, idesc, acc);
+      }
+      mma_commit(&empty[s]);  // stage s free once these MMAs complete
+      const int kn = k + kStages;
+      if (kn < nk) {
+        if (!mbar_wait(&empty[s], ph)) {
+          ok = false;
+          break;
+        }
+        load_stage(kn);
+        issued = kn + 1;
+      }
+    }
+    if (ok) {
+      mma_commit(accbar);
+    } else {
+      // drain: wait (bounded) for every stage load still in flight, then abort
+      atomicExch(prm.err, 1);
+      for (int k = 0; k < issued; ++k) {
+        const int s = k % kStages;
+        (void)mbar_wait(&full[s], (uint32_t)((k / kStages) & 1));
+      }
+      *(volatile int*)abort_flag = 1;
+      mma_commit(accbar);  // still arrives (after any issued MMAs) so waiters wake
+    }
+  }
+
+  // ---- epilogue: all 4 warps, thread tid <-> tile row (target) ------------
+  bool ok_acc = mbar_wait(accbar, 0);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!ok_acc && tid == 0) atomicExch(prm.err, 1);
+  const bool run = ok_acc && (*(volatile int*)abort_flag == 0);
+  const int i = m0 + tid;  // target gene of this thread's TMEM lane
+  const float N = (float)prm.L;
+  float nf = 0.f, np_ = 0.f, nfp = 0.f;
+  if (i < prm.n) {
+    nf = (float)prm.marg[i];
+    np_ = (float)prm.marg[prm.n + i];
+    nfp = (float)prm.marg[2 * prm.n + i];
+  }
+  const float c1_1 = np_, c1_0 = N - np_;
+  const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+  for (int cb = 0; cb < kTile; cb += 16) {
+    uint32_t rc[16], rd[16], re[16];
+    tmem_ld16(lane_base + 0 + cb, rc);
+    tmem_ld16(lane_base + 128 + cb, rd);
+    tmem_ld16(lane_base + 256 + cb, re);
+    tmem_wait_ld();
+    if (!run || i >= prm.n) continue;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int j = n0 + cb + q;  // source gene
+      if (j >= prm.n || j == i) continue;
+      const float npj = (float)prm.marg[prm.n + j];
+      const float C = (float)rc[q], Dv = (float)rd[q], E = (float)re[q];
+      const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
+      float te = 0.f;
+      te += cell_term(C, c1_1, c2a11, c2b11);                                   // [1,1,1]
+      te += cell_term(Dv - C, c1_1, c2a01, c2b11);                              // [0,1,1]
+      te += cell_term(E - C, c1_0, c2a10, c2b01);                               // [1,0,1]
+      te += cell_term(npj - Dv - E + C, c1_0, c2a00, c2b01);                    // [0,0,1]
+      te += cell_term(nfp - C, c1_1, c2a11, c2b10);                             // [1,1,0]
+      te += cell_term(np_ - Dv - nfp + C, c1_1, c2a01, c2b10);                  // [0,1,0]
+      te += cell_term(nf - E - nfp + C, c1_0, c2a10, c2b00);                    // [1,0,0]
+      te += cell_term(N - nf - np_ - npj + nfp + Dv + E - C, c1_0, c2a00, c2b00);  // [0,0,0]
+      prm.out[(int64_t)j * prm.out_ld + i] = (float)((double)te / (double)prm.L);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static std::once_flag once;
+  static EncodeTiledFn fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+static int make_map(CUtensorMap* map, const uint8_t* base, int rows, int Lpad) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return fail(TENEX_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
+  const cuuint64_t dims[2] = {(cuuint64_t)Lpad, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)Lpad};
+  const cuuint32_t box[2] = {16, (cuuint32_t)kTile};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(TENEX_ERR_LAUNCH, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return TENEX_OK;
+}
+
+}  // namespace
+}  // namespace tenex
+
+using namespace tenex;
+
+extern "C" size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t lag) {
+  if (n_vars < 1 || row_len <= lag) return 256;
+  const int64_t L = row_len - lag;
+  const int64_t Lpad = round_up(L, kKt);
+  return (size_t)(round_up(3 * (int64_t)n_vars * Lpad, 256) + round_up(3 * (int64_t)n_vars * 4, 256) +
+                  256);
+}
+
+extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
+                                      int64_t lag, float* out, int64_t out_ld, void* workspace,
+                                      size_t workspace_bytes, void* stream_) {
+  cudaStream_t stream = as_stream(stream_);
+  if (!bins || !out || !workspace) return fail(TENEX_ERR_BADARG, "bins, out, workspace non-NULL");
+  if (n_vars < 2) return fail(TENEX_ERR_BADARG, "n_vars must be >= 2");
+  if (lag < 1 || row_len <= lag)
+    return fail(TENEX_ERR_BADARG, "need 1 <= lag < row_len");
+  if (ld < row_len) return fail(TENEX_ERR_BADARG, "ld must be >= row_len");
+  if (out_ld < n_vars) return fail(TENEX_ERR_BADARG, "out_ld must be >= n_vars");
+  const int64_t L = row_len - lag;
+  if (L >= ((int64_t)1 << 24))
+    return fail(TENEX_ERR_UNSUPPORTED, "L=%lld: float32 cell counts are exact only below 2^24",
+                (long long)L);
+  const int64_t Lpad = round_up(L, kKt);
+  if ((int64_t)workspace_bytes < (int64_t)tenex_b2_workspace_bytes(n_vars, row_len, lag))
+    return fail(TENEX_ERR_OOM, "workspace too small (tenex_b2_workspace_bytes)");
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+    return fail(TENEX_ERR_BADARG, "workspace must be 256-byte aligned");
+  unsigned char* ws = reinterpret_cast<unsigned char*>(workspace);
+  uint8_t* ops = ws;
+  int32_t* marg = reinterpret_cast<int32_t*>(ws + round_up(3 * (int64_t)n_vars * Lpad, 256));
+  int* err = reinterpret_cast<int*>(ws + round_up(3 * (int64_t)n_vars * Lpad, 256) +
+                                    round_up(3 * (int64_t)n_vars * 4, 256));
+  cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return check_cuda(e, "memset");
+  b2_pack_kernel<<<n_vars, 256, 0, stream>>>(bins, ld, n_vars, (int)L, (int)lag, (int)Lpad, ops,
+                                             marg);
+  int st = check_launch("b2_pack_kernel");
+  if (st) return st;
+  B2Maps maps;
+  if ((st = make_map(&maps.F, ops, n_vars, (int)Lpad))) return st;
+  if ((st = make_map(&maps.P, ops + (int64_t)n_vars * Lpad, n_vars, (int)Lpad))) return st;
+  if ((st = make_map(&maps.FP, ops + 2 * (int64_t)n_vars * Lpad, n_vars, (int)Lpad))) return st;
+  B2Params prm;
+  prm.n = n_vars;
+  prm.L = (int)L;
+  prm.Lpad = (int)Lpad;
+  prm.marg = marg;
+  prm.out = out;
+  prm.out_ld = out_ld;
+  prm.err = err;
+  const int smem = kStages * kStageBytes + 1024 + 256;
+  e = cudaFuncSetAttribute(b2_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+  const unsigned tiles = (unsigned)((n_vars + kTile - 1) / kTile);
+  b2_gemm_kernel<<<dim3(tiles, tiles), 128, smem, stream>>>(maps, prm);
+  return check_launch("b2_gemm_kernel");
+}
+
+extern "C" int tenex_b2_status(const void* workspace, int n_vars, int64_t row_len, int64_t lag,
+                               void* stream) {
+  if (!workspace) return fail(TENEX_ERR_BADARG, "workspace is NULL");
+  const int64_t L = row_len - lag;
+  const int64_t Lpad = round_up(L, kKt);
+  const unsigned char* ws = reinterpret_cast<const unsigned char*>(workspace);
+  const int* err = reinterpret_cast<const int*>(ws + round_up(3 * (int64_t)n_vars * Lpad, 256) +
+                                                round_up(3 * (int64_t)n_vars * 4, 256));
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, as_stream(stream));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+  if (e != cudaSuccess) return check_cuda(e, "tenex_b2_status");
+  if (h) return fail(TENEX_ERR_TIMEOUT, "a tensor-core pipeline wait expired; results invalid");
+  return TENEX_OK;
+}

@@ -67,6 +67,10 @@ struct TeParams {
   int64_t counts_stride;
   const int32_t* marg;  // (n, bmax) per-gene marginal over [0, N)
   const int32_t* ydom;  // (n,) most frequent bin of each gene over [0, N)
+  // pair-list mode (pairs != nullptr): item q is pairs[item_start[q] .. item_start[q+1])
+  // of one target; output index = position in the list
+  const int64_t* pairs;
+  const int64_t* item_start;
   WsHeader* ws;
 };
 
@@ -213,8 +217,13 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
   const int bt2 = bt * bt;
   for (int r = g; r < n_src; r += n_groups) {
     const int64_t p = lo + r;
-    const int sl = (int)(p - base);
-    const int src = sl + (sl >= tgt);
+    int src;
+    if (P.pairs) {
+      src = (int)P.pairs[2 * p + 1];
+    } else {
+      const int sl = (int)(p - base);
+      src = sl + (sl >= tgt);
+    }
     const uint32_t bs = (uint32_t)P.npv[src];
     const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
     const uint32_t yd = (uint32_t)P.ydom[src];
@@ -402,27 +411,58 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     __syncthreads();
     const int64_t q = (int64_t)misc[0];
     if (q >= P.n_items) break;
-    const int chunk = (int)(q / P.n_targets);
-    const int tgt = P.t_first + (int)(q % P.n_targets);
-    const int64_t base = (int64_t)tgt * nm1;
-    int64_t lo = base + (int64_t)chunk * P.W;
-    int64_t hi = base + min((int64_t)(chunk + 1) * P.W, (int64_t)nm1);
-    lo = max(lo, P.p0);
-    hi = min(hi, P.p1);
+    int tgt;
+    int64_t lo, hi, base = 0;
+    if (P.pairs) {
+      lo = P.item_start[q];
+      hi = P.item_start[q + 1];
+      if (lo < 0 || hi > P.p1 || lo > hi) {  // malformed item table: skip, report
+        if (tid == 0) atomicExch(&P.ws->bad_data, 2);
+        __syncthreads();
+        continue;
+      }
+      tgt = lo < hi ? (int)P.pairs[2 * lo] : 0;
+    } else {
+      const int chunk = (int)(q / P.n_targets);
+      tgt = P.t_first + (int)(q % P.n_targets);
+      base = (int64_t)tgt * nm1;
+      lo = base + (int64_t)chunk * P.W;
+      hi = base + min((int64_t)(chunk + 1) * P.W, (int64_t)nm1);
+      lo = max(lo, P.p0);
+      hi = min(hi, P.p1);
+    }
     if (lo >= hi) {
       __syncthreads();
       continue;
     }
     const int n_src = (int)(hi - lo);
+    if (P.pairs && (tgt < 0 || tgt >= P.n)) {
+      if (tid == 0) atomicExch(&P.ws->bad_data, 2);
+      __syncthreads();
+      continue;
+    }
     const int bt = P.npv[tgt];
     const int bt2 = bt * bt;
 
-    // ---- max b_s over the item's sources --------------------------------
+    // ---- max b_s over the item's sources (pair lists: also check indices) --
     unsigned my_max = 1;
+    bool bad = tgt < 0 || tgt >= P.n;
     for (int r = tid; r < n_src; r += nthreads) {
-      int sl = (int)(lo + r - base);
-      int src = sl + (sl >= tgt);
+      int src;
+      if (P.pairs) {
+        src = (int)P.pairs[2 * (lo + r) + 1];
+        bad |= P.pairs[2 * (lo + r)] != tgt || src < 0 || src >= P.n;
+        if (src < 0 || src >= P.n) src = 0;
+      } else {
+        int sl = (int)(lo + r - base);
+        src = sl + (sl >= tgt);
+      }
       my_max = max(my_max, (unsigned)P.npv[src]);
+    }
+    if (__syncthreads_or(bad)) {
+      if (tid == 0) atomicExch(&P.ws->bad_data, 2);
+      __syncthreads();
+      continue;
     }
     my_max = dev::warp_max(my_max);
     if ((tid & 31) == 0) reinterpret_cast<unsigned*>(red)[warp] = my_max;
@@ -639,6 +679,10 @@ extern "C" int tenex_workspace_status(const void* workspace, void* stream) {
                                   as_stream(stream));
   if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
   if (e != cudaSuccess) return check_cuda(e, "tenex_workspace_status");
+  if (h.bad_data == 2)
+    return fail(TENEX_ERR_BADDATA,
+                "a pair-list item mixed targets or held an index outside [0, n_vars); those "
+                "pairs were not computed");
   if (h.bad_data)
     return fail(TENEX_ERR_BADDATA,
                 "a bin value was >= its gene's n_per_var, or n_per_var was outside [1, b_max]; "
@@ -648,12 +692,15 @@ extern "C" int tenex_workspace_status(const void* workspace, void* stream) {
   return TENEX_OK;
 }
 
-// Common driver of the TE entry points.
+// Common driver of the TE entry points. pairs/item_start/n_items select the
+// pair-list mode (then p0 must be 0 and n_pairs the list length).
 static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max, int n,
                   int64_t row_len, int64_t lag, int64_t p0, int64_t n_pairs, int out_mode,
                   float* out, int64_t out_ld, const float* obs, double* sum, double* sumsq,
                   int32_t* cnt, int32_t* counts, int64_t counts_stride, void* workspace,
-                  size_t ws_bytes, const tenex_te_config* cfg, void* stream_) {
+                  size_t ws_bytes, const tenex_te_config* cfg, void* stream_,
+                  const int64_t* pairs = nullptr, const int64_t* item_start = nullptr,
+                  int64_t n_items_list = 0) {
   cudaStream_t stream = as_stream(stream_);
   if (!bins || !npv) return fail(TENEX_ERR_BADARG, "bins and n_per_var must be non-NULL");
   if (n < 2) return fail(TENEX_ERR_BADARG, "n_vars must be >= 2 (got %d)", n);
@@ -673,9 +720,11 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
                 "(ld=%lld, row_len=%lld)",
                 (long long)ld, (long long)row_len);
   const int64_t total = (int64_t)n * (n - 1);
-  if (p0 < 0 || n_pairs < 0 || p0 + n_pairs > total)
+  if (!pairs && (p0 < 0 || n_pairs < 0 || p0 + n_pairs > total))
     return fail(TENEX_ERR_BADARG, "pair range [%lld, %lld) outside [0, %lld)", (long long)p0,
                 (long long)(p0 + n_pairs), (long long)total);
+  if (pairs && (!item_start || n_items_list < 0 || n_pairs < 0 || p0 != 0))
+    return fail(TENEX_ERR_BADARG, "pair list needs item_start, n_items >= 0 and n_pairs >= 0");
   if (out_mode != kOutStats && !out) return fail(TENEX_ERR_BADARG, "out must be non-NULL");
   if (out_mode == kOutMatrix && out_ld < n)
     return fail(TENEX_ERR_BADARG, "out_ld (%lld) must be >= n_vars", (long long)out_ld);
@@ -700,13 +749,23 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   P.lag = (int)lag;
   P.p0 = p0;
   P.p1 = p0 + n_pairs;
-  P.t_first = (int)(p0 / (n - 1));
-  const int t_last = (int)((P.p1 - 1) / (n - 1));
-  P.n_targets = t_last - P.t_first + 1;
   P.W = (cfg && cfg->src_chunk) ? cfg->src_chunk : 128;
   if (P.W < 1) return fail(TENEX_ERR_BADARG, "src_chunk must be >= 1");
-  P.n_chunks = (n - 1 + P.W - 1) / P.W;
-  P.n_items = (int64_t)P.n_targets * P.n_chunks;
+  if (pairs) {
+    P.pairs = pairs;
+    P.item_start = item_start;
+    P.n_items = n_items_list;
+    P.t_first = 0;
+    P.n_targets = 1;
+    P.n_chunks = 1;
+  } else {
+    P.t_first = (int)(p0 / (n - 1));
+    const int t_last = (int)((P.p1 - 1) / (n - 1));
+    P.n_targets = t_last - P.t_first + 1;
+    P.n_chunks = (n - 1 + P.W - 1) / P.W;
+    P.n_items = (int64_t)P.n_targets * P.n_chunks;
+  }
+  if (P.n_items == 0) return TENEX_OK;
   if (P.n_items > 0x7fffffffLL - 65536)
     return fail(TENEX_ERR_UNSUPPORTED, "too many work items (%lld); raise src_chunk",
                 (long long)P.n_items);
@@ -788,4 +847,16 @@ extern "C" int tenex_surrogate_accumulate(const uint8_t* bins, int64_t ld,
   return te_run(bins, ld, n_per_var, b_max, n_vars, row_len, lag, pair_offset, n_pairs,
                 kOutStats, nullptr, 0, observed, sum, sumsq, count_ge, nullptr, 0, workspace,
                 workspace_bytes, cfg, stream);
+}
+
+extern "C" int tenex_te_pairs(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                              int b_max, int n_vars, int64_t row_len, int64_t lag,
+                              const int64_t* pairs, int64_t n_pairs, const int64_t* item_start,
+                              int64_t n_items, float* out, void* workspace,
+                              size_t workspace_bytes, const tenex_te_config* cfg,
+                              void* stream) {
+  if (!pairs || !item_start) return fail(TENEX_ERR_BADARG, "pairs and item_start must be non-NULL");
+  return te_run(bins, ld, n_per_var, b_max, n_vars, row_len, lag, 0, n_pairs, kOutPairfree, out,
+                0, nullptr, nullptr, nullptr, nullptr, nullptr, 0, workspace, workspace_bytes,
+                cfg, stream, pairs, item_start, n_items);
 }

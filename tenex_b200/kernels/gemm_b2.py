@@ -1,0 +1,71 @@
+"""GEMM-B2 kernel class: binary (b_max = 2) TE as a tensor-core contraction.
+
+Reference: tenex/kernels/gemm_b2.py (GEMMB2Kernel :565-596, compute_te_gemm_b2
+:307-425). Same name, supports() predicate and compute_matrix() contract
+([i, j] = TE(j -> i), diagonal 0); the counts come from tcgen05 INT8 MMAs with
+int32 accumulators (exact), the 8-cell TE from the TMEM epilogue of the same
+kernel (gemm_b2.cu).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from tenex_b200 import native
+from tenex_b200.kernels import TEKernel
+from tenex_b200.kernels import device as D
+
+
+def te_binary_matrix(db: D.DeviceBins, tau: int = 1, out: torch.Tensor | None = None,
+                     check: bool = True) -> torch.Tensor:
+    """(n, n) float32 device matrix with [src, tgt] = TE(src -> tgt), diagonal 0."""
+    dev = db.data.device
+    n = db.n
+    lag = tau * db.K
+    if out is None:
+        out = torch.zeros((n, n), dtype=torch.float32, device=dev)
+    nb = int(native.lib().tenex_b2_workspace_bytes(n, db.row_len, lag))
+    ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+    s = native.stream_ptr()
+    native.call("tenex_te_binary_matrix", db.data.data_ptr(), db.ld, n, db.row_len, lag,
+                out.data_ptr(), n, ws.data_ptr(), nb, s)
+    if check:
+        native.call("tenex_b2_status", ws.data_ptr(), n, db.row_len, lag, s)
+    return out
+
+
+class GEMMB2Kernel(TEKernel):
+    """Exact binary TE for all pairs from three INT8 tensor-core contractions."""
+
+    @property
+    def name(self) -> str:
+        return "GEMM-B2"
+
+    @property
+    def is_matrix_kernel(self) -> bool:
+        return True
+
+    def supports(self, b_max, on_cuda, smem_optin, smem_bytes, n_per_var,
+                 source_filter) -> bool:
+        return bool(on_cuda) and b_max == 2 and not source_filter
+
+    def compute_matrix_device(self, db: D.DeviceBins, tau: int) -> torch.Tensor:
+        """[src, tgt] = TE(src -> tgt) on the device."""
+        return te_binary_matrix(db, tau)
+
+    def compute_matrix(self, data, n_vars: int, tau: int, device, **kwargs) -> np.ndarray:
+        dev = torch.device(device) if not isinstance(device, torch.device) else device
+        db = D.pack_bins(data, dev, 2)
+        if db.K != 1:
+            raise ValueError(f"GEMM-B2 kernel only supports K=1, got K={db.K}")
+        m = te_binary_matrix(db, tau)
+        return m.t().contiguous().cpu().numpy()  # reference orientation: [i, j] = TE(j -> i)
+
+    def compute_single_gpu(self, bin_arrs, pairs, b_max, n_per_var, tau, batch_size, device,
+                           **kwargs) -> np.ndarray:
+        te = self.compute_matrix(bin_arrs, None, tau, device)
+        p = pairs.cpu().numpy() if isinstance(pairs, torch.Tensor) else np.asarray(pairs)
+        return te[p[:, 0], p[:, 1]]
+
+    def log_description(self, **kwargs) -> str:
+        return "GEMM-B2 (tcgen05 INT8 contractions + fused TE epilogue, exact)"

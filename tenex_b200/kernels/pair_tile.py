@@ -1,0 +1,117 @@
+"""Shared implementation of the Full-SMEM and Adaptive-SMEM kernel classes.
+
+Both reference backends (tenex/kernels/full_smem.py, tenex/kernels/adaptive_smem.py)
+map to one persistent sm_100a kernel (te_pair_tile_kernel): per-gene bin
+counts are read on the device, so a uniform-b run (Full-SMEM) and an uneven
+run (Adaptive-SMEM) are the same launch. The classes keep the reference's
+names, supports() predicates and prepare() (coarsening) so kernel choice and
+the bins the kernel sees are the reference's.
+"""
+from __future__ import annotations
+
+from typing import Optional
+
+import numpy as np
+import torch
+
+from tenex_b200.kernels import TEKernel
+from tenex_b200.kernels import device as D
+
+# Launch shapes the autotuner tries: (threads, ctas_per_sm, src_chunk)
+TUNE_SPACE = [(512, 2, 128), (1024, 1, 128), (512, 1, 128), (256, 2, 64), (1024, 1, 64),
+              (512, 2, 64)]
+DEFAULT_CFG = dict(threads=512, ctas_per_sm=2, src_chunk=128)
+_tune_cache: dict[tuple, dict] = {}
+
+
+def _npv_tensor(n_per_var, device) -> torch.Tensor:
+    return torch.as_tensor(np.asarray(n_per_var.cpu() if isinstance(n_per_var, torch.Tensor)
+                                      else n_per_var), dtype=torch.int32).to(device)
+
+
+def autotune(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int = 1,
+             sample_pairs: int = 400_000, space=TUNE_SPACE) -> dict:
+    """Times each launch shape on a contiguous slice of pair ids (whole targets
+    from the middle of the range) and returns the fastest; cached per
+    (device, n, T, K, b_max, tau, bin-count histogram)."""
+    dev = db.data.device
+    npv_h = npv.cpu().numpy()
+    key = (torch.cuda.get_device_name(dev), db.n, db.T, db.K, int(b_max), int(tau),
+           tuple(np.bincount(np.minimum(npv_h, 64), minlength=65)[::4]))
+    if key in _tune_cache:
+        return _tune_cache[key]
+    n = db.n
+    total = n * (n - 1)
+    cnt = min(total, max(n - 1, (sample_pairs // (n - 1)) * (n - 1)))
+    p0 = ((total - cnt) // 2) // (n - 1) * (n - 1)
+    best, best_t = dict(DEFAULT_CFG), float("inf")
+    for th, cps, w in space:
+        cfg = dict(threads=th, ctas_per_sm=cps, src_chunk=w)
+        try:
+            D.te_pairfree(db, npv, b_max, tau, p0, cnt, cfg=cfg, check_data=False)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            D.te_pairfree(db, npv, b_max, tau, p0, cnt, cfg=cfg, check_data=False)
+            e1.record()
+            e1.synchronize()
+            t = e0.elapsed_time(e1)
+        except Exception:
+            continue
+        if t < best_t:
+            best, best_t = cfg, t
+    _tune_cache[key] = best
+    return best
+
+
+class PairTileKernel(TEKernel):
+    """Pair-free / pair-list TE through the persistent shared-memory kernel."""
+
+    cfg: Optional[dict] = None  # launch shape override (None: tuned or default)
+
+    @property
+    def supports_pairfree(self) -> bool:
+        return True
+
+    def peak_bytes_per_pair(self, b_max, T, K, tau=1):
+        return 4
+
+    def launch_cfg(self, db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int,
+                   autotune_shape: bool) -> dict:
+        if self.cfg is not None:
+            return self.cfg
+        if autotune_shape:
+            return autotune(db, npv, b_max, tau)
+        return DEFAULT_CFG
+
+    def compute_pairfree_device(self, db: D.DeviceBins, n_per_var, b_max: int, tau: int,
+                                pair_offset: int = 0, n_pairs: Optional[int] = None,
+                                matrix: bool = False, out: Optional[torch.Tensor] = None,
+                                autotune_shape: bool = False) -> torch.Tensor:
+        """Device-resident result: pair-free float32 vector, or the (n, n) matrix
+        with [src, tgt] = TE(src -> tgt) when matrix=True."""
+        npv = _npv_tensor(n_per_var, db.data.device)
+        cfg = self.launch_cfg(db, npv, b_max, tau, autotune_shape)
+        return D.te_pairfree(db, npv, int(b_max), tau, pair_offset, n_pairs, out=out,
+                             matrix=matrix, cfg=cfg)
+
+    def compute_pairfree(self, bin_arrs, n_vars: int, b_max: int, n_per_var, tau: int,
+                         device, pair_offset: int = 0,
+                         n_pairs_local: Optional[int] = None) -> np.ndarray:
+        dev = torch.device(device) if not isinstance(device, torch.device) else device
+        db = D.pack_bins(bin_arrs, dev, b_max)
+        if db.n != n_vars:
+            raise ValueError(f"bin_arrs has {db.n} variables, n_vars={n_vars}")
+        te = self.compute_pairfree_device(db, n_per_var, b_max, tau, pair_offset,
+                                          n_pairs_local)
+        return te.cpu().numpy()
+
+    def compute_single_gpu(self, bin_arrs, pairs, b_max, n_per_var, tau, batch_size, device,
+                           **kwargs) -> np.ndarray:
+        from tenex_b200.kernels.pair_list import te_pair_list
+        dev = torch.device(device) if not isinstance(device, torch.device) else device
+        db = D.pack_bins(bin_arrs, dev, b_max)
+        npv = _npv_tensor(n_per_var, dev)
+        pr = pairs.cpu().numpy() if isinstance(pairs, torch.Tensor) else np.asarray(pairs)
+        return te_pair_list(db, npv, int(b_max), tau, pr, cfg=self.cfg).cpu().numpy()

@@ -65,13 +65,22 @@ _SIGS = {
                           ctypes.POINTER(TeConfig), _P],
     "tenex_te_pairfree_counts": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _P, _L, _P, _S,
                                  ctypes.POINTER(TeConfig), _P],
+    "tenex_te_pairs": [_P, _L, _P, _I, _I, _L, _L, _P, _L, _P, _L, _P, _P, _S,
+                       ctypes.POINTER(TeConfig), _P],
     "tenex_surrogate_accumulate": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _P, _P, _P, _P, _S,
                                    ctypes.POINTER(TeConfig), _P],
     "tenex_block_shuffle": [_P, _L, _I, _L, _I, _P, _I, _I, _P, _L, _P],
+    "tenex_fsbwl_bins": [_P, _L, _I, _I, ctypes.c_float, _P, _L, _P, _P],
+    "tenex_remap_dense": [_P, _I, _L, _I, _L, _P, _I, _L, _P, _P, _P],
+    "tenex_coarsen": [_P, _L, _I, _L, _P, _I, _P],
+    "tenex_b2_workspace_bytes": [_I, _L, _L],
+    "tenex_te_binary_matrix": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _P],
+    "tenex_b2_status": [_P, _I, _L, _L, _P],
     "tenex_probe_smem_atomics": [_I, _I, ctypes.POINTER(ctypes.c_int64),
                                  ctypes.POINTER(ctypes.c_float), _P],
 }
-_RESTYPES = {"tenex_te_workspace_bytes": ctypes.c_size_t}
+_RESTYPES = {"tenex_te_workspace_bytes": ctypes.c_size_t,
+             "tenex_b2_workspace_bytes": ctypes.c_size_t}
 
 _lib = None
 _lock = threading.Lock()

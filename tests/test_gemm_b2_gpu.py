@@ -1,0 +1,44 @@
+"""tcgen05 binary TE kernel against the oracle and the reference GEMM-B2 fixture."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tenex_b200 import workloads as W
+from tenex_b200.kernels import device as D
+from tenex_b200.kernels.gemm_b2 import te_binary_matrix
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def _run(x, cuda, tau=1):
+    db = D.pack_bins(x, cuda)
+    m = te_binary_matrix(db, tau).cpu().numpy()
+    torch.cuda.synchronize()
+    return m
+
+
+@pytest.mark.parametrize("n,T", [(5, 40), (130, 300), (257, 1100)])
+def test_binary_matrix_matches_oracle(cuda, n, T):
+    x, _ = W.cfg2_binary(n=n, T=T, seed=n + T, n_planted=min(3, n // 2))
+    m = _run(x, cuda)
+    ref = O.te_matrix(x.astype(np.int32), np.full(n, 2, np.int32))
+    assert np.all(np.diag(m) == 0)
+    assert np.max(np.abs(m - ref)) <= TOL
+
+
+def test_binary_matches_reference_fixture(cuda, golden):
+    g = golden("gemm_b2.npz")
+    m = _run(g["bins"], cuda)
+    assert np.max(np.abs(m - g["te_ij_j_to_i"].T)) <= TOL
+
+
+def test_binary_tau2_constant_rows(cuda):
+    rng = np.random.default_rng(2)
+    x = (rng.random((70, 500)) < 0.3).astype(np.uint8)
+    x[3] = 0
+    x[4] = 1
+    m = _run(x, cuda, tau=2)
+    ref = O.te_matrix(x.astype(np.int32), np.full(70, 2, np.int32), tau=2)
+    assert np.max(np.abs(m - ref)) <= TOL
