@@ -163,6 +163,14 @@ int tenex_remap_dense(const void* raw, int in_bytes, int64_t ldr, int n_vars, in
 int tenex_coarsen(uint8_t* bins, int64_t ld, int n_vars, int64_t row_len, int32_t* n_per_var,
                   int limit, void* stream);
 
+/* Binarisation 1[x > thr_g] (tenex/binarize.py:225-295; kernels of
+ * tenex/csrc/binarize_cuda.cu:14-56): mode 0 nonzero (thr 0), 1 mean (numpy
+ * float32 mean), 2 caller thresholds[g]. out: uint8 padded rows; n_per_var[g]
+ * = 1 for a constant row, else 2 (the reference's max - min + 1). */
+int tenex_binarize(const float* x, int64_t ldx, int n_vars, int T, int mode,
+                   const float* thresholds, uint8_t* out, int64_t ldo, int32_t* n_per_var,
+                   void* stream);
+
 /* Binary (b_max = 2) TE matrix on the tensor cores; replaces compute_te_gemm_b2
  * (tenex/kernels/gemm_b2.py:307-425) and its Triton epilogue (:65-187).
  * bins: uint8 {0,1} padded rows; out[src * out_ld + tgt] = TE(src -> tgt)

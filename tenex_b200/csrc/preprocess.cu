@@ -284,6 +284,47 @@ __global__ void coarsen_kernel(uint8_t* __restrict__ bins, int64_t ld, int64_t r
     row[i] = (uint8_t)(((int)row[i] * limit) / b);
 }
 
+// Binarisation 1[x > thr_g] into uint8 padded rows, one CTA per gene.
+// mode 0: thr = 0 (nonzero); 1: thr = float32 mean with numpy's pairwise sum and
+// float64 division (np.mean on float32 rows); 2: thr = thr_in[g].
+// n_per_var[g] = max - min + 1 of the binary row (1 if constant, else 2).
+__global__ void binarize_kernel(const float* __restrict__ x, int64_t ldx, int T, int mode,
+                                const float* __restrict__ thr_in, uint8_t* __restrict__ out,
+                                int64_t ldo, int32_t* __restrict__ npv) {
+  __shared__ int lstart[kMaxLeaves];
+  __shared__ int llen[kMaxLeaves];
+  __shared__ float lsum[kMaxLeaves];
+  __shared__ float sh_thr;
+  __shared__ int sh_nl;
+  const int g = blockIdx.x;
+  const float* row = x + (int64_t)g * ldx;
+  const int tid = threadIdx.x;
+  if (mode == 1) {
+    if (tid == 0) sh_nl = enum_leaves(T, lstart, llen);
+    __syncthreads();
+    const int nl = sh_nl;
+    for (int k = tid; k < nl; k += blockDim.x) lsum[k] = leaf_sum(row + lstart[k], llen[k]);
+    __syncthreads();
+    if (tid == 0)
+      sh_thr = __double2float_rn(__ddiv_rn((double)combine_leaves(T, lsum), (double)T));
+  } else if (tid == 0) {
+    sh_thr = mode == 0 ? 0.f : thr_in[g];
+  }
+  __syncthreads();
+  const float thr = sh_thr;
+  uint8_t* orow = out + (int64_t)g * ldo;
+  int any1 = 0, any0 = 0;
+  for (int t = tid; t < T; t += blockDim.x) {
+    const uint8_t b = row[t] > thr ? 1 : 0;
+    orow[t] = b;
+    any1 |= b;
+    any0 |= b ^ 1;
+  }
+  any1 = __syncthreads_or(any1);
+  any0 = __syncthreads_or(any0);
+  if (tid == 0) npv[g] = (any1 && any0) ? 2 : 1;
+}
+
 __global__ void coarsen_npv_kernel(int32_t* npv, int n, int limit) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < n && npv[g] > limit) npv[g] = limit;
@@ -360,4 +401,19 @@ extern "C" int tenex_coarsen(uint8_t* bins, int64_t ld, int n_vars, int64_t row_
   if (st) return st;
   coarsen_npv_kernel<<<(n_vars + 255) / 256, 256, 0, s>>>(n_per_var, n_vars, limit);
   return check_launch("coarsen_npv_kernel");
+}
+
+extern "C" int tenex_binarize(const float* x, int64_t ldx, int n_vars, int T, int mode,
+                              const float* thresholds, uint8_t* out, int64_t ldo,
+                              int32_t* n_per_var, void* stream) {
+  if (!x || !out || !n_per_var) return fail(TENEX_ERR_BADARG, "x, out, n_per_var non-NULL");
+  if (n_vars < 1 || T < 1) return fail(TENEX_ERR_BADARG, "empty expression matrix");
+  if (ldx < T || ldo < T) return fail(TENEX_ERR_BADARG, "row strides must be >= T");
+  if (mode < 0 || mode > 2) return fail(TENEX_ERR_BADARG, "mode must be 0, 1 or 2");
+  if (mode == 2 && !thresholds) return fail(TENEX_ERR_BADARG, "mode 2 needs thresholds");
+  if (mode == 1 && (int64_t)T > (int64_t)kMaxLeaves * 56)
+    return fail(TENEX_ERR_UNSUPPORTED, "T=%d too long for the mean binariser", T);
+  binarize_kernel<<<n_vars, 128, 0, as_stream(stream)>>>(x, ldx, T, mode, thresholds, out, ldo,
+                                                         n_per_var);
+  return check_launch("binarize_kernel");
 }

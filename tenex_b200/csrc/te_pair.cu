@@ -634,28 +634,30 @@ struct TeLaunch {
 static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const DevAttr& A,
                           TeLaunch* L, int64_t max_slot_bytes) {
   const int threads = (cfg && cfg->threads) ? cfg->threads : 512;
-  const int cps = (cfg && cfg->ctas_per_sm) ? cfg->ctas_per_sm : 1;
+  int cps = (cfg && cfg->ctas_per_sm) ? cfg->ctas_per_sm : 1;
   if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
     return fail(TENEX_ERR_BADARG, "threads must be 128, 256, 512 or 1024 (got %d)", threads);
   if (cps < 1 || cps * threads > A.max_threads_per_sm)
     return fail(TENEX_ERR_BADARG, "ctas_per_sm=%d x threads=%d exceeds %d threads/SM", cps,
                 threads, A.max_threads_per_sm);
-  int smem = (cfg && cfg->smem_bytes) ? cfg->smem_bytes : 0;
-  if (smem == 0) {
-    // fill the SM: per-SM shared memory minus the 1 KB the driver reserves per CTA
-    smem = (A.smem_per_sm / cps) - 1024;
-    if (smem > A.smem_optin) smem = A.smem_optin;
-  }
-  if (smem > A.smem_optin)
-    return fail(TENEX_ERR_BADARG, "smem_bytes=%d exceeds the device opt-in %d", smem,
+  const int fixed = (cfg && cfg->smem_bytes) ? cfg->smem_bytes : 0;
+  if (fixed > A.smem_optin)
+    return fail(TENEX_ERR_BADARG, "smem_bytes=%d exceeds the device opt-in %d", fixed,
                 A.smem_optin);
-  smem = smem / 16 * 16;
   const SmemLayout SL = smem_layout(P.N, P.zbytes, P.bmax);
-  if ((int64_t)SL.slot_off + max_slot_bytes > smem)
-    return fail(TENEX_ERR_UNSUPPORTED,
-                "histogram of the largest pair (%lld B) plus the staged target (%d B) does not "
-                "fit %d B of shared memory; coarsen bins or shorten the series",
-                (long long)max_slot_bytes, SL.slot_off, smem);
+  int smem = 0;
+  // With shared memory sized automatically, fewer CTAs per SM are used when the
+  // largest pair's histogram would not fit (e.g. 38-bin genes need ~110 KB).
+  for (;; --cps) {
+    smem = fixed ? fixed : std::min((A.smem_per_sm / cps) - 1024, A.smem_optin);
+    smem = smem / 16 * 16;
+    if ((int64_t)SL.slot_off + max_slot_bytes <= smem) break;
+    if (fixed || cps == 1)
+      return fail(TENEX_ERR_UNSUPPORTED,
+                  "histogram of the largest pair (%lld B) plus the staged target (%d B) does "
+                  "not fit %d B of shared memory; coarsen bins or shorten the series",
+                  (long long)max_slot_bytes, SL.slot_off, smem);
+  }
   L->threads = threads;
   L->smem = smem;
   L->grid = A.sm_count * cps;

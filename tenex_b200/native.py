@@ -73,6 +73,7 @@ _SIGS = {
     "tenex_fsbwl_bins": [_P, _L, _I, _I, ctypes.c_float, _P, _L, _P, _P],
     "tenex_remap_dense": [_P, _I, _L, _I, _L, _P, _I, _L, _P, _P, _P],
     "tenex_coarsen": [_P, _L, _I, _L, _P, _I, _P],
+    "tenex_binarize": [_P, _L, _I, _I, _I, _P, _P, _L, _P, _P],
     "tenex_b2_workspace_bytes": [_I, _L, _L],
     "tenex_te_binary_matrix": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _P],
     "tenex_b2_status": [_P, _I, _L, _L, _P],

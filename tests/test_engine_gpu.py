@@ -1,0 +1,123 @@
+"""End-to-end engine and preprocessing kernels against the reference goldens / oracle."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tenex_b200 import TransferEntropyEngine, workloads as W
+from tenex_b200.kernels import device as D
+from tenex_b200.kernels.adaptive_smem import AdaptiveSMEMKernel
+from tenex_b200.preprocess import coarsen_bins, discretize, fsbwl_bins, remap_bins
+from tenex_b200.binarize import binarize
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def test_engine_cfg1_golden(cuda, golden):
+    g = golden("discretize_cfg1.npz")
+    names = np.array([f"g{i}" for i in range(g["x"].shape[0])])
+    res = TransferEntropyEngine(g["x"], names).compute(accelerator="gpu", profile=True)
+    assert res.kernel == "Full-SMEM"
+    assert np.array_equal(res.bin_arrs[:, :, 0].astype(np.int32), g["bins"][:, :, 0])
+    assert np.array_equal(res.n_per_var, g["n_per_var"])
+    assert res.b_max == int(g["b_max"])
+    assert np.max(np.abs(res.matrix - g["matrix"])) <= TOL
+    assert np.all(np.diag(res.matrix) == 0)
+    assert set(res.timings) >= {"total", "discretize", "compute"}
+
+
+@pytest.mark.parametrize("n,T", [(7, 1), (9, 7), (33, 128), (31, 129), (40, 1000), (12, 5003),
+                                 (6, 20001)])
+def test_fsbwl_bitexact_vs_numpy(cuda, n, T):
+    rng = np.random.default_rng(n * T)
+    x = np.log1p(rng.lognormal(0, 1, (n, T)) * (rng.random((n, T)) > 0.6)).astype(np.float32)
+    x[0] = 1.5  # constant row: std 0 -> 1
+    bins, nb = fsbwl_bins(x, 0.5, cuda)
+    rb, rnb = O.fsbwl(x, 0.5)
+    assert np.array_equal(nb.cpu().numpy(), rnb)
+    assert np.array_equal(bins.cpu().numpy(), rb)
+
+
+def test_remap_and_discretize_match_reference(cuda, golden):
+    g = golden("remap.npz")
+    db, npv, bmax = remap_bins(g["raw"], 1, cuda)
+    assert np.array_equal(db.unpadded()[:, :, 0].cpu().numpy().astype(np.int32), g["remapped"])
+    assert np.array_equal(npv.cpu().numpy(), g["n_per_var"])
+    assert bmax == int(g["b_max"])
+    c = golden("discretize_cfg1.npz")
+    db2, nb2, bmax2, npv2 = discretize(c["x"], "FSBW-L", 0.5, cuda)
+    assert np.array_equal(db2.unpadded()[:, :, 0].cpu().numpy().astype(np.int32),
+                          c["bins"][:, :, 0])
+    assert np.array_equal(nb2.cpu().numpy(), c["n_bins"])
+
+
+def test_coarsen_matches_reference(cuda, golden):
+    g = golden("coarsen.npz")
+    db = D.pack_bins(g["bins"], cuda)
+    db, npv, bmax = coarsen_bins(db, torch.as_tensor(g["n_per_var"], device=cuda), int(g["limit"]))
+    assert np.array_equal(db.unpadded()[:, :, 0].cpu().numpy().astype(np.int32), g["out"])
+    assert np.array_equal(npv.cpu().numpy(), g["out_npv"])
+    assert bmax == int(g["out_bmax"])
+
+
+def test_adaptive_prepare_and_heavy_genes(cuda):
+    x, npv = W.multibin(40, 1500, 4, 2, 16, heavy_frac=0.25, heavy_lo=64, heavy_hi=200)
+    db = D.pack_bins(x, cuda)
+    k = AdaptiveSMEMKernel()
+    db2, npv2, bmax2 = k.prepare(db, torch.as_tensor(npv, device=cuda), int(npv.max()), tau=1,
+                                 smem_optin=232448)
+    assert bmax2 == 38
+    cb, cnpv, cbmax = O.coarsen(x, npv, 38)
+    assert np.array_equal(db2.unpadded()[:, :, 0].cpu().numpy().astype(np.int32), cb)
+    te = k.compute_pairfree_device(db2, npv2, bmax2, 1).cpu().numpy()
+    assert np.max(np.abs(te - O.te_pairfree(cb, cnpv))) <= TOL
+
+
+@pytest.mark.parametrize("method", ["nonzero", "mean", "median", "quantile"])
+def test_binarization_routes_to_gemm_b2(cuda, method):
+    x, _ = W.cfg1_expression(n=50, T=400, seed=3)
+    names = np.array([f"g{i}" for i in range(50)])
+    res = TransferEntropyEngine(x, names).compute(accelerator="gpu", binarization=method,
+                                                  binarization_kwargs={"q": 0.7}
+                                                  if method == "quantile" else None)
+    assert res.kernel == "GEMM-B2"
+    b = res.bin_arrs[:, :, 0].astype(np.int32)
+    if method == "nonzero":
+        assert np.array_equal(b, (x > 0).astype(np.int32))
+    elif method == "mean":
+        assert np.array_equal(b, (x > x.mean(axis=1, keepdims=True)).astype(np.int32))
+    ref = O.te_matrix(b, np.full(50, 2, np.int32))
+    assert np.max(np.abs(res.matrix - ref)) <= TOL
+
+
+def test_source_filter_pair_list(cuda, golden):
+    g = golden("discretize_cfg1.npz")
+    n = g["x"].shape[0]
+    names = np.array([f"g{i}" for i in range(n)])
+    srcs = names[[3, 7, 11, 20]]
+    res = TransferEntropyEngine(g["x"], names, sources=srcs).compute(accelerator="gpu")
+    full = g["matrix"]
+    for s in (3, 7, 11, 20):
+        row = full[s].copy()
+        row[s] = 0.0
+        assert np.max(np.abs(res.matrix[s] - row)) <= TOL
+    other = np.setdiff1d(np.arange(n), [3, 7, 11, 20])
+    assert np.all(res.matrix[other] == 0)
+
+
+def test_engine_contracts(cuda):
+    x, _ = W.cfg1_expression(n=10, T=200, seed=1)
+    names = np.array([f"g{i}" for i in range(10)])
+    eng = TransferEntropyEngine(x, names)
+    with pytest.raises(ValueError):
+        eng.compute(accelerator="gpu", kernel="GEMM-B2")
+    with pytest.raises(KeyError):
+        eng.compute(accelerator="gpu", kernel="nope")
+    with pytest.raises(ValueError):
+        eng.compute(accelerator="gpu", tau=0)
+    r = TransferEntropyEngine(x[:1], names[:1]).compute(accelerator="gpu")
+    assert r.matrix.shape == (1, 1) and r.matrix[0, 0] == 0
+    r2 = eng.compute(accelerator="gpu", kernel="Adaptive-SMEM", tau=2)
+    ref = O.te_matrix(r2.bin_arrs, r2.n_per_var, tau=2)
+    assert np.max(np.abs(r2.matrix - ref)) <= TOL
