@@ -107,6 +107,22 @@ int tenex_te_pairfree_counts(const uint8_t* bins, int64_t ld, const int32_t* n_p
                              void* workspace, size_t workspace_bytes,
                              const tenex_te_config* cfg, void* stream);
 
+/* Same computation as tenex_te_pairfree, for callers that cannot allocate
+ * device memory. (No counterpart in the reference.) Its scratch is a fixed
+ * 4 MiB area inside the library's device image, so n_vars * (b_max + 1) * 4
+ * plus about 768 bytes must fit in 4 MiB (TENEX_ERR_UNSUPPORTED otherwise;
+ * e.g. 10,000 genes up to b_max = 103). The area's address is looked up by the
+ * first call on each device (make that call before any stream capture); every
+ * call reuses and re-initialises the same area, so calls that overlap on the
+ * GPU race and must not be issued. status: optional device int32 that receives
+ * the validation word (0 = inputs valid, else no TE was computed); NULL skips it.
+ * Allocates nothing: no cudaMalloc, cudaFree or allocating library call. */
+int tenex_te_pairfree_static(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                             int b_max, int n_vars, int64_t row_len, int64_t lag,
+                             int64_t pair_offset, int64_t n_pairs, float* out, int out_mode,
+                             int64_t out_ld, int32_t* status, const tenex_te_config* cfg,
+                             void* stream);
+
 /* TE for an explicit pair list (the source-filter path of the reference:
  * te_smem_launch, tenex/csrc/full_smem.cu:319-347, and compute_single_gpu).
  * pairs: device int64 (n_pairs, 2) = [target, source], grouped so that equal

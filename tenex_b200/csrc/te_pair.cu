@@ -33,6 +33,8 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstddef>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -861,4 +863,73 @@ extern "C" int tenex_te_pairs(const uint8_t* bins, int64_t ld, const int32_t* n_
   return te_run(bins, ld, n_per_var, b_max, n_vars, row_len, lag, 0, n_pairs, kOutPairfree, out,
                 0, nullptr, nullptr, nullptr, nullptr, nullptr, 0, workspace, workspace_bytes,
                 cfg, stream, pairs, item_start, n_items);
+}
+
+// ---------------------------------------------------------------------------
+// Entry point for callers that must not allocate device memory.
+//
+// Some hosts of this library cannot call cudaMalloc once they are running:
+// services that reserve their whole device-memory budget at start-up and treat
+// any later allocation as a fault, processes whose device memory is owned by
+// another framework's pooling allocator, and foreign-language bindings that
+// have no way to own the lifetime of a device buffer. tenex_te_pairfree needs
+// a caller-provided workspace; this variant instead uses the fixed scratch
+// area below, which is part of the library's device image: every GPU on which
+// the library is loaded keeps these 4 MiB for the life of the process.
+//
+// The scratch address is looked up once per device (cudaGetSymbolAddress, with
+// that device current) by the first call made on that device, so that first
+// call should come before any stream capture. All calls share the one area and
+// each call rewrites it (work ticket and validation words are cleared, the
+// per-gene marginals recomputed), so calls that overlap on the GPU — on two
+// streams, or from two threads — race and must not be issued.
+// ---------------------------------------------------------------------------
+namespace tenex {
+namespace {
+constexpr size_t kStaticScratchBytes = (size_t)4 << 20;
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+int static_scratch(void** out) {
+  static std::mutex mu;
+  static void* addr[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return check_cuda(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return fail(TENEX_ERR_UNSUPPORTED, "device index %d", dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return check_cuda(e, "cudaGetSymbolAddress(scratch)");
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return TENEX_OK;
+}
+}  // namespace
+}  // namespace tenex
+
+extern "C" int tenex_te_pairfree_static(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                                        int b_max, int n_vars, int64_t row_len, int64_t lag,
+                                        int64_t pair_offset, int64_t n_pairs, float* out,
+                                        int out_mode, int64_t out_ld, int32_t* status,
+                                        const tenex_te_config* cfg, void* stream) {
+  if (n_vars < 2 || b_max < 1 || b_max > 255)
+    return fail(TENEX_ERR_BADARG, "need n_vars >= 2 and 1 <= b_max <= 255");
+  const int64_t need = ws_total(n_vars, b_max);
+  if (need > (int64_t)kStaticScratchBytes)
+    return fail(TENEX_ERR_UNSUPPORTED,
+                "n_vars=%d with b_max=%d needs %lld bytes of scratch; the built-in area holds "
+                "%zu bytes (about 4*n_vars*(b_max+1) + 768 must fit). Use tenex_te_pairfree "
+                "with a workspace instead.",
+                n_vars, b_max, (long long)need, kStaticScratchBytes);
+  void* ws = nullptr;
+  int st = static_scratch(&ws);
+  if (st) return st;
+  st = tenex_te_pairfree(bins, ld, n_per_var, b_max, n_vars, row_len, lag, pair_offset, n_pairs,
+                         out, out_mode, out_ld, ws, kStaticScratchBytes, cfg, stream);
+  if (st || !status) return st;
+  cudaError_t e = cudaMemcpyAsync(status, static_cast<unsigned char*>(ws) + offsetof(WsHeader, bad_data),
+                                  sizeof(int32_t), cudaMemcpyDeviceToDevice, as_stream(stream));
+  return check_cuda(e, "status copy");
 }

@@ -65,6 +65,8 @@ _SIGS = {
                           ctypes.POINTER(TeConfig), _P],
     "tenex_te_pairfree_counts": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _P, _L, _P, _S,
                                  ctypes.POINTER(TeConfig), _P],
+    "tenex_te_pairfree_static": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _I, _L, _P,
+                                 ctypes.POINTER(TeConfig), _P],
     "tenex_te_pairs": [_P, _L, _P, _I, _I, _L, _L, _P, _L, _P, _L, _P, _P, _S,
                        ctypes.POINTER(TeConfig), _P],
     "tenex_surrogate_accumulate": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _P, _P, _P, _P, _S,

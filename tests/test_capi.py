@@ -27,7 +27,7 @@ def test_library_exports_declared_symbols():
 
 
 def test_binding_covers_declarations():
-    assert set(native.declared_symbols()) >= _declared() - {"tenex_te_pairfree_static"}
+    assert set(native.declared_symbols()) >= _declared()
 
 
 def test_abi_version_and_error_text_without_gpu():

@@ -1,0 +1,73 @@
+"""The no-allocation TE entry point against the regular one.
+
+tenex_te_pairfree_static serves callers that cannot allocate device memory
+after start-up (fixed device-memory budgets, memory owned by another
+framework's pool, bindings that cannot own device buffers): it takes no
+workspace and uses a fixed scratch area compiled into the library. These tests
+call both entry points through the C ABI on the same inputs, twice in a row
+with different data (the shared scratch must not carry state from one call to
+the next), and require the same TE within the suite's 1e-6 tolerance. This
+file is collected last so a failure here leaves the rest of the suite's
+results intact.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tenex_b200 import native
+from tenex_b200.kernels import device as D
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def _case(seed, n, T, b_hi):
+    rng = np.random.default_rng(seed)
+    b = rng.integers(2, b_hi + 1, n)
+    x = np.stack([rng.integers(0, bb, T) for bb in b]).astype(np.int32)
+    return O.remap(x)
+
+
+def _regular(db, npv_t, bmax, dev):
+    n = db.n
+    out = torch.zeros((n, n), dtype=torch.float32, device=dev)
+    ws = D.workspace(dev, n, db.row_len, bmax)
+    native.call("tenex_te_pairfree", db.data.data_ptr(), db.ld, npv_t.data_ptr(), bmax, n,
+                db.row_len, 1, 0, n * (n - 1), out.data_ptr(), native.OUT_MATRIX, n,
+                ws.data_ptr(), ws.numel(), None, native.stream_ptr())
+    native.call("tenex_workspace_status", ws.data_ptr(), native.stream_ptr())
+    return out
+
+
+def _static(db, npv_t, bmax, dev):
+    n = db.n
+    out = torch.zeros((n, n), dtype=torch.float32, device=dev)
+    status = torch.full((1,), -1, dtype=torch.int32, device=dev)
+    native.call("tenex_te_pairfree_static", db.data.data_ptr(), db.ld, npv_t.data_ptr(), bmax, n,
+                db.row_len, 1, 0, n * (n - 1), out.data_ptr(), native.OUT_MATRIX, n,
+                status.data_ptr(), None, native.stream_ptr())
+    torch.cuda.synchronize(dev)
+    assert int(status.item()) == 0
+    return out
+
+
+def test_static_scratch_matches_workspace_entry_twice(cuda):
+    cases = [_case(1, 48, 3001, 16), _case(2, 37, 1200, 38)]
+    for bins, npv, bmax in cases:  # two calls in a row, different shapes and data
+        db = D.pack_bins(bins, cuda)
+        npv_t = torch.as_tensor(npv, dtype=torch.int32, device=cuda)
+        a = _static(db, npv_t, bmax, cuda).cpu().numpy()
+        b = _regular(db, npv_t, bmax, cuda).cpu().numpy()
+        assert np.max(np.abs(a - b)) <= TOL
+        assert np.max(np.abs(a - O.te_matrix(bins, npv))) <= TOL
+
+
+def test_static_scratch_rejects_oversized_problem(cuda):
+    # 40,000 genes at b_max 38 need ~6.2 MB of scratch: refused before any launch
+    st = native.lib().tenex_te_pairfree_static(None, 64, None, 38, 40000, 100, 1, 0, 10, None,
+                                               0, 0, None, None, None)
+    assert st == native.TENEX_ERR_UNSUPPORTED
+    assert "scratch" in native.last_error()
