@@ -74,7 +74,8 @@ int tenex_device_query(int device, tenex_dev_info* info);
 
 /* Bytes of device workspace the TE / surrogate entry points need: a 256-byte
  * header (work ticket, validation words) plus each gene's bin marginal
- * (n_vars * b_max int32) and most frequent bin (n_vars int32). */
+ * (n_vars * b_max int32), most frequent bin (n_vars int32) and the source
+ * processing order (n_vars int32). */
 size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len, int b_max);
 
 /* Reads back the data-validation word a previous TE call left in the
@@ -109,9 +110,9 @@ int tenex_te_pairfree_counts(const uint8_t* bins, int64_t ld, const int32_t* n_p
 
 /* Same computation as tenex_te_pairfree, for callers that cannot allocate
  * device memory. (No counterpart in the reference.) Its scratch is a fixed
- * 4 MiB area inside the library's device image, so n_vars * (b_max + 1) * 4
- * plus about 768 bytes must fit in 4 MiB (TENEX_ERR_UNSUPPORTED otherwise;
- * e.g. 10,000 genes up to b_max = 103). The area's address is looked up by the
+ * 4 MiB area inside the library's device image, so n_vars * (b_max + 2) * 4
+ * plus about 1 KB must fit in 4 MiB (TENEX_ERR_UNSUPPORTED otherwise;
+ * e.g. 10,000 genes up to b_max = 102). The area's address is looked up by the
  * first call on each device (make that call before any stream capture); every
  * call reuses and re-initialises the same area, so calls that overlap on the
  * GPU race and must not be issued. status: optional device int32 that receives

@@ -69,6 +69,7 @@ struct TeParams {
   int64_t counts_stride;
   const int32_t* marg;  // (n, bmax) per-gene marginal over [0, N)
   const int32_t* ydom;  // (n,) most frequent bin of each gene over [0, N)
+  const int32_t* order; // (n,) genes stably sorted by bin-count class (pair-free mode)
   // pair-list mode (pairs != nullptr): item q is pairs[item_start[q] .. item_start[q+1])
   // of one target; output index = position in the list
   const int64_t* pairs;
@@ -76,13 +77,17 @@ struct TeParams {
   WsHeader* ws;
 };
 
-// Workspace: header | marg (n*bmax int32) | ydom (n int32), 256-byte aligned.
+// Workspace: header | marg (n*bmax int32) | ydom (n int32) | order (n int32),
+// 256-byte aligned.
 __host__ __device__ inline int64_t ws_marg_off() { return (int64_t)sizeof(WsHeader); }
 __host__ __device__ inline int64_t ws_ydom_off(int n, int bmax) {
   return round_up(ws_marg_off() + (int64_t)n * bmax * 4, 256);
 }
-__host__ __device__ inline int64_t ws_total(int n, int bmax) {
+__host__ __device__ inline int64_t ws_order_off(int n, int bmax) {
   return round_up(ws_ydom_off(n, bmax) + (int64_t)n * 4, 256);
+}
+__host__ __device__ inline int64_t ws_total(int n, int bmax) {
+  return round_up(ws_order_off(n, bmax) + (int64_t)n * 4, 256);
 }
 
 #ifdef TENEX_PHASE_TIMERS
@@ -218,13 +223,15 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
   const int nvec = N >> 4;
   const int bt2 = bt * bt;
   for (int r = g; r < n_src; r += n_groups) {
-    const int64_t p = lo + r;
+    int64_t p;
     int src;
     if (P.pairs) {
+      p = lo + r;
       src = (int)P.pairs[2 * p + 1];
     } else {
-      const int sl = (int)(p - base);
-      src = sl + (sl >= tgt);
+      src = P.order[lo + r];
+      p = base + (src < tgt ? src : src - 1);
+      if (src == tgt || p < P.p0 || p >= P.p1) continue;  // group-uniform skip
     }
     const uint32_t bs = (uint32_t)P.npv[src];
     const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
@@ -425,13 +432,16 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       }
       tgt = lo < hi ? (int)P.pairs[2 * lo] : 0;
     } else {
+      // pair-free: chunk `chunk` covers positions [chunk*W, (chunk+1)*W) of the
+      // source order (genes grouped by bin count, so one item's histogram slots
+      // are sized for sources of similar b); sources outside [p0, p1) or equal
+      // to the target are skipped below
       const int chunk = (int)(q / P.n_targets);
       tgt = P.t_first + (int)(q % P.n_targets);
       base = (int64_t)tgt * nm1;
-      lo = base + (int64_t)chunk * P.W;
-      hi = base + min((int64_t)(chunk + 1) * P.W, (int64_t)nm1);
-      lo = max(lo, P.p0);
-      hi = min(hi, P.p1);
+      lo = (int64_t)chunk * P.W;
+      hi = min((int64_t)(chunk + 1) * P.W, (int64_t)P.n);
+      if (base + nm1 <= P.p0 || base >= P.p1) lo = hi;  // target outside the range
     }
     if (lo >= hi) {
       __syncthreads();
@@ -456,8 +466,9 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
         bad |= P.pairs[2 * (lo + r)] != tgt || src < 0 || src >= P.n;
         if (src < 0 || src >= P.n) src = 0;
       } else {
-        int sl = (int)(lo + r - base);
-        src = sl + (sl >= tgt);
+        src = P.order[lo + r];
+        const int64_t p = base + (src < tgt ? src : src - 1);
+        if (src == tgt || p < P.p0 || p >= P.p1) continue;
       }
       my_max = max(my_max, (unsigned)P.npv[src]);
     }
@@ -625,6 +636,51 @@ __global__ void gene_prepass_kernel(const uint8_t* bins, int64_t ld, const int32
   }
 }
 
+// Source order for pair-free items: genes stably sorted by bin-count class
+// (class = b for b <= 40, then bands of 16), so a work item's sources have
+// similar b and its histogram slots are sized for them. One CTA of 1024 threads;
+// deterministic (ballot + block scan, no atomics on the order).
+__device__ __forceinline__ int order_class(int b) {
+  const int c = b <= 40 ? b : 41 + (b - 41) / 16;
+  return c < 0 ? 0 : (c > 56 ? 56 : c);  // out-of-range counts (rejected later) stay in bounds
+}
+
+__global__ void __launch_bounds__(1024) source_order_kernel(const int32_t* __restrict__ npv,
+                                                            int n, int32_t* __restrict__ order) {
+  constexpr int kClasses = 41 + 15 + 1;
+  __shared__ int present[kClasses];
+  __shared__ int wsum[32];
+  __shared__ int base_sh;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+  for (int c = tid; c < kClasses; c += blockDim.x) present[c] = 0;
+  if (tid == 0) base_sh = 0;
+  __syncthreads();
+  for (int g = tid; g < n; g += blockDim.x) present[order_class(npv[g])] = 1;
+  __syncthreads();
+  for (int c = 0; c < kClasses; ++c) {
+    if (!present[c]) continue;  // uniform: read after the barrier above
+    for (int start = 0; start < n; start += blockDim.x) {
+      const int g = start + tid;
+      const int flag = (g < n) && order_class(npv[g]) == c;
+      const unsigned m = __ballot_sync(0xffffffffu, flag);
+      const int pre = __popc(m & ((1u << lane) - 1u));
+      if (lane == 0) wsum[w] = __popc(m);
+      __syncthreads();
+      int wpre = 0, tot = 0;
+      for (int k = 0; k < nw; ++k) {
+        const int v = wsum[k];
+        wpre += k < w ? v : 0;
+        tot += v;
+      }
+      const int b0 = base_sh;
+      if (flag) order[b0 + wpre + pre] = g;
+      __syncthreads();
+      if (tid == 0) base_sh = b0 + tot;
+      __syncthreads();
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -766,7 +822,7 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
     P.t_first = (int)(p0 / (n - 1));
     const int t_last = (int)((P.p1 - 1) / (n - 1));
     P.n_targets = t_last - P.t_first + 1;
-    P.n_chunks = (n - 1 + P.W - 1) / P.W;
+    P.n_chunks = (n + P.W - 1) / P.W;
     P.n_items = (int64_t)P.n_targets * P.n_chunks;
   }
   if (P.n_items == 0) return TENEX_OK;
@@ -788,8 +844,10 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   unsigned char* wsb = reinterpret_cast<unsigned char*>(workspace);
   int32_t* marg = reinterpret_cast<int32_t*>(wsb + ws_marg_off());
   int32_t* ydom = reinterpret_cast<int32_t*>(wsb + ws_ydom_off(n, b_max));
+  int32_t* order = reinterpret_cast<int32_t*>(wsb + ws_order_off(n, b_max));
   P.marg = marg;
   P.ydom = ydom;
+  P.order = order;
 
   // worst case the device can meet: 16-bit halves when N < 65536, else 32-bit
   const int64_t hb = P.N < 65536 ? (b_max + 1) / 2 : b_max;
@@ -807,6 +865,11 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
                                              P.ws);
   st = check_launch("gene_prepass_kernel");
   if (st) return st;
+  if (!pairs) {
+    source_order_kernel<<<1, 1024, 0, stream>>>(npv, n, order);
+    st = check_launch("source_order_kernel");
+    if (st) return st;
+  }
   e = cudaFuncSetAttribute(te_pair_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            L.smem);
   if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
@@ -920,7 +983,7 @@ extern "C" int tenex_te_pairfree_static(const uint8_t* bins, int64_t ld, const i
   if (need > (int64_t)kStaticScratchBytes)
     return fail(TENEX_ERR_UNSUPPORTED,
                 "n_vars=%d with b_max=%d needs %lld bytes of scratch; the built-in area holds "
-                "%zu bytes (about 4*n_vars*(b_max+1) + 768 must fit). Use tenex_te_pairfree "
+                "%zu bytes (about 4*n_vars*(b_max+2) + 1024 must fit). Use tenex_te_pairfree "
                 "with a workspace instead.",
                 n_vars, b_max, (long long)need, kStaticScratchBytes);
   void* ws = nullptr;
