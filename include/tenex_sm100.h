@@ -150,6 +150,12 @@ int tenex_surrogate_accumulate(const uint8_t* bins, int64_t ld, const int32_t* n
                                void* workspace, size_t workspace_bytes,
                                const tenex_te_config* cfg, void* stream);
 
+/* Surrogate accumulation from a finished TE matrix te[src*n + tgt] (the
+ * matrix-kernel path, GEMM-B2): same update as tenex_surrogate_accumulate, off
+ * the diagonal. */
+int tenex_stats_accumulate(const float* te, const float* observed, double* sum, double* sumsq,
+                           int32_t* count_ge, int n_vars, void* stream);
+
 /* Block shuffle of every gene's time axis (tenex/inference/surrogate_test.py:107-162):
  * out[g, t*K + k] = in[g, (perm[g, t/bl]*bl + t%bl)*K + k] for t < n_blocks*bl,
  * tail t >= n_blocks*bl unchanged. bl = 1 with n_blocks = T is the random shuffle.

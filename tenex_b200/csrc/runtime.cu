@@ -87,9 +87,39 @@ __global__ void block_shuffle_kernel(const uint8_t* __restrict__ in, int64_t in_
   }
 }
 
+// sum[m] += te[m]; sumsq[m] += te[m]^2 (float32 widened); count_ge[m] += te[m] >= obs[m],
+// for m off the diagonal of an (n, n) matrix (the diagonal is handled by the caller).
+__global__ void stats_accumulate_kernel(const float* __restrict__ te, const float* __restrict__ obs,
+                                        double* __restrict__ sum, double* __restrict__ sumsq,
+                                        int32_t* __restrict__ cnt, int n) {
+  const int64_t total = (int64_t)n * n;
+  for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < total;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    if (m / n == m % n) continue;
+    const float t = te[m];
+    const double d = (double)t;
+    sum[m] += d;
+    sumsq[m] += d * d;
+    cnt[m] += t >= obs[m] ? 1 : 0;
+  }
+}
+
 }  // namespace tenex
 
 using namespace tenex;
+
+extern "C" int tenex_stats_accumulate(const float* te, const float* observed, double* sum,
+                                      double* sumsq, int32_t* count_ge, int n_vars, void* stream) {
+  if (!te || !observed || !sum || !sumsq || !count_ge)
+    return fail(TENEX_ERR_BADARG, "all pointers must be non-NULL");
+  if (n_vars < 1) return fail(TENEX_ERR_BADARG, "n_vars must be >= 1");
+  const int64_t total = (int64_t)n_vars * n_vars;
+  const int64_t blocks64 = (total + 255) / 256;
+  const int blocks = (int)(blocks64 < 4096 ? blocks64 : 4096);
+  stats_accumulate_kernel<<<blocks, 256, 0, as_stream(stream)>>>(te, observed, sum, sumsq,
+                                                                 count_ge, n_vars);
+  return check_launch("stats_accumulate_kernel");
+}
 
 extern "C" int tenex_abi_version(void) { return 1; }
 

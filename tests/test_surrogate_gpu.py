@@ -1,0 +1,96 @@
+"""Surrogate test on the GPU against the reference fixture and the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tenex_b200 import TransferEntropyEngine, workloads as W
+from tenex_b200.inference import NetWeaver
+from tenex_b200.inference.surrogate_test import (SurrogateAccumulator, build_block_perm,
+                                                 run_surrogates, surrogate_statistics)
+from tenex_b200.kernels import device as D
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def _acc(bins, npv, bmax, obs, cuda, binary=False):
+    db = D.pack_bins(bins, cuda)
+    return SurrogateAccumulator(db, torch.as_tensor(npv, dtype=torch.int32, device=cuda), bmax,
+                                1, torch.as_tensor(obs, dtype=torch.float32, device=cuda),
+                                binary)
+
+
+def test_reference_permutations_reproduce_reference_stats(cuda, golden):
+    """The reference's own CPU run (its RNG, its kernel): our kernels given its
+    block permutations reproduce its mean / std of the surrogate TE."""
+    g = golden("surrogate.npz")
+    perm = torch.as_tensor(g["perm"], device=cuda)
+    acc = _acc(g["bins"], g["n_per_var"], int(g["n_per_var"].max()), g["observed"], cuda)
+    run_surrogates(acc, perm, int(g["block_length"]), use_graph=False)
+    S = perm.shape[0]
+    mean, std, eff, p = surrogate_statistics(g["observed"], acc.sum.cpu().numpy(),
+                                             acc.sumsq.cpu().numpy(), acc.cnt.cpu().numpy(), S,
+                                             "parametric")
+    assert np.max(np.abs(mean - g["mean"])) <= TOL
+    assert np.max(np.abs(std - g["std"])) <= 2e-6
+    assert np.max(np.abs(eff - g["effective"])) <= TOL
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+@pytest.mark.parametrize("bl", [20, 1])
+def test_cuda_rng_surrogates_match_oracle(cuda, use_graph, bl):
+    """Each side compares its surrogate TE with its own observed TE (as the
+    method does): pairs whose shuffle leaves the joint counts unchanged tie
+    exactly on both sides."""
+    x, npv, _ = W.cfg5_bins(n=24, T=600, seed=3, n_planted=3)
+    bmax = int(npv.max())
+    obs_ref = O.te_matrix(x, npv).astype(np.float32)
+    db = D.pack_bins(x, cuda)
+    obs = D.te_pairfree(db, torch.as_tensor(npv, device=cuda), bmax, matrix=True).cpu().numpy()
+    assert np.max(np.abs(obs - obs_ref)) <= TOL
+    S = 6
+    perms, eff_bl, nb = build_block_perm(24, 600, "block", bl if bl > 1 else 600, 0, S, 42, cuda)
+    acc = _acc(x, npv, bmax, obs, cuda)
+    run_surrogates(acc, perms, eff_bl, use_graph=use_graph)
+    s, ss, c = O.surrogate_stats(x, npv, perms.cpu().numpy(), eff_bl, obs_ref)
+    off = ~np.eye(24, dtype=bool)
+    assert np.max(np.abs(acc.sum.cpu().numpy() - s)) <= S * TOL
+    assert np.max(np.abs(acc.sumsq.cpu().numpy() - ss)) <= S * TOL
+    cg = acc.cnt.cpu().numpy()
+    assert np.mean(cg[off] != c[off]) <= 1e-3  # ties within 1e-6 may flip a comparison
+    assert np.max(np.abs(cg[off] - c[off])) <= 1
+
+
+def test_binary_surrogates_use_gemm_path(cuda):
+    x, _ = W.cfg2_binary(n=40, T=700, seed=4, n_planted=3)
+    npv = np.full(40, 2, np.int32)
+    obs = O.te_matrix(x.astype(np.int32), npv).astype(np.float32)
+    perms, bl, _ = build_block_perm(40, 700, "block", 25, 0, 4, 7, cuda)
+    acc = _acc(x, npv, 2, obs, cuda, binary=True)
+    run_surrogates(acc, perms, bl)
+    s, ss, c = O.surrogate_stats(x.astype(np.int32), npv, perms.cpu().numpy(), bl, obs)
+    assert np.max(np.abs(acc.sum.cpu().numpy() - s)) <= 4 * TOL
+
+
+def test_netweaver_surrogate_end_to_end(cuda):
+    x, planted = W.cfg1_expression(n=30, T=500, seed=11, n_planted=4)
+    names = np.array([f"g{i}" for i in range(30)])
+    res = TransferEntropyEngine(x, names).compute(accelerator="gpu")
+    st = NetWeaver(res, fdr=0.05).infer("surrogate_test", device=cuda, n_surrogates=8,
+                                        block_length=20, seed=5)
+    perms, bl, _ = build_block_perm(30, 500, "block", 20, 0, 8, 5, cuda)
+    s, ss, c = O.surrogate_stats(res.bin_arrs.astype(np.int32), res.n_per_var,
+                                 perms.cpu().numpy(), bl, res.matrix)
+    c[np.arange(30), np.arange(30)] += 8
+    mean, std, eff, p = surrogate_statistics(res.matrix, s, ss, c, 8, "parametric")
+    assert np.max(np.abs(st.mean_surrogate_te - mean)) <= TOL
+    assert np.max(np.abs(st.effective_te - eff)) <= TOL
+    assert st.p_values.shape == (30, 30) and np.all(np.diag(st.p_values) == 1.0)
+    st_mc = NetWeaver(res, fdr=0.05).infer("surrogate_test", device=cuda, n_surrogates=8,
+                                           block_length=20, seed=5, p_method="mc")
+    assert np.all((st_mc.p_values > 0) & (st_mc.p_values <= 1))
+    with pytest.raises(ValueError):
+        NetWeaver(res).infer("surrogate_test", device=cuda, n_surrogates=1)
+    with pytest.raises(NotImplementedError):
+        NetWeaver(res).infer("trace", device=cuda)
