@@ -11,8 +11,14 @@ the B200 shared-memory limit (38, the reference rule) and the full TE matrix
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 (torchrun, one process per GPU): the pair-id range is split evenly across
-ranks (no data-path collective); time is the max over ranks.
+Profiling options (not the headline run): --genes / --cells shrink the
+workload, --pairs times only the first pair ids, --launch T,C,W fixes the
+launch shape (threads, CTAs per SM, sources per work item) instead of running
+the autotuner, --no-e2e and --no-cpu-baseline skip those legs.
+
+N > 1 (torchrun, one process per GPU): the pair-id range is split into
+contiguous chunks of ceil(pairs / N), the reference's split (no data-path
+collective); total work is fixed (strong scaling); time is the max over ranks.
 --impl reference: rank 0 times the CPU oracle (a C restatement of the
 reference's counting and TE formula, all host threads) on a bounded sample of
 the same pairs.
@@ -38,9 +44,9 @@ METRIC = "TE pairs/s @10k genes x 20k cells (all ordered pairs, Adaptive-SMEM)"
 WORKLOAD = "cfg4: 10000 genes x 20000 cells, 95% b~U{2..16}, 5% b~U{64..256} coarsened to 38"
 
 
-def make_bins():
+def make_bins(genes: int = N_GENES, cells: int = N_CELLS):
     from tenex_b200 import workloads as W
-    return W.cfg4_bins(N_GENES, N_CELLS, seed=1004)
+    return W.cfg4_bins(genes, cells, seed=1004)
 
 
 class ClockSampler:
@@ -174,16 +180,17 @@ def run_ours(args) -> None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    x, npv = make_bins()
-    total = N_GENES * (N_GENES - 1)
-    p0 = total * rank // world
-    p1 = total * (rank + 1) // world
+    G, C = args.genes, args.cells
+    x, npv = make_bins(G, C)
+    total = G * (G - 1) if args.pairs is None else min(args.pairs, G * (G - 1))
+    from tenex_b200.distributed import pair_range
+    p0, p1 = pair_range(total, rank, world)
     kern = AdaptiveSMEMKernel()
     smem_optin = native.device_info(local).smem_optin
     limit = compute_smem_bin_limit(smem_optin, warps=32)
 
     raw_d = torch.from_numpy(x).to(dev)            # resident raw bins (uint8, 200 MB)
-    out = torch.zeros((N_GENES, N_GENES), dtype=torch.float32, device=dev)
+    out = torch.zeros((G, G), dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     te_times = []
 
@@ -195,7 +202,7 @@ def run_ours(args) -> None:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
         kern.compute_pairfree_device(db, npv_d, bmax, TAU, p0, p1 - p0, matrix=True,
-                                     out=out)                       # 2 launches
+                                     out=out)                       # 3 launches
         if record_te:
             e1.record(stream)
             te_times.append((e0, e1))
@@ -203,9 +210,13 @@ def run_ours(args) -> None:
 
     # launch shape from the autotuner (timed once on a slice of the pair range, cached)
     from tenex_b200.kernels.pair_tile import autotune
-    db0, npv0, bmax0 = step()
-    kern.cfg = autotune(db0, npv0, bmax0, TAU)
-    del db0, npv0
+    if args.launch:
+        th, cps, w = (int(v) for v in args.launch.split(","))
+        kern.cfg = dict(threads=th, ctas_per_sm=cps, src_chunk=w)
+    else:
+        db0, npv0, bmax0 = step()
+        kern.cfg = autotune(db0, npv0, bmax0, TAU)
+        del db0, npv0
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
@@ -233,8 +244,8 @@ def run_ours(args) -> None:
 
     # ---- end to end through the kernel plugin API (host bins -> host matrix) ----
     x_pin = torch.from_numpy(x).pin_memory()
-    out_pin = torch.empty((N_GENES, N_GENES), dtype=torch.float32).pin_memory()
-    e2e_steps = max(1, min(args.steps, 3))
+    out_pin = torch.empty((G, G), dtype=torch.float32).pin_memory()
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
 
     def e2e_step():
         xd = x_pin.to(dev, non_blocking=True)
@@ -243,26 +254,29 @@ def run_ours(args) -> None:
         m = kern.compute_pairfree_device(db, npv_d, bmax, TAU, p0, p1 - p0, matrix=True)
         out_pin.copy_(m, non_blocking=True)
 
-    e2e_step()
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(e2e_steps):
+    e2e = None
+    if e2e_steps:
         e2e_step()
-    b.record(stream)
-    torch.cuda.synchronize(dev)
-    e2e_ms = a.elapsed_time(b)
-    if world > 1:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt[0])
-    e2e = {"value": pairs_per_step * e2e_steps / (e2e_ms / 1e3), "unit": "pairs/s",
-           "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": int(out_pin.numel() * 4),
-           "path": "AdaptiveSMEMKernel: pinned host bins -> remap -> prepare -> "
-                   "compute_pairfree_device -> pinned host matrix"}
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = a.elapsed_time(b)
+        if world > 1:
+            tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_ms = float(tt[0])
+        e2e = {"value": pairs_per_step * e2e_steps / (e2e_ms / 1e3), "unit": "pairs/s",
+               "h2d_bytes_per_step": int(x.nbytes),
+               "d2h_bytes_per_step": int(out_pin.numel() * 4),
+               "path": "AdaptiveSMEMKernel: pinned host bins -> remap -> prepare -> "
+                       "compute_pairfree_device -> pinned host matrix"}
 
     if rank != 0:
         if world > 1:
@@ -270,13 +284,13 @@ def run_ours(args) -> None:
         return
 
     # ---- roofline of the dominant kernel (te_pair_tile_kernel) ----
-    N = N_CELLS - TAU
+    N = C - TAU
     incr = (p1 - p0) * N                                   # histogram increments per launch
     peak_atomic = max(native.probe_smem_atomics(0, 8192) for _ in range(3))
     achieved = incr / (te_ms / 1e3)
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs")
-    compulsory = N_GENES * x.shape[1] + (p1 - p0) * 4      # bins once + fp32 outputs
+    compulsory = G * x.shape[1] + (p1 - p0) * 4            # bins once + fp32 outputs
     roofline = {"bound": "smem_atomic", "achieved": achieved / 1e9, "peak": peak_atomic / 1e9,
                 "unit": "Gincr/s", "frac": achieved / peak_atomic,
                 "traffic": profile_traffic(),
@@ -295,11 +309,14 @@ def run_ours(args) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "genes": N_GENES, "cells": N_CELLS, "tau": TAU,
+            "config": {"workload": WORKLOAD if (G, C, total) == (N_GENES, N_CELLS,
+                                                                 N_GENES * (N_GENES - 1))
+                       else f"cfg4-shaped slice: {G} genes x {C} cells, pair ids [0, {total})",
+                       "genes": G, "cells": C, "tau": TAU,
                        "pairs": total, "step": "remap + coarsen + all-pairs TE matrix",
                        "parallelism": f"pair-range x{world}", "l2": "inputs (200 MB) > L2",
                        "launch": kern.cfg},
-            "gpu_launches": 5 * args.steps,
+            "gpu_launches": 6 * args.steps,  # remap, coarsen x2, prepass, order, TE tile
             "roofline": roofline, "roofline_hbm": roofline_hbm,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
@@ -321,6 +338,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ref-pairs", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--genes", type=int, default=N_GENES)
+    ap.add_argument("--cells", type=int, default=N_CELLS)
+    ap.add_argument("--pairs", type=int, default=None)
+    ap.add_argument("--launch", default=None)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

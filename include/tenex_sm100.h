@@ -150,6 +150,16 @@ int tenex_surrogate_accumulate(const uint8_t* bins, int64_t ld, const int32_t* n
                                void* workspace, size_t workspace_bytes,
                                const tenex_te_config* cfg, void* stream);
 
+/* Surrogate accumulation for an explicit pair list (same pair/item conventions as
+ * tenex_te_pairs; accumulators indexed [src * n + tgt]). */
+int tenex_surrogate_accumulate_pairs(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                                     int b_max, int n_vars, int64_t row_len, int64_t lag,
+                                     const int64_t* pairs, int64_t n_pairs,
+                                     const int64_t* item_start, int64_t n_items,
+                                     const float* observed, double* sum, double* sumsq,
+                                     int32_t* count_ge, void* workspace, size_t workspace_bytes,
+                                     const tenex_te_config* cfg, void* stream);
+
 /* Surrogate accumulation from a finished TE matrix te[src*n + tgt] (the
  * matrix-kernel path, GEMM-B2): same update as tenex_surrogate_accumulate, off
  * the diagonal. */
@@ -208,6 +218,38 @@ int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t 
  * (synchronises `stream`): TENEX_ERR_TIMEOUT if a pipeline wait expired. */
 int tenex_b2_status(const void* workspace, int n_vars, int64_t row_len, int64_t lag,
                     void* stream);
+
+/* ---- Learned null model of the surrogate test (no reference counterpart) ----
+ * MLP 16 -> 64 -> 64 -> 2 (GELU), parameters W1[64][16] b1[64] W2[64][64] b2[64]
+ * W3[2][64] b3[2] (tenex_mlp_param_count() values), BF16 for the forward,
+ * FP32 master copy for training. Outputs: log(mu * N), log(sigma * N) of a
+ * pair's surrogate-TE distribution. */
+int tenex_mlp_param_count(void);
+/* Per-gene features (n_vars x 8 float): log2 b, H(x_t), H(x_{t+lag}, x_t),
+ * 2H - H2, log2 mean run length, 2^H / b (joint terms NaN when b > 64). */
+int tenex_gene_features(const uint8_t* bins, int64_t ld, const int32_t* n_per_var, int n_vars,
+                        int64_t row_len, int64_t lag, float* feat, void* stream);
+/* Raw 16 features of the pairs (tgt[i], src[i]) into X (n_pairs x 16). */
+int tenex_pair_features(const float* gene_feat, const int32_t* tgt, const int32_t* src,
+                        int64_t n_pairs, float log2N, float log2bl, float* X, void* stream);
+/* Prediction for every ordered pair: out_mu[src*n + tgt], out_sigma[...] (log scale;
+ * NaN where a feature is undefined); features standardised by feat_mean/feat_std. */
+int tenex_null_predict(const float* gene_feat, int n_vars, float log2N, float log2bl,
+                       const void* weights_bf16, const float* feat_mean, const float* feat_std,
+                       float* out_mu, float* out_sigma, void* stream);
+/* Scratch floats needed by a training step / gradient call of `batch` samples. */
+size_t tenex_mlp_scratch_floats(int batch);
+/* Gradients of the mean squared error / 2 over a batch (X standardised, Y targets)
+ * w.r.t. all parameters (grad_out, tenex_mlp_param_count() floats); *loss += sum. */
+int tenex_mlp_gradients(const float* X, const float* Y, int batch, const void* weights_bf16,
+                        float* scratch, float* grad_out, float* loss, void* stream);
+/* One Adam step (bias-corrected, decoupled weight decay wd) on the FP32 master
+ * copy; refreshes the BF16 weights. */
+int tenex_mlp_train_step(const float* X, const float* Y, int batch, void* weights_bf16,
+                         float* master, float* adam_m, float* adam_v, float* scratch, float lr,
+                         float beta1, float beta2, float eps, float wd, int step, float* loss,
+                         void* stream);
+int tenex_to_bf16(const float* src, void* dst, int count, void* stream);
 
 /* Roofline probe (no reference counterpart): times `iters` shared-memory
  * atomicAdds per thread on every SM (mode 0 conflict-free int32, 1 conflict-free

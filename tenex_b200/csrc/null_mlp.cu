@@ -1,0 +1,415 @@
+// null_mlp.cu — learned null model of the surrogate test (no reference
+// counterpart): per-gene features, per-pair feature assembly, and a small MLP
+// (16 -> 64 -> 64 -> 2, GELU) with BF16 weights and FP32 accumulation, plus the
+// kernels that train it (forward with stored pre-activations, backward deltas,
+// batch-reduced weight gradients, Adam on an FP32 master copy).
+//
+// Parameter vector (FP32 master and BF16 copy, same order):
+//   W1[64][16] b1[64] W2[64][64] b2[64] W3[2][64] b3[2]   (5378 values)
+// Feature vector of a pair (src -> tgt), before standardisation:
+//   0-5  target: log2 b, H(x_t), H(x_{t+lag}, x_t), 2H - H2 (lag-1 information),
+//        log2 mean run length, 2^H / b
+//   6-11 source: the same six
+//   12 log2 N, 13 log2 block length, 14 log2 of (b_t - 1)(b_s - 1) b_t + 1,
+//   15 log2 of 2^{H2_t} * 2^{H_s}
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace tenex {
+namespace {
+
+constexpr int kIn = 16, kH = 64, kOut = 2;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kH * kIn, kOffW2 = kOffB1 + kH,
+              kOffB2 = kOffW2 + kH * kH, kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kOut * kH,
+              kParams = kOffB3 + kOut;
+constexpr int kGeneFeat = 8;
+
+__device__ __forceinline__ float gelu(float x) {
+  return 0.5f * x * (1.f + erff(x * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float cdf = 0.5f * (1.f + erff(x * 0.70710678118654752f));
+  const float pdf = 0.3989422804014327f * expf(-0.5f * x * x);
+  return cdf + x * pdf;
+}
+
+// ---- per-gene features (one CTA per gene, b <= 64 for the joint entropy) ----
+__global__ void gene_features_kernel(const uint8_t* __restrict__ bins, int64_t ld,
+                                     const int32_t* __restrict__ npv, int n, int N, int lag,
+                                     float* __restrict__ feat) {
+  __shared__ int h1[256];
+  __shared__ int h2[64 * 64];
+  __shared__ int changes;
+  const int g = blockIdx.x;
+  const int b = npv[g];
+  const uint8_t* row = bins + (int64_t)g * ld;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h1[i] = 0;
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) h2[i] = 0;
+  if (threadIdx.x == 0) changes = 0;
+  __syncthreads();
+  const bool joint = b >= 1 && b <= 64;
+  int ch = 0;
+  for (int s = threadIdx.x; s < N; s += blockDim.x) {
+    const int x0 = row[s], x1 = row[s + lag];
+    atomicAdd(&h1[x0], 1);
+    if (joint && x0 < 64 && x1 < 64) atomicAdd(&h2[x1 * 64 + x0], 1);
+    ch += x1 != x0;
+  }
+  atomicAdd(&changes, ch);
+  __syncthreads();
+  __shared__ double part[2][32];
+  double e1 = 0.0, e2 = 0.0;
+  const double invN = 1.0 / (double)N;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    if (h1[i]) {
+      const double p = h1[i] * invN;
+      e1 -= p * log2(p);
+    }
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x)
+    if (h2[i]) {
+      const double p = h2[i] * invN;
+      e2 -= p * log2(p);
+    }
+  e1 = dev::warp_sum(e1);
+  e2 = dev::warp_sum(e2);
+  if ((threadIdx.x & 31) == 0) {
+    part[0][threadIdx.x >> 5] = e1;
+    part[1][threadIdx.x >> 5] = e2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double H1 = 0.0, H2 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      H1 += part[0][w];
+      H2 += part[1][w];
+    }
+    float* f = feat + (int64_t)g * kGeneFeat;
+    const float nan = __int_as_float(0x7fc00000);
+    f[0] = log2f((float)max(b, 1));
+    f[1] = (float)H1;
+    f[2] = joint ? (float)H2 : nan;
+    f[3] = joint ? (float)(2.0 * H1 - H2) : nan;
+    f[4] = log2f((float)N / (float)(changes + 1));
+    f[5] = (float)(exp2(H1) / (double)max(b, 1));
+    f[6] = 0.f;
+    f[7] = 0.f;
+  }
+}
+
+__device__ __forceinline__ void pair_features(const float* __restrict__ gf, int tgt, int src,
+                                              float log2N, float log2bl, float* x) {
+  const float* t = gf + (int64_t)tgt * kGeneFeat;
+  const float* s = gf + (int64_t)src * kGeneFeat;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    x[k] = t[k];
+    x[6 + k] = s[k];
+  }
+  x[12] = log2N;
+  x[13] = log2bl;
+  const float bt = exp2f(t[0]), bs = exp2f(s[0]);
+  x[14] = log2f((bt - 1.f) * (bs - 1.f) * bt + 1.f);
+  x[15] = t[2] + s[1];
+}
+
+// Forward of one sample with weights in shared memory (float). Returns the two
+// outputs; optionally stores z1 and z2 (pre-activations).
+__device__ __forceinline__ void mlp_forward_one(const float* __restrict__ w, const float* x,
+                                                float* z1s, float* z2s, float& o0, float& o1) {
+  float g1[kH];
+#pragma unroll 4
+  for (int i = 0; i < kH; ++i) {
+    float a = w[kOffB1 + i];
+#pragma unroll
+    for (int f = 0; f < kIn; ++f) a = fmaf(w[kOffW1 + i * kIn + f], x[f], a);
+    if (z1s) z1s[i] = a;
+    g1[i] = gelu(a);
+  }
+  o0 = w[kOffB3];
+  o1 = w[kOffB3 + 1];
+  for (int j = 0; j < kH; ++j) {
+    float a = w[kOffB2 + j];
+#pragma unroll 8
+    for (int i = 0; i < kH; ++i) a = fmaf(w[kOffW2 + j * kH + i], g1[i], a);
+    if (z2s) z2s[j] = a;
+    const float g = gelu(a);
+    o0 = fmaf(w[kOffW3 + j], g, o0);
+    o1 = fmaf(w[kOffW3 + kH + j], g, o1);
+  }
+}
+
+__device__ __forceinline__ void load_weights(const __nv_bfloat16* __restrict__ wb, float* ws) {
+  for (int i = threadIdx.x; i < kParams; i += blockDim.x) ws[i] = __bfloat162float(wb[i]);
+}
+
+// Inference over all pairs: mu_log/sigma_log matrices at [src, tgt] (diagonal
+// untouched), features standardised by (fmean, fstd); NaN features give NaN
+// outputs (the caller sends those pairs to the full surrogate test).
+__global__ void __launch_bounds__(128) null_predict_kernel(
+    const float* __restrict__ gf, int n, float log2N, float log2bl,
+    const __nv_bfloat16* __restrict__ wb, const float* __restrict__ fmean,
+    const float* __restrict__ fstd, float* __restrict__ out0, float* __restrict__ out1) {
+  __shared__ float w[kParams];
+  __shared__ float mu[kIn], sd[kIn];
+  load_weights(wb, w);
+  if (threadIdx.x < kIn) {
+    mu[threadIdx.x] = fmean[threadIdx.x];
+    sd[threadIdx.x] = fstd[threadIdx.x];
+  }
+  __syncthreads();
+  const int64_t total = (int64_t)n * n;
+  for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < total;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    const int src = (int)(m / n), tgt = (int)(m - (int64_t)src * n);
+    if (src == tgt) continue;
+    float x[kIn];
+    pair_features(gf, tgt, src, log2N, log2bl, x);
+#pragma unroll
+    for (int f = 0; f < kIn; ++f) x[f] = (x[f] - mu[f]) / sd[f];
+    float o0, o1;
+    mlp_forward_one(w, x, nullptr, nullptr, o0, o1);
+    out0[m] = o0;
+    out1[m] = o1;
+  }
+}
+
+// Raw (unstandardised) features of a pair list.
+__global__ void pair_features_kernel(const float* __restrict__ gf, const int32_t* __restrict__ tgt,
+                                     const int32_t* __restrict__ src, int64_t P, float log2N,
+                                     float log2bl, float* __restrict__ X) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < P;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    float x[kIn];
+    pair_features(gf, tgt[p], src[p], log2N, log2bl, x);
+#pragma unroll
+    for (int f = 0; f < kIn; ++f) X[p * kIn + f] = x[f];
+  }
+}
+
+// Training forward: X (B x 16, standardised), stores z1 (B x 64), z2 (B x 64),
+// out (B x 2) and dout = out - Y; loss[0] += sum of squared errors / 2.
+__global__ void __launch_bounds__(128) mlp_train_forward_kernel(
+    const float* __restrict__ X, const float* __restrict__ Y, int B,
+    const __nv_bfloat16* __restrict__ wb, float* __restrict__ z1, float* __restrict__ z2,
+    float* __restrict__ dout, float* __restrict__ loss) {
+  __shared__ float w[kParams];
+  load_weights(wb, w);
+  __syncthreads();
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0.f;
+  if (b < B) {
+    float x[kIn];
+#pragma unroll
+    for (int f = 0; f < kIn; ++f) x[f] = X[(int64_t)b * kIn + f];
+    float o0, o1;
+    mlp_forward_one(w, x, z1 + (int64_t)b * kH, z2 + (int64_t)b * kH, o0, o1);
+    const float d0 = o0 - Y[2 * b], d1 = o1 - Y[2 * b + 1];
+    dout[2 * b] = d0;
+    dout[2 * b + 1] = d1;
+    l = 0.5f * (d0 * d0 + d1 * d1);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
+}
+
+// Backward deltas per sample: dz2 = (W3^T dout) * gelu'(z2), dz1 = (W2^T dz2) * gelu'(z1).
+// Overwrites z2 with dz2 and z1 with dz1 (the pre-activations are not needed after).
+__global__ void __launch_bounds__(128) mlp_train_deltas_kernel(
+    const __nv_bfloat16* __restrict__ wb, const float* __restrict__ dout, int B,
+    float* __restrict__ z1, float* __restrict__ z2) {
+  __shared__ float w[kParams];
+  load_weights(wb, w);
+  __syncthreads();
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const float d0 = dout[2 * b], d1 = dout[2 * b + 1];
+  float* zz2 = z2 + (int64_t)b * kH;
+  float* zz1 = z1 + (int64_t)b * kH;
+  float dz2[kH];
+#pragma unroll 8
+  for (int j = 0; j < kH; ++j) {
+    const float dg = w[kOffW3 + j] * d0 + w[kOffW3 + kH + j] * d1;
+    dz2[j] = dg * gelu_grad(zz2[j]);
+    zz2[j] = dz2[j];
+  }
+  for (int i = 0; i < kH; ++i) {
+    float dg = 0.f;
+#pragma unroll 8
+    for (int j = 0; j < kH; ++j) dg = fmaf(w[kOffW2 + j * kH + i], dz2[j], dg);
+    zz1[i] = dg * gelu_grad(zz1[i]);
+  }
+}
+
+// Weight gradients as batch reductions, one thread per parameter, averaged over B.
+// Needs the layer inputs: x (X), g1 = gelu(z1_pre) and g2 = gelu(z2_pre), recomputed
+// from stored copies z1p / z2p of the pre-activations.
+__global__ void mlp_weight_grads_kernel(const float* __restrict__ X, const float* __restrict__ z1p,
+                                        const float* __restrict__ z2p,
+                                        const float* __restrict__ dz1, const float* __restrict__ dz2,
+                                        const float* __restrict__ dout, int B,
+                                        float* __restrict__ grad) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kParams) return;
+  float acc = 0.f;
+  if (p < kOffB1) {  // W1[i][f]
+    const int i = p / kIn, f = p - i * kIn;
+    for (int b = 0; b < B; ++b) acc = fmaf(dz1[(int64_t)b * kH + i], X[(int64_t)b * kIn + f], acc);
+  } else if (p < kOffW2) {  // b1[i]
+    const int i = p - kOffB1;
+    for (int b = 0; b < B; ++b) acc += dz1[(int64_t)b * kH + i];
+  } else if (p < kOffB2) {  // W2[j][i]
+    const int q = p - kOffW2, j = q / kH, i = q - j * kH;
+    for (int b = 0; b < B; ++b)
+      acc = fmaf(dz2[(int64_t)b * kH + j], gelu(z1p[(int64_t)b * kH + i]), acc);
+  } else if (p < kOffW3) {  // b2[j]
+    const int j = p - kOffB2;
+    for (int b = 0; b < B; ++b) acc += dz2[(int64_t)b * kH + j];
+  } else if (p < kOffB3) {  // W3[k][j]
+    const int q = p - kOffW3, k = q / kH, j = q - k * kH;
+    for (int b = 0; b < B; ++b) acc = fmaf(dout[2 * b + k], gelu(z2p[(int64_t)b * kH + j]), acc);
+  } else {  // b3[k]
+    const int k = p - kOffB3;
+    for (int b = 0; b < B; ++b) acc += dout[2 * b + k];
+  }
+  grad[p] = acc / (float)B;
+}
+
+// Adam on the FP32 master copy, then the BF16 copy used by the forward kernels.
+__global__ void mlp_adam_kernel(float* __restrict__ master, const float* __restrict__ grad,
+                                float* __restrict__ m, float* __restrict__ v, float lr, float b1,
+                                float b2, float eps, float bc1, float bc2, float wd,
+                                __nv_bfloat16* __restrict__ wb) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= kParams) return;
+  const float g = grad[p] + wd * master[p];
+  const float mm = b1 * m[p] + (1.f - b1) * g;
+  const float vv = b2 * v[p] + (1.f - b2) * g * g;
+  m[p] = mm;
+  v[p] = vv;
+  const float upd = (mm / bc1) / (sqrtf(vv / bc2) + eps);
+  const float w = master[p] - lr * upd;
+  master[p] = w;
+  wb[p] = __float2bfloat16_rn(w);
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst,
+                               int count) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < count) dst[p] = __float2bfloat16_rn(src[p]);
+}
+
+}  // namespace
+}  // namespace tenex
+
+using namespace tenex;
+
+extern "C" int tenex_mlp_param_count(void) { return kParams; }
+
+extern "C" int tenex_gene_features(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                                   int n_vars, int64_t row_len, int64_t lag, float* feat,
+                                   void* stream) {
+  if (!bins || !n_per_var || !feat) return fail(TENEX_ERR_BADARG, "null pointer");
+  if (n_vars < 1 || lag < 1 || row_len <= lag) return fail(TENEX_ERR_BADARG, "bad shape");
+  gene_features_kernel<<<n_vars, 256, 0, as_stream(stream)>>>(bins, ld, n_per_var, n_vars,
+                                                              (int)(row_len - lag), (int)lag, feat);
+  return check_launch("gene_features_kernel");
+}
+
+extern "C" int tenex_pair_features(const float* gene_feat, const int32_t* tgt, const int32_t* src,
+                                   int64_t n_pairs, float log2N, float log2bl, float* X,
+                                   void* stream) {
+  if (!gene_feat || !tgt || !src || !X) return fail(TENEX_ERR_BADARG, "null pointer");
+  if (n_pairs <= 0) return TENEX_OK;
+  const int blocks = (int)std::min<int64_t>((n_pairs + 255) / 256, 8192);
+  pair_features_kernel<<<blocks, 256, 0, as_stream(stream)>>>(gene_feat, tgt, src, n_pairs, log2N,
+                                                              log2bl, X);
+  return check_launch("pair_features_kernel");
+}
+
+extern "C" int tenex_null_predict(const float* gene_feat, int n_vars, float log2N, float log2bl,
+                                  const void* weights_bf16, const float* feat_mean,
+                                  const float* feat_std, float* out_mu, float* out_sigma,
+                                  void* stream) {
+  if (!gene_feat || !weights_bf16 || !feat_mean || !feat_std || !out_mu || !out_sigma)
+    return fail(TENEX_ERR_BADARG, "null pointer");
+  if (n_vars < 2) return fail(TENEX_ERR_BADARG, "n_vars must be >= 2");
+  DevAttr A;
+  int st = current_device_attr(&A);
+  if (st) return st;
+  null_predict_kernel<<<A.sm_count * 8, 128, 0, as_stream(stream)>>>(
+      gene_feat, n_vars, log2N, log2bl, static_cast<const __nv_bfloat16*>(weights_bf16),
+      feat_mean, feat_std, out_mu, out_sigma);
+  return check_launch("null_predict_kernel");
+}
+
+extern "C" int tenex_mlp_train_step(const float* X, const float* Y, int batch, void* weights_bf16,
+                                    float* master, float* adam_m, float* adam_v, float* scratch,
+                                    float lr, float beta1, float beta2, float eps, float wd,
+                                    int step, float* loss, void* stream) {
+  if (!X || !Y || !weights_bf16 || !master || !adam_m || !adam_v || !scratch || !loss)
+    return fail(TENEX_ERR_BADARG, "null pointer");
+  if (batch < 1 || step < 1) return fail(TENEX_ERR_BADARG, "batch and step must be >= 1");
+  cudaStream_t s = as_stream(stream);
+  // scratch layout: z1 | z2 | z1 copy | z2 copy | dout | grad
+  float* z1 = scratch;
+  float* z2 = z1 + (int64_t)batch * kH;
+  float* z1p = z2 + (int64_t)batch * kH;
+  float* z2p = z1p + (int64_t)batch * kH;
+  float* dout = z2p + (int64_t)batch * kH;
+  float* grad = dout + (int64_t)batch * kOut;
+  __nv_bfloat16* wb = static_cast<__nv_bfloat16*>(weights_bf16);
+  const int blocks = (batch + 127) / 128;
+  mlp_train_forward_kernel<<<blocks, 128, 0, s>>>(X, Y, batch, wb, z1, z2, dout, loss);
+  cudaError_t e = cudaMemcpyAsync(z1p, z1, sizeof(float) * 2 * (size_t)batch * kH,
+                                  cudaMemcpyDeviceToDevice, s);  // z1|z2 -> z1p|z2p
+  if (e != cudaSuccess) return check_cuda(e, "copy pre-activations");
+  mlp_train_deltas_kernel<<<blocks, 128, 0, s>>>(wb, dout, batch, z1, z2);
+  mlp_weight_grads_kernel<<<(kParams + 127) / 128, 128, 0, s>>>(X, z1p, z2p, z1, z2, dout, batch,
+                                                                grad);
+  const float bc1 = 1.f - powf(beta1, (float)step), bc2 = 1.f - powf(beta2, (float)step);
+  mlp_adam_kernel<<<(kParams + 127) / 128, 128, 0, s>>>(master, grad, adam_m, adam_v, lr, beta1,
+                                                        beta2, eps, bc1, bc2, wd, wb);
+  return check_launch("mlp train step");
+}
+
+extern "C" size_t tenex_mlp_scratch_floats(int batch) {
+  return (size_t)batch * (4 * kH + kOut) + kParams;
+}
+
+extern "C" int tenex_mlp_gradients(const float* X, const float* Y, int batch,
+                                   const void* weights_bf16, float* scratch, float* grad_out,
+                                   float* loss, void* stream) {
+  if (!X || !Y || !weights_bf16 || !scratch || !grad_out || !loss)
+    return fail(TENEX_ERR_BADARG, "null pointer");
+  cudaStream_t s = as_stream(stream);
+  float* z1 = scratch;
+  float* z2 = z1 + (int64_t)batch * kH;
+  float* z1p = z2 + (int64_t)batch * kH;
+  float* z2p = z1p + (int64_t)batch * kH;
+  float* dout = z2p + (int64_t)batch * kH;
+  const __nv_bfloat16* wb = static_cast<const __nv_bfloat16*>(weights_bf16);
+  const int blocks = (batch + 127) / 128;
+  mlp_train_forward_kernel<<<blocks, 128, 0, s>>>(X, Y, batch, wb, z1, z2, dout, loss);
+  cudaError_t e = cudaMemcpyAsync(z1p, z1, sizeof(float) * 2 * (size_t)batch * kH,
+                                  cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return check_cuda(e, "copy pre-activations");
+  mlp_train_deltas_kernel<<<blocks, 128, 0, s>>>(wb, dout, batch, z1, z2);
+  mlp_weight_grads_kernel<<<(kParams + 127) / 128, 128, 0, s>>>(X, z1p, z2p, z1, z2, dout, batch,
+                                                                grad_out);
+  return check_launch("mlp gradients");
+}
+
+extern "C" int tenex_to_bf16(const float* src, void* dst, int count, void* stream) {
+  if (!src || !dst || count < 0) return fail(TENEX_ERR_BADARG, "bad arguments");
+  if (count == 0) return TENEX_OK;
+  to_bf16_kernel<<<(count + 255) / 256, 256, 0, as_stream(stream)>>>(
+      src, static_cast<__nv_bfloat16*>(dst), count);
+  return check_launch("to_bf16_kernel");
+}

@@ -928,6 +928,18 @@ extern "C" int tenex_te_pairs(const uint8_t* bins, int64_t ld, const int32_t* n_
                 cfg, stream, pairs, item_start, n_items);
 }
 
+extern "C" int tenex_surrogate_accumulate_pairs(
+    const uint8_t* bins, int64_t ld, const int32_t* n_per_var, int b_max, int n_vars,
+    int64_t row_len, int64_t lag, const int64_t* pairs, int64_t n_pairs,
+    const int64_t* item_start, int64_t n_items, const float* observed, double* sum,
+    double* sumsq, int32_t* count_ge, void* workspace, size_t workspace_bytes,
+    const tenex_te_config* cfg, void* stream) {
+  if (!pairs || !item_start) return fail(TENEX_ERR_BADARG, "pairs and item_start must be non-NULL");
+  return te_run(bins, ld, n_per_var, b_max, n_vars, row_len, lag, 0, n_pairs, kOutStats, nullptr,
+                0, observed, sum, sumsq, count_ge, nullptr, 0, workspace, workspace_bytes, cfg,
+                stream, pairs, item_start, n_items);
+}
+
 // ---------------------------------------------------------------------------
 // Entry point for callers that must not allocate device memory.
 //

@@ -1,0 +1,453 @@
+"""Learned null model for the surrogate test (no reference counterpart).
+
+The block-shuffle surrogate test spends S full TE matrices to estimate, per
+pair, the mean and spread of TE under the null. That distribution depends on
+cheap per-gene statistics (bin counts, marginal and lag-1 joint entropies,
+autocorrelation, run lengths) and on N and the block length, not on the
+pair's coupling. A small MLP (16 -> 64 -> 64 -> 2, GELU, BF16 weights, FP32
+accumulation; kernels in null_mlp.cu) predicts log(mu*N) and log(sigma*N) of
+the null from those features.
+
+Training: synthetic datasets from generator seeds disjoint from evaluation
+(2000-2019 by default); each is run through the full surrogate test (S
+shuffles, permutation seeds disjoint from evaluation too), and the per-pair
+surrogate mean / std are the targets. Everything runs on the GPU through this
+package's kernels (features, forward, backward, Adam).
+
+Inference (null="learned" in SurrogateTestMethod.infer): predicted mu, sigma
+give z = (TE_obs - mu) / sigma and parametric p-values; the BH-FDR threshold of
+those p-values gives z_FDR. Every pair with z >= z_FDR - band (the band is
+calibrated on held-out seeds and stored with the model), every pair whose genes
+fall outside the features seen in training, and every pair with undefined
+features goes to the full block-shuffle surrogate test (pair-list kernel, the
+full test's own permutations, so those pairs get exactly the full test's
+statistics). BH is then recomputed over the mixed p-values and the screen is
+widened while z_FDR - band keeps falling. Called edges are therefore always
+verified by the full test; the band only decides how many true edges could be
+missed (pairs whose predicted z falls more than `band` below z_FDR).
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from tenex_b200 import _log, native
+from tenex_b200.kernels import device as D
+
+GENE_FEAT = 8
+N_IN = 16
+DEFAULT_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "null_model_cfg5.npz")
+
+
+def n_params() -> int:
+    return int(native.lib().tenex_mlp_param_count())
+
+
+def init_params(rng: np.random.Generator) -> np.ndarray:
+    """He-style initialisation of W1, W2, W3 (biases zero), FP32."""
+    H = 64
+    w1 = rng.normal(0, np.sqrt(2.0 / N_IN), (H, N_IN))
+    w2 = rng.normal(0, np.sqrt(2.0 / H), (H, H))
+    w3 = rng.normal(0, np.sqrt(1.0 / H), (2, H))
+    return np.concatenate([w1.ravel(), np.zeros(H), w2.ravel(), np.zeros(H), w3.ravel(),
+                           np.zeros(2)]).astype(np.float32)
+
+
+@dataclass
+class NullModel:
+    params: np.ndarray            # FP32 master parameters
+    feat_mean: np.ndarray         # (16,)
+    feat_std: np.ndarray          # (16,)
+    gene_lo: np.ndarray           # (6,) per-gene feature range seen in training
+    gene_hi: np.ndarray
+    meta: dict = field(default_factory=dict)
+
+    def save(self, path: str) -> None:
+        np.savez(path, params=self.params, feat_mean=self.feat_mean, feat_std=self.feat_std,
+                 gene_lo=self.gene_lo, gene_hi=self.gene_hi,
+                 meta=np.array(repr(self.meta)))
+
+    @staticmethod
+    def load(path: str = DEFAULT_MODEL) -> "NullModel":
+        if not os.path.exists(path):
+            raise FileNotFoundError(
+                f"{path} not found; train a model with "
+                f"`python -m tenex_b200.inference.learned_null --train`")
+        z = np.load(path, allow_pickle=False)
+        import ast
+        return NullModel(z["params"].astype(np.float32), z["feat_mean"], z["feat_std"],
+                         z["gene_lo"], z["gene_hi"], ast.literal_eval(str(z["meta"])))
+
+    def device_weights(self, dev) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        master = torch.from_numpy(self.params).to(dev)
+        wb = torch.empty(master.numel(), dtype=torch.bfloat16, device=dev)
+        native.call("tenex_to_bf16", master.data_ptr(), wb.data_ptr(), master.numel(),
+                    native.stream_ptr())
+        return (wb, torch.from_numpy(self.feat_mean.astype(np.float32)).to(dev),
+                torch.from_numpy(self.feat_std.astype(np.float32)).to(dev))
+
+
+def gene_features(db: D.DeviceBins, npv: torch.Tensor, tau: int) -> torch.Tensor:
+    """(n, 8) float32 per-gene features on the device."""
+    feat = torch.empty((db.n, GENE_FEAT), dtype=torch.float32, device=db.data.device)
+    native.call("tenex_gene_features", db.data.data_ptr(), db.ld, npv.data_ptr(), db.n,
+                db.row_len, tau * db.K, feat.data_ptr(), native.stream_ptr())
+    return feat
+
+
+def pair_features(gf: torch.Tensor, tgt: torch.Tensor, src: torch.Tensor, N: int,
+                  block_length: int) -> torch.Tensor:
+    P = int(tgt.numel())
+    X = torch.empty((P, N_IN), dtype=torch.float32, device=gf.device)
+    native.call("tenex_pair_features", gf.data_ptr(), tgt.data_ptr(), src.data_ptr(), P,
+                float(np.log2(N)), float(np.log2(block_length)), X.data_ptr(),
+                native.stream_ptr())
+    return X
+
+
+def predict(model: NullModel, db: D.DeviceBins, npv: torch.Tensor, tau: int, block_length: int,
+            gf: torch.Tensor | None = None):
+    """Null mean and std of TE for every ordered pair ([src, tgt], float32 device
+    tensors, NaN where undefined) and a per-gene in-range flag."""
+    dev = db.data.device
+    n = db.n
+    N = (db.T - tau) * db.K
+    if gf is None:
+        gf = gene_features(db, npv, tau)
+    wb, fm, fs = model.device_weights(dev)
+    lmu = torch.full((n, n), float("nan"), dtype=torch.float32, device=dev)
+    lsg = torch.full((n, n), float("nan"), dtype=torch.float32, device=dev)
+    native.call("tenex_null_predict", gf.data_ptr(), n, float(np.log2(N)),
+                float(np.log2(block_length)), wb.data_ptr(), fm.data_ptr(), fs.data_ptr(),
+                lmu.data_ptr(), lsg.data_ptr(), native.stream_ptr())
+    mu = torch.exp(lmu) / N
+    sigma = torch.exp(lsg) / N
+    lo = torch.from_numpy(model.gene_lo.astype(np.float32)).to(dev)
+    hi = torch.from_numpy(model.gene_hi.astype(np.float32)).to(dev)
+    g6 = gf[:, :6]
+    in_range = ((g6 >= lo) & (g6 <= hi)).all(dim=1) & torch.isfinite(g6).all(dim=1)
+    meta = model.meta
+    if "N" in meta and abs(np.log2(N) - np.log2(meta["N"])) > 0.5:
+        in_range[:] = False
+    if "block_length" in meta and abs(np.log2(block_length) - np.log2(meta["block_length"])) > 0.5:
+        in_range[:] = False
+    return mu, sigma, in_range
+
+
+# --------------------------------------------------------------------------- training
+def surrogate_moments(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int, S: int,
+                      block_length: int, seed: int) -> tuple[torch.Tensor, torch.Tensor]:
+    """Per-pair mean and population std of the surrogate TE ([src, tgt], device)."""
+    from tenex_b200.inference.surrogate_test import (SurrogateAccumulator, build_block_perm,
+                                                     run_surrogates)
+    n = db.n
+    obs = torch.zeros((n, n), dtype=torch.float32, device=db.data.device)
+    acc = SurrogateAccumulator(db, npv, b_max, tau, obs, b_max == 2)
+    perms, bl, _ = build_block_perm(n, db.T, "block", block_length, 0, S, seed, db.data.device)
+    run_surrogates(acc, perms, bl, use_graph=True)
+    mean = acc.sum / S
+    var = acc.sumsq / S - mean * mean
+    return mean.float(), torch.sqrt(torch.clamp(var, min=0.0)).float()
+
+
+def training_set(seeds, n: int, T: int, S: int, block_length: int, pairs_per_dataset: int,
+                 dev, tau: int = 1):
+    """Raw features X (P, 16) and targets Y (P, 2) = log(mu*N), log(sigma*N) on the device."""
+    from tenex_b200 import workloads as W
+    Xs, Ys, G = [], [], []
+    N = T - tau
+    rng = np.random.default_rng(12345)
+    for sd in seeds:
+        x, npv, _ = W.cfg5_bins(n=n, T=T, seed=int(sd))
+        db = D.pack_bins(x, dev)
+        npv_t = torch.as_tensor(npv, dtype=torch.int32, device=dev)
+        b_max = int(npv.max())
+        mean, std = surrogate_moments(db, npv_t, b_max, tau, S, block_length, 10_000 + int(sd))
+        gf = gene_features(db, npv_t, tau)
+        t = rng.integers(0, n, pairs_per_dataset)
+        s = rng.integers(0, n - 1, pairs_per_dataset)
+        s = s + (s >= t)
+        tt = torch.as_tensor(t, dtype=torch.int32, device=dev)
+        ss = torch.as_tensor(s, dtype=torch.int32, device=dev)
+        X = pair_features(gf, tt, ss, N, block_length)
+        mu = mean[ss.long(), tt.long()]
+        sg = std[ss.long(), tt.long()]
+        ok = torch.isfinite(X).all(dim=1) & (mu > 0) & (sg > 0)
+        Y = torch.stack([torch.log(mu * N), torch.log(sg * N)], dim=1)
+        Xs.append(X[ok])
+        Ys.append(Y[ok])
+        G.append(gf[:, :6])
+        _log.vprint(f"[TENEX] null training data: seed {sd}, {int(ok.sum())} pairs")
+    return torch.cat(Xs), torch.cat(Ys), torch.cat(G)
+
+
+def train(X: torch.Tensor, Y: torch.Tensor, G: torch.Tensor, steps: int = 3000, batch: int = 8192,
+          lr: float = 3e-3, wd: float = 1e-5, seed: int = 0, Xval=None, Yval=None,
+          meta: dict | None = None) -> tuple[NullModel, dict]:
+    """Adam on the MLP with this package's training kernels; cosine-decayed lr."""
+    dev = X.device
+    fm = X.mean(dim=0)
+    fs = X.std(dim=0).clamp(min=1e-3)
+    Xn = ((X - fm) / fs).contiguous()
+    Yc = Y.contiguous()
+    rng = np.random.default_rng(seed)
+    master = torch.from_numpy(init_params(rng)).to(dev)
+    P = master.numel()
+    wb = torch.empty(P, dtype=torch.bfloat16, device=dev)
+    native.call("tenex_to_bf16", master.data_ptr(), wb.data_ptr(), P, native.stream_ptr())
+    m = torch.zeros(P, dtype=torch.float32, device=dev)
+    v = torch.zeros(P, dtype=torch.float32, device=dev)
+    scratch = torch.empty(int(native.lib().tenex_mlp_scratch_floats(batch)), dtype=torch.float32,
+                          device=dev)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    n = Xn.shape[0]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    hist = []
+    since = 0
+    t0 = time.time()
+    for step in range(1, steps + 1):
+        idx = torch.randint(0, n, (batch,), device=dev, generator=gen)
+        xb = Xn[idx].contiguous()
+        yb = Yc[idx].contiguous()
+        lr_t = 0.5 * lr * (1 + np.cos(np.pi * (step - 1) / steps))
+        native.call("tenex_mlp_train_step", xb.data_ptr(), yb.data_ptr(), batch, wb.data_ptr(),
+                    master.data_ptr(), m.data_ptr(), v.data_ptr(), scratch.data_ptr(),
+                    float(lr_t), 0.9, 0.999, 1e-8, float(wd), step, loss.data_ptr(),
+                    native.stream_ptr())
+        since += 1
+        if step % 250 == 0 or step == steps:
+            hist.append((step, float(loss.item()) / (since * batch)))
+            loss.zero_()
+            since = 0
+    report = {"train_seconds": time.time() - t0, "loss_history": hist}
+    gene_lo = G.min(dim=0).values.cpu().numpy()
+    gene_hi = G.max(dim=0).values.cpu().numpy()
+    model = NullModel(master.cpu().numpy(), fm.cpu().numpy(), fs.cpu().numpy(), gene_lo, gene_hi,
+                      dict(meta or {}))
+    if Xval is not None:
+        report["val_mse"] = evaluate(model, Xval, Yval)
+    return model, report
+
+
+def evaluate(model: NullModel, Xraw: torch.Tensor, Y: torch.Tensor) -> list[float]:
+    """Mean squared error of the two outputs on raw features (through the kernels)."""
+    dev = Xraw.device
+    wb, fm, fs = model.device_weights(dev)
+    Xn = ((Xraw - fm) / fs).contiguous()
+    B = Xn.shape[0]
+    scratch = torch.empty(int(native.lib().tenex_mlp_scratch_floats(B)), dtype=torch.float32,
+                          device=dev)
+    grad = torch.empty(n_params(), dtype=torch.float32, device=dev)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    native.call("tenex_mlp_gradients", Xn.data_ptr(), Y.contiguous().data_ptr(), B, wb.data_ptr(),
+                scratch.data_ptr(), grad.data_ptr(), loss.data_ptr(), native.stream_ptr())
+    z2off = 3 * B * 64 + B * 64  # dout lives after z1 | z2 | z1p | z2p
+    dout = scratch[z2off:z2off + 2 * B].view(B, 2)
+    return [float((dout[:, 0] ** 2).mean()), float((dout[:, 1] ** 2).mean())]
+
+
+def train_default(device="cuda", seeds=range(2000, 2018), val_seeds=(2018, 2019), n=2000,
+                  T=5000, S=100, block_length=50, pairs_per_dataset=150_000, steps=4000,
+                  out=DEFAULT_MODEL) -> dict:
+    dev = torch.device(device)
+    t0 = time.time()
+    X, Y, G = training_set(list(seeds), n, T, S, block_length, pairs_per_dataset, dev)
+    Xv, Yv, Gv = training_set(list(val_seeds), n, T, S, block_length, 50_000, dev)
+    t_data = time.time() - t0
+    meta = {"N": T - 1, "block_length": block_length, "n_surrogates": S,
+            "train_seeds": [int(s) for s in seeds], "val_seeds": [int(s) for s in val_seeds],
+            "generator": "cfg5_bins", "n": n, "T": T}
+    model, rep = train(X, Y, torch.cat([G, Gv]), steps=steps, Xval=Xv, Yval=Yv, meta=meta)
+    rep["data_seconds"] = t_data
+    rep["train_pairs"] = int(X.shape[0])
+    model.meta["report"] = {k: rep[k] for k in ("val_mse", "train_pairs")}
+    model.save(out)
+    return rep
+
+
+# --------------------------------------------------------------------------- inference
+def _pair_items(pairs_ts: np.ndarray, run: int = 128):
+    from tenex_b200.kernels.pair_list import item_table
+    order = np.argsort(pairs_ts[:, 0], kind="stable")
+    sp = np.ascontiguousarray(pairs_ts[order])
+    return sp, item_table(sp[:, 0], run)
+
+
+def fallback_surrogates(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int,
+                        pairs_ts: np.ndarray, obs: torch.Tensor, perms: torch.Tensor, bl: int,
+                        use_graph: bool = True):
+    """Full surrogate statistics (all S = perms.shape[0] shuffles, the same
+    permutations as the full test) for the listed [tgt, src] pairs only: device
+    (n, n) float64 sum, sum of squares and int32 count_ge, indexed [src, tgt];
+    entries of other pairs stay zero."""
+    dev = db.data.device
+    n = db.n
+    S = perms.shape[0]
+    sp, items = _pair_items(pairs_ts)
+    pairs_d = torch.from_numpy(sp).to(dev)
+    items_d = torch.from_numpy(items).to(dev)
+    shuf = D.empty_bins(n, db.T, db.K, dev)
+    ssum = torch.zeros((n, n), dtype=torch.float64, device=dev)
+    ssq = torch.zeros((n, n), dtype=torch.float64, device=dev)
+    cnt = torch.zeros((n, n), dtype=torch.int32, device=dev)
+    ws = D.workspace(dev, n, db.row_len, b_max)
+
+    def one(k):
+        D.block_shuffle(db, perms[k], bl, out=shuf)
+        native.call("tenex_surrogate_accumulate_pairs", shuf.data.data_ptr(), shuf.ld,
+                    npv.data_ptr(), int(b_max), n, shuf.row_len, tau * db.K, pairs_d.data_ptr(),
+                    sp.shape[0], items_d.data_ptr(), items.shape[0] - 1, obs.data_ptr(),
+                    ssum.data_ptr(), ssq.data_ptr(), cnt.data_ptr(), ws.data_ptr(), ws.numel(),
+                    None, native.stream_ptr())
+
+    one(0)
+    native.call("tenex_workspace_status", ws.data_ptr(), native.stream_ptr())
+    if use_graph and S > 1:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for k in range(1, S):
+                one(k)
+        g.replay()
+        torch.cuda.synchronize(dev)
+        del g
+    else:
+        for k in range(1, S):
+            one(k)
+    native.call("tenex_workspace_status", ws.data_ptr(), native.stream_ptr())
+    return ssum, ssq, cnt
+
+
+def bh_cut(p: torch.Tensor, fdr: float) -> float:
+    """Largest p-value that BH-FDR at level fdr calls significant (adjusted
+    p < fdr) among the 1-D p-values p, or 0.0 when none is."""
+    from tenex_b200.inference.grn import bh_fdr_gpu
+    if p.numel() == 0:
+        return 0.0
+    sig = bh_fdr_gpu(p, fdr) < fdr
+    return float(p[sig].max()) if bool(sig.any()) else 0.0
+
+
+def z_of_p(p: float, m: int, fdr: float) -> float:
+    """Upper-tail normal quantile of p (of fdr / m when p is 0: nothing significant)."""
+    from scipy.special import ndtri
+    q = p if p > 0.0 else fdr / max(m, 1)
+    return float(ndtri(1.0 - min(max(q, 1e-300), 1.0 - 1e-16)))
+
+
+def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n_per_var, b_max,
+                           kernel_name, tau, n_surrogates, shuffle_method, block_length, p_method,
+                           fdr, seed, kwargs):
+    """Surrogate test with the learned null screening the pairs (see module doc).
+
+    Pairs whose predicted z reaches z_FDR - band (z_FDR from BH over the current
+    p-values), and pairs the model cannot score, run the full S-shuffle test with
+    the full test's permutations, so their statistics equal the full test's; the
+    rest keep the predicted null. BH is recomputed on the mixed p-values and the
+    screen widened until z_FDR - band stops falling (at most max_rounds times)."""
+    from scipy.special import erfc
+    from tenex_b200.inference.grn import build_pairs
+    from tenex_b200.inference.surrogate_test import (SurrogateTestResult, bh_edges,
+                                                     build_block_perm, pair_statistics)
+    t0 = time.time()
+    model = kwargs.get("null_model")
+    if model is None:
+        model = NullModel.load(kwargs.get("null_model_path", DEFAULT_MODEL))
+    band = float(kwargs.get("fallback_band", model.meta.get("band", 1.0)))
+    max_rounds = int(kwargs.get("max_rounds", 4))
+    use_graph = bool(kwargs.get("use_graph", True))
+    n, T = bin_data.shape[0], bin_data.shape[1]
+    db = D.pack_bins(bin_data, dev)
+    npv = torch.as_tensor(np.asarray(n_per_var), dtype=torch.int32).to(dev)
+    bl_eff = 1 if (shuffle_method == "random" or block_length <= 1
+                   or block_length >= T) else block_length
+    mu_d, sg_d, in_range = predict(model, db, npv, tau, max(bl_eff, 2))
+    obs_d = torch.as_tensor(observed_te, dtype=torch.float32, device=dev).contiguous()
+    z_d = (obs_d - mu_d) / torch.clamp(sg_d, min=1e-12)
+    sources = kwargs.get("sources")
+    if sources is not None:
+        pb = build_pairs(np.asarray(variable_names), sources)
+        tested_np = np.zeros((n, n), dtype=bool)
+        tested_np[pb[:, 0], pb[:, 1]] = True
+        tested = torch.from_numpy(tested_np).to(dev)
+    else:
+        tested = ~torch.eye(n, dtype=torch.bool, device=dev)
+    valid = torch.isfinite(z_d) & in_range[None, :] & in_range[:, None]
+    p_mix = 0.5 * torch.special.erfc(z_d.double() / np.sqrt(2.0))
+    p_mix = torch.where(valid, p_mix, torch.ones_like(p_mix))
+    mean_s = mu_d.clone()
+    std_s = sg_d.clone()
+    eff_s = obs_d - mean_s
+    count = torch.zeros((n, n), dtype=torch.int32, device=dev)
+    verified = torch.zeros((n, n), dtype=torch.bool, device=dev)
+    m_tested = int(tested.sum())
+    t_pred = time.time() - t0
+    perms = None
+    rounds, z_cuts, t_verify = 0, [], 0.0
+    for _ in range(max_rounds):
+        z_cut = z_of_p(bh_cut(p_mix[tested], fdr), m_tested, fdr)
+        z_cuts.append(z_cut)
+        new = tested & ~verified & (~valid | (z_d >= z_cut - band))
+        idx = torch.nonzero(new)                                   # (src, tgt)
+        if idx.shape[0] == 0:
+            break
+        tv = time.time()
+        if perms is None:
+            perms, bl, _ = build_block_perm(n, T, shuffle_method, block_length, 0, n_surrogates,
+                                            seed, dev)
+        idx_np = idx.cpu().numpy()
+        pairs_ts = np.ascontiguousarray(idx_np[:, ::-1]).astype(np.int64)
+        ssum, ssq, cnt = fallback_surrogates(db, npv, b_max, tau, pairs_ts, obs_d, perms, bl,
+                                             use_graph)
+        si, ti = idx[:, 0], idx[:, 1]
+        ms, ss_, ef, pv = pair_statistics(observed_te[idx_np[:, 0], idx_np[:, 1]],
+                                          ssum[si, ti].cpu().numpy(), ssq[si, ti].cpu().numpy(),
+                                          cnt[si, ti].cpu().numpy(), n_surrogates, p_method)
+        mean_s[si, ti] = torch.from_numpy(ms).to(dev)
+        std_s[si, ti] = torch.from_numpy(ss_).to(dev)
+        eff_s[si, ti] = torch.from_numpy(ef).to(dev)
+        p_mix[si, ti] = torch.from_numpy(pv).to(dev).double()
+        count[si, ti] = cnt[si, ti]
+        verified |= new
+        rounds += 1
+        t_verify += time.time() - tv
+    diag = torch.arange(n, device=dev)
+    p_mix[diag, diag] = 1.0
+    mean_s[diag, diag] = 0.0
+    std_s[diag, diag] = 0.0
+    eff_s[diag, diag] = obs_d[diag, diag]
+    p_values = p_mix.float().cpu().numpy()
+    mean_np = mean_s.cpu().numpy()
+    std_np = std_s.cpu().numpy()
+    effective = eff_s.cpu().numpy()
+    grn, _ = bh_edges(p_values, effective, variable_names, sources, fdr, dev)
+    n_ver = int(verified.sum())
+    info = {"n_fallback": n_ver, "fallback_fraction": n_ver / max(m_tested, 1),
+            "n_invalid": int((tested & ~valid).sum()), "z_cuts": z_cuts, "band": band,
+            "rounds": rounds, "seconds_predict": t_pred, "seconds_verify": t_verify,
+            "seconds_total": time.time() - t0,
+            "n_out_of_range_genes": int((~in_range).sum().item())}
+    _log.vprint(f"[TENEX] learned null: {n_ver} pairs ({100 * info['fallback_fraction']:.3f}%) "
+                f"verified by the full surrogate test in {rounds} round(s); {len(grn)} edges")
+    return SurrogateTestResult(observed_te=observed_te, mean_surrogate_te=mean_np,
+                               std_surrogate_te=std_np, effective_te=effective, p_values=p_values,
+                               grn=grn, n_surrogates=n_surrogates, shuffle_method=shuffle_method,
+                               block_length=block_length if shuffle_method == "block" else None,
+                               p_method=p_method, fdr=fdr, null_model="learned", info=info)
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", action="store_true")
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--out", default=DEFAULT_MODEL)
+    a = ap.parse_args()
+    if a.train:
+        _log.set_verbose(True)
+        rep = train_default(steps=a.steps, out=a.out)
+        print(rep)

@@ -140,6 +140,15 @@ def surrogate_statistics(observed_te: np.ndarray, sum_surr: np.ndarray, sum_sq_s
                          count_ge: np.ndarray, n_surrogates: int, p_method: str):
     """mean, std (population), effective TE and p-values, computed with the
     reference's numpy expressions (tenex/inference/surrogate_test.py:890-912)."""
+    out = pair_statistics(observed_te, sum_surr, sum_sq_surr, count_ge, n_surrogates, p_method)
+    np.fill_diagonal(out[3], 1.0)
+    return out
+
+
+def pair_statistics(observed_te: np.ndarray, sum_surr: np.ndarray, sum_sq_surr: np.ndarray,
+                    count_ge: np.ndarray, n_surrogates: int, p_method: str):
+    """The elementwise part of surrogate_statistics, for arrays of any shape
+    (the learned null applies it to its verified pairs only)."""
     mean_surr = (sum_surr / n_surrogates).astype(np.float32)
     var_surr = sum_sq_surr / n_surrogates - (sum_surr / n_surrogates) ** 2
     std_surr = np.sqrt(np.maximum(var_surr, 0.0)).astype(np.float32)
@@ -151,7 +160,6 @@ def surrogate_statistics(observed_te: np.ndarray, sum_surr: np.ndarray, sum_sq_s
         p_values = (0.5 * erfc(z / np.sqrt(2.0))).astype(np.float32)
     else:
         p_values = ((1.0 + count_ge) / (1.0 + n_surrogates)).astype(np.float32)
-    np.fill_diagonal(p_values, 1.0)
     return mean_surr, std_surr, effective_te, p_values
 
 

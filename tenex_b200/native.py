@@ -73,6 +73,8 @@ _SIGS = {
                                    ctypes.POINTER(TeConfig), _P],
     "tenex_block_shuffle": [_P, _L, _I, _L, _I, _P, _I, _I, _P, _L, _P],
     "tenex_stats_accumulate": [_P, _P, _P, _P, _P, _I, _P],
+    "tenex_surrogate_accumulate_pairs": [_P, _L, _P, _I, _I, _L, _L, _P, _L, _P, _L, _P, _P, _P,
+                                         _P, _P, _S, ctypes.POINTER(TeConfig), _P],
     "tenex_fsbwl_bins": [_P, _L, _I, _I, ctypes.c_float, _P, _L, _P, _P],
     "tenex_remap_dense": [_P, _I, _L, _I, _L, _P, _I, _L, _P, _P, _P],
     "tenex_coarsen": [_P, _L, _I, _L, _P, _I, _P],
@@ -80,11 +82,21 @@ _SIGS = {
     "tenex_b2_workspace_bytes": [_I, _L, _L],
     "tenex_te_binary_matrix": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _P],
     "tenex_b2_status": [_P, _I, _L, _L, _P],
+    "tenex_mlp_param_count": [],
+    "tenex_gene_features": [_P, _L, _P, _I, _L, _L, _P, _P],
+    "tenex_pair_features": [_P, _P, _P, _L, ctypes.c_float, ctypes.c_float, _P, _P],
+    "tenex_null_predict": [_P, _I, ctypes.c_float, ctypes.c_float, _P, _P, _P, _P, _P, _P],
+    "tenex_mlp_scratch_floats": [_I],
+    "tenex_mlp_gradients": [_P, _P, _I, _P, _P, _P, _P, _P],
+    "tenex_mlp_train_step": [_P, _P, _I, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float,
+                             ctypes.c_float, ctypes.c_float, ctypes.c_float, _I, _P, _P],
+    "tenex_to_bf16": [_P, _P, _I, _P],
     "tenex_probe_smem_atomics": [_I, _I, ctypes.POINTER(ctypes.c_int64),
                                  ctypes.POINTER(ctypes.c_float), _P],
 }
 _RESTYPES = {"tenex_te_workspace_bytes": ctypes.c_size_t,
-             "tenex_b2_workspace_bytes": ctypes.c_size_t}
+             "tenex_b2_workspace_bytes": ctypes.c_size_t,
+             "tenex_mlp_scratch_floats": ctypes.c_size_t}
 
 _lib = None
 _lock = threading.Lock()
