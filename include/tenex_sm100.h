@@ -229,12 +229,24 @@ int tenex_mlp_param_count(void);
  * 2H - H2, log2 mean run length, 2^H / b (joint terms NaN when b > 64). */
 int tenex_gene_features(const uint8_t* bins, int64_t ld, const int32_t* n_per_var, int n_vars,
                         int64_t row_len, int64_t lag, float* feat, void* stream);
-/* Raw 16 features of the pairs (tgt[i], src[i]) into X (n_pairs x 16). */
-int tenex_pair_features(const float* gene_feat, const int32_t* tgt, const int32_t* src,
-                        int64_t n_pairs, float log2N, float log2bl, float* X, void* stream);
+/* Independence bias of every ordered pair, eiid[src*n + tgt] (float, NaN when
+ * b_t or b_s > 64): E_iid = sum_{a,b} g(n_a q_b) - sum_{x,b} g(n_x q_b) with n_a the
+ * counts of the target's (x_{t+lag}, x_t) states, n_x of x_t, q_b the source's
+ * marginal over the same N = row_len - lag positions and g(m) = E[C ln C] - m ln m
+ * for C ~ Poisson(m) (the expected plug-in bias of N ln2 * TE under independence).
+ * Workspace: tenex_eiid_workspace_bytes(n_vars) bytes, 16-byte aligned. */
+size_t tenex_eiid_workspace_bytes(int n_vars);
+int tenex_eiid_matrix(const uint8_t* bins, int64_t ld, const int32_t* n_per_var, int n_vars,
+                      int64_t row_len, int64_t lag, float* eiid, void* workspace,
+                      size_t workspace_bytes, void* stream);
+/* Raw 16 features of the pairs (tgt[i], src[i]) into X (n_pairs x 16); eiid is the
+ * (n_vars x n_vars) matrix of tenex_eiid_matrix. */
+int tenex_pair_features(const float* gene_feat, const float* eiid, int n_vars,
+                        const int32_t* tgt, const int32_t* src, int64_t n_pairs, float log2bl,
+                        float* X, void* stream);
 /* Prediction for every ordered pair: out_mu[src*n + tgt], out_sigma[...] (log scale;
  * NaN where a feature is undefined); features standardised by feat_mean/feat_std. */
-int tenex_null_predict(const float* gene_feat, int n_vars, float log2N, float log2bl,
+int tenex_null_predict(const float* gene_feat, const float* eiid, int n_vars, float log2bl,
                        const void* weights_bf16, const float* feat_mean, const float* feat_std,
                        float* out_mu, float* out_sigma, void* stream);
 /* Scratch floats needed by a training step / gradient call of `batch` samples. */

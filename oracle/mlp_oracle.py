@@ -2,7 +2,8 @@
 
 float64 numpy forward / backward of the 16 -> 64 -> 64 -> 2 GELU MLP whose
 kernels live in the package (null_mlp.cu), on the same BF16-rounded weights,
-plus a numpy restatement of the per-gene features. Used only by tests to check
+plus numpy restatements of the per-gene features, the pair independence bias
+E_iid and the pair features. Used only by tests to check
 the kernels' outputs and gradients.
 """
 from __future__ import annotations
@@ -87,3 +88,64 @@ def gene_features(bins: np.ndarray, npv: np.ndarray, lag: int = 1) -> np.ndarray
         b = max(int(npv[g]), 1)
         out[g] = [np.log2(b), H1, H2, 2 * H1 - H2, np.log2(N / (ch + 1)), 2 ** H1 / b]
     return out
+
+
+def g_poisson(m: np.ndarray) -> np.ndarray:
+    """g(m) = E[C ln C] - m ln m for C ~ Poisson(m), by direct summation of the
+    Poisson series (float64, log-space probabilities)."""
+    from scipy.special import gammaln
+    m = np.atleast_1d(np.asarray(m, np.float64)).ravel()
+    out = np.zeros_like(m)
+    pos = m > 0
+    if not pos.any():
+        return out
+    mp = m[pos]
+    kmax = int(mp.max() + 14 * np.sqrt(mp.max()) + 60)
+    k = np.arange(1, kmax + 1, dtype=np.float64)
+    klk = k * np.log(k)
+    lg = gammaln(k + 1)
+    for i0 in range(0, mp.size, 512):
+        mm = mp[i0:i0 + 512, None]
+        pmf = np.exp(k[None, :] * np.log(mm) - mm - lg[None, :])
+        out_i = (pmf * klk[None, :]).sum(1) - mm[:, 0] * np.log(mm[:, 0])
+        idx = np.flatnonzero(pos)[i0:i0 + 512]
+        out[idx] = out_i
+    return out
+
+
+def eiid(bins: np.ndarray, npv: np.ndarray, lag: int = 1) -> np.ndarray:
+    """(n, n) [src, tgt] independence bias sum_{a,b} g(n_a q_b) - sum_{x,b} g(n_x q_b)
+    (NaN when either gene has more than 64 states; diagonal NaN)."""
+    n, T = bins.shape
+    N = T - lag
+    out = np.full((n, n), np.nan)
+    for t in range(n):
+        bt = int(npv[t])
+        if bt > 64:
+            continue
+        x0 = bins[t, :N].astype(np.int64)
+        x1 = bins[t, lag:lag + N].astype(np.int64)
+        na = np.bincount(x1 * bt + x0, minlength=bt * bt).astype(np.float64)
+        nx = np.bincount(x0, minlength=bt).astype(np.float64)
+        na, nx = na[na > 0], nx[nx > 0]
+        for s in range(n):
+            if s == t or int(npv[s]) > 64:
+                continue
+            q = np.bincount(bins[s, :N].astype(np.int64)) / N
+            q = q[q > 0]
+            out[s, t] = g_poisson(np.outer(na, q).ravel()).sum() - \
+                g_poisson(np.outer(nx, q).ravel()).sum()
+    return out
+
+
+def pair_features(gf6: np.ndarray, eiid_m: np.ndarray, tgt, src, block_length: int) -> np.ndarray:
+    """Raw (P, 16) pair features from the (n, 6) gene features and the E_iid matrix."""
+    tgt = np.asarray(tgt)
+    src = np.asarray(src)
+    a, b = gf6[tgt], gf6[src]
+    bt, bs = 2.0 ** a[:, 0], 2.0 ** b[:, 0]
+    e = eiid_m[src, tgt]
+    return np.concatenate([a, b, np.log2(np.maximum(e, 1e-6))[:, None],
+                           np.full((tgt.size, 1), np.log2(block_length)),
+                           np.log2((bt - 1) * (bs - 1) * bt + 1)[:, None],
+                           (a[:, 2] + b[:, 1])[:, None]], axis=1)

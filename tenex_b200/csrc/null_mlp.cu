@@ -10,8 +10,17 @@
 //   0-5  target: log2 b, H(x_t), H(x_{t+lag}, x_t), 2H - H2 (lag-1 information),
 //        log2 mean run length, 2^H / b
 //   6-11 source: the same six
-//   12 log2 N, 13 log2 block length, 14 log2 of (b_t - 1)(b_s - 1) b_t + 1,
-//   15 log2 of 2^{H2_t} * 2^{H_s}
+//   12 log2 of the pair's independence bias E_iid (below), 13 log2 block length,
+//   14 log2 of (b_t - 1)(b_s - 1) b_t + 1, 15 log2 of 2^{H2_t} * 2^{H_s}
+//
+// E_iid is the expected plug-in bias of N ln2 * TE when source and target are
+// independent and each joint cell count is Poisson with its independence mean:
+//   E_iid = sum_{a,b} g(n_a q_b) - sum_{x,b} g(n_x q_b),
+// n_a = count of target state a = (x_{t+lag}, x_t), n_x = count of x_t, q_b =
+// source marginal over the same N positions, g(m) = E[C ln C] - m ln m for
+// C ~ Poisson(m). (The m ln m parts cancel against the target's own entropy
+// terms, so E_iid is the whole expectation under that model.) It carries the
+// small-count behaviour of sparse tables that per-gene summaries miss.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -102,8 +111,118 @@ __global__ void gene_features_kernel(const uint8_t* __restrict__ bins, int64_t l
   }
 }
 
-__device__ __forceinline__ void pair_features(const float* __restrict__ gf, int tgt, int src,
-                                              float log2N, float log2bl, float* x) {
+// ---- E_iid: g table, source marginals, per-pair double sum ------------------
+constexpr int kGTable = 1024;
+constexpr float kGLo = -10.f, kGHi = 8.f;  // table covers m in [2^-10, 2^8]
+constexpr int kEiidMaxB = 64;
+
+// g(m) = E[C ln C] - m ln m, C ~ Poisson(m), on a log2 grid (float64 series).
+__global__ void g_table_kernel(float* __restrict__ table) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kGTable) return;
+  const double m = exp2((double)kGLo + (double)(kGHi - kGLo) * i / (kGTable - 1));
+  const int kmax = (int)(m + 14.0 * sqrt(m) + 60.0);
+  double p = exp(-m), acc = 0.0;
+  for (int k = 1; k <= kmax; ++k) {
+    p *= m / k;
+    acc += p * k * log((double)k);
+  }
+  table[i] = (float)(acc - m * log(m));
+}
+
+// g(m) from the table, with its two limits outside it: -m ln m + m^2 ln 2 for
+// small m, 1/2 + 1/(12m) + 1/(12m^2) for large m.
+__device__ __forceinline__ float g_poisson(float m, const float* __restrict__ tab) {
+  if (m <= 0.f) return 0.f;
+  if (m < 9.765625e-4f) return m * (0.69314718f * m - __logf(m));
+  if (m > 256.f) {
+    const float r = 1.f / m;
+    return 0.5f + r * (0.083333333f + 0.083333333f * r);
+  }
+  const float pos = (__log2f(m) - kGLo) * ((kGTable - 1) / (kGHi - kGLo));
+  const int i = max(0, min((int)pos, kGTable - 2));
+  const float f = pos - (float)i;
+  return fmaf(f, tab[i + 1] - tab[i], tab[i]);
+}
+
+// q[g][b] = count of y_s = b over s < N, / N (b < 64; genes with b > 64 unused).
+__global__ void source_marginal_kernel(const uint8_t* __restrict__ bins, int64_t ld, int N,
+                                       float* __restrict__ q) {
+  __shared__ int h[256];
+  const int g = blockIdx.x;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const uint8_t* row = bins + (int64_t)g * ld;
+  for (int s = threadIdx.x; s < N; s += blockDim.x) atomicAdd(&h[row[s]], 1);
+  __syncthreads();
+  if (threadIdx.x < kEiidMaxB) q[(int64_t)g * kEiidMaxB + threadIdx.x] = (float)h[threadIdx.x] / N;
+}
+
+// One CTA per target: its non-zero n_a and n_x in shared memory, threads over
+// sources. out[src * n + tgt] = E_iid (NaN when b_t or b_s > 64).
+__global__ void __launch_bounds__(256) eiid_kernel(const uint8_t* __restrict__ bins, int64_t ld,
+                                                   const int32_t* __restrict__ npv, int n, int N,
+                                                   int lag, const float* __restrict__ q,
+                                                   const float* __restrict__ gtab,
+                                                   float* __restrict__ out) {
+  __shared__ int hz[kEiidMaxB * kEiidMaxB];
+  __shared__ int hx[kEiidMaxB];
+  __shared__ float la[kEiidMaxB * kEiidMaxB + kEiidMaxB];
+  __shared__ float tab[kGTable];
+  __shared__ int nz, nx;
+  const int t = blockIdx.x;
+  const int bt = npv[t];
+  const float nan = __int_as_float(0x7fc00000);
+  if (bt < 1 || bt > kEiidMaxB) {
+    for (int s = threadIdx.x; s < n; s += blockDim.x)
+      if (s != t) out[(int64_t)s * n + t] = nan;
+    return;
+  }
+  for (int i = threadIdx.x; i < bt * bt; i += blockDim.x) hz[i] = 0;
+  for (int i = threadIdx.x; i < kEiidMaxB; i += blockDim.x) hx[i] = 0;
+  for (int i = threadIdx.x; i < kGTable; i += blockDim.x) tab[i] = gtab[i];
+  if (threadIdx.x == 0) nz = nx = 0;
+  __syncthreads();
+  const uint8_t* row = bins + (int64_t)t * ld;
+  for (int s = threadIdx.x; s < N; s += blockDim.x) {
+    const int x0 = row[s], x1 = row[s + lag];
+    if (x0 < bt && x1 < bt) {
+      atomicAdd(&hz[x1 * bt + x0], 1);
+      atomicAdd(&hx[x0], 1);
+    }
+  }
+  __syncthreads();
+  // compact lists: the non-zero n_a, then the non-zero n_x after them
+  for (int i = threadIdx.x; i < bt * bt; i += blockDim.x)
+    if (hz[i]) la[atomicAdd(&nz, 1)] = (float)hz[i];
+  __syncthreads();
+  const int kz = nz;
+  for (int i = threadIdx.x; i < bt; i += blockDim.x)
+    if (hx[i]) la[kz + atomicAdd(&nx, 1)] = (float)hx[i];
+  __syncthreads();
+  const int kx = nx;
+  for (int s = threadIdx.x; s < n; s += blockDim.x) {
+    if (s == t) continue;
+    const int bs = npv[s];
+    float acc = nan;
+    if (bs >= 1 && bs <= kEiidMaxB) {
+      acc = 0.f;
+      const float* qs = q + (int64_t)s * kEiidMaxB;
+      for (int b = 0; b < bs; ++b) {
+        const float qb = qs[b];
+        if (qb <= 0.f) continue;
+        float part = 0.f;
+        for (int a = 0; a < kz; ++a) part += g_poisson(la[a] * qb, tab);
+        for (int a = 0; a < kx; ++a) part -= g_poisson(la[kz + a] * qb, tab);
+        acc += part;
+      }
+    }
+    out[(int64_t)s * n + t] = acc;
+  }
+}
+
+__device__ __forceinline__ void pair_features(const float* __restrict__ gf, float eiid, int tgt,
+                                              int src, float log2bl, float* x) {
   const float* t = gf + (int64_t)tgt * kGeneFeat;
   const float* s = gf + (int64_t)src * kGeneFeat;
 #pragma unroll
@@ -111,7 +230,7 @@ __device__ __forceinline__ void pair_features(const float* __restrict__ gf, int 
     x[k] = t[k];
     x[6 + k] = s[k];
   }
-  x[12] = log2N;
+  x[12] = eiid != eiid ? eiid : log2f(fmaxf(eiid, 1e-6f));
   x[13] = log2bl;
   const float bt = exp2f(t[0]), bs = exp2f(s[0]);
   x[14] = log2f((bt - 1.f) * (bs - 1.f) * bt + 1.f);
@@ -152,7 +271,7 @@ __device__ __forceinline__ void load_weights(const __nv_bfloat16* __restrict__ w
 // untouched), features standardised by (fmean, fstd); NaN features give NaN
 // outputs (the caller sends those pairs to the full surrogate test).
 __global__ void __launch_bounds__(128) null_predict_kernel(
-    const float* __restrict__ gf, int n, float log2N, float log2bl,
+    const float* __restrict__ gf, const float* __restrict__ eiid, int n, float log2bl,
     const __nv_bfloat16* __restrict__ wb, const float* __restrict__ fmean,
     const float* __restrict__ fstd, float* __restrict__ out0, float* __restrict__ out1) {
   __shared__ float w[kParams];
@@ -169,7 +288,7 @@ __global__ void __launch_bounds__(128) null_predict_kernel(
     const int src = (int)(m / n), tgt = (int)(m - (int64_t)src * n);
     if (src == tgt) continue;
     float x[kIn];
-    pair_features(gf, tgt, src, log2N, log2bl, x);
+    pair_features(gf, eiid[m], tgt, src, log2bl, x);
 #pragma unroll
     for (int f = 0; f < kIn; ++f) x[f] = (x[f] - mu[f]) / sd[f];
     float o0, o1;
@@ -180,13 +299,15 @@ __global__ void __launch_bounds__(128) null_predict_kernel(
 }
 
 // Raw (unstandardised) features of a pair list.
-__global__ void pair_features_kernel(const float* __restrict__ gf, const int32_t* __restrict__ tgt,
-                                     const int32_t* __restrict__ src, int64_t P, float log2N,
-                                     float log2bl, float* __restrict__ X) {
+__global__ void pair_features_kernel(const float* __restrict__ gf, const float* __restrict__ eiid,
+                                     int n, const int32_t* __restrict__ tgt,
+                                     const int32_t* __restrict__ src, int64_t P, float log2bl,
+                                     float* __restrict__ X) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < P;
        p += (int64_t)gridDim.x * blockDim.x) {
     float x[kIn];
-    pair_features(gf, tgt[p], src[p], log2N, log2bl, x);
+    const int t = tgt[p], s = src[p];
+    pair_features(gf, eiid[(int64_t)s * n + t], t, s, log2bl, x);
 #pragma unroll
     for (int f = 0; f < kIn; ++f) X[p * kIn + f] = x[f];
   }
@@ -322,29 +443,54 @@ extern "C" int tenex_gene_features(const uint8_t* bins, int64_t ld, const int32_
   return check_launch("gene_features_kernel");
 }
 
-extern "C" int tenex_pair_features(const float* gene_feat, const int32_t* tgt, const int32_t* src,
-                                   int64_t n_pairs, float log2N, float log2bl, float* X,
-                                   void* stream) {
-  if (!gene_feat || !tgt || !src || !X) return fail(TENEX_ERR_BADARG, "null pointer");
+extern "C" size_t tenex_eiid_workspace_bytes(int n_vars) {
+  return n_vars < 1 ? 0 : (size_t)n_vars * kEiidMaxB * sizeof(float) + kGTable * sizeof(float);
+}
+
+extern "C" int tenex_eiid_matrix(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
+                                 int n_vars, int64_t row_len, int64_t lag, float* eiid,
+                                 void* workspace, size_t workspace_bytes, void* stream) {
+  if (!bins || !n_per_var || !eiid || !workspace) return fail(TENEX_ERR_BADARG, "null pointer");
+  if (n_vars < 2 || lag < 1 || row_len <= lag) return fail(TENEX_ERR_BADARG, "bad shape");
+  if (row_len - lag >= ((int64_t)1 << 31)) return fail(TENEX_ERR_UNSUPPORTED, "N >= 2^31");
+  if (workspace_bytes < tenex_eiid_workspace_bytes(n_vars))
+    return fail(TENEX_ERR_BADARG, "workspace of %zu bytes < %zu", workspace_bytes,
+                tenex_eiid_workspace_bytes(n_vars));
+  if (reinterpret_cast<uintptr_t>(workspace) % 16)
+    return fail(TENEX_ERR_BADARG, "workspace must be 16-byte aligned");
+  cudaStream_t s = as_stream(stream);
+  float* q = static_cast<float*>(workspace);
+  float* tab = q + (size_t)n_vars * kEiidMaxB;
+  const int N = (int)(row_len - lag);
+  g_table_kernel<<<kGTable / 256, 256, 0, s>>>(tab);
+  source_marginal_kernel<<<n_vars, 256, 0, s>>>(bins, ld, N, q);
+  eiid_kernel<<<n_vars, 256, 0, s>>>(bins, ld, n_per_var, n_vars, N, (int)lag, q, tab, eiid);
+  return check_launch("eiid kernels");
+}
+
+extern "C" int tenex_pair_features(const float* gene_feat, const float* eiid, int n_vars,
+                                   const int32_t* tgt, const int32_t* src, int64_t n_pairs,
+                                   float log2bl, float* X, void* stream) {
+  if (!gene_feat || !eiid || !tgt || !src || !X) return fail(TENEX_ERR_BADARG, "null pointer");
   if (n_pairs <= 0) return TENEX_OK;
   const int blocks = (int)std::min<int64_t>((n_pairs + 255) / 256, 8192);
-  pair_features_kernel<<<blocks, 256, 0, as_stream(stream)>>>(gene_feat, tgt, src, n_pairs, log2N,
-                                                              log2bl, X);
+  pair_features_kernel<<<blocks, 256, 0, as_stream(stream)>>>(gene_feat, eiid, n_vars, tgt, src,
+                                                              n_pairs, log2bl, X);
   return check_launch("pair_features_kernel");
 }
 
-extern "C" int tenex_null_predict(const float* gene_feat, int n_vars, float log2N, float log2bl,
-                                  const void* weights_bf16, const float* feat_mean,
+extern "C" int tenex_null_predict(const float* gene_feat, const float* eiid, int n_vars,
+                                  float log2bl, const void* weights_bf16, const float* feat_mean,
                                   const float* feat_std, float* out_mu, float* out_sigma,
                                   void* stream) {
-  if (!gene_feat || !weights_bf16 || !feat_mean || !feat_std || !out_mu || !out_sigma)
+  if (!gene_feat || !eiid || !weights_bf16 || !feat_mean || !feat_std || !out_mu || !out_sigma)
     return fail(TENEX_ERR_BADARG, "null pointer");
   if (n_vars < 2) return fail(TENEX_ERR_BADARG, "n_vars must be >= 2");
   DevAttr A;
   int st = current_device_attr(&A);
   if (st) return st;
   null_predict_kernel<<<A.sm_count * 8, 128, 0, as_stream(stream)>>>(
-      gene_feat, n_vars, log2N, log2bl, static_cast<const __nv_bfloat16*>(weights_bf16),
+      gene_feat, eiid, n_vars, log2bl, static_cast<const __nv_bfloat16*>(weights_bf16),
       feat_mean, feat_std, out_mu, out_sigma);
   return check_launch("null_predict_kernel");
 }

@@ -6,7 +6,10 @@ cheap per-gene statistics (bin counts, marginal and lag-1 joint entropies,
 autocorrelation, run lengths) and on N and the block length, not on the
 pair's coupling. A small MLP (16 -> 64 -> 64 -> 2, GELU, BF16 weights, FP32
 accumulation; kernels in null_mlp.cu) predicts log(mu*N) and log(sigma*N) of
-the null from those features.
+the null from those features and one pair-level statistic, E_iid: the
+expected plug-in bias of N ln2 * TE under independence with Poisson cell
+counts, sum_{a,b} g(n_a q_b) - sum_{x,b} g(n_x q_b), g(m) = E[C ln C] - m ln m
+(the small-count behaviour of sparse tables; tenex_eiid_matrix).
 
 Training: synthetic datasets from generator seeds disjoint from evaluation
 (2000-2019 by default); each is run through the full surrogate test (S
@@ -100,12 +103,25 @@ def gene_features(db: D.DeviceBins, npv: torch.Tensor, tau: int) -> torch.Tensor
     return feat
 
 
-def pair_features(gf: torch.Tensor, tgt: torch.Tensor, src: torch.Tensor, N: int,
+def eiid_matrix(db: D.DeviceBins, npv: torch.Tensor, tau: int) -> torch.Tensor:
+    """(n, n) float32 [src, tgt] independence bias E_iid of every ordered pair."""
+    dev = db.data.device
+    out = torch.empty((db.n, db.n), dtype=torch.float32, device=dev)
+    ws = torch.empty(int(native.lib().tenex_eiid_workspace_bytes(db.n)), dtype=torch.uint8,
+                     device=dev)
+    native.call("tenex_eiid_matrix", db.data.data_ptr(), db.ld, npv.data_ptr(), db.n,
+                db.row_len, tau * db.K, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                native.stream_ptr())
+    return out
+
+
+def pair_features(gf: torch.Tensor, eiid: torch.Tensor, tgt: torch.Tensor, src: torch.Tensor,
                   block_length: int) -> torch.Tensor:
+    """Raw (n_pairs, 16) features of the [tgt, src] pairs."""
     P = int(tgt.numel())
     X = torch.empty((P, N_IN), dtype=torch.float32, device=gf.device)
-    native.call("tenex_pair_features", gf.data_ptr(), tgt.data_ptr(), src.data_ptr(), P,
-                float(np.log2(N)), float(np.log2(block_length)), X.data_ptr(),
+    native.call("tenex_pair_features", gf.data_ptr(), eiid.data_ptr(), int(eiid.shape[0]),
+                tgt.data_ptr(), src.data_ptr(), P, float(np.log2(block_length)), X.data_ptr(),
                 native.stream_ptr())
     return X
 
@@ -119,10 +135,11 @@ def predict(model: NullModel, db: D.DeviceBins, npv: torch.Tensor, tau: int, blo
     N = (db.T - tau) * db.K
     if gf is None:
         gf = gene_features(db, npv, tau)
+    eiid = eiid_matrix(db, npv, tau)
     wb, fm, fs = model.device_weights(dev)
     lmu = torch.full((n, n), float("nan"), dtype=torch.float32, device=dev)
     lsg = torch.full((n, n), float("nan"), dtype=torch.float32, device=dev)
-    native.call("tenex_null_predict", gf.data_ptr(), n, float(np.log2(N)),
+    native.call("tenex_null_predict", gf.data_ptr(), eiid.data_ptr(), n,
                 float(np.log2(block_length)), wb.data_ptr(), fm.data_ptr(), fs.data_ptr(),
                 lmu.data_ptr(), lsg.data_ptr(), native.stream_ptr())
     mu = torch.exp(lmu) / N
@@ -169,12 +186,13 @@ def training_set(seeds, n: int, T: int, S: int, block_length: int, pairs_per_dat
         b_max = int(npv.max())
         mean, std = surrogate_moments(db, npv_t, b_max, tau, S, block_length, 10_000 + int(sd))
         gf = gene_features(db, npv_t, tau)
+        eiid = eiid_matrix(db, npv_t, tau)
         t = rng.integers(0, n, pairs_per_dataset)
         s = rng.integers(0, n - 1, pairs_per_dataset)
         s = s + (s >= t)
         tt = torch.as_tensor(t, dtype=torch.int32, device=dev)
         ss = torch.as_tensor(s, dtype=torch.int32, device=dev)
-        X = pair_features(gf, tt, ss, N, block_length)
+        X = pair_features(gf, eiid, tt, ss, block_length)
         mu = mean[ss.long(), tt.long()]
         sg = std[ss.long(), tt.long()]
         ok = torch.isfinite(X).all(dim=1) & (mu > 0) & (sg > 0)
@@ -252,9 +270,87 @@ def evaluate(model: NullModel, Xraw: torch.Tensor, Y: torch.Tensor) -> list[floa
     return [float((dout[:, 0] ** 2).mean()), float((dout[:, 1] ** 2).mean())]
 
 
+BANDS = tuple(np.round(np.arange(0.25, 4.01, 0.25), 2))
+
+
+def analytic_null(db: D.DeviceBins, npv: torch.Tensor, tau: int):
+    """The null without the network: the plug-in bias read as a scaled chi-square,
+    2 N ln2 * TE ~ chi2(df) with df = 2 E_iid, so mu = E_iid / (N ln2) and
+    sigma = sqrt(E_iid) / (N ln2). Same return form as predict()."""
+    N = (db.T - tau) * db.K
+    e = eiid_matrix(db, npv, tau)
+    c = 1.0 / (N * np.log(2.0))
+    mu = e * c
+    sigma = torch.sqrt(torch.clamp(e, min=0.0)) * c
+    ok = npv <= 64
+    return mu, sigma, ok
+
+
+def screen_recall(model, x: np.ndarray, npv: np.ndarray, dev, S: int, block_length: int,
+                  seed: int, fdr: float = 0.05, tau: int = 1) -> dict:
+    """On one dataset: the full S-shuffle test's BH-FDR edge set (parametric p) and,
+    for each band in BANDS, the fraction of those edges the screen (predicted z >=
+    z_FDR(predicted) - band) sends to verification, and the fraction of all pairs
+    it sends. model is a NullModel, or "analytic" for analytic_null."""
+    from tenex_b200.inference.grn import bh_fdr_gpu
+    from tenex_b200.kernels.full_smem import FullSMEMKernel
+    db = D.pack_bins(x, dev)
+    npv_t = torch.as_tensor(npv, dtype=torch.int32, device=dev)
+    b_max = int(npv.max())
+    obs = FullSMEMKernel().compute_pairfree_device(db, npv_t, b_max, tau, matrix=True)
+    from tenex_b200.inference.surrogate_test import (SurrogateAccumulator, build_block_perm,
+                                                     run_surrogates)
+    acc = SurrogateAccumulator(db, npv_t, b_max, tau, obs, b_max == 2)
+    perms, bl, _ = build_block_perm(db.n, db.T, "block", block_length, 0, S, seed, dev)
+    run_surrogates(acc, perms, bl, use_graph=True)
+    mean = (acc.sum / S).float()
+    std = torch.sqrt(torch.clamp(acc.sumsq / S - (acc.sum / S) ** 2, min=0.0)).float()
+    off = ~torch.eye(db.n, dtype=torch.bool, device=dev)
+    z_full = (obs - mean) / torch.clamp(std, min=1e-12)
+    p_full = 0.5 * torch.special.erfc(z_full.double() / np.sqrt(2.0))
+    sig = torch.zeros_like(off)
+    sig[off] = bh_fdr_gpu(p_full[off], fdr) < fdr
+    sig &= (obs - mean) > 0
+    if isinstance(model, str) and model == "analytic":
+        mu, sg, ok = analytic_null(db, npv_t, tau)
+    else:
+        mu, sg, ok = predict(model, db, npv_t, tau, block_length)
+    z_pred = (obs - mu) / torch.clamp(sg, min=1e-12)
+    valid = torch.isfinite(z_pred) & ok[None, :] & ok[:, None]
+    p_pred = torch.where(valid, 0.5 * torch.special.erfc(z_pred.double() / np.sqrt(2.0)),
+                         torch.ones_like(p_full))
+    z_cut = z_of_p(bh_cut(p_pred[off], fdr), int(off.sum()), fdr)
+    n_edges = int(sig.sum())
+    out = {"n_edges": n_edges, "z_cut_pred": z_cut, "recall": {}, "verified": {}}
+    for band in BANDS:
+        screen = off & (~valid | (z_pred >= z_cut - band))
+        out["recall"][band] = float((screen & sig).sum()) / max(n_edges, 1)
+        out["verified"][band] = float(screen.sum()) / float(off.sum())
+    return out
+
+
+def calibrate_band(model: NullModel, seeds, dev, n=2000, T=5000, S=100, block_length=50,
+                   target: float = 0.995) -> dict:
+    """Smallest band of BANDS whose screen keeps >= target of the full test's edges
+    on every held-out dataset (generator seeds `seeds`, permutation seeds 20000+)."""
+    from tenex_b200 import workloads as W
+    per = []
+    for sd in seeds:
+        x, npv, _ = W.cfg5_bins(n=n, T=T, seed=int(sd))
+        per.append(screen_recall(model, x, npv, dev, S, block_length, 20_000 + int(sd)))
+    band = next((b for b in BANDS if all(r["recall"][b] >= target for r in per)), BANDS[-1])
+    return {"band": float(band), "target_recall": target,
+            "recall": [r["recall"][band] for r in per],
+            "verified_fraction": [r["verified"][band] for r in per],
+            "n_edges": [r["n_edges"] for r in per]}
+
+
 def train_default(device="cuda", seeds=range(2000, 2018), val_seeds=(2018, 2019), n=2000,
                   T=5000, S=100, block_length=50, pairs_per_dataset=150_000, steps=4000,
                   out=DEFAULT_MODEL) -> dict:
+    """Trains on generator seeds `seeds`, reports the MSE on `val_seeds` and
+    calibrates the fallback band on them (all disjoint from the evaluation seeds
+    1000-1005)."""
     dev = torch.device(device)
     t0 = time.time()
     X, Y, G = training_set(list(seeds), n, T, S, block_length, pairs_per_dataset, dev)
@@ -266,7 +362,11 @@ def train_default(device="cuda", seeds=range(2000, 2018), val_seeds=(2018, 2019)
     model, rep = train(X, Y, torch.cat([G, Gv]), steps=steps, Xval=Xv, Yval=Yv, meta=meta)
     rep["data_seconds"] = t_data
     rep["train_pairs"] = int(X.shape[0])
-    model.meta["report"] = {k: rep[k] for k in ("val_mse", "train_pairs")}
+    model.save(out)
+    cal = calibrate_band(model, val_seeds, dev, n, T, S, block_length)
+    rep["calibration"] = cal
+    model.meta["band"] = cal["band"]
+    model.meta["report"] = {k: rep[k] for k in ("val_mse", "train_pairs", "calibration")}
     model.save(out)
     return rep
 

@@ -84,8 +84,10 @@ _SIGS = {
     "tenex_b2_status": [_P, _I, _L, _L, _P],
     "tenex_mlp_param_count": [],
     "tenex_gene_features": [_P, _L, _P, _I, _L, _L, _P, _P],
-    "tenex_pair_features": [_P, _P, _P, _L, ctypes.c_float, ctypes.c_float, _P, _P],
-    "tenex_null_predict": [_P, _I, ctypes.c_float, ctypes.c_float, _P, _P, _P, _P, _P, _P],
+    "tenex_eiid_workspace_bytes": [_I],
+    "tenex_eiid_matrix": [_P, _L, _P, _I, _L, _L, _P, _P, _S, _P],
+    "tenex_pair_features": [_P, _P, _I, _P, _P, _L, ctypes.c_float, _P, _P],
+    "tenex_null_predict": [_P, _P, _I, ctypes.c_float, _P, _P, _P, _P, _P, _P],
     "tenex_mlp_scratch_floats": [_I],
     "tenex_mlp_gradients": [_P, _P, _I, _P, _P, _P, _P, _P],
     "tenex_mlp_train_step": [_P, _P, _I, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float,
@@ -96,7 +98,8 @@ _SIGS = {
 }
 _RESTYPES = {"tenex_te_workspace_bytes": ctypes.c_size_t,
              "tenex_b2_workspace_bytes": ctypes.c_size_t,
-             "tenex_mlp_scratch_floats": ctypes.c_size_t}
+             "tenex_mlp_scratch_floats": ctypes.c_size_t,
+             "tenex_eiid_workspace_bytes": ctypes.c_size_t}
 
 _lib = None
 _lock = threading.Lock()

@@ -24,7 +24,10 @@ CONFIGS = {
 
 
 def _planted(rng, n: int, k: int) -> np.ndarray:
-    """k distinct (regulator, target) pairs with regulator != target."""
+    """k distinct (regulator, target) pairs with regulator != target and distinct
+    targets (so k <= n)."""
+    if k > n:
+        raise ValueError(f"{k} planted pairs need at least {k} genes (n={n})")
     out, seen = [], set()
     while len(out) < k:
         r, t = (int(v) for v in rng.integers(0, n, 2))

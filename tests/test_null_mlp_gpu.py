@@ -42,6 +42,23 @@ def test_mlp_gradients_match_float64_oracle(cuda):
     assert np.max(np.abs(g - g_ref)) <= 2e-4 * np.max(np.abs(g_ref)) + 1e-6
 
 
+def test_eiid_matches_float64_series(cuda):
+    # E_iid = sum g(n_a q_b) - sum g(n_x q_b); the kernel's g is a 1024-point table
+    # with its two analytic limits, the oracle sums the Poisson series directly.
+    x, npv, _ = W.cfg5_bins(n=30, T=800, seed=9)
+    npv = npv.copy()
+    x[3] = (np.arange(800) * 7 % 70).astype(np.uint8)   # one gene with 70 states: NaN row/col
+    npv[3] = 70
+    db = D.pack_bins(x, cuda)
+    got = LN.eiid_matrix(db, torch.as_tensor(npv, dtype=torch.int32, device=cuda), 1).cpu().numpy()
+    ref = M.eiid(x, npv, 1)
+    off = ~np.eye(30, dtype=bool)
+    assert np.array_equal(np.isnan(got[off]), np.isnan(ref[off]))
+    ok = off & ~np.isnan(ref)
+    assert np.isnan(got[3, 5]) and np.isnan(got[5, 3])
+    assert np.allclose(got[ok], ref[ok], rtol=2e-4, atol=1e-3)
+
+
 def test_null_predict_matches_float64_forward(cuda):
     x, npv, _ = W.cfg5_bins(n=30, T=800, seed=9)
     db = D.pack_bins(x, cuda)
@@ -56,9 +73,13 @@ def test_null_predict_matches_float64_forward(cuda):
     t, s = np.meshgrid(np.arange(30), np.arange(30), indexing="ij")
     m = t != s
     tt, ss = t[m], s[m]
-    Xr = LN.pair_features(LN.gene_features(db, npv_t, 1),
-                          torch.as_tensor(tt, dtype=torch.int32, device=cuda),
-                          torch.as_tensor(ss, dtype=torch.int32, device=cuda), 799, 50).cpu().numpy()
+    gf = LN.gene_features(db, npv_t, 1)
+    eiid = LN.eiid_matrix(db, npv_t, 1)
+    Xr = LN.pair_features(gf, eiid, torch.as_tensor(tt, dtype=torch.int32, device=cuda),
+                          torch.as_tensor(ss, dtype=torch.int32, device=cuda), 50).cpu().numpy()
+    # the kernel's features equal the oracle's restatement on the kernel's inputs
+    Xo = M.pair_features(gf.cpu().numpy()[:, :6], eiid.cpu().numpy(), tt, ss, 50)
+    assert np.allclose(Xr, Xo, rtol=1e-5, atol=1e-5)
     out = M.forward(M.bf16_round(model.params), Xr.astype(np.float64) / 4.0)
     N = 799
     ref_mu = np.exp(out[:, 0]) / N
