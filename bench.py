@@ -14,7 +14,9 @@ the B200 shared-memory limit (38, the reference rule) and the full TE matrix
 Profiling options (not the headline run): --genes / --cells shrink the
 workload, --pairs times only the first pair ids, --launch T,C,W fixes the
 launch shape (threads, CTAs per SM, sources per work item) instead of running
-the autotuner, --no-e2e and --no-cpu-baseline skip those legs.
+the autotuner, --no-e2e, --no-cpu-baseline and --no-surrogate skip those legs.
+The line's "surrogate" object times NetWeaver's surrogate test on cfg5 (full
+100-shuffle test against the learned null, wall seconds, edge agreement).
 
 N > 1 (torchrun, one process per GPU): the pair-id range is split into
 contiguous chunks of ceil(pairs / N), the reference's split (no data-path
@@ -305,6 +307,7 @@ def run_ours(args) -> None:
                     "note": "compulsory bytes (bins read once + float32 outputs) / launch time; "
                             "peak = MEASURED_PEAKS.json hbm_gbs (of measured)"}
     cpu = cpu_baseline(*_coarsened_host(x, npv, limit)) if not args.no_cpu_baseline else None
+    sur = surrogate_leg(dev) if (world == 1 and not args.no_surrogate) else None
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
@@ -318,10 +321,57 @@ def run_ours(args) -> None:
                        "launch": kern.cfg},
             "gpu_launches": 6 * args.steps,  # remap, coarsen x2, prepass, order, TE tile
             "roofline": roofline, "roofline_hbm": roofline_hbm,
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary()}
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "surrogate": sur}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def surrogate_leg(dev, reps: int = 2) -> dict:
+    """Wall seconds of NetWeaver's surrogate test on cfg5 (2,000 genes x 5,000 cells,
+    100 block shuffles of length 50, seed 42, BH-FDR 0.05, parametric p): the full
+    test against the learned null, each after one warm-up call, with the edge-set
+    agreement of the two."""
+    import torch
+
+    from tenex_b200 import workloads as W
+    from tenex_b200.inference.surrogate_test import SurrogateTestMethod
+    from tenex_b200.kernels import device as D
+    from tenex_b200.kernels.full_smem import FullSMEMKernel
+    x, npv, _ = W.cfg5_bins(seed=1005)
+    n = x.shape[0]
+    names = np.array([f"g{i}" for i in range(n)])
+    db = D.pack_bins(x, dev)
+    obs = FullSMEMKernel().compute_pairfree_device(
+        db, torch.as_tensor(npv, device=dev), int(npv.max()), 1, matrix=True).cpu().numpy()
+    kw = dict(bin_data=x, n_per_var=npv, b_max=int(npv.max()), kernel="Full-SMEM", tau=1,
+              n_surrogates=100, block_length=50, fdr=0.05, seed=42)
+    m = SurrogateTestMethod()
+
+    def timed(**extra):
+        ts, res = [], None
+        for _ in range(reps + 1):                      # first call is the warm-up
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            res = m.infer(obs, names, dev, **kw, **extra)
+            torch.cuda.synchronize(dev)
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts[1:]), res
+
+    t_full, full = timed()
+    t_lrn, lrn = timed(null="learned")
+    e1 = set(map(tuple, full.grn.pairs.tolist()))
+    e2 = set(map(tuple, lrn.grn.pairs.tolist()))
+    inter = len(e1 & e2)
+    return {"workload": "cfg5: 2000 genes x 5000 cells, b~U{2..16} Markov, 100 block shuffles "
+                        "(block length 50, seed 42), BH-FDR 0.05, parametric p",
+            "metric": "surrogate_test wall seconds (median of %d after a warm-up call)" % reps,
+            "full_s": t_full, "learned_s": t_lrn, "speedup": t_full / t_lrn,
+            "n_edges_full": len(e1), "n_edges_learned": len(e2),
+            "jaccard": inter / max(1, len(e1 | e2)), "precision": inter / max(1, len(e2)),
+            "recall": inter / max(1, len(e1)),
+            "verified_fraction": lrn.info.get("fallback_fraction"),
+            "band": lrn.info.get("band")}
 
 
 def _coarsened_host(x, npv, limit):
@@ -339,6 +389,7 @@ def main():
     ap.add_argument("--ref-pairs", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--genes", type=int, default=N_GENES)
     ap.add_argument("--cells", type=int, default=N_CELLS)
     ap.add_argument("--pairs", type=int, default=None)

@@ -110,9 +110,9 @@ int tenex_te_pairfree_counts(const uint8_t* bins, int64_t ld, const int32_t* n_p
 
 /* Same computation as tenex_te_pairfree, for callers that cannot allocate
  * device memory. (No counterpart in the reference.) Its scratch is a fixed
- * 4 MiB area inside the library's device image, so n_vars * (b_max + 2) * 4
- * plus about 1 KB must fit in 4 MiB (TENEX_ERR_UNSUPPORTED otherwise;
- * e.g. 10,000 genes up to b_max = 102). The area's address is looked up by the
+ * 4 MiB area inside the library's device image, so n_vars * 4 plus about
+ * 512 bytes must fit in 4 MiB (TENEX_ERR_UNSUPPORTED otherwise; up to about
+ * 1,048,000 genes). The area's address is looked up by the
  * first call on each device (make that call before any stream capture); every
  * call reuses and re-initialises the same area, so calls that overlap on the
  * GPU race and must not be issued. status: optional device int32 that receives

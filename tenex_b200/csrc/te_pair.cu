@@ -16,17 +16,14 @@
 //     for the item (b_t^2 * b_s cells); a slot belongs to a group of G warps
 //     (G = 1: warp-private histograms for the common small pairs). Counters are
 //     32-bit when the slots fit, else 16-bit halves of a word (N < 65536).
-//   * Shared-memory atomics serialise on bank conflicts and on lanes hitting
-//     the same word, and the hottest words are the cells of the most frequent
-//     values. The kernel therefore never counts a sample whose target state is
-//     the target's most frequent state z_dom or whose source bin is the
-//     source's most frequent value y_dom. Those cells are exact by subtraction:
-//       c3[z, y_dom]    = c2a[z] - sum_{y != y_dom} c3[z, y]        (z != z_dom)
-//       c3[z_dom, y]    = m_src[y] - sum_{z != z_dom} c3[z, y]      (all y)
-//     where m_src is the source's marginal over [0, N) (a per-gene pre-pass).
-//     On skewed bins this halves the wavefronts per atomic.
+//   * Every sample is one predicated-free red.shared.add (16 samples per
+//     uint4 of source bins). Skipping the most frequent cells and deriving them
+//     by subtraction (fewer same-word collisions) was measured slower on every
+//     workload, binary ones included: the derivation passes cost more than the
+//     collisions they avoid.
 //   * The entropy pass reads each slot column once to form c2b, once more to
-//     form the terms, and clears the slot for the next source.
+//     form the terms (ratio c3 * (1/c2b) * (c1/c2a), lg2.approx; exact 0 where
+//     c3*c1 == c2a*c2b), and clears the slot for the next source.
 //   * Items are handed out by an atomic ticket in chunk-major order, so the
 //     CTAs resident at one moment share a small set of source rows in L2.
 #include <cuda_runtime.h>
@@ -67,8 +64,6 @@ struct TeParams {
   int32_t* cnt_ge;
   int32_t* counts_dbg;
   int64_t counts_stride;
-  const int32_t* marg;  // (n, bmax) per-gene marginal over [0, N)
-  const int32_t* ydom;  // (n,) most frequent bin of each gene over [0, N)
   const int32_t* order; // (n,) genes stably sorted by bin-count class (pair-free mode)
   // pair-list mode (pairs != nullptr): item q is pairs[item_start[q] .. item_start[q+1])
   // of one target; output index = position in the list
@@ -77,14 +72,12 @@ struct TeParams {
   WsHeader* ws;
 };
 
-// Workspace: header | marg (n*bmax int32) | ydom (n int32) | order (n int32),
-// 256-byte aligned.
-__host__ __device__ inline int64_t ws_marg_off() { return (int64_t)sizeof(WsHeader); }
-__host__ __device__ inline int64_t ws_ydom_off(int n, int bmax) {
-  return round_up(ws_marg_off() + (int64_t)n * bmax * 4, 256);
-}
+// Workspace: header | order (n int32), 256-byte aligned (bmax kept in the
+// signature for callers; the layout no longer depends on it).
 __host__ __device__ inline int64_t ws_order_off(int n, int bmax) {
-  return round_up(ws_ydom_off(n, bmax) + (int64_t)n * 4, 256);
+  (void)n;
+  (void)bmax;
+  return round_up((int64_t)sizeof(WsHeader), 256);
 }
 __host__ __device__ inline int64_t ws_total(int n, int bmax) {
   return round_up(ws_order_off(n, bmax) + (int64_t)n * 4, 256);
@@ -104,7 +97,7 @@ namespace {
 constexpr int kMaxWarps = 32;
 
 struct SmemLayout {
-  int z_off, c2a_off, c1_off, red_off, misc_off, slot_off;
+  int z_off, c2a_off, c1_off, q_off, red_off, misc_off, slot_off;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(int N, int zbytes, int bmax) {
@@ -114,6 +107,7 @@ __host__ __device__ inline SmemLayout smem_layout(int N, int zbytes, int bmax) {
   L.red_off = off;   off += kMaxWarps * 8;                    // double red[32]
   L.c1_off = off;    off += (int)round_up((int64_t)bmax * 4, 16);
   L.c2a_off = off;   off += (int)round_up((int64_t)bmax * bmax * 4, 16);
+  L.q_off = off;     off += (int)round_up((int64_t)bmax * bmax * 8, 16);  // {c1/c2a, c2a}
   L.z_off = off;     off += (int)round_up((int64_t)N * zbytes, 16);
   L.slot_off = (int)round_up(off, 128);
   return L;
@@ -131,23 +125,12 @@ __device__ __forceinline__ uint32_t cell_get(const uint32_t* slot, uint32_t z, u
   return slot[z * bs + y];
 }
 
-template <bool PACK16>
-__device__ __forceinline__ void cell_add(uint32_t* slot, uint32_t z, uint32_t y, uint32_t bs,
-                                         uint32_t hb, uint32_t v) {
-  if (PACK16) {
-    atomicAdd(slot + (z * hb + (y >> 1)), v << ((y & 1u) << 4));
-  } else {
-    atomicAdd(slot + (z * bs + y), v);
-  }
-}
-
-// Counts one sample unless it belongs to the derived row (z_dom) or column
-// (y_dom). The skip is a predicate on a single red.shared instruction (inline
-// PTX) so the compiler cannot turn the 16 unrolled updates into branches.
-// slot32 is the slot's 32-bit shared-window address.
+// Counts one sample: one red.shared.add per sample (inline PTX, no return value);
+// PACK16 adds 1 or 1 << 16 to the word holding the cell's 16-bit half. slot32 is
+// the slot's 32-bit shared-window address.
 template <bool PACK16>
 __device__ __forceinline__ void hist_add(uint32_t slot32, uint32_t z, uint32_t y, uint32_t bs,
-                                         uint32_t hb, uint32_t zdom, uint32_t yd) {
+                                         uint32_t hb) {
   uint32_t addr, inc;
   if (PACK16) {
     addr = slot32 + ((z * hb + (y >> 1)) << 2);
@@ -156,18 +139,12 @@ __device__ __forceinline__ void hist_add(uint32_t slot32, uint32_t z, uint32_t y
     addr = slot32 + ((z * bs + y) << 2);
     inc = 1u;
   }
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.u32 p, %2, %3;\n\t"
-      "setp.ne.and.u32 p, %4, %5, p;\n\t"
-      "@p red.shared.add.u32 [%0], %1;\n\t}"
-      ::"r"(addr), "r"(inc), "r"(z), "r"(zdom), "r"(y), "r"(yd)
-      : "memory");
+  asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(inc) : "memory");
 }
 
 template <bool PACK16>
 __device__ __forceinline__ void hist16_z8(uint32_t slot, uint4 yv, uint4 zv, uint32_t bs,
-                                          uint32_t hb, uint32_t zdom, uint32_t yd) {
+                                          uint32_t hb) {
   const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
   const uint32_t zs[4] = {zv.x, zv.y, zv.z, zv.w};
 #pragma unroll
@@ -176,15 +153,14 @@ __device__ __forceinline__ void hist16_z8(uint32_t slot, uint4 yv, uint4 zv, uin
     for (int b = 0; b < 4; ++b) {
       const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
       const uint32_t z = __byte_perm(zs[w], 0, 0x4440 + b);
-      hist_add<PACK16>(slot, z, y, bs, hb, zdom, yd);
+      hist_add<PACK16>(slot, z, y, bs, hb);
     }
   }
 }
 
 template <bool PACK16>
 __device__ __forceinline__ void hist16_z16(uint32_t slot, uint4 yv, uint4 za, uint4 zb,
-                                           uint32_t bs, uint32_t hb, uint32_t zdom,
-                                           uint32_t yd) {
+                                           uint32_t bs, uint32_t hb) {
   const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
   const uint32_t zs[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
 #pragma unroll
@@ -194,15 +170,48 @@ __device__ __forceinline__ void hist16_z16(uint32_t slot, uint4 yv, uint4 za, ui
       const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
       const uint32_t zw = zs[(w * 4 + b) >> 1];
       const uint32_t z = (b & 1) ? (zw >> 16) : (zw & 0xffffu);
-      hist_add<PACK16>(slot, z, y, bs, hb, zdom, yd);
+      hist_add<PACK16>(slot, z, y, bs, hb);
     }
   }
 }
 
-__device__ __forceinline__ float te_term(float c3, float c1, float c2a, float c2b) {
-  // The reference's per-cell term (full_smem.cu:124-127),
-  // c3 * log2((c3*c1) / (c2a*c2b)), with IEEE division and an accurate log2.
-  return c3 * log2f(__fdiv_rn(c3 * c1, c2a * c2b));
+// Histogram of one source against the staged target (all group lanes).
+template <bool PACK16>
+__device__ __forceinline__ void hist_source(uint32_t slot32, const unsigned char* zsm, bool z8,
+                                            const uint8_t* srow, int N, int lane_g,
+                                            int gthreads, uint32_t bs, uint32_t hb) {
+  const int nvec = N >> 4;
+  const uint4* yv = reinterpret_cast<const uint4*>(srow);
+  const uint4* zv = reinterpret_cast<const uint4*>(zsm);
+  int v = lane_g;
+  if (z8) {
+    if (v < nvec) {
+      uint4 ycur = dev::ldg_nc_v4(yv + v);
+      for (; v < nvec; v += gthreads) {
+        const int vn = v + gthreads;
+        uint4 ynext = ycur;
+        if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
+        hist16_z8<PACK16>(slot32, ycur, zv[v], bs, hb);
+        ycur = ynext;
+      }
+    }
+    for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
+      hist_add<PACK16>(slot32, zsm[s], srow[s], bs, hb);
+  } else {
+    const uint16_t* z16 = reinterpret_cast<const uint16_t*>(zsm);
+    if (v < nvec) {
+      uint4 ycur = dev::ldg_nc_v4(yv + v);
+      for (; v < nvec; v += gthreads) {
+        const int vn = v + gthreads;
+        uint4 ynext = ycur;
+        if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
+        hist16_z16<PACK16>(slot32, ycur, zv[2 * v], zv[2 * v + 1], bs, hb);
+        ycur = ynext;
+      }
+    }
+    for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
+      hist_add<PACK16>(slot32, z16[s], srow[s], bs, hb);
+  }
 }
 
 __device__ __forceinline__ void group_sync(int G, int g, int gthreads) {
@@ -215,12 +224,10 @@ template <bool PACK16>
 __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, int G, int g,
                                             int n_groups, int lane_g, int tid, int warp,
                                             int tgt, int64_t lo, int64_t base, int n_src,
-                                            int bt, uint32_t zdom, const unsigned char* zsm,
-                                            bool z8, const float* c1s, const float* c2as,
-                                            double* red) {
+                                            int bt, const unsigned char* zsm, bool z8,
+                                            const float* c1s, const float2* qa, double* red) {
   const int gthreads = G * 32;
   const int N = P.N;
-  const int nvec = N >> 4;
   const int bt2 = bt * bt;
   for (int r = g; r < n_src; r += n_groups) {
     int64_t p;
@@ -235,84 +242,14 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
     }
     const uint32_t bs = (uint32_t)P.npv[src];
     const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
-    const uint32_t yd = (uint32_t)P.ydom[src];
     const uint8_t* srow = P.bins + (int64_t)src * P.ld;
-    const uint4* yv = reinterpret_cast<const uint4*>(srow);
     const uint32_t slot32 = (uint32_t)__cvta_generic_to_shared(slot);
     PHASE_MARK(t0);
 
-    // -- histogram of the counted cells ------------------------------------
-    if (z8) {
-      const uint4* zv = reinterpret_cast<const uint4*>(zsm);
-      int v = lane_g;
-      if (v < nvec) {
-        uint4 ycur = dev::ldg_nc_v4(yv + v);
-        for (; v < nvec; v += gthreads) {
-          const int vn = v + gthreads;
-          uint4 ynext = ycur;
-          if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
-          hist16_z8<PACK16>(slot32, ycur, zv[v], bs, hb, zdom, yd);
-          ycur = ynext;
-        }
-      }
-      for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
-        hist_add<PACK16>(slot32, zsm[s], srow[s], bs, hb, zdom, yd);
-    } else {
-      const uint4* zv = reinterpret_cast<const uint4*>(zsm);
-      const uint16_t* z16 = reinterpret_cast<const uint16_t*>(zsm);
-      int v = lane_g;
-      if (v < nvec) {
-        uint4 ycur = dev::ldg_nc_v4(yv + v);
-        for (; v < nvec; v += gthreads) {
-          const int vn = v + gthreads;
-          uint4 ynext = ycur;
-          if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
-          hist16_z16<PACK16>(slot32, ycur, zv[2 * v], zv[2 * v + 1], bs, hb, zdom, yd);
-          ycur = ynext;
-        }
-      }
-      for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
-        hist_add<PACK16>(slot32, z16[s], srow[s], bs, hb, zdom, yd);
-    }
+    // -- histogram of every sample -----------------------------------------
+    hist_source<PACK16>(slot32, zsm, z8, srow, N, lane_g, gthreads, bs, hb);
     group_sync(G, g, gthreads);
     PHASE_MARK(t1);
-
-    // -- derived cells: column y_dom from the row sums c2a, then row z_dom
-    //    from the source marginal ------------------------------------------
-    for (int z = lane_g; z < bt2; z += gthreads) {
-      if ((uint32_t)z == zdom) continue;
-      uint32_t rs = 0;
-      for (uint32_t y = 0; y < bs; ++y) rs += cell_get<PACK16>(slot, z, y, bs, hb);
-      cell_add<PACK16>(slot, z, yd, bs, hb, (uint32_t)c2as[z] - rs);
-    }
-    group_sync(G, g, gthreads);
-    // row z_dom: partial column sums over z != z_dom are accumulated into the
-    // (still empty) z_dom row by all lanes, then each word of the row is
-    // finalised by one lane as m_src[y] - sum.
-    const int32_t* msrc = P.marg + (int64_t)src * P.bmax;
-    const int nparts = max(1, gthreads / (int)bs);
-    for (int idx = lane_g; idx < (int)bs * nparts; idx += gthreads) {
-      const int part = idx / (int)bs;
-      const uint32_t y = (uint32_t)(idx - part * (int)bs);
-      uint32_t cs = 0;
-      for (int z = part; z < bt2; z += nparts)
-        if ((uint32_t)z != zdom) cs += cell_get<PACK16>(slot, z, y, bs, hb);
-      if (cs) cell_add<PACK16>(slot, zdom, y, bs, hb, cs);
-    }
-    group_sync(G, g, gthreads);
-    for (int w = lane_g; w < (int)hb; w += gthreads) {
-      uint32_t* wp = slot + zdom * hb + w;
-      if (PACK16) {
-        const uint32_t cur = *wp;
-        const uint32_t y0 = 2u * w, y1 = 2u * w + 1u;
-        const uint32_t lo = (uint32_t)msrc[y0] - (cur & 0xffffu);
-        const uint32_t hi = y1 < bs ? (uint32_t)msrc[y1] - (cur >> 16) : 0u;
-        *wp = lo | (hi << 16);
-      } else {
-        *wp = (uint32_t)msrc[w] - *wp;
-      }
-    }
-    group_sync(G, g, gthreads);
     PHASE_MARK(t2);
 
     // -- optional raw-count export (parity checks only) --------------------
@@ -327,6 +264,11 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
     }
 
     // -- entropy pass: column (xt=j, word wk) over xt1=i, clearing the slot --
+    // term = c3 * log2(c3 * c1 / (c2a * c2b)). The ratio is formed as
+    // c3 * (1/c2b) * (c1/c2a) (one reciprocal per column, c1/c2a staged per
+    // target) except where c3 * c1 == c2a * c2b, whose term is exactly 0 as in
+    // the reference's formula (constant or duplicated sources give TE = 0, not a
+    // rounding residue). Empty cells take log2(1) = 0 (no branch).
     float acc = 0.f;
     const int ncols = bt * (int)hb;
     for (int col = lane_g; col < ncols; col += gthreads) {
@@ -337,27 +279,33 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
       if (s == 0u) continue;
       const float c1j = c1s[j];
       if (PACK16) {
-        const float c2b_lo = (float)(s & 0xffffu), c2b_hi = (float)(s >> 16);
+        const float blo = (float)(s & 0xffffu), bhi = (float)(s >> 16);
+        const float inv_lo = __frcp_rn(blo), inv_hi = __frcp_rn(bhi);
         for (int i = 0; i < bt; ++i) {
           const int idx = (i * bt + j) * hb + wk;
           const uint32_t w = slot[idx];
-          if (w != 0u) {
-            slot[idx] = 0u;
-            const float c2a = c2as[i * bt + j];
-            const uint32_t clo = w & 0xffffu, chi = w >> 16;
-            if (clo) acc += te_term((float)clo, c1j, c2a, c2b_lo);
-            if (chi) acc += te_term((float)chi, c1j, c2a, c2b_hi);
-          }
+          slot[idx] = 0u;
+          const float2 q = qa[i * bt + j];  // {c1/c2a, c2a}
+          const float clo = (float)(w & 0xffffu), chi = (float)(w >> 16);
+          const bool elo = clo == 0.f || clo * c1j == q.y * blo;
+          const bool ehi = chi == 0.f || chi * c1j == q.y * bhi;
+          const float rlo = elo ? 1.f : clo * inv_lo * q.x;
+          const float rhi = ehi ? 1.f : chi * inv_hi * q.x;
+          acc = fmaf(clo, __log2f(rlo), acc);
+          acc = fmaf(chi, __log2f(rhi), acc);
         }
       } else {
-        const float c2b = (float)s;
+        const float b = (float)s;
+        const float inv = __frcp_rn(b);
         for (int i = 0; i < bt; ++i) {
           const int idx = (i * bt + j) * hb + wk;
           const uint32_t w = slot[idx];
-          if (w != 0u) {
-            slot[idx] = 0u;
-            acc += te_term((float)w, c1j, c2as[i * bt + j], c2b);
-          }
+          slot[idx] = 0u;
+          const float2 q = qa[i * bt + j];
+          const float c = (float)w;
+          const bool e = w == 0u || c * c1j == q.y * b;
+          const float r = e ? 1.f : c * inv * q.x;
+          acc = fmaf(c, __log2f(r), acc);
         }
       }
     }
@@ -401,6 +349,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   double* red = reinterpret_cast<double*>(smem + SL.red_off);
   float* c1s = reinterpret_cast<float*>(smem + SL.c1_off);
   float* c2as = reinterpret_cast<float*>(smem + SL.c2a_off);
+  float2* qa = reinterpret_cast<float2*>(smem + SL.q_off);
   int* c2a_cnt = reinterpret_cast<int*>(smem + SL.c2a_off);
   unsigned char* zsm = smem + SL.z_off;
   uint32_t* slots = reinterpret_cast<uint32_t*>(smem + SL.slot_off);
@@ -505,33 +454,9 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       }
     }
     __syncthreads();
-    // z_dom = most frequent target state (ties: smallest z). Key = count<<11 | (2047 - z)
-    // (count <= N < 2^21 when packed this way; z < bt2 <= 65025 needs 16 bits, so use 64-bit)
-    unsigned long long key = 0ull;
-    for (int z = tid; z < bt2; z += nthreads) {
-      const unsigned long long k =
-          ((unsigned long long)(unsigned)c2a_cnt[z] << 32) | (0xffffffffu - (unsigned)z);
-      key = k > key ? k : key;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long w = __shfl_xor_sync(0xffffffffu, key, o);
-      key = w > key ? w : key;
-    }
-    if ((tid & 31) == 0) reinterpret_cast<unsigned long long*>(red)[warp] = key;
     const int bsmax = misc[1];
     for (int i = tid; i < bt2; i += nthreads) c2as[i] = (float)c2a_cnt[i];
     __syncthreads();
-    if (tid < 32) {
-      unsigned long long v =
-          tid < n_warps ? reinterpret_cast<unsigned long long*>(red)[tid] : 0ull;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-        v = w > v ? w : v;
-      }
-      if (tid == 0) misc[2] = (int)(0xffffffffu - (unsigned)(v & 0xffffffffull));
-    }
     for (int j = tid; j < bt; j += nthreads) {
       float s = 0.f;
       for (int i = 0; i < bt; ++i) s += c2as[i * bt + j];
@@ -560,80 +485,44 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     uint32_t* slot = slots + (int64_t)g * slot_words;
     for (int i = tid; i < n_groups * slot_words; i += nthreads) slots[i] = 0u;
     __syncthreads();
-    const uint32_t zdom = (uint32_t)misc[2];
+    for (int z = tid; z < bt2; z += nthreads) {
+      const float c2a = c2as[z];
+      qa[z] = make_float2(c2a > 0.f ? __fdiv_rn(c1s[z % bt], c2a) : 0.f, c2a);
+    }
+    __syncthreads();
 
     if (pack16)
       run_sources<true>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src, bt,
-                        zdom, zsm, z8, c1s, c2as, red);
+                        zsm, z8, c1s, qa, red);
     else
       run_sources<false>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src, bt,
-                         zdom, zsm, z8, c1s, c2as, red);
+                         zsm, z8, c1s, qa, red);
     __syncthreads();
   }
 }
 
 // Per-gene pre-pass: validation (every bin of gene g in [0, row_len) below
-// n_per_var[g], and 1 <= n_per_var[g] <= b_max; sets ws->bad_data otherwise),
-// the marginal m[g][y] over samples [0, N) and its most frequent bin ydom[g]
-// (ties: smallest y). One CTA per gene.
+// n_per_var[g], and 1 <= n_per_var[g] <= b_max; sets ws->bad_data otherwise).
+// One CTA per gene.
 __global__ void gene_prepass_kernel(const uint8_t* bins, int64_t ld, const int32_t* npv,
-                                    int b_max, int n, int64_t row_len, int N, int32_t* marg,
-                                    int32_t* ydom, WsHeader* ws) {
-  __shared__ int h[256];
-  __shared__ unsigned long long wkey[32];
+                                    int b_max, int n, int64_t row_len, WsHeader* ws) {
   const int g = blockIdx.x;
   if (g >= n) return;
   const int b = npv[g];
-  const bool bad_b = b < 1 || b > b_max;
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
-  __syncthreads();
   const uint8_t* row = bins + (int64_t)g * ld;
   const int64_t nvec = row_len >> 4;
-  bool bad = bad_b;
+  bool bad = b < 1 || b > b_max;
   const uint4* rv = reinterpret_cast<const uint4*>(row);
   for (int64_t v = threadIdx.x; v < nvec; v += blockDim.x) {
     const uint4 q = __ldg(rv + v);
     const uint32_t w[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 4; ++k)
 #pragma unroll
-      for (int bb = 0; bb < 4; ++bb) {
-        const uint32_t val = (w[k] >> (8 * bb)) & 0xffu;
-        bad |= val >= (uint32_t)b;
-        if (v * 16 + k * 4 + bb < N) atomicAdd(&h[val], 1);
-      }
-    }
+      for (int bb = 0; bb < 4; ++bb) bad |= ((w[k] >> (8 * bb)) & 0xffu) >= (uint32_t)b;
   }
-  for (int64_t i = (nvec << 4) + threadIdx.x; i < row_len; i += blockDim.x) {
-    bad |= row[i] >= b;
-    if (i < N) atomicAdd(&h[row[i]], 1);
-  }
-  if (__syncthreads_or(bad)) {
-    if (threadIdx.x == 0) atomicExch(&ws->bad_data, 1);
-    return;
-  }
-  unsigned long long key = 0ull;
-  for (int y = threadIdx.x; y < b; y += blockDim.x) {
-    marg[(int64_t)g * b_max + y] = h[y];
-    const unsigned long long k = ((unsigned long long)(unsigned)h[y] << 32) | (255u - (unsigned)y);
-    key = k > key ? k : key;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long w = __shfl_xor_sync(0xffffffffu, key, o);
-    key = w > key ? w : key;
-  }
-  if ((threadIdx.x & 31) == 0) wkey[threadIdx.x >> 5] = key;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    unsigned long long v = threadIdx.x < (blockDim.x >> 5) ? wkey[threadIdx.x] : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-      v = w > v ? w : v;
-    }
-    if (threadIdx.x == 0) ydom[g] = (int32_t)(255u - (unsigned)(v & 0xffull));
-  }
+  for (int64_t i = (nvec << 4) + threadIdx.x; i < row_len; i += blockDim.x) bad |= row[i] >= b;
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(&ws->bad_data, 1);
 }
 
 // Source order for pair-free items: genes stably sorted by bin-count class
@@ -842,11 +731,7 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   P.counts_stride = counts_stride;
   P.ws = reinterpret_cast<WsHeader*>(workspace);
   unsigned char* wsb = reinterpret_cast<unsigned char*>(workspace);
-  int32_t* marg = reinterpret_cast<int32_t*>(wsb + ws_marg_off());
-  int32_t* ydom = reinterpret_cast<int32_t*>(wsb + ws_ydom_off(n, b_max));
   int32_t* order = reinterpret_cast<int32_t*>(wsb + ws_order_off(n, b_max));
-  P.marg = marg;
-  P.ydom = ydom;
   P.order = order;
 
   // worst case the device can meet: 16-bit halves when N < 65536, else 32-bit
@@ -861,8 +746,7 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
 
   cudaError_t e = cudaMemsetAsync(workspace, 0, sizeof(WsHeader), stream);
   if (e != cudaSuccess) return check_cuda(e, "workspace reset");
-  gene_prepass_kernel<<<n, 256, 0, stream>>>(bins, ld, npv, b_max, n, row_len, P.N, marg, ydom,
-                                             P.ws);
+  gene_prepass_kernel<<<n, 256, 0, stream>>>(bins, ld, npv, b_max, n, row_len, P.ws);
   st = check_launch("gene_prepass_kernel");
   if (st) return st;
   if (!pairs) {
@@ -956,7 +840,7 @@ extern "C" int tenex_surrogate_accumulate_pairs(
 // that device current) by the first call made on that device, so that first
 // call should come before any stream capture. All calls share the one area and
 // each call rewrites it (work ticket and validation words are cleared, the
-// per-gene marginals recomputed), so calls that overlap on the GPU — on two
+// source order recomputed), so calls that overlap on the GPU — on two
 // streams, or from two threads — race and must not be issued.
 // ---------------------------------------------------------------------------
 namespace tenex {
@@ -995,7 +879,7 @@ extern "C" int tenex_te_pairfree_static(const uint8_t* bins, int64_t ld, const i
   if (need > (int64_t)kStaticScratchBytes)
     return fail(TENEX_ERR_UNSUPPORTED,
                 "n_vars=%d with b_max=%d needs %lld bytes of scratch; the built-in area holds "
-                "%zu bytes (about 4*n_vars*(b_max+2) + 1024 must fit). Use tenex_te_pairfree "
+                "%zu bytes (about 4*n_vars + 512 must fit). Use tenex_te_pairfree "
                 "with a workspace instead.",
                 n_vars, b_max, (long long)need, kStaticScratchBytes);
   void* ws = nullptr;

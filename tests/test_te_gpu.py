@@ -127,6 +127,19 @@ def test_constant_source_gives_zero(cuda):
         assert te[t * 5 + sl] == 0.0
 
 
+def test_duplicate_source_gives_zero(cuda):
+    # source == target's own series: y_t = x_t, so every cell has c3*c1 == c2a*c2b and
+    # TE(src -> tgt) = I(x_{t+1}; x_t | x_t) = 0 exactly, as in the reference's formula
+    rng = np.random.default_rng(5)
+    bins, npv, bmax = _rand_bins(rng, 6, 700, 2, 9)
+    bins[4] = bins[1]
+    npv = npv.copy()
+    npv[4] = npv[1]
+    te = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
+    assert te[1 * 5 + 3] == 0.0            # target 1, source 4 (src_local 3)
+    assert te[4 * 5 + 1] == 0.0            # target 4, source 1
+
+
 def test_bad_bins_raise_without_fault(cuda):
     rng = np.random.default_rng(4)
     bins, npv, bmax = _rand_bins(rng, 6, 300, 2, 5)

@@ -66,8 +66,8 @@ def test_static_scratch_matches_workspace_entry_twice(cuda):
 
 
 def test_static_scratch_rejects_oversized_problem(cuda):
-    # 40,000 genes at b_max 38 need ~6.2 MB of scratch: refused before any launch
-    st = native.lib().tenex_te_pairfree_static(None, 64, None, 38, 40000, 100, 1, 0, 10, None,
-                                               0, 0, None, None, None)
+    # 1,500,000 genes need ~6 MB of scratch (4 bytes each): refused before any launch
+    st = native.lib().tenex_te_pairfree_static(None, 64, None, 38, 1_500_000, 100, 1, 0, 10,
+                                               None, 0, 0, None, None, None)
     assert st == native.TENEX_ERR_UNSUPPORTED
     assert "scratch" in native.last_error()
