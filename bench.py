@@ -16,7 +16,9 @@ workload, --pairs times only the first pair ids, --launch T,C,W fixes the
 launch shape (threads, CTAs per SM, sources per work item) instead of running
 the autotuner, --no-e2e, --no-cpu-baseline and --no-surrogate skip those legs.
 The line's "surrogate" object times NetWeaver's surrogate test on cfg5 (full
-100-shuffle test against the learned null, wall seconds, edge agreement).
+100-shuffle test against the learned null, wall seconds, edge agreement), and
+"binary_path" the cfg2 GEMM-B2 matrix against the measured INT8 tensor peak
+(both skipped by --no-surrogate).
 
 N > 1 (torchrun, one process per GPU): the pair-id range is split into
 contiguous chunks of ceil(pairs / N), the reference's split (no data-path
@@ -308,6 +310,7 @@ def run_ours(args) -> None:
                             "peak = MEASURED_PEAKS.json hbm_gbs (of measured)"}
     cpu = cpu_baseline(*_coarsened_host(x, npv, limit)) if not args.no_cpu_baseline else None
     sur = surrogate_leg(dev) if (world == 1 and not args.no_surrogate) else None
+    binl = binary_leg(dev) if (world == 1 and not args.no_surrogate) else None
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
@@ -321,7 +324,8 @@ def run_ours(args) -> None:
                        "launch": kern.cfg},
             "gpu_launches": 6 * args.steps,  # remap, coarsen x2, prepass, order, TE tile
             "roofline": roofline, "roofline_hbm": roofline_hbm,
-            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "surrogate": sur}
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "surrogate": sur,
+            "binary_path": binl}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -374,6 +378,44 @@ def surrogate_leg(dev, reps: int = 2) -> dict:
             "band": lrn.info.get("band")}
 
 
+def binary_leg(dev, reps: int = 5) -> dict:
+    """cfg2 binary path (2,000 genes x 5,000 cells, GEMM-B2 on tcgen05): device time of
+    one full TE matrix (pack kernel + INT8 GEMM with the TE epilogue), against the
+    live INT8 tensor-pipe probe."""
+    import torch
+
+    from tenex_b200 import native, workloads as W
+    from tenex_b200.kernels import device as D
+    from tenex_b200.kernels.gemm_b2 import te_binary_matrix
+    x, _ = W.cfg2_binary()
+    n, T = x.shape
+    db = D.pack_bins(x, dev)
+    out = torch.zeros((n, n), dtype=torch.float32, device=dev)
+    for _ in range(3):
+        te_binary_matrix(db, 1, out=out)
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(reps)]
+    for a, b in ev:
+        a.record()
+        te_binary_matrix(db, 1, out=out, check=False)
+        b.record()
+    torch.cuda.synchronize(dev)
+    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    L = T - 1
+    Lpad = -(-L // 128) * 128
+    tiles = -(-n // 128)
+    ops = 6.0 * (tiles * 128) ** 2 * Lpad          # 3 int8 GEMMs of (n x Lpad) x (Lpad x n)
+    peak = max(native.probe_tc_int8(100_000) for _ in range(2))
+    return {"workload": "cfg2: 2000 genes x 5000 cells, binary Markov bins, GEMM-B2",
+            "pairs_per_s": n * (n - 1) / (ms / 1e3), "ms": ms,
+            "roofline": {"bound": "tensor", "achieved": ops / (ms / 1e3) / 1e12,
+                         "peak": peak / 1e12, "unit": "TOP/s (int8)",
+                         "frac": ops / (ms / 1e3) / peak,
+                         "note": "achieved = 6*n_pad^2*L_pad int8 ops (C, D, E) / device time of "
+                                 "pack + GEMM; peak = tenex_probe_tc_int8 measured live"}}
+
+
 def _coarsened_host(x, npv, limit):
     from oracle import oracle as O
     cb, cnpv, bmax = O.coarsen(x, npv, limit)
@@ -390,6 +432,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--only", choices=["binary", "surrogate"], default=None,
+                    help="run one side leg alone and print its JSON object (profiling)")
     ap.add_argument("--genes", type=int, default=N_GENES)
     ap.add_argument("--cells", type=int, default=N_CELLS)
     ap.add_argument("--pairs", type=int, default=None)
@@ -399,6 +443,12 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.only == "binary":
+        import torch
+        print(json.dumps(binary_leg(torch.device("cuda", 0))), flush=True)
+    elif args.only == "surrogate":
+        import torch
+        print(json.dumps(surrogate_leg(torch.device("cuda", 0))), flush=True)
     else:
         run_ours(args)
 

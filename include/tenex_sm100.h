@@ -268,6 +268,11 @@ int tenex_to_bf16(const float* src, void* dst, int count, void* stream);
  * 16-bit halves, 2 random words, 3 the same 32 words from every warp) and returns the increment count and the
  * milliseconds. Synchronises `stream`. */
 int tenex_probe_smem_atomics(int mode, int iters, int64_t* increments, float* ms, void* stream);
+/* Roofline probe (no reference counterpart): dense INT8 tensor-pipe rate. One CTA per SM
+ * issues `iters` tcgen05.mma.kind::i8 (M=128, N=256, K=32) from shared-memory operands
+ * into TMEM; returns the operation count (2*M*N*K per MMA) and the milliseconds.
+ * Synchronises `stream`; TENEX_ERR_TIMEOUT if the bounded completion wait expired. */
+int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stream);
 
 #ifdef __cplusplus
 }

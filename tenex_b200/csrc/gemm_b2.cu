@@ -10,14 +10,18 @@
 //     operands F, P, FP (rows padded to a multiple of 128 bytes, zero filled)
 //     and the per-gene counts nf, np, nfp.
 //   * GEMM kernel: one CTA per 128 x 128 (target x source) output tile.
-//     TMA (cp.async.bulk.tensor.2d, no multicast) brings 16-byte x 128-row
-//     planes of FP, P, F (targets) and P (sources) into shared memory in the
-//     K-major SWIZZLE_NONE canonical layout; one thread issues, per 32-byte
+//     TMA (cp.async.bulk.tensor.2d, no multicast) brings one 128-byte x
+//     128-row box of each of FP, P, F (targets) and P (sources) per stage into
+//     shared memory, 128-byte swizzled (the K-major SWIZZLE_128B layout the MMA
+//     descriptors name); one thread issues, per 32-byte
 //     K step, three tcgen05.mma.kind::i8 (FP x P^T -> C, P x P^T -> D,
 //     F x P^T -> E) into int32 accumulators in TMEM (3 x 128 columns). The
 //     counts are exact integers (int32, N < 2^31).
-//   * Epilogue: four warps read their 32 TMEM lanes (one target row each) with
-//     tcgen05.ld, form the 8 cells and write TE(src -> tgt) to out[src, tgt].
+//   * Epilogue: sixteen warps; warp w reads TMEM lanes 32*(w%4).. (one target row
+//     per lane) and a quarter of the 128 columns with tcgen05.ld, forms the 8
+//     cells and writes TE(src -> tgt) to out[src, tgt] (the other twelve warps
+//     only wait for the accumulators: four warps alone left the epilogue, not
+//     the MMAs, as the kernel's critical path).
 //   * Every mbarrier wait is bounded; on expiry the kernel records an error
 //     word, drains the copies it issued (bounded), frees TMEM and returns.
 #include <cuda.h>
@@ -27,6 +31,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "tcgen05.cuh"
 
 namespace tenex {
 namespace {
@@ -34,11 +39,9 @@ namespace {
 constexpr int kTile = 128;     // M = N = 128
 constexpr int kKt = 128;       // bytes of K per pipeline stage (4 MMA K-steps of 32)
 constexpr int kStages = 3;
-constexpr int kPlane = 16 * kTile;             // one 16-byte x 128-row plane
 constexpr int kOpBytes = kKt * kTile;          // one operand tile per stage (16 KB)
 constexpr int kStageBytes = 4 * kOpBytes;      // FP, P, F (targets) + P (sources)
 constexpr int kTmemCols = 512;
-constexpr uint32_t kSpinLimit = 1u << 22;      // bounded mbarrier polling (seconds at most)
 
 struct B2Params {
   int n;            // genes
@@ -49,80 +52,6 @@ struct B2Params {
   int64_t out_ld;
   int* err;         // device error word (1 = a wait expired)
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-// Polls the phase `parity` of an mbarrier at most kSpinLimit times; false on expiry.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
-                                            uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, "
-      "{%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-      : "memory");
-}
-
-// K-major SWIZZLE_NONE shared-memory descriptor (version 1 for sm_100):
-// start >> 4 in [0,14), LBO >> 4 in [16,30), SBO >> 4 in [32,46), version 1 at [46,48).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t start, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((start >> 4) & 0x3fffu);
-  d |= (uint64_t)((lbo >> 4) & 0x3fffu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3fffu) << 32;
-  d |= (uint64_t)1 << 46;
-  return d;  // base_offset 0, lbo_mode 0, layout_type 0 (SWIZZLE_NONE)
-}
-
-// Instruction descriptor, kind::i8: D s32 (bits 4-5 = 2), A/B unsigned 8-bit (0),
-// K-major A and B, N >> 3 at bit 17, M >> 4 at bit 24.
-__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
-  return (2u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
@@ -138,8 +67,13 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// c * log2(c * c1 / (c2a * c2b)); exactly 0 for an empty cell and where the two
+// products are equal (the reference's ratio is exactly 1 there); otherwise the
+// ratio by approximate division (2 ulp) and lg2.approx, far below the 1e-6 TE budget.
 __device__ __forceinline__ float cell_term(float c, float c1, float c2a, float c2b) {
-  return c > 0.f ? c * log2f(__fdiv_rn(c * c1, c2a * c2b)) : 0.f;
+  const float num = c * c1, den = c2a * c2b;
+  const float r = (c > 0.f && num != den) ? __fdividef(num, den) : 1.f;
+  return c * __log2f(r);
 }
 
 // Pack: F[g, t] = x[g, t+lag], P[g, t] = x[g, t], FP = F & P for t < L (0 beyond),
@@ -191,7 +125,9 @@ struct B2Maps {
   CUtensorMap F, P, FP;
 };
 
-__global__ void __launch_bounds__(128, 1)
+constexpr int kB2Threads = 512;
+
+__global__ void __launch_bounds__(kB2Threads, 1)
     b2_gemm_kernel(const __grid_constant__ B2Maps maps, B2Params prm) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte align the operand region
@@ -240,12 +176,11 @@ __global__ void __launch_bounds__(128, 1)
       unsigned char* buf = stage_base + s * kStageBytes;
       mbar_expect_tx(&full[s], kStageBytes);
       const int x0 = k * kKt;
-      for (int c = 0; c < kKt / 16; ++c) {
-        tma_load_2d(buf + 0 * kOpBytes + c * kPlane, &maps.FP, x0 + 16 * c, m0, &full[s]);
-        tma_load_2d(buf + 1 * kOpBytes + c * kPlane, &maps.P, x0 + 16 * c, m0, &full[s]);
-        tma_load_2d(buf + 2 * kOpBytes + c * kPlane, &maps.F, x0 + 16 * c, m0, &full[s]);
-        tma_load_2d(buf + 3 * kOpBytes + c * kPlane, &maps.P, x0 + 16 * c, n0, &full[s]);
-      }
+      // one 128-byte x 128-row box per operand, 128-byte swizzled
+      tma_load_2d(buf + 0 * kOpBytes, &maps.FP, x0, m0, &full[s]);
+      tma_load_2d(buf + 1 * kOpBytes, &maps.P, x0, m0, &full[s]);
+      tma_load_2d(buf + 2 * kOpBytes, &maps.F, x0, m0, &full[s]);
+      tma_load_2d(buf + 3 * kOpBytes, &maps.P, x0, n0, &full[s]);
     };
     const int pre = nk < kStages ? nk : kStages;
     for (int k = 0; k < pre; ++k) load_stage(k);
@@ -265,12 +200,12 @@ __global__ void __launch_bounds__(128, 1)
       const uint32_t bP = smem_u32(buf + 3 * kOpBytes);
 #pragma unroll
       for (int kk = 0; kk < kKt / 32; ++kk) {
-        const uint32_t off = kk * 2 * kPlane;  // two 16-byte planes per 32-byte K step
-        const uint64_t bd = smem_desc(bP + off, kPlane, 128);
+        const uint32_t off = kk * 32;  // 32-byte K step inside the 128-byte swizzle row
+        const uint64_t bd = smem_desc_sw128(bP + off);
         const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
-        mma_i8(tmem + 0, smem_desc(aFP + off, kPlane, 128), bd, idesc, acc);
-        mma_i8(tmem + 128, smem_desc(aP + off, kPlane, 128), bd, idesc, acc);
-        mma_i8(tmem + 256, smem_desc(aF + off, kPlane, 128), bd, idesc, acc);
+        mma_i8(tmem + 0, smem_desc_sw128(aFP + off), bd, idesc, acc);
+        mma_i8(tmem + 128, smem_desc_sw128(aP + off), bd, idesc, acc);
+        mma_i8(tmem + 256, smem_desc_sw128(aF + off), bd, idesc, acc);
       }
       mma_commit(&empty[s]);  // stage s free once these MMAs complete
       const int kn = k + kStages;
@@ -297,13 +232,14 @@ __global__ void __launch_bounds__(128, 1)
     }
   }
 
-  // ---- epilogue: all 4 warps, thread tid <-> tile row (target) ------------
-  bool ok_acc = mbar_wait(accbar, 0);
+  // ---- epilogue: 16 warps; lane quarter warp % 4, column quarter warp / 4 ---
+  bool ok_acc = tid == 0 ? mbar_wait(accbar, 0) : mbar_wait_sleep(accbar, 0, 200);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!ok_acc && tid == 0) atomicExch(prm.err, 1);
   const bool run = ok_acc && (*(volatile int*)abort_flag == 0);
-  const int i = m0 + tid;  // target gene of this thread's TMEM lane
+  const int lq = warp & 3, cq = warp >> 2;
+  const int i = m0 + lq * 32 + (tid & 31);  // target gene of this thread's TMEM lane
   const float N = (float)prm.L;
   float nf = 0.f, np_ = 0.f, nfp = 0.f;
   if (i < prm.n) {
@@ -313,8 +249,8 @@ __global__ void __launch_bounds__(128, 1)
   }
   const float c1_1 = np_, c1_0 = N - np_;
   const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
-  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-  for (int cb = 0; cb < kTile; cb += 16) {
+  const uint32_t lane_base = tmem + ((uint32_t)(lq * 32) << 16);
+  for (int cb = cq * (kTile / 4); cb < (cq + 1) * (kTile / 4); cb += 16) {
     uint32_t rc[16], rd[16], re[16];
     tmem_ld16(lane_base + 0 + cb, rc);
     tmem_ld16(lane_base + 128 + cb, rd);
@@ -374,10 +310,10 @@ static int make_map(CUtensorMap* map, const uint8_t* base, int rows, int Lpad) {
   if (!enc) return fail(TENEX_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
   const cuuint64_t dims[2] = {(cuuint64_t)Lpad, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)Lpad};
-  const cuuint32_t box[2] = {16, (cuuint32_t)kTile};
+  const cuuint32_t box[2] = {(cuuint32_t)kKt, (cuuint32_t)kTile};
   const cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(TENEX_ERR_LAUNCH, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return TENEX_OK;
@@ -442,7 +378,7 @@ extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_var
   e = cudaFuncSetAttribute(b2_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
   const unsigned tiles = (unsigned)((n_vars + kTile - 1) / kTile);
-  b2_gemm_kernel<<<dim3(tiles, tiles), 128, smem, stream>>>(maps, prm);
+  b2_gemm_kernel<<<dim3(tiles, tiles), kB2Threads, smem, stream>>>(maps, prm);
   return check_launch("b2_gemm_kernel");
 }
 

@@ -11,10 +11,18 @@
 //           across consecutive instructions).
 // The entry point times the kernel with CUDA events on `stream` and returns the
 // number of increments and the milliseconds (synchronises the stream).
+//
+// tc_int8_probe: dense INT8 tensor-pipe throughput, the roofline of the GEMM-B2
+// path. One CTA per SM (its shared-memory request admits one), one thread issues
+// back-to-back tcgen05.mma.cta_group::1.kind::i8 of M = 128, N = 256, K = 32 from
+// fixed shared-memory operands into two alternating int32 TMEM accumulators
+// (512 columns), commits to an mbarrier and waits for it (bounded); nothing is
+// loaded from global memory, so this is the issue-limited MMA rate.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "common.cuh"
+#include "tcgen05.cuh"
 
 namespace tenex {
 
@@ -51,9 +59,94 @@ __global__ void __launch_bounds__(1024, 1) smem_atomic_probe(int mode, int iters
   if (acc == 0xffffffffu) sink[0] = acc;  // keeps the work observable
 }
 
+constexpr int kProbeM = 128, kProbeN = 256, kProbeK = 32;
+constexpr int kProbeSmem = 120 * 1024;  // > half of an SM's shared memory: one CTA per SM
+
+__global__ void __launch_bounds__(128, 1) tc_int8_probe(int iters, int* err) {
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  unsigned char* sm = (unsigned char*)(((uintptr_t)sm_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* a = sm;                                  // 128 rows x 32 B: 2 planes of 2 KB
+  unsigned char* b = sm + kProbeM * kProbeK;              // 256 rows x 32 B: 2 planes of 4 KB
+  uint64_t* bar = reinterpret_cast<uint64_t*>(b + kProbeN * kProbeK);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < (kProbeM + kProbeN) * kProbeK / 4; i += blockDim.x)
+    reinterpret_cast<uint32_t*>(a)[i] = 0x01010101u * (uint32_t)(i & 3);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // operands visible to the MMA
+  if (tid < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  if (tid == 0) {
+    const uint32_t idesc = idesc_i8(kProbeM, kProbeN);
+    const uint64_t ad = smem_desc(smem_u32(a), kProbeM * 16, 128);
+    const uint64_t bd = smem_desc(smem_u32(b), kProbeN * 16, 128);
+    for (int it = 0; it < iters; ++it)
+      mma_i8(tmem + (uint32_t)((it & 1) * kProbeN), ad, bd, idesc, it >= 2 ? 1u : 0u);
+    mma_commit(bar);
+    if (!mbar_wait(bar, 0)) atomicExch(err, 1);
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (tid < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512)
+                 : "memory");
+}
+
 }  // namespace tenex
 
 using namespace tenex;
+
+extern "C" int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stream_) {
+  if (iters < 1 || !ops || !ms) return fail(TENEX_ERR_BADARG, "iters >= 1, outputs non-NULL");
+  DevAttr A;
+  int st = current_device_attr(&A);
+  if (st) return st;
+  cudaStream_t s = as_stream(stream_);
+  int* err = nullptr;
+  cudaError_t e = cudaMallocAsync(&err, sizeof(int), s);
+  if (e != cudaSuccess) return check_cuda(e, "cudaMallocAsync");
+  cudaMemsetAsync(err, 0, sizeof(int), s);
+  e = cudaFuncSetAttribute(tc_int8_probe, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kProbeSmem + 1024);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(err, s);
+    return check_cuda(e, "cudaFuncSetAttribute");
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  tc_int8_probe<<<A.sm_count, 128, kProbeSmem + 1024, s>>>(iters < 64 ? iters : 64, err);
+  cudaEventRecord(e0, s);
+  tc_int8_probe<<<A.sm_count, 128, kProbeSmem + 1024, s>>>(iters, err);
+  cudaEventRecord(e1, s);
+  st = check_launch("tc_int8_probe");
+  e = cudaEventSynchronize(e1);
+  if (!st && e != cudaSuccess) st = check_cuda(e, "cudaEventSynchronize");
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  int h = 0;
+  cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(err, s);
+  if (st) return st;
+  if (h) return fail(TENEX_ERR_TIMEOUT, "tensor-pipe probe: commit wait expired");
+  *ms = t;
+  *ops = 2.0 * kProbeM * kProbeN * kProbeK * (double)iters * A.sm_count;
+  return TENEX_OK;
+}
 
 extern "C" int tenex_probe_smem_atomics(int mode, int iters, int64_t* increments, float* ms,
                                         void* stream_) {

@@ -51,6 +51,7 @@ struct TeParams {
   int n_targets;
   int W;          // sources per item
   int n_chunks;   // items per target
+  int tblock;     // targets per L2 block of the item order (pair-free mode)
   int64_t n_items;
   int zbytes;     // bytes per z entry reserved (1 or 2)
   int bmax;       // max n_per_var (sizes the c2a/c1 region and the marginal rows)
@@ -385,8 +386,16 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       // source order (genes grouped by bin count, so one item's histogram slots
       // are sized for sources of similar b); sources outside [p0, p1) or equal
       // to the target are skipped below
-      const int chunk = (int)(q / P.n_targets);
-      tgt = P.t_first + (int)(q % P.n_targets);
+      // Item order: targets in blocks of tblock rows (sized to stay in L2); within
+      // a block, chunk-major, so one source chunk is shared by the CTAs resident
+      // at one moment and the block's target rows are re-read from L2, not HBM.
+      const int64_t per_block = (int64_t)P.tblock * P.n_chunks;
+      const int blk = (int)(q / per_block);
+      const int tb0 = blk * P.tblock;
+      const int tbs = min(P.tblock, P.n_targets - tb0);
+      const int64_t rem = q - (int64_t)blk * per_block;
+      const int chunk = (int)(rem / tbs);
+      tgt = P.t_first + tb0 + (int)(rem - (int64_t)chunk * tbs);
       base = (int64_t)tgt * nm1;
       lo = (int64_t)chunk * P.W;
       hi = min((int64_t)(chunk + 1) * P.W, (int64_t)P.n);
@@ -707,12 +716,16 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
     P.t_first = 0;
     P.n_targets = 1;
     P.n_chunks = 1;
+    P.tblock = 1;
   } else {
     P.t_first = (int)(p0 / (n - 1));
     const int t_last = (int)((P.p1 - 1) / (n - 1));
     P.n_targets = t_last - P.t_first + 1;
     P.n_chunks = (n + P.W - 1) / P.W;
     P.n_items = (int64_t)P.n_targets * P.n_chunks;
+    // about 40% of L2 for the block's target rows
+    const int64_t rows = (int64_t)A.l2_bytes * 2 / 5 / std::max<int64_t>(ld, 1);
+    P.tblock = (int)std::max<int64_t>(1, std::min<int64_t>(P.n_targets, rows));
   }
   if (P.n_items == 0) return TENEX_OK;
   if (P.n_items > 0x7fffffffLL - 65536)

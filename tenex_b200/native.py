@@ -95,6 +95,8 @@ _SIGS = {
     "tenex_to_bf16": [_P, _P, _I, _P],
     "tenex_probe_smem_atomics": [_I, _I, ctypes.POINTER(ctypes.c_int64),
                                  ctypes.POINTER(ctypes.c_float), _P],
+    "tenex_probe_tc_int8": [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float),
+                            _P],
 }
 _RESTYPES = {"tenex_te_workspace_bytes": ctypes.c_size_t,
              "tenex_b2_workspace_bytes": ctypes.c_size_t,
@@ -167,3 +169,11 @@ def probe_smem_atomics(mode: int = 0, iters: int = 4096) -> float:
     call("tenex_probe_smem_atomics", int(mode), int(iters), ctypes.byref(inc), ctypes.byref(ms),
          stream_ptr())
     return inc.value / (ms.value * 1e-3)
+
+
+def probe_tc_int8(iters: int = 100_000) -> float:
+    """Measured dense INT8 tensor-pipe operations per second over all SMs."""
+    ops = ctypes.c_double()
+    ms = ctypes.c_float()
+    call("tenex_probe_tc_int8", int(iters), ctypes.byref(ops), ctypes.byref(ms), stream_ptr())
+    return ops.value / (ms.value * 1e-3)
