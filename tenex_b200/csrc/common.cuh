@@ -41,7 +41,8 @@ struct WsHeader {
   unsigned int ticket;
   int bad_data;
   int bad_item;
-  int pad[13];
+  unsigned int ov_ticket;  // work ticket of the global-memory overflow launch
+  int pad[12];
   unsigned long long phase_cycles[8];
   int pad2[32];
 };

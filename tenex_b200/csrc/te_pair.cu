@@ -52,6 +52,11 @@ struct TeParams {
   int W;          // sources per item
   int n_chunks;   // items per target
   int tblock;     // targets per L2 block of the item order (pair-free mode)
+  // global-memory overflow launch: pairs whose histogram does not fit shared
+  // memory (only with coarsening off), one 32-bit slot of gslot_words per CTA
+  int gmem;
+  uint32_t* gslots;
+  int64_t gslot_words;
   int64_t n_items;
   int zbytes;     // bytes per z entry reserved (1 or 2)
   int bmax;       // max n_per_var (sizes the c2a/c1 region and the marginal rows)
@@ -126,25 +131,29 @@ __device__ __forceinline__ uint32_t cell_get(const uint32_t* slot, uint32_t z, u
   return slot[z * bs + y];
 }
 
-// Counts one sample: one red.shared.add per sample (inline PTX, no return value);
-// PACK16 adds 1 or 1 << 16 to the word holding the cell's 16-bit half. slot32 is
-// the slot's 32-bit shared-window address.
-template <bool PACK16>
-__device__ __forceinline__ void hist_add(uint32_t slot32, uint32_t z, uint32_t y, uint32_t bs,
+// Counts one sample: one reduction per sample (inline PTX, no return value);
+// PACK16 adds 1 or 1 << 16 to the word holding the cell's 16-bit half. base is
+// the slot's address: the 32-bit shared window address, or (GMEM, the
+// global-memory overflow slot) the global address.
+template <bool PACK16, bool GMEM>
+__device__ __forceinline__ void hist_add(uint64_t base, uint32_t z, uint32_t y, uint32_t bs,
                                          uint32_t hb) {
-  uint32_t addr, inc;
+  uint32_t off, inc;
   if (PACK16) {
-    addr = slot32 + ((z * hb + (y >> 1)) << 2);
+    off = (z * hb + (y >> 1)) << 2;
     inc = (y & 1u) * 0xffffu + 1u;
   } else {
-    addr = slot32 + ((z * bs + y) << 2);
+    off = (z * bs + y) << 2;
     inc = 1u;
   }
-  asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(inc) : "memory");
+  if (GMEM)
+    asm volatile("red.global.add.u32 [%0], %1;" ::"l"(base + off), "r"(inc) : "memory");
+  else
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"((uint32_t)base + off), "r"(inc) : "memory");
 }
 
-template <bool PACK16>
-__device__ __forceinline__ void hist16_z8(uint32_t slot, uint4 yv, uint4 zv, uint32_t bs,
+template <bool PACK16, bool GMEM>
+__device__ __forceinline__ void hist16_z8(uint64_t slot, uint4 yv, uint4 zv, uint32_t bs,
                                           uint32_t hb) {
   const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
   const uint32_t zs[4] = {zv.x, zv.y, zv.z, zv.w};
@@ -154,13 +163,13 @@ __device__ __forceinline__ void hist16_z8(uint32_t slot, uint4 yv, uint4 zv, uin
     for (int b = 0; b < 4; ++b) {
       const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
       const uint32_t z = __byte_perm(zs[w], 0, 0x4440 + b);
-      hist_add<PACK16>(slot, z, y, bs, hb);
+      hist_add<PACK16, GMEM>(slot, z, y, bs, hb);
     }
   }
 }
 
-template <bool PACK16>
-__device__ __forceinline__ void hist16_z16(uint32_t slot, uint4 yv, uint4 za, uint4 zb,
+template <bool PACK16, bool GMEM>
+__device__ __forceinline__ void hist16_z16(uint64_t slot, uint4 yv, uint4 za, uint4 zb,
                                            uint32_t bs, uint32_t hb) {
   const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
   const uint32_t zs[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
@@ -171,14 +180,14 @@ __device__ __forceinline__ void hist16_z16(uint32_t slot, uint4 yv, uint4 za, ui
       const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
       const uint32_t zw = zs[(w * 4 + b) >> 1];
       const uint32_t z = (b & 1) ? (zw >> 16) : (zw & 0xffffu);
-      hist_add<PACK16>(slot, z, y, bs, hb);
+      hist_add<PACK16, GMEM>(slot, z, y, bs, hb);
     }
   }
 }
 
 // Histogram of one source against the staged target (all group lanes).
-template <bool PACK16>
-__device__ __forceinline__ void hist_source(uint32_t slot32, const unsigned char* zsm, bool z8,
+template <bool PACK16, bool GMEM>
+__device__ __forceinline__ void hist_source(uint64_t slot32, const unsigned char* zsm, bool z8,
                                             const uint8_t* srow, int N, int lane_g,
                                             int gthreads, uint32_t bs, uint32_t hb) {
   const int nvec = N >> 4;
@@ -192,12 +201,12 @@ __device__ __forceinline__ void hist_source(uint32_t slot32, const unsigned char
         const int vn = v + gthreads;
         uint4 ynext = ycur;
         if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
-        hist16_z8<PACK16>(slot32, ycur, zv[v], bs, hb);
+        hist16_z8<PACK16, GMEM>(slot32, ycur, zv[v], bs, hb);
         ycur = ynext;
       }
     }
     for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
-      hist_add<PACK16>(slot32, zsm[s], srow[s], bs, hb);
+      hist_add<PACK16, GMEM>(slot32, zsm[s], srow[s], bs, hb);
   } else {
     const uint16_t* z16 = reinterpret_cast<const uint16_t*>(zsm);
     if (v < nvec) {
@@ -206,12 +215,12 @@ __device__ __forceinline__ void hist_source(uint32_t slot32, const unsigned char
         const int vn = v + gthreads;
         uint4 ynext = ycur;
         if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
-        hist16_z16<PACK16>(slot32, ycur, zv[2 * v], zv[2 * v + 1], bs, hb);
+        hist16_z16<PACK16, GMEM>(slot32, ycur, zv[2 * v], zv[2 * v + 1], bs, hb);
         ycur = ynext;
       }
     }
     for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
-      hist_add<PACK16>(slot32, z16[s], srow[s], bs, hb);
+      hist_add<PACK16, GMEM>(slot32, z16[s], srow[s], bs, hb);
   }
 }
 
@@ -220,13 +229,26 @@ __device__ __forceinline__ void group_sync(int G, int g, int gthreads) {
   else dev::named_bar(1 + g, gthreads);
 }
 
-// One group's pass over its sources of the current item.
-template <bool PACK16>
+// Whether pair (bt, bs) fits one group's shared-memory slot of slot_region bytes
+// (32-bit counters, or 16-bit halves when N < 65536); pairs that do not go to
+// the global-memory overflow launch. Same rule on host and device.
+__host__ __device__ inline bool slot_fits(int64_t bt, int64_t bs, int N, int64_t slot_region) {
+  const int64_t w32 = round_up(bt * bt * bs, 4);
+  if (w32 * 4 <= slot_region) return true;
+  const int64_t w16 = round_up(bt * bt * ((bs + 1) / 2), 4);
+  return N < 65536 && w16 * 4 <= slot_region;
+}
+
+// One group's pass over its sources of the current item. GMEM: the global-memory
+// overflow launch (one slot per CTA in the workspace, only pairs that do not fit
+// shared memory); otherwise only pairs that fit.
+template <bool PACK16, bool GMEM>
 __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, int G, int g,
                                             int n_groups, int lane_g, int tid, int warp,
                                             int tgt, int64_t lo, int64_t base, int n_src,
                                             int bt, const unsigned char* zsm, bool z8,
-                                            const float* c1s, const float2* qa, double* red) {
+                                            const float* c1s, const float2* qa, double* red,
+                                            int slot_region) {
   const int gthreads = G * 32;
   const int N = P.N;
   const int bt2 = bt * bt;
@@ -242,13 +264,16 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
       if (src == tgt || p < P.p0 || p >= P.p1) continue;  // group-uniform skip
     }
     const uint32_t bs = (uint32_t)P.npv[src];
+    if (slot_fits(bt, bs, N, slot_region) == GMEM) continue;  // the other launch's pair
     const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
     const uint8_t* srow = P.bins + (int64_t)src * P.ld;
-    const uint32_t slot32 = (uint32_t)__cvta_generic_to_shared(slot);
+    uint64_t slot_addr;
+    if (GMEM) asm("cvta.to.global.u64 %0, %1;" : "=l"(slot_addr) : "l"(slot));
+    else slot_addr = (uint64_t)__cvta_generic_to_shared(slot);
     PHASE_MARK(t0);
 
     // -- histogram of every sample -----------------------------------------
-    hist_source<PACK16>(slot32, zsm, z8, srow, N, lane_g, gthreads, bs, hb);
+    hist_source<PACK16, GMEM>(slot_addr, zsm, z8, srow, N, lane_g, gthreads, bs, hb);
     group_sync(G, g, gthreads);
     PHASE_MARK(t1);
     PHASE_MARK(t2);
@@ -364,9 +389,14 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   const int N = P.N;
 
   if (*(volatile int*)&P.ws->bad_data != 0) return;  // validation failed: do nothing
+  uint32_t* gslot = P.gmem ? P.gslots + (int64_t)blockIdx.x * P.gslot_words : nullptr;
+  if (P.gmem) {
+    for (int64_t i = tid; i < P.gslot_words; i += nthreads) gslot[i] = 0u;
+    __syncthreads();
+  }
 
   for (;;) {
-    if (tid == 0) misc[0] = (int)atomicAdd(&P.ws->ticket, 1u);
+    if (tid == 0) misc[0] = (int)atomicAdd(P.gmem ? &P.ws->ov_ticket : &P.ws->ticket, 1u);
     __syncthreads();
     const int64_t q = (int64_t)misc[0];
     if (q >= P.n_items) break;
@@ -400,6 +430,12 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       lo = (int64_t)chunk * P.W;
       hi = min((int64_t)(chunk + 1) * P.W, (int64_t)P.n);
       if (base + nm1 <= P.p0 || base >= P.p1) lo = hi;  // target outside the range
+      // sources are sorted by bin count: skip a chunk this launch has no pair of
+      if (lo < hi) {
+        const int btq = P.npv[tgt];
+        if (!P.gmem && !slot_fits(btq, P.npv[P.order[lo]], N, slot_region)) lo = hi;
+        if (P.gmem && slot_fits(btq, P.npv[P.order[hi - 1]], N, slot_region)) lo = hi;
+      }
     }
     if (lo >= hi) {
       __syncthreads();
@@ -414,8 +450,9 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     const int bt = P.npv[tgt];
     const int bt2 = bt * bt;
 
-    // ---- max b_s over the item's sources (pair lists: also check indices) --
+    // ---- max b_s over this launch's sources (pair lists: also check indices) --
     unsigned my_max = 1;
+    int mine = 0;
     bool bad = tgt < 0 || tgt >= P.n;
     for (int r = tid; r < n_src; r += nthreads) {
       int src;
@@ -428,13 +465,17 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
         const int64_t p = base + (src < tgt ? src : src - 1);
         if (src == tgt || p < P.p0 || p >= P.p1) continue;
       }
-      my_max = max(my_max, (unsigned)P.npv[src]);
+      const int bsrc = P.npv[src];
+      if (!bad && slot_fits(bt, bsrc, N, slot_region) == (P.gmem != 0)) continue;
+      my_max = max(my_max, (unsigned)bsrc);
+      mine = 1;
     }
     if (__syncthreads_or(bad)) {
       if (tid == 0) atomicExch(&P.ws->bad_data, 2);
       __syncthreads();
       continue;
     }
+    if (!__syncthreads_or(mine)) continue;  // no pair of this launch (uniform)
     my_max = dev::warp_max(my_max);
     if ((tid & 31) == 0) reinterpret_cast<unsigned*>(red)[warp] = my_max;
     for (int i = tid; i < bt2; i += nthreads) c2a_cnt[i] = 0;
@@ -473,11 +514,12 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     }
 
     // ---- carve slots: 32-bit counters when groups of <= 4 warps fit --------
+    // (the overflow launch: the whole CTA on one 32-bit slot in global memory)
     const int words32 = (int)round_up((int64_t)bt2 * bsmax, 4);
     const int words16 = (int)round_up((int64_t)bt2 * ((bsmax + 1) >> 1), 4);
-    const int fit32 = slot_region / (words32 * 4);
-    const int fit16 = slot_region / (words16 * 4);
-    const bool pack16 = (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
+    const int fit32 = P.gmem ? 1 : slot_region / (words32 * 4);
+    const int fit16 = P.gmem ? 0 : slot_region / (words16 * 4);
+    const bool pack16 = !P.gmem && (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
     const int fit = pack16 ? fit16 : fit32;
     const int slot_words = pack16 ? words16 : words32;
     if (fit < 1) {
@@ -491,8 +533,9 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     const int n_groups = n_warps / G;
     const int g = warp / G;
     const int lane_g = tid - g * G * 32;
-    uint32_t* slot = slots + (int64_t)g * slot_words;
-    for (int i = tid; i < n_groups * slot_words; i += nthreads) slots[i] = 0u;
+    uint32_t* slot = P.gmem ? gslot : slots + (int64_t)g * slot_words;
+    if (!P.gmem)
+      for (int i = tid; i < n_groups * slot_words; i += nthreads) slots[i] = 0u;
     __syncthreads();
     for (int z = tid; z < bt2; z += nthreads) {
       const float c2a = c2as[z];
@@ -500,12 +543,15 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     }
     __syncthreads();
 
-    if (pack16)
-      run_sources<true>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src, bt,
-                        zsm, z8, c1s, qa, red);
+    if (P.gmem)
+      run_sources<false, true>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src,
+                               bt, zsm, z8, c1s, qa, red, slot_region);
+    else if (pack16)
+      run_sources<true, false>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src,
+                               bt, zsm, z8, c1s, qa, red, slot_region);
     else
-      run_sources<false>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src, bt,
-                         zsm, z8, c1s, qa, red);
+      run_sources<false, false>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src,
+                                bt, zsm, z8, c1s, qa, red, slot_region);
     __syncthreads();
   }
 }
@@ -534,18 +580,17 @@ __global__ void gene_prepass_kernel(const uint8_t* bins, int64_t ld, const int32
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicExch(&ws->bad_data, 1);
 }
 
-// Source order for pair-free items: genes stably sorted by bin-count class
-// (class = b for b <= 40, then bands of 16), so a work item's sources have
-// similar b and its histogram slots are sized for them. One CTA of 1024 threads;
+// Source order for pair-free items: genes stably sorted by bin count, so a work
+// item's sources have similar b (its histogram slots are sized for them) and the
+// pairs that overflow shared memory form a suffix of every target's order. One CTA of 1024 threads;
 // deterministic (ballot + block scan, no atomics on the order).
 __device__ __forceinline__ int order_class(int b) {
-  const int c = b <= 40 ? b : 41 + (b - 41) / 16;
-  return c < 0 ? 0 : (c > 56 ? 56 : c);  // out-of-range counts (rejected later) stay in bounds
+  return b < 0 ? 0 : (b > 255 ? 255 : b);  // out-of-range counts (rejected later) stay in bounds
 }
 
 __global__ void __launch_bounds__(1024) source_order_kernel(const int32_t* __restrict__ npv,
                                                             int n, int32_t* __restrict__ order) {
-  constexpr int kClasses = 41 + 15 + 1;
+  constexpr int kClasses = 256;
   __shared__ int present[kClasses];
   __shared__ int wsum[32];
   __shared__ int base_sh;
@@ -604,20 +649,36 @@ static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const D
   int smem = 0;
   // With shared memory sized automatically, fewer CTAs per SM are used when the
   // largest pair's histogram would not fit (e.g. 38-bin genes need ~110 KB).
+  // Pairs that still do not fit at one CTA per SM go to the global-memory
+  // overflow launch (te_run).
   for (;; --cps) {
     smem = fixed ? fixed : std::min((A.smem_per_sm / cps) - 1024, A.smem_optin);
     smem = smem / 16 * 16;
     if ((int64_t)SL.slot_off + max_slot_bytes <= smem) break;
-    if (fixed || cps == 1)
-      return fail(TENEX_ERR_UNSUPPORTED,
-                  "histogram of the largest pair (%lld B) plus the staged target (%d B) does "
-                  "not fit %d B of shared memory; coarsen bins or shorten the series",
-                  (long long)max_slot_bytes, SL.slot_off, smem);
+    if (fixed || cps == 1) break;
   }
+  if ((int64_t)SL.slot_off + 1024 > smem)
+    return fail(TENEX_ERR_UNSUPPORTED,
+                "the staged target (%d B of shared memory for N = %d samples) leaves no room "
+                "for histograms in %d B; shorten the series", SL.slot_off, P.N, smem);
   L->threads = threads;
   L->smem = smem;
   L->grid = A.sm_count * cps;
   return TENEX_OK;
+}
+
+// Global-memory overflow slots (bytes, 0 if every pair of b_max fits shared
+// memory with N samples at one CTA per SM): one b_max^3 32-bit slot per overflow
+// CTA, as many CTAs as fit 1 GiB (at least one, at most one per SM).
+static int64_t gmem_slot_count(int b_max, const DevAttr& A) {
+  const int64_t words = (int64_t)b_max * b_max * b_max;
+  return std::max<int64_t>(1, std::min<int64_t>(A.sm_count, ((int64_t)1 << 30) / (words * 4)));
+}
+static int64_t gmem_bytes(int b_max, int N, int zbytes, const DevAttr& A) {
+  const SmemLayout SL = smem_layout(N, zbytes, b_max);
+  const int smem = std::min(A.smem_per_sm - 1024, A.smem_optin) / 16 * 16;
+  if (slot_fits(b_max, b_max, N, (int64_t)smem - SL.slot_off)) return 0;
+  return round_up(gmem_slot_count(b_max, A) * (int64_t)b_max * b_max * b_max * 4, 256);
 }
 
 }  // namespace tenex
@@ -625,9 +686,12 @@ static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const D
 using namespace tenex;
 
 extern "C" size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len, int b_max) {
-  (void)row_len;
   if (n_vars < 1 || b_max < 1) return sizeof(WsHeader);
-  return (size_t)ws_total(n_vars, b_max);
+  size_t total = (size_t)ws_total(n_vars, b_max);
+  DevAttr A;
+  if (row_len > 1 && row_len < ((int64_t)1 << 24) && current_device_attr(&A) == TENEX_OK)
+    total += (size_t)gmem_bytes(b_max, (int)row_len, b_max <= 16 ? 1 : 2, A);
+  return total;
 }
 
 extern "C" int tenex_workspace_status(const void* workspace, void* stream) {
@@ -754,6 +818,22 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   st = plan_te_launch(P, cfg, A, &L, worst_slot);
   if (st) return st;
   P.smem_bytes = L.smem;
+  // pairs whose histogram does not fit shared memory: global-memory overflow launch
+  const SmemLayout SLh = smem_layout(P.N, P.zbytes, P.bmax);
+  const bool overflow = !slot_fits(b_max, b_max, P.N, (int64_t)L.smem - SLh.slot_off);
+  int64_t n_gslots = 0;
+  if (overflow) {
+    P.gslot_words = (int64_t)b_max * b_max * b_max;
+    n_gslots = gmem_slot_count(b_max, A);
+    const int64_t need = ws_total(n, b_max) + round_up(n_gslots * P.gslot_words * 4, 256);
+    if ((int64_t)ws_bytes < need)
+      return fail(TENEX_ERR_UNSUPPORTED,
+                  "pairs with b up to %d do not fit shared memory and need %lld bytes of "
+                  "global-memory slots in the workspace (%lld given; size it with "
+                  "tenex_te_workspace_bytes)", b_max, (long long)need, (long long)ws_bytes);
+    P.gslots = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(workspace) +
+                                           ws_total(n, b_max));
+  }
   int64_t grid = L.grid;
   if (grid > P.n_items) grid = P.n_items;
 
@@ -770,8 +850,14 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   e = cudaFuncSetAttribute(te_pair_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            L.smem);
   if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+  P.gmem = 0;
   te_pair_tile_kernel<<<(int)grid, L.threads, L.smem, stream>>>(P);
-  return check_launch("te_pair_tile_kernel");
+  st = check_launch("te_pair_tile_kernel");
+  if (st || !overflow) return st;
+  P.gmem = 1;
+  te_pair_tile_kernel<<<(int)std::min<int64_t>(n_gslots, P.n_items), L.threads, L.smem,
+                        stream>>>(P);
+  return check_launch("te_pair_tile_kernel (global-memory overflow)");
 }
 
 extern "C" int tenex_te_pairfree(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,

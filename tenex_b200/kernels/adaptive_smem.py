@@ -10,6 +10,8 @@ from __future__ import annotations
 
 import torch
 
+from tenex_b200 import _log
+
 from tenex_b200.kernels import _next_pow2
 from tenex_b200.kernels.pair_tile import PairTileKernel
 
@@ -55,8 +57,15 @@ class AdaptiveSMEMKernel(PairTileKernel):
         if b_max <= limit:
             return bin_arrs, n_per_var, b_max
         if use_coarsening is False:
-            raise ValueError(
-                f"coarsening=False but b_max={b_max} exceeds the shared-memory bin limit "
-                f"{limit}; the global-memory overflow path is not part of this build. "
-                f"Use coarsening=None (default).")
+            # as the reference (tenex/kernels/adaptive_smem.py:1252-1262): bins stay
+            # as they are and the pairs whose histogram does not fit shared memory
+            # run in the kernel's global-memory overflow launch; bins are uint8 here
+            if b_max >= 256:
+                raise ValueError(
+                    f"coarsening=False but b_max={b_max} >= 256, which the global-memory "
+                    f"overflow path cannot hold in uint8 bins. Use coarsening=None (default) "
+                    f"or kp<0.5 to reduce bins.")
+            _log.vprint("[TENEX] bin coarsening disabled: shared-memory kernel + global-memory "
+                        "overflow")
+            return bin_arrs, n_per_var, b_max
         return coarsen_bins(bin_arrs, n_per_var, limit)

@@ -74,6 +74,23 @@ def test_adaptive_prepare_and_heavy_genes(cuda):
     assert np.max(np.abs(te - O.te_pairfree(cb, cnpv))) <= TOL
 
 
+def test_adaptive_no_coarsening_uses_overflow(cuda):
+    # use_coarsening=False: heavy genes keep all their bins; their pairs run in the
+    # global-memory overflow launch and TE equals the oracle on the raw bins
+    x, npv = W.multibin(24, 1200, 6, 2, 12, heavy_frac=0.25, heavy_lo=60, heavy_hi=120)
+    db = D.pack_bins(x, cuda)
+    k = AdaptiveSMEMKernel()
+    bmax = int(npv.max())
+    db2, npv2, bmax2 = k.prepare(db, torch.as_tensor(npv, device=cuda), bmax, tau=1,
+                                 use_coarsening=False, smem_optin=232448)
+    assert bmax2 == bmax > 38
+    te = k.compute_pairfree_device(db2, npv2, bmax2, 1).cpu().numpy()
+    assert np.max(np.abs(te - O.te_pairfree(x, npv))) <= TOL
+    with pytest.raises(ValueError, match="256"):
+        k.prepare(db, torch.as_tensor(npv, device=cuda), 256, tau=1, use_coarsening=False,
+                  smem_optin=232448)
+
+
 @pytest.mark.parametrize("method", ["nonzero", "mean", "median", "quantile"])
 def test_binarization_routes_to_gemm_b2(cuda, method):
     x, _ = W.cfg1_expression(n=50, T=400, seed=3)

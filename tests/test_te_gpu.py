@@ -48,6 +48,36 @@ def test_counts_bitexact_and_te(cuda, b_lo, b_hi, T, threads):
     assert np.max(np.abs(te - ref_te)) <= TOL
 
 
+@pytest.mark.parametrize("T,b_big", [(900, 90), (70000, 41)])
+def test_global_memory_overflow_counts(cuda, T, b_big):
+    # genes whose b_t^2 * b_s histogram cannot fit shared memory (no coarsening): those
+    # pairs run in the global-memory overflow launch, the rest in shared memory. T=70000
+    # makes N >= 65536 (32-bit counters only, so 41 bins already overflow).
+    rng = np.random.default_rng(T + b_big)
+    bvals = [3, b_big, 5, b_big - 7, 2]
+    n = len(bvals)
+    x = np.stack([rng.integers(0, b, T) for b in bvals]).astype(np.int32)
+    bins, npv, bmax = O.remap(x)
+    bins = bins.reshape(n, T, 1)
+    P = n * (n - 1)
+    stride = bmax ** 3
+    counts = torch.full((P, stride), -1, dtype=torch.int32, device=cuda)
+    te = _gpu_te(bins, npv, bmax, cuda, counts=counts, counts_stride=stride).cpu().numpy()
+    cnt = counts.cpu().numpy()
+    for p in range(P):
+        t, sl = divmod(p, n - 1)
+        s = sl + (sl >= t)
+        ref = O.counts(bins, 1, t, s, npv).reshape(-1)
+        assert np.array_equal(cnt[p, :ref.size], ref), (p, t, s)
+    assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
+    # pair-list mode (source filter) takes the same two launches
+    pairs = np.array([[1, 0], [1, 3], [0, 1], [4, 3], [3, 1]], np.int64)
+    from tenex_b200.kernels.pair_list import te_pair_list
+    db = D.pack_bins(bins, cuda)
+    got = te_pair_list(db, torch.as_tensor(npv, device=cuda), bmax, 1, pairs).cpu().numpy()
+    assert np.max(np.abs(got - O.te_pairs(bins, npv, pairs))) <= TOL
+
+
 @pytest.mark.parametrize("tau,K", [(1, 1), (2, 1), (1, 2), (3, 2)])
 def test_tau_and_k(cuda, tau, K):
     rng = np.random.default_rng(tau * 10 + K)
