@@ -17,6 +17,11 @@ product to the reference's own CPU code paths:
   surrogate.npz         SurrogateTestMethod.infer on CPU (scatter_add kernel, block
                         shuffles) plus the block permutations its RNG schedule draws
   smem_limit.npz        compute_smem_bin_limit for a few SMEM sizes
+  multilag.npz          Pipeline._combine_surrogate_multi_lag (max, adaptive_select,
+                        weighted_sum) on three synthetic per-lag surrogate results
+
+`python tests/golden/make_golden.py /path/to/reference multilag` writes only the
+last one.
 """
 from __future__ import annotations
 
@@ -134,5 +139,51 @@ def main(ref: str) -> None:
     print("golden fixtures written to", HERE)
 
 
+def multilag(ref: str) -> None:
+    """The reference's multi-lag combine on synthetic per-lag surrogate results."""
+    sys.path.insert(0, ref)
+    os.environ.setdefault("TENEX_CPU_ONLY", "1")
+    import torch
+    from tenex.pipeline import Pipeline
+    from tenex.inference import make_grn
+    from tenex.inference.surrogate_test import SurrogateTestResult
+
+    rng = np.random.default_rng(21)
+    n, taus = 15, [1, 2, 3]
+    names = np.array([f"g{i}" for i in range(n)])
+    stacks = {k: [] for k in ("observed", "mean", "std", "effective", "p")}
+    results = []
+    for _ in taus:
+        obs = (rng.random((n, n)) * 0.05).astype(np.float32)
+        np.fill_diagonal(obs, 0.0)
+        mean = (rng.random((n, n)) * 0.03).astype(np.float32)
+        std = (rng.random((n, n)) * 0.01 + 1e-3).astype(np.float32)
+        eff = (obs - mean).astype(np.float32)
+        p = (rng.random((n, n)) ** 4).astype(np.float32)
+        np.fill_diagonal(p, 1.0)
+        for k, v in zip(stacks, (obs, mean, std, eff, p)):
+            stacks[k].append(v)
+        results.append(SurrogateTestResult(
+            observed_te=obs, mean_surrogate_te=mean, std_surrogate_te=std, effective_te=eff,
+            p_values=p, grn=make_grn(names, np.zeros((0, 2), np.int64), np.zeros(0)),
+            n_surrogates=10, shuffle_method="block", block_length=5, p_method="parametric",
+            fdr=0.05))
+    out = {k: np.stack(v) for k, v in stacks.items()}
+    for combine in ("max", "adaptive_select", "weighted_sum"):
+        r = Pipeline._combine_surrogate_multi_lag(results, taus, combine, names,
+                                                  torch.device("cpu"))
+        for f in ("observed_te", "mean_surrogate_te", "std_surrogate_te", "effective_te",
+                  "p_values"):
+            out[f"{combine}_{f}"] = getattr(r, f)
+        out[f"{combine}_pairs"] = r.grn.pairs
+    np.savez_compressed(os.path.join(HERE, "multilag.npz"), taus=np.array(taus), **out)
+    print("multilag.npz written to", HERE)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref_dir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) > 2 and sys.argv[2] == "multilag":
+        multilag(ref_dir)
+    else:
+        main(ref_dir)
+        multilag(ref_dir)
