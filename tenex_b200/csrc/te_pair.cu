@@ -54,7 +54,7 @@ struct TeParams {
   int tblock;     // targets per L2 block of the item order (pair-free mode)
   // global-memory overflow launch: pairs whose histogram does not fit shared
   // memory (only with coarsening off), one 32-bit slot of gslot_words per CTA
-  int gmem;
+  int overflow;   // an overflow launch exists: both launches filter pairs by slot_fits
   uint32_t* gslots;
   int64_t gslot_words;
   int64_t n_items;
@@ -264,7 +264,7 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
       if (src == tgt || p < P.p0 || p >= P.p1) continue;  // group-uniform skip
     }
     const uint32_t bs = (uint32_t)P.npv[src];
-    if (slot_fits(bt, bs, N, slot_region) == GMEM) continue;  // the other launch's pair
+    if (P.overflow && slot_fits(bt, bs, N, slot_region) == GMEM) continue;  // other launch's
     const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
     const uint8_t* srow = P.bins + (int64_t)src * P.ld;
     uint64_t slot_addr;
@@ -368,6 +368,9 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
 
 }  // namespace
 
+// GMEM = false: the shared-memory launch; true: the global-memory overflow launch
+// (separate code, so the common kernel carries none of the overflow path).
+template <bool GMEM>
 __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   const SmemLayout SL = smem_layout(P.N, P.zbytes, P.bmax);
@@ -389,14 +392,14 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   const int N = P.N;
 
   if (*(volatile int*)&P.ws->bad_data != 0) return;  // validation failed: do nothing
-  uint32_t* gslot = P.gmem ? P.gslots + (int64_t)blockIdx.x * P.gslot_words : nullptr;
-  if (P.gmem) {
+  uint32_t* gslot = GMEM ? P.gslots + (int64_t)blockIdx.x * P.gslot_words : nullptr;
+  if (GMEM) {
     for (int64_t i = tid; i < P.gslot_words; i += nthreads) gslot[i] = 0u;
     __syncthreads();
   }
 
   for (;;) {
-    if (tid == 0) misc[0] = (int)atomicAdd(P.gmem ? &P.ws->ov_ticket : &P.ws->ticket, 1u);
+    if (tid == 0) misc[0] = (int)atomicAdd(GMEM ? &P.ws->ov_ticket : &P.ws->ticket, 1u);
     __syncthreads();
     const int64_t q = (int64_t)misc[0];
     if (q >= P.n_items) break;
@@ -431,10 +434,10 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       hi = min((int64_t)(chunk + 1) * P.W, (int64_t)P.n);
       if (base + nm1 <= P.p0 || base >= P.p1) lo = hi;  // target outside the range
       // sources are sorted by bin count: skip a chunk this launch has no pair of
-      if (lo < hi) {
+      if (P.overflow && lo < hi) {
         const int btq = P.npv[tgt];
-        if (!P.gmem && !slot_fits(btq, P.npv[P.order[lo]], N, slot_region)) lo = hi;
-        if (P.gmem && slot_fits(btq, P.npv[P.order[hi - 1]], N, slot_region)) lo = hi;
+        if (!GMEM && !slot_fits(btq, P.npv[P.order[lo]], N, slot_region)) lo = hi;
+        if (GMEM && slot_fits(btq, P.npv[P.order[hi - 1]], N, slot_region)) lo = hi;
       }
     }
     if (lo >= hi) {
@@ -466,7 +469,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
         if (src == tgt || p < P.p0 || p >= P.p1) continue;
       }
       const int bsrc = P.npv[src];
-      if (!bad && slot_fits(bt, bsrc, N, slot_region) == (P.gmem != 0)) continue;
+      if (!bad && P.overflow && slot_fits(bt, bsrc, N, slot_region) == GMEM) continue;
       my_max = max(my_max, (unsigned)bsrc);
       mine = 1;
     }
@@ -475,7 +478,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       __syncthreads();
       continue;
     }
-    if (!__syncthreads_or(mine)) continue;  // no pair of this launch (uniform)
+    if (P.overflow && !__syncthreads_or(mine)) continue;  // no pair of this launch (uniform)
     my_max = dev::warp_max(my_max);
     if ((tid & 31) == 0) reinterpret_cast<unsigned*>(red)[warp] = my_max;
     for (int i = tid; i < bt2; i += nthreads) c2a_cnt[i] = 0;
@@ -517,9 +520,9 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     // (the overflow launch: the whole CTA on one 32-bit slot in global memory)
     const int words32 = (int)round_up((int64_t)bt2 * bsmax, 4);
     const int words16 = (int)round_up((int64_t)bt2 * ((bsmax + 1) >> 1), 4);
-    const int fit32 = P.gmem ? 1 : slot_region / (words32 * 4);
-    const int fit16 = P.gmem ? 0 : slot_region / (words16 * 4);
-    const bool pack16 = !P.gmem && (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
+    const int fit32 = GMEM ? 1 : slot_region / (words32 * 4);
+    const int fit16 = GMEM ? 0 : slot_region / (words16 * 4);
+    const bool pack16 = !GMEM && (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
     const int fit = pack16 ? fit16 : fit32;
     const int slot_words = pack16 ? words16 : words32;
     if (fit < 1) {
@@ -533,8 +536,8 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     const int n_groups = n_warps / G;
     const int g = warp / G;
     const int lane_g = tid - g * G * 32;
-    uint32_t* slot = P.gmem ? gslot : slots + (int64_t)g * slot_words;
-    if (!P.gmem)
+    uint32_t* slot = GMEM ? gslot : slots + (int64_t)g * slot_words;
+    if (!GMEM)
       for (int i = tid; i < n_groups * slot_words; i += nthreads) slots[i] = 0u;
     __syncthreads();
     for (int z = tid; z < bt2; z += nthreads) {
@@ -543,7 +546,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     }
     __syncthreads();
 
-    if (P.gmem)
+    if (GMEM)
       run_sources<false, true>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src,
                                bt, zsm, z8, c1s, qa, red, slot_region);
     else if (pack16)
@@ -834,6 +837,7 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
     P.gslots = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(workspace) +
                                            ws_total(n, b_max));
   }
+  P.overflow = overflow ? 1 : 0;
   int64_t grid = L.grid;
   if (grid > P.n_items) grid = P.n_items;
 
@@ -847,15 +851,16 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
     st = check_launch("source_order_kernel");
     if (st) return st;
   }
-  e = cudaFuncSetAttribute(te_pair_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(te_pair_tile_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            L.smem);
   if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
-  P.gmem = 0;
-  te_pair_tile_kernel<<<(int)grid, L.threads, L.smem, stream>>>(P);
+  te_pair_tile_kernel<false><<<(int)grid, L.threads, L.smem, stream>>>(P);
   st = check_launch("te_pair_tile_kernel");
   if (st || !overflow) return st;
-  P.gmem = 1;
-  te_pair_tile_kernel<<<(int)std::min<int64_t>(n_gslots, P.n_items), L.threads, L.smem,
+  e = cudaFuncSetAttribute(te_pair_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           L.smem);
+  if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+  te_pair_tile_kernel<true><<<(int)std::min<int64_t>(n_gslots, P.n_items), L.threads, L.smem,
                         stream>>>(P);
   return check_launch("te_pair_tile_kernel (global-memory overflow)");
 }
