@@ -76,8 +76,12 @@ __device__ __forceinline__ float cell_term(float c, float c1, float c2a, float c
   return c * __log2f(r);
 }
 
-// Pack: F[g, t] = x[g, t+lag], P[g, t] = x[g, t], FP = F & P for t < L (0 beyond),
-// plus nf, np, nfp. One CTA per gene.
+// Pack: F[g, t] = x[g, t+lag] != 0, P[g, t] = x[g, t] != 0, FP = F & P for t < L
+// (0 beyond, up to Lpad), plus nf, np, nfp. One CTA per gene; each thread makes
+// 16 bytes of each operand from 16-byte loads (F's source window is shifted by
+// lag, taken from two aligned loads), with a scalar path for the row end.
+__device__ __forceinline__ uint32_t nz01(uint32_t w) { return __vcmpne4(w, 0u) & 0x01010101u; }
+
 __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L,
                                int lag, int Lpad, uint8_t* __restrict__ ops,
                                int32_t* __restrict__ marg) {
@@ -87,18 +91,52 @@ __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int
   uint8_t* Pr = ops + ((int64_t)1 * n + g) * Lpad;
   uint8_t* FPr = ops + ((int64_t)2 * n + g) * Lpad;
   int nf = 0, np = 0, nfp = 0;
-  for (int t = threadIdx.x; t < Lpad; t += blockDim.x) {
-    uint8_t f = 0, p = 0;
-    if (t < L) {
-      f = row[t + lag] ? 1 : 0;
-      p = row[t] ? 1 : 0;
+  const int sh = lag & 15;
+  for (int t = threadIdx.x * 16; t < Lpad; t += blockDim.x * 16) {
+    uint32_t f[4], p[4];
+    const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;  // aligned start of F's window
+    if (t + 16 <= L && fa + 32 <= ld) {
+      const uint4 pv = *reinterpret_cast<const uint4*>(row + t);
+      const uint4 a = *reinterpret_cast<const uint4*>(row + fa);
+      const uint4 b = *reinterpret_cast<const uint4*>(row + fa + 16);
+      const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      const uint32_t pw[4] = {pv.x, pv.y, pv.z, pv.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        // bytes sh + 4k .. sh + 4k + 3 of the 32-byte window
+        const int byte = sh + 4 * k;
+        const uint32_t lo = w[byte >> 2], hi = w[(byte >> 2) + 1];
+        const uint32_t fw = __funnelshift_r(lo, hi, (byte & 3) * 8);
+        f[k] = nz01(fw);
+        p[k] = nz01(pw[k]);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        uint32_t fk = 0, pk = 0;
+        for (int j = 0; j < 4; ++j) {
+          const int tt = t + 4 * k + j;
+          if (tt < L) {
+            fk |= (row[tt + lag] ? 1u : 0u) << (8 * j);
+            pk |= (row[tt] ? 1u : 0u) << (8 * j);
+          }
+        }
+        f[k] = fk;
+        p[k] = pk;
+      }
     }
-    Fr[t] = f;
-    Pr[t] = p;
-    FPr[t] = f & p;
-    nf += f;
-    np += p;
-    nfp += f & p;
+    const uint4 fv = make_uint4(f[0], f[1], f[2], f[3]);
+    const uint4 pv4 = make_uint4(p[0], p[1], p[2], p[3]);
+    const uint4 fpv = make_uint4(f[0] & p[0], f[1] & p[1], f[2] & p[2], f[3] & p[3]);
+    *reinterpret_cast<uint4*>(Fr + t) = fv;
+    *reinterpret_cast<uint4*>(Pr + t) = pv4;
+    *reinterpret_cast<uint4*>(FPr + t) = fpv;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      nf += __popc(f[k]);
+      np += __popc(p[k]);
+      nfp += __popc(f[k] & p[k]);
+    }
   }
   __shared__ int red[3][32];
 #pragma unroll
@@ -341,6 +379,8 @@ extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_var
   if (lag < 1 || row_len <= lag)
     return fail(TENEX_ERR_BADARG, "need 1 <= lag < row_len");
   if (ld < row_len) return fail(TENEX_ERR_BADARG, "ld must be >= row_len");
+  if ((ld & 15) || (reinterpret_cast<uintptr_t>(bins) & 15))
+    return fail(TENEX_ERR_BADARG, "bins and ld must be 16-byte aligned");
   if (out_ld < n_vars) return fail(TENEX_ERR_BADARG, "out_ld must be >= n_vars");
   const int64_t L = row_len - lag;
   if (L >= ((int64_t)1 << 24))
