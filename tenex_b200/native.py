@@ -141,11 +141,41 @@ def check(status: int, where: str) -> None:
         raise TenexError(status, where, last_error())
 
 
+_FAULT_CODES = {"bad_arg": TENEX_ERR_BADARG, "bad_shape": TENEX_ERR_BADARG,
+                "unsupported": TENEX_ERR_UNSUPPORTED, "oom": TENEX_ERR_OOM,
+                "launch_fail": TENEX_ERR_LAUNCH, "timeout": TENEX_ERR_TIMEOUT,
+                "bad_data": TENEX_ERR_BADDATA}
+
+
+def _injected_fault(name: str) -> int:
+    """Host-side fault injection: TENEX_FAULT="kind[:symbol]" (kind in _FAULT_CODES)
+    makes call() raise that status for `symbol` (every status-returning entry
+    point if omitted) without running it, so the error paths can be exercised
+    with no GPU fault."""
+    spec = os.environ.get("TENEX_FAULT")
+    if not spec:
+        return TENEX_OK
+    kind, _, sym = spec.partition(":")
+    if sym and sym != name:
+        return TENEX_OK
+    if kind not in _FAULT_CODES:
+        raise ValueError(f"TENEX_FAULT kind {kind!r} not in {sorted(_FAULT_CODES)}")
+    return _FAULT_CODES[kind]
+
+
 def call(name: str, *args) -> None:
+    fault = _injected_fault(name)
+    if fault:
+        raise TenexError(fault, name, f"injected by TENEX_FAULT={os.environ['TENEX_FAULT']}")
     check(getattr(lib(), name)(*args), name)
 
 
 def stream_ptr(stream: torch.cuda.Stream | None = None) -> int:
+    """The stream handle for the C ABI (the current stream; 0, the legacy default
+    stream, when this process sees no CUDA device, in which case every entry point
+    fails with its own status)."""
+    if stream is None and not torch.cuda.is_available():
+        return 0
     s = stream if stream is not None else torch.cuda.current_stream()
     return int(s.cuda_stream)
 

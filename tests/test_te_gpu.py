@@ -184,11 +184,18 @@ def test_bad_bins_raise_without_fault(cuda):
 
 
 def test_determinism(cuda):
+    # items are handed out by an atomic ticket, but each pair's counts and the order
+    # of its entropy sum are fixed: repeated runs give identical integers and float bits
     rng = np.random.default_rng(8)
     bins, npv, bmax = _rand_bins(rng, 30, 2000, 2, 16)
-    a = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
-    b = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
-    assert np.array_equal(a, b)
+    P, stride = 30 * 29, bmax ** 3
+    runs = []
+    for _ in range(2):
+        counts = torch.zeros((P, stride), dtype=torch.int32, device=cuda)
+        te = _gpu_te(bins, npv, bmax, cuda, counts=counts, counts_stride=stride)
+        runs.append((te.cpu().numpy().view(np.uint32), counts.cpu().numpy()))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
 
 
 def test_skewed_bins_dominant_value_derivation(cuda):
