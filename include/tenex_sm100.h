@@ -219,6 +219,16 @@ int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t 
 int tenex_b2_status(const void* workspace, int n_vars, int64_t row_len, int64_t lag,
                     void* stream);
 
+/* DPI trimming of the FDR method's network; replaces the row-batched torch loop
+ * of _trim (tenex/inference/fdr.py:61-133). te: n x n float (kept edges, 0
+ * elsewhere), row stride ld. out[i*out_ld + j] = te[i][j] if keep_all[i], else
+ * te[i][j] when te[i][j] >= max(0, max_{k: mediator[k]} min(te[i][k], te[k][j]))
+ * + trim_threshold, else 0 (float32 sum and compare as in the reference).
+ * mediator / keep_all: n bytes each, NULL = all k / no row. out must not alias te. */
+int tenex_dpi_trim(const float* te, int64_t ld, int n_vars, const uint8_t* mediator,
+                   const uint8_t* keep_all, float trim_threshold, float* out, int64_t out_ld,
+                   void* stream);
+
 /* ---- Learned null model of the surrogate test (no reference counterpart) ----
  * MLP 16 -> 64 -> 64 -> 2 (GELU), parameters W1[64][16] b1[64] W2[64][64] b2[64]
  * W3[2][64] b3[2] (tenex_mlp_param_count() values), BF16 for the forward,

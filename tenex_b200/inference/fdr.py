@@ -1,0 +1,138 @@
+"""FDR inference: z-score -> Benjamini-Hochberg -> optional DPI trimming.
+
+Mirrors FDRMethod (tenex/inference/fdr.py:16-58) and the thresholding helpers
+of tenex/inference/__init__.py:129-162 with the same arguments (fdr=0.01,
+links=0, sources, is_trimming=True, trim_threshold=0.0, batch_size=512) and
+return values (GRN, or (GRN, trimmed GRN) with trimming). Thresholding runs on
+the device as the reference's GPU branch does (z-score with the unbiased std,
+p = erfc(z / sqrt 2) / 2, BH, keep adjusted p < fdr; or the `links` largest);
+the trimming step's (max, min) matrix product over the mediators is the CUDA
+kernel tenex_dpi_trim.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from tenex_b200 import _log, native
+from tenex_b200.inference.grn import bh_fdr_gpu, build_pairs, make_grn
+
+
+def fdr_threshold_gpu(te: torch.Tensor, pairs: torch.Tensor, fdr: float):
+    """Edges whose BH-adjusted one-sided z-score p-value is below `fdr`
+    (tenex/inference/__init__.py:129-139)."""
+    std = te.std()
+    if std == 0:
+        return torch.empty(0, device=te.device), pairs[:0]
+    z = (te - te.mean()) / std
+    pval = 0.5 * torch.erfc(z / 1.4142135623730951)
+    adj = bh_fdr_gpu(pval, 0.05)
+    mask = adj < fdr
+    return te[mask], pairs[mask]
+
+
+def threshold_pairs(te: torch.Tensor, pairs: torch.Tensor, fdr: float = 0.01, links: int = 0):
+    """Top-`links` or FDR thresholding (tenex/inference/__init__.py:155-170);
+    returns numpy (te_cut, pairs_cut)."""
+    if links > 0:
+        k = min(links, len(te))
+        _, idx = te.topk(k)
+        idx = idx[te[idx].argsort(descending=True)]
+        return te[idx].cpu().numpy(), pairs[idx].cpu().numpy()
+    te_c, p_c = fdr_threshold_gpu(te, pairs, fdr)
+    return te_c.cpu().numpy(), p_c.cpu().numpy()
+
+
+def dpi_trim_matrix(arr: torch.Tensor, mediator: torch.Tensor | None = None,
+                    keep_all: torch.Tensor | None = None, trim_threshold: float = 0.0,
+                    out: torch.Tensor | None = None) -> torch.Tensor:
+    """tenex_dpi_trim on a float32 (n, n) device matrix: entries that survive the
+    DPI test (or whole rows flagged keep_all), zero elsewhere."""
+    if arr.dim() != 2 or arr.shape[0] != arr.shape[1] or arr.dtype != torch.float32:
+        raise ValueError("arr must be a square float32 matrix")
+    if arr.device.type != "cuda":
+        raise RuntimeError("DPI trimming runs on a CUDA device; got " + str(arr.device))
+    arr = arr.contiguous()
+    n = arr.shape[0]
+    if out is None:
+        out = torch.empty_like(arr)
+
+    def _mask(m):
+        if m is None:
+            return None
+        m = m.to(device=arr.device, dtype=torch.uint8).contiguous()
+        if m.numel() != n:
+            raise ValueError("mediator / keep_all must have n entries")
+        return m
+    med, keep = _mask(mediator), _mask(keep_all)
+    native.call("tenex_dpi_trim", arr.data_ptr(), n, n,
+                med.data_ptr() if med is not None else None,
+                keep.data_ptr() if keep is not None else None,
+                ctypes.c_float(trim_threshold), out.data_ptr(), out.stride(0), native.stream_ptr())
+    return out
+
+
+def dpi_trim(n: int, variable_names, pairs: np.ndarray, te_values: np.ndarray,
+             device: torch.device, batch_size: int = 512, trim_threshold: float = 0.0):
+    """Trimmed GRN of the kept edges (tenex/inference/fdr.py:61-133): mediators
+    are rows with a positive sum; row batches of `batch_size` without an active
+    mediator are kept whole; the rest keep A[i,j] >= indirect + trim_threshold."""
+    pairs = np.asarray(pairs)
+    arr = torch.zeros((n, n), dtype=torch.float32, device=device)
+    if len(pairs):
+        p = torch.as_tensor(pairs, dtype=torch.long, device=device)
+        arr[p[:, 0], p[:, 1]] = torch.as_tensor(np.asarray(te_values, np.float32), device=device)
+    mediator = arr.sum(dim=1) > 0
+    if not bool(mediator.any()):
+        return make_grn(variable_names, pairs, np.asarray(te_values))
+    # a batch is active when one of its nonzero columns is a mediator
+    row_active = ((arr != 0) & mediator[None, :]).any(dim=1)
+    nb = (n + batch_size - 1) // batch_size
+    pad = nb * batch_size - n
+    batch_active = torch.nn.functional.pad(row_active, (0, pad)).view(nb, batch_size).any(dim=1)
+    keep_all = (~batch_active).repeat_interleave(batch_size)[:n]
+    out = dpi_trim_matrix(arr, mediator, keep_all, trim_threshold)
+    rows, cols = torch.nonzero(out, as_tuple=True)
+    if rows.numel() == 0:
+        return make_grn(variable_names, np.empty((0, 2), dtype=np.int32),
+                        np.empty(0, dtype=np.float32))
+    vals = out[rows, cols].cpu().numpy()
+    kept = torch.stack((rows, cols), dim=1).cpu().numpy()
+    return make_grn(variable_names, kept, vals)
+
+
+class FDRMethod:
+    """'fdr' inference method (tenex/inference/fdr.py:16-58)."""
+
+    @property
+    def name(self) -> str:
+        return "fdr"
+
+    def infer(self, te_matrix, variable_names, device, **kwargs):
+        fdr = kwargs.get("fdr", 0.01)
+        links = kwargs.get("links", 0)
+        sources = kwargs.get("sources", None)
+        is_trimming = kwargs.get("is_trimming", True)
+        trim_threshold = kwargs.get("trim_threshold", 0.0)
+        batch_size = kwargs.get("batch_size", 512)
+        device = torch.device(device)
+        if device.type != "cuda":
+            raise RuntimeError("the fdr method runs on a CUDA device in this package; got "
+                               f"{device}")
+        variable_names = np.asarray(variable_names)
+        pairs_np = build_pairs(variable_names, sources)
+        te_matrix = np.asarray(te_matrix, dtype=np.float32)
+        pairs_t = torch.from_numpy(np.ascontiguousarray(pairs_np)).to(device, dtype=torch.long)
+        M = torch.from_numpy(te_matrix).to(device)
+        te_t = M[pairs_t[:, 0], pairs_t[:, 1]]
+        te_cut, pairs_cut = threshold_pairs(te_t, pairs_t, fdr=fdr, links=links)
+        grn = make_grn(variable_names, pairs_cut, te_cut)
+        _log.vprint(f"[TENEX] inference(fdr): {len(grn)} links after thresholding")
+        if not is_trimming:
+            return grn
+        trimmed = dpi_trim(te_matrix.shape[0], variable_names, pairs_cut, te_cut, device,
+                           batch_size=batch_size, trim_threshold=trim_threshold)
+        _log.vprint(f"[TENEX] inference(fdr): {len(trimmed)} links after trimming")
+        return grn, trimmed

@@ -35,13 +35,18 @@ class NetWeaver:
         self.is_trimming = is_trimming
         self.trim_threshold = trim_threshold
 
-    def infer(self, method: str = "surrogate_test", device=None, verbose: bool = False, **kwargs):
+    def infer(self, method: str = "fdr", device=None, verbose: bool = False, **kwargs):
+        """'fdr' -> GRN, or (GRN, trimmed GRN) with trimming; 'surrogate_test' ->
+        SurrogateTestResult (tenex/inference/netweaver.py:77-165)."""
         from tenex_b200.inference import get_method
         _log.set_verbose(verbose)
         dev = torch.device(device) if device is not None else torch.device("cuda", 0)
         m = get_method(method)
-        params = dict(fdr=self.fdr, sources=self.sources)
+        params = dict(fdr=self.fdr, links=self.links, sources=self.sources,
+                      is_trimming=self.is_trimming, trim_threshold=self.trim_threshold)
         if method == "surrogate_test":
+            for drop in ("links", "is_trimming", "trim_threshold"):
+                params.pop(drop)
             if "bin_data" not in kwargs and self.bin_arrs is not None:
                 params["bin_data"] = self.bin_arrs
             if "n_per_var" not in kwargs and self.n_per_var is not None:

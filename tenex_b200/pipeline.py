@@ -7,9 +7,9 @@ _combine_surrogate_multi_lag :316-410), which re-runs the TE hot path and the
 surrogate test once per lag and merges the per-lag results per pair ("max":
 lag with the largest effective TE; "adaptive_select": smallest p; "weighted_sum":
 effective TE summed with weights -log p for p < 0.05), with a Bonferroni p
-(K * min p) and BH-FDR over the off-diagonal pairs. Only the surrogate test is an
-inference method here (the matrix methods FDR/CLR/ND/POINT are outside this
-build and raise NotImplementedError).
+(K * min p) and BH-FDR over the off-diagonal pairs. infer() dispatches to the
+registered methods ('surrogate_test', 'fdr'); CLR/ND/TRACE/POINT are not part of
+this package and raise NotImplementedError.
 """
 from __future__ import annotations
 
@@ -108,23 +108,22 @@ class Pipeline:
         if taus is not None:
             return self._infer_multi_lag(taus=taus, combine=lag_combine,
                                          inference_method=method, **kwargs)
-        if method not in _FUSED_METHODS:
-            raise NotImplementedError(f"inference method {method!r} is outside this build; "
-                                      f"available: {sorted(_FUSED_METHODS)}")
         from tenex_b200.inference import get_method
         params = {**self._defaults, **kwargs}
+        method_obj = get_method(method)
         te = self.te_result
         device = params.pop("device", None)
         device = torch.device("cuda", 0) if device is None else torch.device(device)
-        params.setdefault("bin_data", te.bin_arrs)
-        params.setdefault("n_per_var", te.n_per_var)
-        params.setdefault("b_max", te.b_max)
-        params.setdefault("kernel", te.kernel)
-        params.setdefault("tau", te.tau)
+        if method in _FUSED_METHODS:
+            params.setdefault("bin_data", te.bin_arrs)
+            params.setdefault("n_per_var", te.n_per_var)
+            params.setdefault("b_max", te.b_max)
+            params.setdefault("kernel", te.kernel)
+            params.setdefault("tau", te.tau)
         sources = getattr(self.engine, "_sources", None)
         if sources is not None:
             params.setdefault("sources", sources)
-        return get_method(method).infer(te.matrix, te.variable_names, device, **params)
+        return method_obj.infer(te.matrix, te.variable_names, device, **params)
 
     def _infer_multi_lag(self, taus: list[int], combine: str = "max",
                          inference_method: str = "surrogate_test", **kwargs) -> Any:

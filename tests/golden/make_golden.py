@@ -19,9 +19,12 @@ product to the reference's own CPU code paths:
   smem_limit.npz        compute_smem_bin_limit for a few SMEM sizes
   multilag.npz          Pipeline._combine_surrogate_multi_lag (max, adaptive_select,
                         weighted_sum) on three synthetic per-lag surrogate results
+  fdr_trim.npz          the FDR method's thresholding (fdr_threshold_gpu, top-K) and
+                        DPI trimming (_trim) on CPU tensors, for a synthetic TE matrix
+                        with planted direct and indirect edges
 
-`python tests/golden/make_golden.py /path/to/reference multilag` writes only the
-last one.
+`python tests/golden/make_golden.py /path/to/reference multilag` (or `fdr`) writes
+only that one.
 """
 from __future__ import annotations
 
@@ -180,10 +183,71 @@ def multilag(ref: str) -> None:
     print("multilag.npz written to", HERE)
 
 
+def fdr_te_matrix(n: int = 150, seed: int = 31) -> tuple[np.ndarray, list]:
+    """Synthetic TE matrix: small background, planted chains a -> b -> c with a
+    weaker direct a -> c (an indirect edge DPI removes), a few exact ties and
+    exact zeros."""
+    rng = np.random.default_rng(seed)
+    m = (rng.gamma(2.0, 0.002, (n, n))).astype(np.float32)
+    m[rng.random((n, n)) < 0.05] = 0.0
+    chains = []
+    for c in range(12):
+        a, b, d = rng.choice(n, 3, replace=False)
+        ab, bd = np.float32(0.2 + 0.02 * c), np.float32(0.15 + 0.01 * c)
+        m[a, b], m[b, d] = ab, bd
+        m[a, d] = np.float32(0.1) if c % 3 else bd     # c % 3 == 0: a tie with min(ab, bd)
+        chains.append((a, b, d))
+    np.fill_diagonal(m, 0.0)
+    return m, chains
+
+
+def fdr(ref: str) -> None:
+    """The reference's FDR thresholding and DPI trimming on CPU tensors."""
+    sys.path.insert(0, ref)
+    os.environ.setdefault("TENEX_CPU_ONLY", "1")
+    import torch
+    from tenex.inference import build_pairs, fdr_threshold_gpu, threshold_pairs
+    from tenex.inference.fdr import _trim
+
+    cpu = torch.device("cpu")
+    m, _ = fdr_te_matrix()
+    n = m.shape[0]
+    names = np.array([f"g{i}" for i in range(n)])
+    pairs = build_pairs(names)
+    te = m[pairs[:, 0], pairs[:, 1]]
+    out = {"matrix": m}
+    cases = [("a", dict(fdr=0.01, links=0, thr=0.0, bs=512)),
+             ("b", dict(fdr=0.05, links=0, thr=0.001, bs=7)),
+             ("c", dict(fdr=0.01, links=300, thr=0.0, bs=64)),
+             ("d", dict(fdr=0.2, links=0, thr=-0.01, bs=33)),
+             ("e", dict(fdr=0.05, links=0, thr=0.15, bs=5))]
+    for tag, c in cases:
+        te_t = torch.from_numpy(te)
+        pairs_t = torch.from_numpy(pairs).long()
+        if c["links"]:
+            te_cut, pairs_cut = threshold_pairs(te_t, pairs_t, cpu, fdr=c["fdr"], links=c["links"])
+        else:
+            tc, pc = fdr_threshold_gpu(te_t, pairs_t, c["fdr"])
+            te_cut, pairs_cut = tc.numpy(), pc.numpy()
+        grn = _trim(m, names, pairs_cut, te_cut, device=cpu, batch_size=c["bs"],
+                    trim_threshold=c["thr"])
+        out[f"{tag}_cfg"] = np.array([c["fdr"], c["links"], c["thr"], c["bs"]], np.float64)
+        out[f"{tag}_cut_pairs"] = np.asarray(pairs_cut)
+        out[f"{tag}_cut_te"] = np.asarray(te_cut, np.float32)
+        out[f"{tag}_trim_pairs"] = np.asarray(grn.pairs)
+        out[f"{tag}_trim_te"] = np.asarray(grn.te, np.float32)
+    np.savez_compressed(os.path.join(HERE, "fdr_trim.npz"), **out)
+    print("fdr_trim.npz written to", HERE)
+
+
 if __name__ == "__main__":
     ref_dir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    if len(sys.argv) > 2 and sys.argv[2] == "multilag":
+    only = sys.argv[2] if len(sys.argv) > 2 else None
+    if only == "multilag":
         multilag(ref_dir)
+    elif only == "fdr":
+        fdr(ref_dir)
     else:
         main(ref_dir)
         multilag(ref_dir)
+        fdr(ref_dir)
