@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kThreads, 2) dpi_trim_kernel(DpiArgs P) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) acc[r][c] = 0.f;
 
-  float ra[8], rb[8];
+  float ra[8] = {}, rb[8] = {};
   auto stage = [&](int buf) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) As[buf][(t & 1) * 8 + q][t >> 1] = ra[q];
