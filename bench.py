@@ -311,6 +311,7 @@ def run_ours(args) -> None:
     cpu = cpu_baseline(*_coarsened_host(x, npv, limit)) if not args.no_cpu_baseline else None
     sur = surrogate_leg(dev) if (world == 1 and not args.no_surrogate) else None
     binl = binary_leg(dev) if (world == 1 and not args.no_surrogate) else None
+    fdrl = fdr_leg(dev, out) if (world == 1 and not args.no_fdr and total == G * (G - 1)) else None
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
@@ -325,7 +326,7 @@ def run_ours(args) -> None:
             "gpu_launches": 6 * args.steps,  # remap, coarsen x2, prepass, order, TE tile
             "roofline": roofline, "roofline_hbm": roofline_hbm,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "surrogate": sur,
-            "binary_path": binl}
+            "binary_path": binl, "fdr": fdrl}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -416,6 +417,55 @@ def binary_leg(dev, reps: int = 5) -> dict:
                                  "pack + GEMM; peak = tenex_probe_tc_int8 measured live"}}
 
 
+def fdr_leg(dev, mat, reps: int = 2) -> dict:
+    """NetWeaver's default method on the TE matrix just computed: z-score, BH-FDR
+    0.01 and DPI trimming (FDRMethod.infer from a host matrix, wall seconds, median
+    of `reps` after a warm-up call), and the DPI kernel's device time on the
+    thresholded network against the live FP32 min/max probe."""
+    import torch
+
+    from tenex_b200 import native
+    from tenex_b200.inference.fdr import FDRMethod, dpi_trim_matrix
+    n = mat.shape[0]
+    names = np.array([f"g{i}" for i in range(n)])
+    host = mat.cpu().numpy()
+    m = FDRMethod()
+    ts = []
+    for _ in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        grn, trimmed = m.infer(host, names, dev, fdr=0.01)
+        torch.cuda.synchronize(dev)
+        ts.append(time.perf_counter() - t0)
+    arr = torch.zeros((n, n), dtype=torch.float32, device=dev)
+    if len(grn):
+        p = torch.as_tensor(grn.pairs, dtype=torch.long, device=dev)
+        arr[p[:, 0], p[:, 1]] = torch.as_tensor(grn.te, device=dev)
+    med = arr.sum(dim=1) > 0
+    res = torch.empty_like(arr)
+    dpi_trim_matrix(arr, med, None, 0.0, out=res)
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(reps)]
+    for a, b in ev:
+        a.record()
+        dpi_trim_matrix(arr, med, None, 0.0, out=res)
+        b.record()
+    torch.cuda.synchronize(dev)
+    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    instr = 1.5 * float(n) ** 3          # one min per k, one three-input max per two k
+    peak = max(native.probe_minmax() for _ in range(2))
+    return {"workload": f"TE matrix of {n} genes, fdr=0.01, DPI trimming (threshold 0)",
+            "metric": "FDRMethod.infer wall seconds from a host matrix (median of %d after a "
+                      "warm-up call)" % reps,
+            "seconds": statistics.median(ts[1:]), "edges": len(grn), "edges_trimmed": len(trimmed),
+            "density": len(grn) / float(n * (n - 1)), "dpi_ms": ms,
+            "roofline": {"bound": "fp32 min/max issue", "achieved": instr / (ms / 1e3) / 1e12,
+                         "peak": peak / 1e12, "unit": "T instr/s", "frac": instr / (ms / 1e3) / peak,
+                         "note": "achieved = 1.5 n^3 min/max instructions / DPI kernel device "
+                                 "time; peak = tenex_probe_minmax measured live"}}
+
+
 def _coarsened_host(x, npv, limit):
     from oracle import oracle as O
     cb, cnpv, bmax = O.coarsen(x, npv, limit)
@@ -432,7 +482,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
-    ap.add_argument("--only", choices=["binary", "surrogate"], default=None,
+    ap.add_argument("--no-fdr", action="store_true")
+    ap.add_argument("--only", choices=["binary", "surrogate", "fdr"], default=None,
                     help="run one side leg alone and print its JSON object (profiling)")
     ap.add_argument("--genes", type=int, default=N_GENES)
     ap.add_argument("--cells", type=int, default=N_CELLS)
@@ -449,6 +500,17 @@ def main():
     elif args.only == "surrogate":
         import torch
         print(json.dumps(surrogate_leg(torch.device("cuda", 0))), flush=True)
+    elif args.only == "fdr":
+        import torch
+
+        from tenex_b200 import workloads as W
+        from tenex_b200.kernels import device as D
+        from tenex_b200.kernels.full_smem import FullSMEMKernel
+        dev = torch.device("cuda", 0)
+        x, npv, _ = W.cfg5_bins(seed=1005)
+        mat = FullSMEMKernel().compute_pairfree_device(
+            D.pack_bins(x, dev), torch.as_tensor(npv, device=dev), int(npv.max()), 1, matrix=True)
+        print(json.dumps(fdr_leg(dev, mat)), flush=True)
     else:
         run_ours(args)
 

@@ -283,6 +283,11 @@ int tenex_probe_smem_atomics(int mode, int iters, int64_t* increments, float* ms
  * into TMEM; returns the operation count (2*M*N*K per MMA) and the milliseconds.
  * Synchronises `stream`; TENEX_ERR_TIMEOUT if the bounded completion wait expired. */
 int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stream);
+/* Roofline probe (no reference counterpart): FP32 min/max issue rate, the bound of
+ * tenex_dpi_trim. Every thread of 2 CTAs x 1024 threads per SM runs `iters` steps
+ * of 8 independent chains (two min.f32 and one three-input max.f32 each); returns
+ * the instruction count and the milliseconds. Synchronises `stream`. */
+int tenex_probe_minmax(int iters, double* instructions, float* ms, void* stream);
 
 #ifdef __cplusplus
 }

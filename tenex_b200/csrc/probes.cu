@@ -179,3 +179,60 @@ extern "C" int tenex_probe_smem_atomics(int mode, int iters, int64_t* increments
   *increments = (int64_t)grid * block * iters;
   return st;
 }
+
+// ---- FP32 min/max issue rate (denominator of the DPI trimming kernel) -------
+// Eight independent chains per thread, each step one three-input max.f32 and two
+// min.f32 (the DPI kernel's instruction mix); volatile asm keeps every
+// instruction. 2 CTAs of 1024 threads per SM.
+namespace {
+__global__ void __launch_bounds__(1024, 2) minmax_probe(int iters, float seed, float* sink) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = seed + (float)(threadIdx.x + k);
+  const float x = seed * 0.5f, y = seed * 0.25f;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      float m1, m2;
+      asm volatile("min.f32 %0, %1, %2;" : "=f"(m1) : "f"(a[k]), "f"(x));
+      asm volatile("min.f32 %0, %1, %2;" : "=f"(m2) : "f"(a[(k + 1) & 7]), "f"(y));
+      asm volatile("max.f32 %0, %1, %2, %3;" : "=f"(a[k]) : "f"(a[k]), "f"(m1), "f"(m2));
+    }
+  }
+  float t = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) t += a[k];
+  if (t == 12345.678f) sink[0] = t;  // never true for the probe's inputs; keeps the chains live
+}
+}  // namespace
+
+extern "C" int tenex_probe_minmax(int iters, double* instructions, float* ms, void* stream_) {
+  if (iters < 1 || !instructions || !ms)
+    return fail(TENEX_ERR_BADARG, "iters >= 1, outputs non-NULL");
+  DevAttr A;
+  int st = current_device_attr(&A);
+  if (st) return st;
+  cudaStream_t s = as_stream(stream_);
+  float* sink = nullptr;
+  cudaError_t e = cudaMallocAsync(&sink, sizeof(float), s);
+  if (e != cudaSuccess) return check_cuda(e, "cudaMallocAsync");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int grid = 2 * A.sm_count, block = 1024;
+  minmax_probe<<<grid, block, 0, s>>>(iters, 1.5f, sink);  // warm-up
+  cudaEventRecord(e0, s);
+  minmax_probe<<<grid, block, 0, s>>>(iters, 1.5f, sink);
+  cudaEventRecord(e1, s);
+  st = check_launch("minmax_probe");
+  e = cudaEventSynchronize(e1);
+  if (!st && e != cudaSuccess) st = check_cuda(e, "cudaEventSynchronize");
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(sink, s);
+  *ms = t;
+  *instructions = (double)grid * block * iters * 8.0 * 3.0;
+  return st;
+}

@@ -33,6 +33,33 @@ def fdr_threshold_gpu(te: torch.Tensor, pairs: torch.Tensor, fdr: float):
     return te[mask], pairs[mask]
 
 
+class _LazyPairs:
+    """(src, tgt) rows of the all-pairs list for pair ids, computed on indexing
+    (src = id // (n-1), tgt = id % (n-1) skipping the diagonal)."""
+
+    def __init__(self, n: int, device):
+        self.n, self.device = n, device
+
+    def __len__(self):
+        return self.n * (self.n - 1)
+
+    def __getitem__(self, idx):
+        if isinstance(idx, torch.Tensor) and idx.dtype == torch.bool:
+            idx = idx.nonzero(as_tuple=True)[0]
+        elif isinstance(idx, slice):
+            idx = torch.arange(len(self), device=self.device)[idx]
+        idx = torch.as_tensor(idx, device=self.device, dtype=torch.long)
+        src = idx // max(self.n - 1, 1)
+        t = idx - src * (self.n - 1)
+        return torch.stack((src, t + (t >= src).long()), dim=1)
+
+
+def _offdiag(M: torch.Tensor):
+    n = M.shape[0]
+    te = M[~torch.eye(n, dtype=torch.bool, device=M.device)]
+    return te, _LazyPairs(n, M.device)
+
+
 def threshold_pairs(te: torch.Tensor, pairs: torch.Tensor, fdr: float = 0.01, links: int = 0):
     """Top-`links` or FDR thresholding (tenex/inference/__init__.py:155-170);
     returns numpy (te_cut, pairs_cut)."""
@@ -122,11 +149,17 @@ class FDRMethod:
             raise RuntimeError("the fdr method runs on a CUDA device in this package; got "
                                f"{device}")
         variable_names = np.asarray(variable_names)
-        pairs_np = build_pairs(variable_names, sources)
         te_matrix = np.asarray(te_matrix, dtype=np.float32)
-        pairs_t = torch.from_numpy(np.ascontiguousarray(pairs_np)).to(device, dtype=torch.long)
-        M = torch.from_numpy(te_matrix).to(device)
-        te_t = M[pairs_t[:, 0], pairs_t[:, 1]]
+        M = torch.as_tensor(te_matrix).to(device)
+        if sources is None:
+            # build_pairs' all-pairs order is the row-major off-diagonal order of
+            # M[src, tgt]: select it on the device instead of materialising the
+            # n(n-1) x 2 index array on the host
+            te_t, pairs_t = _offdiag(M)
+        else:
+            pairs_np = build_pairs(variable_names, sources)
+            pairs_t = torch.from_numpy(np.ascontiguousarray(pairs_np)).to(device, dtype=torch.long)
+            te_t = M[pairs_t[:, 0], pairs_t[:, 1]]
         te_cut, pairs_cut = threshold_pairs(te_t, pairs_t, fdr=fdr, links=links)
         grn = make_grn(variable_names, pairs_cut, te_cut)
         _log.vprint(f"[TENEX] inference(fdr): {len(grn)} links after thresholding")

@@ -98,6 +98,8 @@ _SIGS = {
                                  ctypes.POINTER(ctypes.c_float), _P],
     "tenex_probe_tc_int8": [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float),
                             _P],
+    "tenex_probe_minmax": [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float),
+                           _P],
 }
 _RESTYPES = {"tenex_te_workspace_bytes": ctypes.c_size_t,
              "tenex_b2_workspace_bytes": ctypes.c_size_t,
@@ -208,3 +210,11 @@ def probe_tc_int8(iters: int = 100_000) -> float:
     ms = ctypes.c_float()
     call("tenex_probe_tc_int8", int(iters), ctypes.byref(ops), ctypes.byref(ms), stream_ptr())
     return ops.value / (ms.value * 1e-3)
+
+
+def probe_minmax(iters: int = 20_000) -> float:
+    """Measured FP32 min/max instructions per second over all SMs."""
+    ins = ctypes.c_double()
+    ms = ctypes.c_float()
+    call("tenex_probe_minmax", int(iters), ctypes.byref(ins), ctypes.byref(ms), stream_ptr())
+    return ins.value / (ms.value * 1e-3)
