@@ -228,6 +228,14 @@ int tenex_b2_status(const void* workspace, int n_vars, int64_t row_len, int64_t 
 int tenex_dpi_trim(const float* te, int64_t ld, int n_vars, const uint8_t* mediator,
                    const uint8_t* keep_all, float trim_threshold, float* out, int64_t out_ld,
                    void* stream);
+/* Sparse form of tenex_dpi_trim (same rule, same results) for networks given in
+ * CSR: row_ptr[n_vars + 1] (int64), col / val the nonzero entries (columns
+ * ascending within a row). keep[e] = 1 if entry e survives, else 0. Work is
+ * sum over k of (positive entries into k) x (positive entries out of k); one row
+ * of n_vars floats must fit shared memory (TENEX_ERR_UNSUPPORTED otherwise). */
+int tenex_dpi_trim_sparse(const int64_t* row_ptr, const int32_t* col, const float* val,
+                          int n_vars, const uint8_t* mediator, const uint8_t* keep_all,
+                          float trim_threshold, uint8_t* keep, void* stream);
 
 /* ---- Learned null model of the surrogate test (no reference counterpart) ----
  * MLP 16 -> 64 -> 64 -> 2 (GELU), parameters W1[64][16] b1[64] W2[64][64] b2[64]

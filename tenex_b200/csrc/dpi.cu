@@ -13,7 +13,7 @@
 // active mediator, which the reference keeps unfiltered (fdr.py:98-104).
 // min/max select one of their inputs, so the result is exact in float32.
 //
-// The (max, min) product runs on the FP32 min/max pipe: 128 x 128 output tile
+// Dense form: the (max, min) product runs on the FP32 min/max pipe: 128 x 128 output tile
 // per CTA, 8 x 8 per thread, K slices of 16 staged through double-buffered
 // shared memory. Two k steps share one three-input max (sm_100 max.f32 with
 // three sources): three min/max instructions per (i, j) and two k.
@@ -139,10 +139,81 @@ __global__ void __launch_bounds__(kThreads, 2) dpi_trim_kernel(DpiArgs P) {
   }
 }
 
+// ---- sparse form ------------------------------------------------------------
+// Only positive A[i][k] and A[k][j] can raise indirect[i][j] above its starting
+// zero, so the product needs, for each row i, the rows k of its positive entries
+// (k a mediator) and their positive entries: sum_k indeg(k) * outdeg(k) updates
+// instead of n^3. The network is given in CSR (row_ptr, col, val: the nonzero
+// entries, columns ascending within a row). One CTA per row i keeps
+// indirect[i][.] in shared memory as the bit patterns of non-negative floats,
+// whose unsigned order is their numeric order, so atomicMax on them is the float
+// maximum; each warp takes one entry (k, v) of row i at a time and its lanes walk
+// row k. The result is one keep flag per CSR entry with the dense kernel's rule
+// (entries whose column lies outside [0, n) are ignored and never kept).
+constexpr int kSparseThreads = 256;
+
+__global__ void __launch_bounds__(kSparseThreads) dpi_trim_sparse_kernel(
+    const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+    const float* __restrict__ val, int n, const uint8_t* __restrict__ mediator,
+    const uint8_t* __restrict__ keep_all, float thr, uint8_t* __restrict__ keep) {
+  extern __shared__ uint32_t ind[];  // n words: max(0, max_k min(A[i][k], A[k][j])) as bits
+  const int i = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n_warps = kSparseThreads / 32;
+  for (int j = tid; j < n; j += kSparseThreads) ind[j] = 0u;
+  __syncthreads();
+  const int64_t e0 = row_ptr[i], e1 = row_ptr[i + 1];
+  for (int64_t e = e0 + warp; e < e1; e += n_warps) {
+    const int k = col[e];
+    const float v = val[e];
+    if ((unsigned)k >= (unsigned)n || !(v > 0.f) || (mediator != nullptr && mediator[k] == 0))
+      continue;  // warp-uniform
+    const int64_t f1 = row_ptr[k + 1];
+    for (int64_t f = row_ptr[k] + lane; f < f1; f += 32) {
+      const float w = val[f];
+      const int j = col[f];
+      if (w > 0.f && (unsigned)j < (unsigned)n) atomicMax(&ind[j], __float_as_uint(fminf(v, w)));
+    }
+  }
+  __syncthreads();
+  const bool all = keep_all != nullptr && keep_all[i] != 0;
+  for (int64_t e = e0 + tid; e < e1; e += kSparseThreads) {
+    const int j = col[e];
+    if ((unsigned)j >= (unsigned)n) {  // malformed entry: never kept
+      keep[e] = 0;
+      continue;
+    }
+    const float a = val[e];
+    const float t = __uint_as_float(ind[j]) + thr;
+    keep[e] = (all || a >= t) ? 1 : 0;
+  }
+}
+
 }  // namespace
 }  // namespace tenex
 
 using namespace tenex;
+
+extern "C" int tenex_dpi_trim_sparse(const int64_t* row_ptr, const int32_t* col, const float* val,
+                                     int n_vars, const uint8_t* mediator, const uint8_t* keep_all,
+                                     float trim_threshold, uint8_t* keep, void* stream) {
+  if (!row_ptr || !col || !val || !keep)
+    return fail(TENEX_ERR_BADARG, "row_ptr, col, val and keep must be non-NULL");
+  if (n_vars < 1) return fail(TENEX_ERR_BADARG, "n_vars must be >= 1");
+  DevAttr A;
+  int st = current_device_attr(&A);
+  if (st) return st;
+  const int64_t smem = (int64_t)n_vars * 4;
+  if (smem > A.smem_optin)
+    return fail(TENEX_ERR_UNSUPPORTED, "n_vars=%d: the row of %lld bytes exceeds shared memory "
+                "(%d bytes); use tenex_dpi_trim", n_vars, (long long)smem, A.smem_optin);
+  cudaError_t e = cudaFuncSetAttribute(dpi_trim_sparse_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+  dpi_trim_sparse_kernel<<<n_vars, kSparseThreads, (size_t)smem, as_stream(stream)>>>(
+      row_ptr, col, val, n_vars, mediator, keep_all, trim_threshold, keep);
+  return check_launch("dpi_trim_sparse_kernel");
+}
 
 extern "C" int tenex_dpi_trim(const float* te, int64_t ld, int n_vars, const uint8_t* mediator,
                               const uint8_t* keep_all, float trim_threshold, float* out,

@@ -6,8 +6,9 @@ links=0, sources, is_trimming=True, trim_threshold=0.0, batch_size=512) and
 return values (GRN, or (GRN, trimmed GRN) with trimming). Thresholding runs on
 the device as the reference's GPU branch does (z-score with the unbiased std,
 p = erfc(z / sqrt 2) / 2, BH, keep adjusted p < fdr; or the `links` largest);
-the trimming step's (max, min) matrix product over the mediators is the CUDA
-kernel tenex_dpi_trim.
+the trimming step's (max, min) matrix product over the mediators is a CUDA
+kernel, dense (tenex_dpi_trim) or over the nonzero entries
+(tenex_dpi_trim_sparse), whichever does less work.
 """
 from __future__ import annotations
 
@@ -101,11 +102,53 @@ def dpi_trim_matrix(arr: torch.Tensor, mediator: torch.Tensor | None = None,
     return out
 
 
+def dpi_trim_sparse(arr: torch.Tensor, mediator: torch.Tensor | None = None,
+                    keep_all: torch.Tensor | None = None, trim_threshold: float = 0.0):
+    """tenex_dpi_trim_sparse on the nonzero entries of a float32 (n, n) device
+    matrix; returns (rows, cols, vals) of the surviving entries, row-major."""
+    if arr.device.type != "cuda":
+        raise RuntimeError("DPI trimming runs on a CUDA device; got " + str(arr.device))
+    n = arr.shape[0]
+    rows, cols = torch.nonzero(arr, as_tuple=True)
+    if rows.numel() == 0:
+        return rows, cols, arr[rows, cols]
+    vals = arr[rows, cols].contiguous()
+    row_ptr = torch.zeros(n + 1, dtype=torch.int64, device=arr.device)
+    row_ptr[1:] = torch.cumsum(torch.bincount(rows, minlength=n), 0)
+    col32 = cols.to(torch.int32).contiguous()
+    keep = torch.empty(rows.numel(), dtype=torch.uint8, device=arr.device)
+    med = None if mediator is None else mediator.to(torch.uint8).contiguous()
+    ka = None if keep_all is None else keep_all.to(torch.uint8).contiguous()
+    native.call("tenex_dpi_trim_sparse", row_ptr.data_ptr(), col32.data_ptr(), vals.data_ptr(), n,
+                med.data_ptr() if med is not None else None,
+                ka.data_ptr() if ka is not None else None, ctypes.c_float(trim_threshold),
+                keep.data_ptr(), native.stream_ptr())
+    k = keep.bool()
+    return rows[k], cols[k], vals[k]
+
+
+def _sparse_pays(arr: torch.Tensor, mediator: torch.Tensor) -> bool:
+    """The sparse form's updates (sum over mediators k of positive in-degree x
+    positive out-degree) against 1.5 n^3 dense min/max instructions; an update
+    (a gather and a shared atomicMax) costs ~10 dense instructions."""
+    n = arr.shape[0]
+    if n * 4 > native.device_info(arr.device.index).smem_optin:
+        return False
+    pos = arr > 0
+    work = (pos.sum(0).double() * pos.sum(1).double() * mediator.double()).sum().item()
+    return work * 10.0 < 1.5 * float(n) ** 3
+
+
 def dpi_trim(n: int, variable_names, pairs: np.ndarray, te_values: np.ndarray,
-             device: torch.device, batch_size: int = 512, trim_threshold: float = 0.0):
+             device: torch.device, batch_size: int = 512, trim_threshold: float = 0.0,
+             method: str = "auto"):
     """Trimmed GRN of the kept edges (tenex/inference/fdr.py:61-133): mediators
     are rows with a positive sum; row batches of `batch_size` without an active
-    mediator are kept whole; the rest keep A[i,j] >= indirect + trim_threshold."""
+    mediator are kept whole; the rest keep A[i,j] >= indirect + trim_threshold.
+    method: "dense" (tenex_dpi_trim), "sparse" (tenex_dpi_trim_sparse) or "auto"
+    (sparse when its work is the smaller); both give the same edges."""
+    if method not in ("auto", "dense", "sparse"):
+        raise ValueError(f"method must be 'auto', 'dense' or 'sparse' (got {method!r})")
     pairs = np.asarray(pairs)
     arr = torch.zeros((n, n), dtype=torch.float32, device=device)
     if len(pairs):
@@ -120,14 +163,17 @@ def dpi_trim(n: int, variable_names, pairs: np.ndarray, te_values: np.ndarray,
     pad = nb * batch_size - n
     batch_active = torch.nn.functional.pad(row_active, (0, pad)).view(nb, batch_size).any(dim=1)
     keep_all = (~batch_active).repeat_interleave(batch_size)[:n]
-    out = dpi_trim_matrix(arr, mediator, keep_all, trim_threshold)
-    rows, cols = torch.nonzero(out, as_tuple=True)
+    if method == "sparse" or (method == "auto" and _sparse_pays(arr, mediator)):
+        rows, cols, vals = dpi_trim_sparse(arr, mediator, keep_all, trim_threshold)
+    else:
+        out = dpi_trim_matrix(arr, mediator, keep_all, trim_threshold)
+        rows, cols = torch.nonzero(out, as_tuple=True)
+        vals = out[rows, cols]
     if rows.numel() == 0:
         return make_grn(variable_names, np.empty((0, 2), dtype=np.int32),
                         np.empty(0, dtype=np.float32))
-    vals = out[rows, cols].cpu().numpy()
     kept = torch.stack((rows, cols), dim=1).cpu().numpy()
-    return make_grn(variable_names, kept, vals)
+    return make_grn(variable_names, kept, vals.cpu().numpy())
 
 
 class FDRMethod:
@@ -144,6 +190,7 @@ class FDRMethod:
         is_trimming = kwargs.get("is_trimming", True)
         trim_threshold = kwargs.get("trim_threshold", 0.0)
         batch_size = kwargs.get("batch_size", 512)
+        dpi_method = kwargs.get("dpi_method", "auto")
         device = torch.device(device)
         if device.type != "cuda":
             raise RuntimeError("the fdr method runs on a CUDA device in this package; got "
@@ -166,6 +213,7 @@ class FDRMethod:
         if not is_trimming:
             return grn
         trimmed = dpi_trim(te_matrix.shape[0], variable_names, pairs_cut, te_cut, device,
-                           batch_size=batch_size, trim_threshold=trim_threshold)
+                           batch_size=batch_size, trim_threshold=trim_threshold,
+                           method=dpi_method)
         _log.vprint(f"[TENEX] inference(fdr): {len(trimmed)} links after trimming")
         return grn, trimmed

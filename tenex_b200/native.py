@@ -83,6 +83,7 @@ _SIGS = {
     "tenex_te_binary_matrix": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _P],
     "tenex_b2_status": [_P, _I, _L, _L, _P],
     "tenex_dpi_trim": [_P, _L, _I, _P, _P, ctypes.c_float, _P, _L, _P],
+    "tenex_dpi_trim_sparse": [_P, _P, _P, _I, _P, _P, ctypes.c_float, _P, _P],
     "tenex_mlp_param_count": [],
     "tenex_gene_features": [_P, _L, _P, _I, _L, _L, _P, _P],
     "tenex_eiid_workspace_bytes": [_I],

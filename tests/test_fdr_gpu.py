@@ -8,7 +8,10 @@ import torch
 
 from oracle import fdr_oracle as F
 from tenex_b200.inference import NetWeaver, get_method
-from tenex_b200.inference.fdr import dpi_trim, dpi_trim_matrix
+import ctypes
+
+from tenex_b200 import native
+from tenex_b200.inference.fdr import dpi_trim, dpi_trim_matrix, dpi_trim_sparse
 from tenex_b200.inference.grn import build_pairs
 
 pytestmark = pytest.mark.gpu
@@ -42,6 +45,41 @@ def test_dpi_kernel_bitexact(cuda, n, density, thr):
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 
+@pytest.mark.parametrize("n,density,thr", [(1, 1.0, 0.0), (7, 0.6, 0.0), (200, 0.05, 0.0),
+                                           (513, 0.02, 0.003), (300, 0.4, -0.01)])
+def test_dpi_sparse_equals_dense(cuda, n, density, thr):
+    rng = np.random.default_rng(1000 + n)
+    a = _sparse_net(rng, n, density, neg=True)
+    med = rng.random(n) < 0.85
+    keep = rng.random(n) < 0.1
+    A = torch.from_numpy(a).to(cuda)
+    for m_, k_ in ((None, None), (med, keep)):
+        mt = None if m_ is None else torch.from_numpy(m_).to(cuda)
+        kt = None if k_ is None else torch.from_numpy(k_).to(cuda)
+        dense = dpi_trim_matrix(A, mt, kt, thr)
+        r, c = torch.nonzero(dense, as_tuple=True)
+        rs, cs, vs = dpi_trim_sparse(A, mt, kt, thr)
+        assert torch.equal(rs, r) and torch.equal(cs, c)
+        assert torch.equal(vs.view(torch.int32), dense[r, c].view(torch.int32))
+
+
+def test_dpi_sparse_guards(cuda):
+    # an entry whose column is out of range is ignored (no fault) and never kept
+    row_ptr = torch.tensor([0, 2, 3], dtype=torch.int64, device=cuda)
+    col = torch.tensor([1, 5, 0], dtype=torch.int32, device=cuda)
+    val = torch.tensor([0.5, 0.7, 0.25], dtype=torch.float32, device=cuda)
+    keep = torch.full((3,), 7, dtype=torch.uint8, device=cuda)
+    native.call("tenex_dpi_trim_sparse", row_ptr.data_ptr(), col.data_ptr(), val.data_ptr(), 2,
+                None, None, ctypes.c_float(0.0), keep.data_ptr(), native.stream_ptr())
+    assert keep.tolist() == [1, 0, 1]
+    big = 200_000                                      # a row of 800 KB cannot fit shared memory
+    rp = torch.zeros(big + 1, dtype=torch.int64, device=cuda)
+    with pytest.raises(native.TenexError) as ei:
+        native.call("tenex_dpi_trim_sparse", rp.data_ptr(), col.data_ptr(), val.data_ptr(), big,
+                    None, None, ctypes.c_float(0.0), keep.data_ptr(), native.stream_ptr())
+    assert ei.value.status == native.TENEX_ERR_UNSUPPORTED
+
+
 def test_dpi_kernel_large_rows(cuda):
     n = 2000
     rng = np.random.default_rng(5)
@@ -66,15 +104,17 @@ def _assert_cut_close(grn, te, pairs, fdr):
         assert abs(adj[idx[p]] - fdr) <= 1e-4 * fdr, p
 
 
+@pytest.mark.parametrize("dpi_method", ["dense", "sparse", "auto"])
 @pytest.mark.parametrize("case", "abcde")
-def test_fdr_method_against_reference(cuda, case):
+def test_fdr_method_against_reference(cuda, case, dpi_method):
     z = np.load(GOLD)
     m = z["matrix"]
     n = m.shape[0]
     names = np.array([f"g{i}" for i in range(n)])
     fdr, links, thr, bs = z[f"{case}_cfg"]
     grn, trimmed = get_method("fdr").infer(m, names, cuda, fdr=fdr, links=int(links),
-                                           trim_threshold=thr, batch_size=int(bs))
+                                           trim_threshold=thr, batch_size=int(bs),
+                                           dpi_method=dpi_method)
     gp, gt = z[f"{case}_cut_pairs"], z[f"{case}_cut_te"]
     if links:
         order = lambda p, t: np.lexsort((p[:, 1], p[:, 0], -t.astype(np.float64)))
