@@ -57,7 +57,9 @@ typedef struct {
   int max_threads_per_sm;
 } tenex_dev_info;
 
-/* Launch shape of the persistent histogram kernels (0 fields = defaults). */
+/* Launch shape of the persistent histogram kernels (0 fields, or a NULL config,
+ * = defaults: 512 threads, 2 CTAs per SM, 128 sources per item; fewer CTAs per
+ * SM when the largest pair's histogram does not fit). */
 typedef struct {
   int threads;      /* threads per CTA: 128, 256, 512 or 1024          */
   int ctas_per_sm;  /* resident CTAs per SM (grid = sm_count * this)    */

@@ -638,7 +638,7 @@ struct TeLaunch {
 static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const DevAttr& A,
                           TeLaunch* L, int64_t max_slot_bytes) {
   const int threads = (cfg && cfg->threads) ? cfg->threads : 512;
-  int cps = (cfg && cfg->ctas_per_sm) ? cfg->ctas_per_sm : 1;
+  int cps = (cfg && cfg->ctas_per_sm) ? cfg->ctas_per_sm : 2;  // lowered below if slots do not fit
   if (threads != 128 && threads != 256 && threads != 512 && threads != 1024)
     return fail(TENEX_ERR_BADARG, "threads must be 128, 256, 512 or 1024 (got %d)", threads);
   if (cps < 1 || cps * threads > A.max_threads_per_sm)

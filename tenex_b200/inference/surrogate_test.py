@@ -272,6 +272,10 @@ class SurrogateTestMethod:
         from tenex_b200.kernels import get_kernel
         kobj = get_kernel(kernel_name)
         cfg = getattr(kobj, "cfg", None)
+        if cfg is None and not binary and hasattr(kobj, "launch_cfg"):
+            # launch shape tuned once on the observed bins (the shuffles keep every
+            # gene's bin counts, so the tuned shape carries over)
+            cfg = kobj.launch_cfg(db, npv, b_max, tau, autotune_shape=True)
         acc = SurrogateAccumulator(db, npv, b_max, tau, obs_d, binary, cfg, pair_offset, n_pairs)
         perms, bl, _ = build_block_perm(n_vars, T, shuffle_method, block_length, k_start,
                                         k_start + n_surrogates, seed, dev)

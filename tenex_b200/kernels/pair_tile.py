@@ -19,7 +19,7 @@ from tenex_b200.kernels import device as D
 
 # Launch shapes the autotuner tries: (threads, ctas_per_sm, src_chunk)
 TUNE_SPACE = [(512, 2, 128), (1024, 1, 128), (512, 1, 128), (256, 2, 64), (1024, 1, 64),
-              (512, 2, 64)]
+              (512, 2, 64), (512, 2, 256), (256, 4, 128), (256, 4, 256)]
 DEFAULT_CFG = dict(threads=512, ctas_per_sm=2, src_chunk=128)
 _tune_cache: dict[tuple, dict] = {}
 
