@@ -192,14 +192,35 @@ __global__ void __launch_bounds__(256) eiid_kernel(const uint8_t* __restrict__ b
     }
   }
   __syncthreads();
-  // compact lists: the non-zero n_a, then the non-zero n_x after them
-  for (int i = threadIdx.x; i < bt * bt; i += blockDim.x)
-    if (hz[i]) la[atomicAdd(&nz, 1)] = (float)hz[i];
+  // compact lists: the non-zero n_a, then the non-zero n_x after them, in index
+  // order (one warp, ballot + prefix count), so every run sums the terms below
+  // in the same order and E_iid is bitwise reproducible
+  if (threadIdx.x < 32) {
+    const unsigned lane = threadIdx.x;
+    const unsigned below = (1u << lane) - 1u;
+    int base = 0;
+    for (int i0 = 0; i0 < bt * bt; i0 += 32) {
+      const int i = i0 + (int)lane;
+      const bool nzv = i < bt * bt && hz[i] != 0;
+      const unsigned m = __ballot_sync(0xffffffffu, nzv);
+      if (nzv) la[base + __popc(m & below)] = (float)hz[i];
+      base += __popc(m);
+    }
+    const int kz0 = base;
+    for (int i0 = 0; i0 < bt; i0 += 32) {
+      const int i = i0 + (int)lane;
+      const bool nzv = i < bt && hx[i] != 0;
+      const unsigned m = __ballot_sync(0xffffffffu, nzv);
+      if (nzv) la[base + __popc(m & below)] = (float)hx[i];
+      base += __popc(m);
+    }
+    if (lane == 0) {
+      nz = kz0;
+      nx = base - kz0;
+    }
+  }
   __syncthreads();
   const int kz = nz;
-  for (int i = threadIdx.x; i < bt; i += blockDim.x)
-    if (hx[i]) la[kz + atomicAdd(&nx, 1)] = (float)hx[i];
-  __syncthreads();
   const int kx = nx;
   for (int s = threadIdx.x; s < n; s += blockDim.x) {
     if (s == t) continue;

@@ -23,8 +23,10 @@ those p-values gives z_FDR. Every pair with z >= z_FDR - band (the band is
 calibrated on held-out seeds and stored with the model), every pair whose genes
 fall outside the features seen in training, and every pair with undefined
 features goes to the full block-shuffle surrogate test (pair-list kernel, the
-full test's own permutations, so those pairs get exactly the full test's
-statistics). BH is then recomputed over the mixed p-values and the screen is
+full test's own permutations and the same per-pair histogram counts, so those
+pairs get the full test's statistics up to the float rounding of each pair's
+entropy sum, whose reduction order follows the launch's warp grouping). BH is
+then recomputed over the mixed p-values and the screen is
 widened while z_FDR - band keeps falling. Called edges are therefore always
 verified by the full test; the band only decides how many true edges could be
 missed (pairs whose predicted z falls more than `band` below z_FDR).
@@ -69,6 +71,7 @@ class NullModel:
     gene_lo: np.ndarray           # (6,) per-gene feature range seen in training
     gene_hi: np.ndarray
     meta: dict = field(default_factory=dict)
+    _dev_cache: dict = field(default_factory=dict, repr=False, compare=False)
 
     def save(self, path: str) -> None:
         np.savez(path, params=self.params, feat_mean=self.feat_mean, feat_std=self.feat_std,
@@ -87,6 +90,13 @@ class NullModel:
                          z["gene_lo"], z["gene_hi"], ast.literal_eval(str(z["meta"])))
 
     def device_weights(self, dev) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        """BF16 weights and the feature standardisation on `dev` (made once per device)."""
+        key = str(torch.device(dev))
+        if key not in self._dev_cache:
+            self._dev_cache[key] = self._to_device(dev)
+        return self._dev_cache[key]
+
+    def _to_device(self, dev):
         master = torch.from_numpy(self.params).to(dev)
         wb = torch.empty(master.numel(), dtype=torch.bfloat16, device=dev)
         native.call("tenex_to_bf16", master.data_ptr(), wb.data_ptr(), master.numel(),
@@ -381,7 +391,7 @@ def _pair_items(pairs_ts: np.ndarray, run: int = 128):
 
 def fallback_surrogates(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int,
                         pairs_ts: np.ndarray, obs: torch.Tensor, perms: torch.Tensor, bl: int,
-                        use_graph: bool = True):
+                        use_graph: bool = True, cfg=None):
     """Full surrogate statistics (all S = perms.shape[0] shuffles, the same
     permutations as the full test) for the listed [tgt, src] pairs only: device
     (n, n) float64 sum, sum of squares and int32 count_ge, indexed [src, tgt];
@@ -404,7 +414,7 @@ def fallback_surrogates(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: in
                     npv.data_ptr(), int(b_max), n, shuf.row_len, tau * db.K, pairs_d.data_ptr(),
                     sp.shape[0], items_d.data_ptr(), items.shape[0] - 1, obs.data_ptr(),
                     ssum.data_ptr(), ssq.data_ptr(), cnt.data_ptr(), ws.data_ptr(), ws.numel(),
-                    None, native.stream_ptr())
+                    D._cfg(cfg), native.stream_ptr())
 
     one(0)
     native.call("tenex_workspace_status", ws.data_ptr(), native.stream_ptr())
@@ -425,12 +435,19 @@ def fallback_surrogates(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: in
 
 def bh_cut(p: torch.Tensor, fdr: float) -> float:
     """Largest p-value that BH-FDR at level fdr calls significant (adjusted
-    p < fdr) among the 1-D p-values p, or 0.0 when none is."""
-    from tenex_b200.inference.grn import bh_fdr_gpu
-    if p.numel() == 0:
+    p < fdr) among the 1-D p-values p, or 0.0 when none is. The BH-adjusted
+    value of the k-th smallest p is the minimum over k' >= k of p_(k') m / k'
+    (clamped at 1), so the significant set is the K smallest p-values, K the
+    last rank with p_(K) m / K < fdr (the same expression as bh_fdr_gpu), and
+    the cut is p_(K): one sort, no scatter back."""
+    m = p.numel()
+    if m == 0:
         return 0.0
-    sig = bh_fdr_gpu(p, fdr) < fdr
-    return float(p[sig].max()) if bool(sig.any()) else 0.0
+    sp = p.sort().values
+    rank = torch.arange(1, m + 1, device=p.device, dtype=p.dtype)
+    ok = (sp * m / rank).clamp(max=1.0) < fdr
+    last = int(torch.where(ok, rank, torch.zeros_like(rank)).max().item())
+    return float(sp[last - 1].item()) if last > 0 else 0.0
 
 
 def z_of_p(p: float, m: int, fdr: float) -> float:
@@ -440,6 +457,27 @@ def z_of_p(p: float, m: int, fdr: float) -> float:
     return float(ndtri(1.0 - min(max(q, 1e-300), 1.0 - 1e-16)))
 
 
+# launch shape of the verification pass (pair lists: few sources per target, so
+# small CTAs keep the per-item barriers short)
+VERIFY_CFG = None
+
+
+def bh_edges_device(p: torch.Tensor, eff: torch.Tensor, tested: torch.Tensor, variable_names,
+                    fdr: float):
+    """bh_edges on device matrices: BH over p[tested] (row-major, float32), edges
+    with adjusted p < fdr and effective TE > 0; the same edges as bh_edges gives
+    for the same float32 values."""
+    from tenex_b200.inference.grn import bh_fdr_gpu, make_grn
+    adj = bh_fdr_gpu(p[tested], alpha=fdr)
+    sig = torch.zeros_like(tested)
+    sig[tested] = adj < fdr
+    sig &= eff > 0
+    idx = torch.nonzero(sig)
+    pairs = idx.cpu().numpy().astype(np.int64)
+    te = eff[idx[:, 0], idx[:, 1]].cpu().numpy()
+    return make_grn(np.asarray(variable_names), pairs, te)
+
+
 def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n_per_var, b_max,
                            kernel_name, tau, n_surrogates, shuffle_method, block_length, p_method,
                            fdr, seed, kwargs):
@@ -447,20 +485,22 @@ def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n
 
     Pairs whose predicted z reaches z_FDR - band (z_FDR from BH over the current
     p-values), and pairs the model cannot score, run the full S-shuffle test with
-    the full test's permutations, so their statistics equal the full test's; the
+    the full test's permutations, so their statistics are the full test's (to the
+    float rounding of each pair's entropy sum); the
     rest keep the predicted null. BH is recomputed on the mixed p-values and the
     screen widened until z_FDR - band stops falling (at most max_rounds times)."""
-    from scipy.special import erfc
     from tenex_b200.inference.grn import build_pairs
-    from tenex_b200.inference.surrogate_test import (SurrogateTestResult, bh_edges,
-                                                     build_block_perm, pair_statistics)
+    from tenex_b200.inference.surrogate_test import (SurrogateTestResult, build_block_perm,
+                                                     pair_statistics)
     t0 = time.time()
     model = kwargs.get("null_model")
     if model is None:
         model = NullModel.load(kwargs.get("null_model_path", DEFAULT_MODEL))
     band = float(kwargs.get("fallback_band", model.meta.get("band", 1.0)))
     max_rounds = int(kwargs.get("max_rounds", 4))
-    use_graph = bool(kwargs.get("use_graph", True))
+    # the verification pass launches 2 x S kernels of ~0.25 ms each: eager launches
+    # cost less than capturing and instantiating a graph for one replay
+    use_graph = bool(kwargs.get("use_graph", False))
     n, T = bin_data.shape[0], bin_data.shape[1]
     db = D.pack_bins(bin_data, dev)
     npv = torch.as_tensor(np.asarray(n_per_var), dtype=torch.int32).to(dev)
@@ -503,7 +543,7 @@ def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n
         idx_np = idx.cpu().numpy()
         pairs_ts = np.ascontiguousarray(idx_np[:, ::-1]).astype(np.int64)
         ssum, ssq, cnt = fallback_surrogates(db, npv, b_max, tau, pairs_ts, obs_d, perms, bl,
-                                             use_graph)
+                                             use_graph, kwargs.get("verify_cfg", VERIFY_CFG))
         si, ti = idx[:, 0], idx[:, 1]
         ms, ss_, ef, pv = pair_statistics(observed_te[idx_np[:, 0], idx_np[:, 1]],
                                           ssum[si, ti].cpu().numpy(), ssq[si, ti].cpu().numpy(),
@@ -521,11 +561,10 @@ def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n
     mean_s[diag, diag] = 0.0
     std_s[diag, diag] = 0.0
     eff_s[diag, diag] = obs_d[diag, diag]
-    p_values = p_mix.float().cpu().numpy()
-    mean_np = mean_s.cpu().numpy()
-    std_np = std_s.cpu().numpy()
-    effective = eff_s.cpu().numpy()
-    grn, _ = bh_edges(p_values, effective, variable_names, sources, fdr, dev)
+    p32 = p_mix.float()
+    grn = bh_edges_device(p32, eff_s, tested, variable_names, fdr)
+    host = torch.stack((p32, mean_s.float(), std_s.float(), eff_s.float())).cpu().numpy()
+    p_values, mean_np, std_np, effective = host[0], host[1], host[2], host[3]
     n_ver = int(verified.sum())
     info = {"n_fallback": n_ver, "fallback_fraction": n_ver / max(m_tested, 1),
             "n_invalid": int((tested & ~valid).sum()), "z_cuts": z_cuts, "band": band,

@@ -63,11 +63,33 @@ def test_learned_null_agrees_with_full_test(cuda, data):
     assert E2 <= E1                       # every called edge was verified by the full test
     assert len(E1 & E2) / len(E1 | E2) >= 0.99
     assert lrn.info["fallback_fraction"] < 0.1
-    # verified pairs carry exactly the full test's statistics
+    # verified pairs carry the full test's statistics (same permutations and counts; a
+    # pair's float entropy sum may differ in its last bits between launch groupings)
     ver = np.isin(np.arange(N_GENES * N_GENES),
                   np.ravel_multi_index(tuple(np.array(sorted(E2)).T), (N_GENES, N_GENES)))
     ver = ver.reshape(N_GENES, N_GENES)
-    assert np.array_equal(lrn.p_values[ver], full.p_values[ver])
-    assert np.array_equal(lrn.mean_surrogate_te[ver], full.mean_surrogate_te[ver])
+    assert np.allclose(lrn.p_values[ver], full.p_values[ver], rtol=1e-4, atol=1e-6)
+    assert np.allclose(lrn.mean_surrogate_te[ver], full.mean_surrogate_te[ver], rtol=1e-5,
+                       atol=1e-7)
     pl = {(int(a), int(b)) for a, b in planted}
     assert len(pl & E2) == len(pl & E1)
+
+
+def test_learned_null_is_reproducible(cuda, data):
+    # the same inputs give bitwise the same result (E_iid sums its terms in a fixed order)
+    x, npv, _ = data
+    db = D.pack_bins(x, cuda)
+    npv_t = torch.as_tensor(npv, dtype=torch.int32, device=cuda)
+    e1 = LN.eiid_matrix(db, npv_t, 1).cpu().numpy()
+    e2 = LN.eiid_matrix(db, npv_t, 1).cpu().numpy()
+    assert np.array_equal(e1.view(np.uint32), e2.view(np.uint32))
+    obs = FullSMEMKernel().compute_pairfree_device(db, npv_t, int(npv.max()), 1,
+                                                   matrix=True).cpu().numpy()
+    names = np.array([f"g{i}" for i in range(N_GENES)])
+    kw = dict(bin_data=x, n_per_var=npv, b_max=int(npv.max()), kernel="Full-SMEM", tau=1,
+              n_surrogates=100, block_length=50, fdr=0.05, seed=42, null="learned")
+    m = SurrogateTestMethod()
+    a, b = m.infer(obs, names, cuda, **kw), m.infer(obs, names, cuda, **kw)
+    for f in ("p_values", "mean_surrogate_te", "std_surrogate_te", "effective_te"):
+        assert np.array_equal(getattr(a, f), getattr(b, f), equal_nan=True), f
+    assert np.array_equal(a.grn.pairs, b.grn.pairs)
