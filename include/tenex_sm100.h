@@ -92,7 +92,8 @@ int tenex_workspace_status(const void* workspace, void* stream);
  * one kernel covers both Full-SMEM (uniform b) and Adaptive-SMEM (per-gene b).
  * b_max = max(n_per_var) (the reference's B argument), 1..255; every
  * n_per_var[g] must lie in [1, b_max] and every bin of gene g below n_per_var[g]
- * (checked on the device; see tenex_workspace_status). */
+ * (checked on the device; see tenex_workspace_status). n_pairs == 0 returns
+ * TENEX_OK without touching out or the workspace (either may then be NULL). */
 int tenex_te_pairfree(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
                       int b_max, int n_vars, int64_t row_len, int64_t lag,
                       int64_t pair_offset, int64_t n_pairs,

@@ -750,6 +750,7 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
                 (long long)(p0 + n_pairs), (long long)total);
   if (pairs && (!item_start || n_items_list < 0 || n_pairs < 0 || p0 != 0))
     return fail(TENEX_ERR_BADARG, "pair list needs item_start, n_items >= 0 and n_pairs >= 0");
+  if (n_pairs == 0) return TENEX_OK;  // an empty range touches no output (NULL allowed)
   if (out_mode != kOutStats && !out) return fail(TENEX_ERR_BADARG, "out must be non-NULL");
   if (out_mode == kOutMatrix && out_ld < n)
     return fail(TENEX_ERR_BADARG, "out_ld (%lld) must be >= n_vars", (long long)out_ld);
@@ -760,7 +761,6 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
                 (long long)ws_total(n, b_max));
   if (counts && counts_stride < (int64_t)b_max * b_max * b_max)
     return fail(TENEX_ERR_BADARG, "counts_stride must be >= b_max^3");
-  if (n_pairs == 0) return TENEX_OK;
   DevAttr A;
   int st = current_device_attr(&A);
   if (st) return st;

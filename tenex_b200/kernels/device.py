@@ -107,6 +107,8 @@ def te_pairfree(db: DeviceBins, n_per_var: torch.Tensor, b_max: int, tau: int = 
     if out is None:
         out = (torch.zeros((n, n), dtype=torch.float32, device=dev) if matrix
                else torch.empty(max(n_pairs, 0), dtype=torch.float32, device=dev))
+    if n_pairs == 0:
+        return out                   # nothing to compute (the C entry point is a no-op too)
     ws = workspace(dev, n, db.row_len, b_max)
     s = native.stream_ptr()
     lag = tau * db.K

@@ -48,3 +48,18 @@ def test_registry_priority_matches_reference():
         get_kernel("scatter_add")
     with pytest.raises(RuntimeError):
         auto_select(4, False, 0, 0, None, False)
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="needs a CUDA-less host")
+def test_device_contract_without_cuda():
+    # the reference's device contract (tests/test_device_contract.py): an explicitly
+    # requested GPU must raise instead of computing elsewhere; this package has no
+    # CPU path, so accelerator='auto' raises too rather than falling back
+    x = np.random.RandomState(0).randn(12, 80).astype(np.float32)
+    eng = TransferEntropyEngine(x, np.array([f"g{i}" for i in range(12)]))
+    for kw in (dict(accelerator="gpu"), dict(accelerator="gpu", devices=[0]),
+               dict(accelerator="auto")):
+        with pytest.raises((RuntimeError, ValueError)):
+            eng.compute(binning_method="FSBW-L", kp=0.5, tau=1, **kw)
+    with pytest.raises((ValueError, RuntimeError)):
+        eng.compute(accelerator="npu", binning_method="FSBW-L", kp=0.5, tau=1)

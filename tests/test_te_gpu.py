@@ -114,6 +114,19 @@ def test_pair_ranges_and_launch_shapes(cuda):
         for p0, cnt in ((0, n * (n - 1)), (5, 77), (n * (n - 1) - 13, 13), (123, 1)):
             te = D.te_pairfree(db, npv_t, bmax, pair_offset=p0, n_pairs=cnt, cfg=cfg)
             assert np.max(np.abs(te.cpu().numpy() - ref[p0:p0 + cnt])) <= TOL, (cfg, p0)
+    # an empty range is a no-op, not an error
+    assert D.te_pairfree(db, npv_t, bmax, pair_offset=17, n_pairs=0).numel() == 0
+
+
+@pytest.mark.parametrize("T", [2, 3, 17])
+def test_shortest_series(cuda, T):
+    # N = T - 1 samples, down to one: TE of a single sample is 0
+    rng = np.random.default_rng(T)
+    bins, npv, bmax = _rand_bins(rng, 6, T, 1, 4)
+    te = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
+    assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
+    if T == 2:
+        assert np.all(te == 0)
 
 
 @pytest.mark.parametrize("threads", [256, 1024])
