@@ -98,7 +98,7 @@ def te_matrix_sharded(kernel, db, n_per_var: torch.Tensor, b_max: int, tau: int,
 
 
 def surrogate_sharded(db, n_per_var: torch.Tensor, b_max: int, tau: int, observed: torch.Tensor,
-                      perms: torch.Tensor, block_length: int, cfg=None, use_graph: bool = True,
+                      perms: torch.Tensor, block_length: int, cfg=None, use_graph: bool = False,
                       group=None):
     """Surrogate sum / sum of squares / count_ge ((n, n) device tensors, all
     pairs) with each rank running every surrogate on its own pair chunk."""

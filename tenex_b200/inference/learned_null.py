@@ -176,7 +176,7 @@ def surrogate_moments(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int,
     obs = torch.zeros((n, n), dtype=torch.float32, device=db.data.device)
     acc = SurrogateAccumulator(db, npv, b_max, tau, obs, b_max == 2)
     perms, bl, _ = build_block_perm(n, db.T, "block", block_length, 0, S, seed, db.data.device)
-    run_surrogates(acc, perms, bl, use_graph=True)
+    run_surrogates(acc, perms, bl)
     mean = acc.sum / S
     var = acc.sumsq / S - mean * mean
     return mean.float(), torch.sqrt(torch.clamp(var, min=0.0)).float()
@@ -312,7 +312,7 @@ def screen_recall(model, x: np.ndarray, npv: np.ndarray, dev, S: int, block_leng
                                                      run_surrogates)
     acc = SurrogateAccumulator(db, npv_t, b_max, tau, obs, b_max == 2)
     perms, bl, _ = build_block_perm(db.n, db.T, "block", block_length, 0, S, seed, dev)
-    run_surrogates(acc, perms, bl, use_graph=True)
+    run_surrogates(acc, perms, bl)
     mean = (acc.sum / S).float()
     std = torch.sqrt(torch.clamp(acc.sumsq / S - (acc.sum / S) ** 2, min=0.0)).float()
     off = ~torch.eye(db.n, dtype=torch.bool, device=dev)
@@ -391,7 +391,7 @@ def _pair_items(pairs_ts: np.ndarray, run: int = 128):
 
 def fallback_surrogates(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int,
                         pairs_ts: np.ndarray, obs: torch.Tensor, perms: torch.Tensor, bl: int,
-                        use_graph: bool = True, cfg=None):
+                        use_graph: bool = False, cfg=None):
     """Full surrogate statistics (all S = perms.shape[0] shuffles, the same
     permutations as the full test) for the listed [tgt, src] pairs only: device
     (n, n) float64 sum, sum of squares and int32 count_ge, indexed [src, tgt];

@@ -114,7 +114,7 @@ class SurrogateAccumulator:
 
 
 def run_surrogates(acc: SurrogateAccumulator, perms: torch.Tensor, block_length: int,
-                   use_graph: bool = True) -> None:
+                   use_graph: bool = False) -> None:
     """Adds all surrogates of `perms` (S, n, n_blocks) into `acc`."""
     S = perms.shape[0]
     if S == 0:
@@ -263,7 +263,7 @@ class SurrogateTestMethod:
 
     @staticmethod
     def accumulate(observed_te, dev, bin_data, n_per_var, b_max, kernel_name, tau, n_surrogates,
-                   shuffle_method, block_length, seed, use_graph=True, k_start=0,
+                   shuffle_method, block_length, seed, use_graph=False, k_start=0,
                    pair_offset=0, n_pairs=None):
         """float64 sum, sum of squares and int32 count_ge (numpy, (n, n)) over
         surrogates [k_start, k_start + n_surrogates), diagonal count included."""
