@@ -83,8 +83,67 @@ class TEKernel(ABC):
         """Full (n, n) matrix with [i, j] = TE(j -> i). Override for matrix kernels."""
         raise NotImplementedError(f"{self.name} is a pair-based kernel")
 
+    def compute_multi_gpu(self, bin_arrs_cpu, pairs_np, b_max: int, n_per_var_cpu, tau: int,
+                          batch_size: Optional[int], device_ids: list, **kwargs) -> np.ndarray:
+        """Pair list over several devices (tenex/kernels/__init__.py:148-236): contiguous
+        chunks of ceil(P / n_devices) pairs, one host thread per device, each with its
+        own copy of the bins calling compute_single_gpu; results in the caller's pair
+        order. The devices work independently (no collectives)."""
+        from concurrent.futures import ThreadPoolExecutor
+        pairs_np = np.asarray(pairs_np)
+        P = pairs_np.shape[0]
+        ids = [int(d) for d in device_ids]
+        if not ids:
+            raise ValueError("device_ids must name at least one device")
+        chunk = -(-P // len(ids)) if P else 0
+
+        def run(rank: int) -> np.ndarray:
+            beg, end = rank * chunk, min(P, (rank + 1) * chunk)
+            if beg >= end:
+                return np.empty(0, np.float32)
+            torch.cuda.set_device(ids[rank])
+            dev = torch.device("cuda", ids[rank])
+            return self.compute_single_gpu(bin_arrs_cpu, pairs_np[beg:end], b_max, n_per_var_cpu,
+                                           tau, batch_size, dev, **kwargs)
+
+        with ThreadPoolExecutor(max_workers=len(ids)) as ex:
+            parts = list(ex.map(run, range(len(ids))))
+        return np.concatenate(parts) if parts else np.empty(0, np.float32)
+
+    def compute_matrix_multi_gpu(self, data, n_vars: int, tau: int, device_ids: list,
+                                 **kwargs) -> np.ndarray:
+        """Full matrix over several devices. Override for matrix kernels."""
+        raise NotImplementedError(f"{self.name} is a pair-based kernel")
+
     def peak_batch_bytes(self, b_max: int, T: int, K: int, batch_size: int, tau: int = 1) -> int:
         return batch_size * 4 + batch_size * 2 * 8
+
+    def peak_bytes_per_pair(self, b_max: int, T: int, K: int, tau: int = 1) -> int:
+        """Device bytes per pair of a pair-list launch: the float32 result and the
+        (target, source) int64 pair. Histograms live in shared memory."""
+        return 4 + 2 * 8
+
+    def heuristic_batch_size(self, bin_arrs, b_max: int, tau: int = 1) -> int:
+        """Pairs per pair-list launch that fit 80% of the free device memory
+        (tenex/kernels/__init__.py:266-322 sizes batches the same way). The
+        persistent kernels take any number of pairs in one launch, so the batch
+        only bounds the pair and result buffers."""
+        device = getattr(bin_arrs, "device", torch.device("cpu"))
+        if device.type != "cuda":
+            return 2048
+        shape = tuple(bin_arrs.shape)
+        T, K = int(shape[1]), int(shape[2]) if len(shape) > 2 else 1
+        free = torch.cuda.mem_get_info(device)[0]
+        budget = max(0, int(free * 0.8) - (256 << 20))
+        return max(1024, budget // self.peak_bytes_per_pair(b_max, T, K, tau))
+
+    def autotune_batch_size(self, bin_arrs, b_max: int, n_per_var, tau: int,
+                            device: torch.device) -> int:
+        """The batch size does not change the persistent kernel's speed (work is
+        handed out by an atomic ticket inside one launch), so the tuned value is
+        the memory heuristic's; the launch shape is tuned separately
+        (tenex_b200.kernels.pair_tile.autotune)."""
+        return self.heuristic_batch_size(bin_arrs, b_max, tau)
 
     def prepare(self, bin_arrs, n_per_var, b_max: int, **kwargs):
         """Optional preprocessing hook (e.g. bin coarsening). Default: no-op."""

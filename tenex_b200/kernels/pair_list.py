@@ -18,16 +18,18 @@ from tenex_b200.kernels import device as D
 
 def item_table(tgt_sorted: np.ndarray, run: int = 128) -> np.ndarray:
     """Start offsets of runs of equal targets, each at most `run` long (+ end)."""
+    tgt_sorted = np.asarray(tgt_sorted)
     P = tgt_sorted.shape[0]
     if P == 0:
         return np.zeros(1, np.int64)
     change = np.flatnonzero(np.diff(tgt_sorted)) + 1
-    starts = np.concatenate([[0], change, [P]])
-    out = []
-    for a, b in zip(starts[:-1], starts[1:]):
-        out.extend(range(int(a), int(b), run))
-    out.append(P)
-    return np.asarray(out, np.int64)
+    starts = np.concatenate([[0], change]).astype(np.int64)
+    lens = np.diff(np.concatenate([starts, [P]]))
+    nchunk = (lens + run - 1) // run
+    first = np.cumsum(nchunk) - nchunk                 # index of each segment's first item
+    k = np.arange(int(nchunk.sum()), dtype=np.int64) - np.repeat(first, nchunk)
+    items = np.repeat(starts, nchunk) + run * k
+    return np.concatenate([items, [P]]).astype(np.int64)
 
 
 def te_pair_list(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int, pairs: np.ndarray,

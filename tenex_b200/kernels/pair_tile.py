@@ -14,6 +14,7 @@ from typing import Optional
 import numpy as np
 import torch
 
+from tenex_b200 import native
 from tenex_b200.kernels import TEKernel
 from tenex_b200.kernels import device as D
 
@@ -74,9 +75,6 @@ class PairTileKernel(TEKernel):
     def supports_pairfree(self) -> bool:
         return True
 
-    def peak_bytes_per_pair(self, b_max, T, K, tau=1):
-        return 4
-
     def launch_cfg(self, db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int,
                    autotune_shape: bool) -> dict:
         if self.cfg is not None:
@@ -106,6 +104,40 @@ class PairTileKernel(TEKernel):
         te = self.compute_pairfree_device(db, n_per_var, b_max, tau, pair_offset,
                                           n_pairs_local)
         return te.cpu().numpy()
+
+    def compute_pairfree_cross(self, bin_arrs, n_per_var, n_tgt: int, n_src: int, tau: int,
+                               device, pair_offset: int = 0,
+                               n_pairs_local: Optional[int] = None) -> np.ndarray:
+        """TE between two disjoint gene blocks (tenex/kernels/adaptive_smem.py:1114-1160,
+        the variable-blocking path): bin_arrs rows [0, n_tgt) are the targets and
+        [n_tgt, n_tgt + n_src) the sources; pair id = tgt_local * n_src + src_local,
+        value TE(source -> target). Runs as a pair list built on the device."""
+        from tenex_b200.kernels.pair_list import item_table
+        dev = torch.device(device) if not isinstance(device, torch.device) else device
+        total = int(n_tgt) * int(n_src)
+        if n_pairs_local is None:
+            n_pairs_local = total - pair_offset
+        if pair_offset < 0 or n_pairs_local < 0 or pair_offset + n_pairs_local > total:
+            raise ValueError(f"pair range [{pair_offset}, {pair_offset + n_pairs_local}) "
+                             f"outside [0, {total})")
+        out = torch.empty(n_pairs_local, dtype=torch.float32, device=dev)
+        if n_pairs_local == 0:
+            return out.cpu().numpy()
+        b_max = int(torch.as_tensor(n_per_var).max())
+        db = D.pack_bins(bin_arrs, dev, b_max)
+        npv = _npv_tensor(n_per_var, dev)
+        ids = torch.arange(pair_offset, pair_offset + n_pairs_local, device=dev, dtype=torch.int64)
+        tgt = ids // n_src
+        pairs = torch.stack((tgt, n_tgt + ids - tgt * n_src), dim=1).contiguous()
+        items = torch.from_numpy(item_table(tgt.cpu().numpy(), 128)).to(dev)
+        ws = D.workspace(dev, db.n, db.row_len, b_max)
+        s = native.stream_ptr()
+        native.call("tenex_te_pairs", db.data.data_ptr(), db.ld, npv.data_ptr(), b_max, db.n,
+                    db.row_len, tau * db.K, pairs.data_ptr(), n_pairs_local, items.data_ptr(),
+                    items.numel() - 1, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                    D._cfg(self.cfg), s)
+        native.call("tenex_workspace_status", ws.data_ptr(), s)
+        return out.cpu().numpy()
 
     def compute_single_gpu(self, bin_arrs, pairs, b_max, n_per_var, tau, batch_size, device,
                            **kwargs) -> np.ndarray:

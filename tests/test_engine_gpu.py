@@ -138,3 +138,39 @@ def test_engine_contracts(cuda):
     r2 = eng.compute(accelerator="gpu", kernel="Adaptive-SMEM", tau=2)
     ref = O.te_matrix(r2.bin_arrs, r2.n_per_var, tau=2)
     assert np.max(np.abs(r2.matrix - ref)) <= TOL
+
+
+def test_multi_device_and_cross_block_entry_points(cuda):
+    from oracle import oracle as O
+    from tenex_b200.kernels import get_kernel
+    rng = np.random.default_rng(12)
+    n, T = 30, 900
+    b = rng.integers(2, 12, n)
+    x = np.stack([rng.integers(0, bb, T) for bb in b]).astype(np.int32)
+    bins, npv, bmax = O.remap(x)
+    ref = O.te_matrix(bins, npv)                      # [src, tgt]
+    k = get_kernel("Adaptive-SMEM")
+    pairs = np.stack(np.nonzero(~np.eye(n, dtype=bool)), axis=1)[::3][:, ::-1].copy()  # [tgt, src]
+    bt = torch.from_numpy(bins.reshape(n, T, 1).astype(np.uint8))
+    npv_t = torch.from_numpy(npv.astype(np.int32))
+    single = k.compute_single_gpu(bt, pairs, bmax, npv_t, 1, None, cuda)
+    for ids in ([0], [0, 0]):                         # two host threads may share a device
+        multi = k.compute_multi_gpu(bt, pairs, bmax, npv_t, 1, None, ids)
+        assert np.array_equal(multi, single)
+    assert np.max(np.abs(single - ref[pairs[:, 1], pairs[:, 0]])) <= 1e-6
+    # cross block: targets 0..9 against sources 20..29, pair id = tgt_local * n_src + src_local
+    tg, sr = np.arange(10), np.arange(20, 30)
+    sub = np.concatenate([tg, sr])
+    cross = k.compute_pairfree_cross(bt[sub], npv_t[sub], 10, 10, 1, cuda)
+    want = ref[np.ix_(sr, tg)].T.reshape(-1)          # [tgt_local, src_local]
+    assert np.max(np.abs(cross - want)) <= 1e-6
+    part = k.compute_pairfree_cross(bt[sub], npv_t[sub], 10, 10, 1, cuda, pair_offset=37,
+                                    n_pairs_local=21)
+    assert np.array_equal(part, cross[37:58])
+    # the binary matrix kernel's multi-device entry
+    xb = (rng.random((20, 400)) < 0.4).astype(np.int32)
+    xb[:, :2] = [1, 0]
+    g = get_kernel("GEMM-B2")
+    m1 = g.compute_matrix(xb[..., None], 20, 1, cuda)
+    m2 = g.compute_matrix_multi_gpu(xb[..., None], 20, 1, [0])
+    assert np.array_equal(m1, m2)
