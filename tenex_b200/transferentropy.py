@@ -10,9 +10,11 @@ leave the device until the result is wrapped.
 Differences from the reference, by design:
   * accelerator="cpu" is rejected: this build has no CPU path (the TE kernels
     are sm_100a code); "auto" requires CUDA.
-  * One process drives one GPU. Several GPUs are driven by one process each
-    (tenex_b200.distributed shards the pair-id range); devices= lists with
-    more than one id are rejected here.
+  * devices= with several ids splits the pair-id range into contiguous chunks,
+    one host thread and one copy of the bins per device (the reference's
+    in-process split, tenex/transferentropy.py:360-440); the devices share no
+    data path. Several processes (one per GPU, torchrun) use
+    tenex_b200.distributed instead.
   * Bins are always the numpy/FastTENET FSBW-L bins (the reference's GPU torch
     binning differs from them in the last float32 bit of std).
 """
@@ -128,10 +130,6 @@ class TransferEntropyEngine:
         else:
             raise TypeError(f"devices must be 'auto', int, list[int], or None "
                             f"(got {type(devices).__name__})")
-        if len(ids) > 1:
-            raise NotImplementedError(
-                "one process drives one GPU: launch one process per GPU "
-                "(torchrun) and use tenex_b200.distributed.compute_sharded")
         return ids
 
     # ------------------------------------------------------------------ bins
@@ -245,7 +243,7 @@ class TransferEntropyEngine:
         kobj = self._select_kernel(kernel, b_max, True, smem_optin, smem_bytes, npv,
                                    source_filter)
         info = {"n_vars": n_vars, "T": T, "K": K, "tau": tau, "n_pairs": n_vars * (n_vars - 1),
-                "device_ids": device_ids, "n_gpus": 1,
+                "device_ids": device_ids, "n_gpus": len(device_ids),
                 "binning_method": binning_method if binarization is None else binarization,
                 "binarization": binarization, "kp": kp, "b_max_before_coarsen": b_max,
                 "b_max": b_max, "kernel": kobj.name, "smem_optin": smem_optin,
@@ -257,9 +255,15 @@ class TransferEntropyEngine:
         if kobj.is_matrix_kernel:
             info.update(mode="matrix", pair_free=False, coarsened=False)
             mark(4)
-            m = kobj.compute_matrix_device(db, tau)  # [src, tgt] = TE(src -> tgt)
-            mark(5)
-            self._result_matrix = m.cpu().numpy()
+            if len(device_ids) > 1:
+                # [i, j] = TE(j -> i) from the matrix kernels' multi-device entry
+                self._result_matrix = kobj.compute_matrix_multi_gpu(
+                    self._host_bins(db), n_vars, tau, device_ids).T.copy()
+                mark(5)
+            else:
+                m = kobj.compute_matrix_device(db, tau)  # [src, tgt] = TE(src -> tgt)
+                mark(5)
+                self._result_matrix = m.cpu().numpy()
             self._finish(info, db, npv, b_max, ev, stream, t0, "matrix")
             return self._wrap_result()
 
@@ -275,22 +279,69 @@ class TransferEntropyEngine:
         if source_filter:
             info.update(mode="pair", pair_free=False)
             pairs = self._build_pairs(n_vars)
-            from tenex_b200.kernels.pair_list import te_pair_list
-            te = te_pair_list(work, npv_w, b_max_w, tau, pairs,
-                              cfg=getattr(kobj, "cfg", None))
-            mark(6)
-            te_h = te.cpu().numpy()
+            if len(device_ids) > 1:
+                te_h = kobj.compute_multi_gpu(self._host_bins(work), pairs, b_max_w,
+                                              npv_w.cpu(), tau, batch_size, device_ids)
+                mark(6)
+            else:
+                from tenex_b200.kernels.pair_list import te_pair_list
+                te = te_pair_list(work, npv_w, b_max_w, tau, pairs,
+                                  cfg=getattr(kobj, "cfg", None))
+                mark(6)
+                te_h = te.cpu().numpy()
             rm = np.zeros((n_vars, n_vars), dtype=np.float32)
             rm[pairs[:, 0], pairs[:, 1]] = te_h
             self._result_matrix = rm.T.copy()
         else:
             info.update(mode="pairfree", pair_free=True)
-            m = kobj.compute_pairfree_device(work, npv_w, b_max_w, tau, matrix=True,
-                                             autotune_shape=autotune)
-            mark(6)
-            self._result_matrix = m.cpu().numpy()
+            if len(device_ids) > 1:
+                self._result_matrix = self._pairfree_multi_device(
+                    kobj, work, npv_w, b_max_w, tau, device_ids, autotune)
+                mark(6)
+            else:
+                m = kobj.compute_pairfree_device(work, npv_w, b_max_w, tau, matrix=True,
+                                                 autotune_shape=autotune)
+                mark(6)
+                self._result_matrix = m.cpu().numpy()
         self._finish(info, work, npv_w, b_max_w, ev, stream, t0, "pair")
         return self._wrap_result()
+
+    @staticmethod
+    def _host_bins(db: D.DeviceBins) -> np.ndarray:
+        """(n, T, K) host copy of device bins (the padding dropped)."""
+        return db.data[:, :db.row_len].cpu().numpy().reshape(db.n, db.T, db.K)
+
+    @staticmethod
+    def _pairfree_multi_device(kobj, work: D.DeviceBins, npv: torch.Tensor, b_max: int,
+                               tau: int, device_ids: list, autotune: bool) -> np.ndarray:
+        """All-pairs TE split over devices: contiguous pair-id chunks of
+        ceil(n(n-1) / devices), one host thread per device with its own copy of the
+        prepared bins; the per-device matrices hold disjoint entries and are summed
+        (exactly: every entry has one non-zero contributor)."""
+        from concurrent.futures import ThreadPoolExecutor
+        from tenex_b200.distributed import pair_range
+        n = work.n
+        total = n * (n - 1)
+        host = work.data.cpu()
+        npv_h = npv.cpu()
+
+        def run(rank: int):
+            p0, p1 = pair_range(total, rank, len(device_ids))
+            if p1 <= p0:
+                return None
+            torch.cuda.set_device(device_ids[rank])
+            dev = torch.device("cuda", device_ids[rank])
+            db = D.DeviceBins(host.to(dev), n, work.T, work.K)
+            m = kobj.compute_pairfree_device(db, npv_h.to(dev), b_max, tau, p0, p1 - p0,
+                                             matrix=True, autotune_shape=autotune)
+            return m.cpu().numpy()
+
+        with ThreadPoolExecutor(max_workers=len(device_ids)) as ex:
+            parts = [p for p in ex.map(run, range(len(device_ids))) if p is not None]
+        out = parts[0].copy()
+        for p in parts[1:]:
+            out += p
+        return out
 
     def _finish(self, info, db, npv, b_max, ev, stream, t0, mode):
         if ev is not None:

@@ -174,3 +174,25 @@ def test_multi_device_and_cross_block_entry_points(cuda):
     m1 = g.compute_matrix(xb[..., None], 20, 1, cuda)
     m2 = g.compute_matrix_multi_gpu(xb[..., None], 20, 1, [0])
     assert np.array_equal(m1, m2)
+
+
+def test_compute_over_several_devices(cuda):
+    # devices=[0, 0]: two host threads, two pair-id chunks (one device here, the
+    # same code path as two GPUs); equal to the single-device matrix
+    x, _ = W.cfg1_expression(n=40, T=300, seed=3)
+    names = np.array([f"g{i}" for i in range(40)])
+    one = TransferEntropyEngine(x, names).compute(accelerator="gpu", devices=[0]).matrix
+    two = TransferEntropyEngine(x, names).compute(accelerator="gpu", devices=[0, 0])
+    assert np.max(np.abs(two.matrix - one)) <= 1e-6
+    assert np.all(np.diag(two.matrix) == 0)
+    tf = names[:6]
+    a = TransferEntropyEngine(x, names, sources=tf).compute(accelerator="gpu", devices=[0]).matrix
+    b = TransferEntropyEngine(x, names, sources=tf).compute(accelerator="gpu", devices=[0, 0]).matrix
+    assert np.max(np.abs(a - b)) <= 1e-6
+    xb = (np.random.default_rng(4).random((25, 300)) < 0.4).astype(np.float32)
+    nb = np.array([f"b{i}" for i in range(25)])
+    c = TransferEntropyEngine(xb, nb).compute(accelerator="gpu", devices=[0],
+                                              binarization="nonzero").matrix
+    d = TransferEntropyEngine(xb, nb).compute(accelerator="gpu", devices=[0, 0],
+                                              binarization="nonzero").matrix
+    assert np.array_equal(c, d)
