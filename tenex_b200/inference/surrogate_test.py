@@ -232,10 +232,8 @@ class SurrogateTestMethod:
         if dev.type != "cuda":
             raise RuntimeError("the surrogate test runs on a CUDA device")
         devices = kwargs.get("devices")
-        if devices:
-            if len(devices) > 1:
-                raise NotImplementedError("one process drives one GPU")
-            dev = torch.device("cuda", int(devices[0]))
+        device_ids = [int(d) for d in devices] if devices else [dev.index or 0]
+        dev = torch.device("cuda", device_ids[0])
         torch.cuda.set_device(dev)
         observed_te = np.asarray(te_matrix, dtype=np.float32)
         if null == "learned":
@@ -246,9 +244,16 @@ class SurrogateTestMethod:
                                           fdr, seed, kwargs)
         _log.vprint(f"[TENEX] surrogate_test: {n_surrogates} shuffles (method={shuffle_method}, "
                     f"block_length={block_length}, kernel={kernel_name}, p={p_method})")
-        sum_surr, sum_sq_surr, count_ge = self.accumulate(
-            observed_te, dev, bin_data, n_per_var, int(b_max), kernel_name, tau, n_surrogates,
-            shuffle_method, block_length, seed, use_graph)
+        # the binary path updates the whole matrix per surrogate (sub-millisecond each):
+        # it stays on the first device
+        if len(device_ids) == 1 or kernel_name == "GEMM-B2":
+            sum_surr, sum_sq_surr, count_ge = self.accumulate(
+                observed_te, dev, bin_data, n_per_var, int(b_max), kernel_name, tau,
+                n_surrogates, shuffle_method, block_length, seed, use_graph)
+        else:
+            sum_surr, sum_sq_surr, count_ge = self._accumulate_devices(
+                observed_te, device_ids, bin_data, n_per_var, int(b_max), kernel_name, tau,
+                n_surrogates, shuffle_method, block_length, seed, use_graph)
         mean_surr, std_surr, effective_te, p_values = surrogate_statistics(
             observed_te, sum_surr, sum_sq_surr, count_ge, n_surrogates, p_method)
         grn, _ = bh_edges(p_values, effective_te, variable_names, kwargs.get("sources"), fdr,
@@ -261,10 +266,38 @@ class SurrogateTestMethod:
                                    block_length=block_length if shuffle_method == "block"
                                    else None, p_method=p_method, fdr=fdr)
 
+    @classmethod
+    def _accumulate_devices(cls, observed_te, device_ids, bin_data, n_per_var, b_max,
+                            kernel_name, tau, n_surrogates, shuffle_method, block_length, seed,
+                            use_graph=False):
+        """The reference's multi-GPU split of the fused path
+        (tenex/inference/surrogate_test.py:812-842): pair-id boundaries
+        linspace(0, n(n-1), devices + 1), one host thread per device running every
+        surrogate on its pairs; the disjoint per-device sums add exactly, and the
+        diagonal's count_ge is added once."""
+        from concurrent.futures import ThreadPoolExecutor
+        n = bin_data.shape[0]
+        bnd = np.linspace(0, n * (n - 1), len(device_ids) + 1, dtype=np.int64)
+
+        def work(rank: int):
+            torch.cuda.set_device(device_ids[rank])
+            d = torch.device("cuda", device_ids[rank])
+            return cls.accumulate(observed_te, d, bin_data, n_per_var, b_max, kernel_name, tau,
+                                  n_surrogates, shuffle_method, block_length, seed, use_graph,
+                                  pair_offset=int(bnd[rank]),
+                                  n_pairs=int(bnd[rank + 1] - bnd[rank]), diag_count=False)
+
+        with ThreadPoolExecutor(max_workers=len(device_ids)) as ex:
+            parts = list(ex.map(work, range(len(device_ids))))
+        s1, s2, c = (sum(p[i] for p in parts) for i in range(3))
+        diag = np.arange(n)
+        c[diag, diag] += n_surrogates
+        return s1, s2, c
+
     @staticmethod
     def accumulate(observed_te, dev, bin_data, n_per_var, b_max, kernel_name, tau, n_surrogates,
                    shuffle_method, block_length, seed, use_graph=False, k_start=0,
-                   pair_offset=0, n_pairs=None):
+                   pair_offset=0, n_pairs=None, diag_count=True):
         """float64 sum, sum of squares and int32 count_ge (numpy, (n, n)) over
         surrogates [k_start, k_start + n_surrogates), diagonal count included."""
         n_vars, T, K = bin_data.shape
@@ -284,6 +317,7 @@ class SurrogateTestMethod:
                                         k_start + n_surrogates, seed, dev)
         run_surrogates(acc, perms, bl, use_graph)
         count = acc.cnt.cpu().numpy()
-        diag = np.arange(n_vars)
-        count[diag, diag] += n_surrogates  # te_k >= observed holds on the diagonal (0 >= 0)
+        if diag_count:
+            diag = np.arange(n_vars)
+            count[diag, diag] += n_surrogates  # te_k >= observed holds on the diagonal (0 >= 0)
         return acc.sum.cpu().numpy(), acc.sumsq.cpu().numpy(), count

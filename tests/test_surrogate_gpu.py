@@ -116,3 +116,24 @@ def test_pipeline_multi_lag_surrogate(cuda):
         assert np.array_equal(multi.p_values, ref.p_values)
         assert np.array_equal(multi.effective_te, ref.effective_te)
         assert np.array_equal(multi.grn.pairs, ref.grn.pairs)
+
+
+def test_surrogate_over_several_devices(cuda):
+    # devices=[0, 0]: the pair range split over two host threads (one GPU here, the
+    # same code path as two); the same statistics as one device up to float rounding
+    from tenex_b200 import workloads as W
+    from tenex_b200.kernels import device as Dv
+    from tenex_b200.kernels.full_smem import FullSMEMKernel
+    x, npv, _ = W.cfg5_bins(n=60, T=600, seed=77)
+    obs = FullSMEMKernel().compute_pairfree_device(
+        Dv.pack_bins(x, cuda), torch.as_tensor(npv, device=cuda), int(npv.max()), 1,
+        matrix=True).cpu().numpy()
+    names = np.array([f"g{i}" for i in range(60)])
+    kw = dict(bin_data=x, n_per_var=npv, b_max=int(npv.max()), kernel="Full-SMEM", tau=1,
+              n_surrogates=12, block_length=20, fdr=0.05, seed=5)
+    one = NetWeaver((obs, names), fdr=0.05).infer("surrogate_test", device=cuda, **kw)
+    two = NetWeaver((obs, names), fdr=0.05).infer("surrogate_test", device=cuda,
+                                                   devices=[0, 0], **kw)
+    assert np.allclose(one.mean_surrogate_te, two.mean_surrogate_te, rtol=1e-6, atol=1e-8)
+    assert np.allclose(one.p_values, two.p_values, rtol=1e-4, atol=1e-6)
+    assert np.array_equal(one.grn.pairs, two.grn.pairs)
