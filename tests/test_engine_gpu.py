@@ -8,7 +8,6 @@ from tenex_b200 import TransferEntropyEngine, workloads as W
 from tenex_b200.kernels import device as D
 from tenex_b200.kernels.adaptive_smem import AdaptiveSMEMKernel
 from tenex_b200.preprocess import coarsen_bins, discretize, fsbwl_bins, remap_bins
-from tenex_b200.binarize import binarize
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-6

@@ -4,7 +4,6 @@ import pytest
 import torch
 
 from oracle import mlp_oracle as M
-from oracle import oracle as O
 from tenex_b200 import native, workloads as W
 from tenex_b200.inference import learned_null as LN
 from tenex_b200.kernels import device as D

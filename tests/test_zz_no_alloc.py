@@ -10,7 +10,6 @@ the next), and require the same TE within the suite's 1e-6 tolerance. This
 file is collected last so a failure here leaves the rest of the suite's
 results intact.
 """
-import ctypes
 
 import numpy as np
 import pytest
