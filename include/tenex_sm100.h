@@ -209,16 +209,17 @@ int tenex_binarize(const float* x, int64_t ldx, int n_vars, int T, int mode,
 
 /* Binary (b_max = 2) TE matrix on the tensor cores; replaces compute_te_gemm_b2
  * (tenex/kernels/gemm_b2.py:307-425) and its Triton epilogue (:65-187).
- * bins: uint8 {0,1} padded rows; out[src * out_ld + tgt] = TE(src -> tgt)
- * (diagonal untouched; the caller zeroes it). L = row_len - lag < 2^24.
- * workspace: tenex_b2_workspace_bytes(), 256-byte aligned (operand copies and
- * per-gene counts). */
+ * bins: uint8 {0,1} padded rows (read in place by TMA: 16-byte aligned rows);
+ * out[src * out_ld + tgt] = TE(src -> tgt) (diagonal untouched; the caller
+ * zeroes it). L = row_len - lag < 2^24. workspace: tenex_b2_workspace_bytes(),
+ * 256-byte aligned (the lag-shifted operand copy and per-gene counts). */
 size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t lag);
 int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
                            int64_t lag, float* out, int64_t out_ld, void* workspace,
                            size_t workspace_bytes, void* stream);
 /* Error word of the last tenex_te_binary_matrix call on this workspace
- * (synchronises `stream`): TENEX_ERR_TIMEOUT if a pipeline wait expired. */
+ * (synchronises `stream`): TENEX_ERR_BADDATA if a bin was not 0 or 1,
+ * TENEX_ERR_TIMEOUT if a pipeline wait expired. */
 int tenex_b2_status(const void* workspace, int n_vars, int64_t row_len, int64_t lag,
                     void* stream);
 

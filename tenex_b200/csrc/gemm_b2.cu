@@ -41,6 +41,8 @@ constexpr int kKt = 128;       // bytes of K per pipeline stage (4 MMA K-steps o
 constexpr int kStages = 3;
 constexpr int kOpBytes = kKt * kTile;          // one operand tile per stage (16 KB)
 constexpr int kStageBytes = 4 * kOpBytes;      // FP, P, F (targets) + P (sources)
+constexpr int kTmaBytes = 3 * kOpBytes;        // P, F, P by TMA; FP = F & P made in smem
+constexpr int kFpWarps = 8;                    // warps 8..15 form FP during the main loop
 constexpr int kTmemCols = 512;
 
 struct B2Params {
@@ -50,7 +52,7 @@ struct B2Params {
   const int32_t* marg;  // (3, n): nf, np, nfp
   float* out;       // (n, n): out[src * ld + tgt]
   int64_t out_ld;
-  int* err;         // device error word (1 = a wait expired)
+  int* err;         // device error word (1 = a wait expired, 2 = a bin was not 0/1)
 };
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
@@ -76,21 +78,21 @@ __device__ __forceinline__ float cell_term(float c, float c1, float c2a, float c
   return c * __log2f(r);
 }
 
-// Pack: F[g, t] = x[g, t+lag] != 0, P[g, t] = x[g, t] != 0, FP = F & P for t < L
-// (0 beyond, up to Lpad), plus nf, np, nfp. One CTA per gene; each thread makes
-// 16 bytes of each operand from 16-byte loads (F's source window is shifted by
-// lag, taken from two aligned loads), with a scalar path for the row end.
-__device__ __forceinline__ uint32_t nz01(uint32_t w) { return __vcmpne4(w, 0u) & 0x01010101u; }
-
+// Pack: F[g, t] = x[g, t+lag] for t < L (0 beyond, up to Lpad), the lag-shifted
+// operand TMA cannot address (its copies start on 16-byte boundaries), plus the
+// per-gene counts nf, np, nfp (P = x[g, t] is read from the bins directly, FP =
+// F & P is formed in shared memory). One CTA per gene; each thread makes 16
+// bytes of F from two aligned 16-byte loads, with a scalar path for the row end.
+// Every bin must be 0 or 1 (the GEMM sums the raw bytes): a larger value sets
+// the error word to 2.
 __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L,
                                int lag, int Lpad, uint8_t* __restrict__ ops,
-                               int32_t* __restrict__ marg) {
+                               int32_t* __restrict__ marg, int* __restrict__ err) {
   const int g = blockIdx.x;
   const uint8_t* row = bins + (int64_t)g * ld;
-  uint8_t* Fr = ops + ((int64_t)0 * n + g) * Lpad;
-  uint8_t* Pr = ops + ((int64_t)1 * n + g) * Lpad;
-  uint8_t* FPr = ops + ((int64_t)2 * n + g) * Lpad;
+  uint8_t* Fr = ops + (int64_t)g * Lpad;
   int nf = 0, np = 0, nfp = 0;
+  uint32_t high = 0;  // any bit above bit 0 of a byte: a bin other than 0/1
   const int sh = lag & 15;
   for (int t = threadIdx.x * 16; t < Lpad; t += blockDim.x * 16) {
     uint32_t f[4], p[4];
@@ -107,8 +109,9 @@ __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int
         const int byte = sh + 4 * k;
         const uint32_t lo = w[byte >> 2], hi = w[(byte >> 2) + 1];
         const uint32_t fw = __funnelshift_r(lo, hi, (byte & 3) * 8);
-        f[k] = nz01(fw);
-        p[k] = nz01(pw[k]);
+        high |= (fw | pw[k]) & 0xfefefefeu;
+        f[k] = fw;
+        p[k] = pw[k];
       }
     } else {
 #pragma unroll
@@ -117,20 +120,16 @@ __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int
         for (int j = 0; j < 4; ++j) {
           const int tt = t + 4 * k + j;
           if (tt < L) {
-            fk |= (row[tt + lag] ? 1u : 0u) << (8 * j);
-            pk |= (row[tt] ? 1u : 0u) << (8 * j);
+            fk |= (uint32_t)row[tt + lag] << (8 * j);
+            pk |= (uint32_t)row[tt] << (8 * j);
           }
         }
+        high |= (fk | pk) & 0xfefefefeu;
         f[k] = fk;
         p[k] = pk;
       }
     }
-    const uint4 fv = make_uint4(f[0], f[1], f[2], f[3]);
-    const uint4 pv4 = make_uint4(p[0], p[1], p[2], p[3]);
-    const uint4 fpv = make_uint4(f[0] & p[0], f[1] & p[1], f[2] & p[2], f[3] & p[3]);
-    *reinterpret_cast<uint4*>(Fr + t) = fv;
-    *reinterpret_cast<uint4*>(Pr + t) = pv4;
-    *reinterpret_cast<uint4*>(FPr + t) = fpv;
+    *reinterpret_cast<uint4*>(Fr + t) = make_uint4(f[0], f[1], f[2], f[3]);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       nf += __popc(f[k]);
@@ -156,11 +155,13 @@ __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
     marg[(int64_t)threadIdx.x * n + g] = s;
   }
+  if (high) atomicExch(err, 2);
 }
 
-// Tensor maps of the three operand matrices (each n x Lpad bytes).
+// Tensor maps of the operands: F (packed, n x Lpad) and P (the bins themselves,
+// n x L with row stride ld; TMA fills columns >= L and rows >= n with zeros).
 struct B2Maps {
-  CUtensorMap F, P, FP;
+  CUtensorMap F, P;
 };
 
 constexpr int kB2Threads = 512;
@@ -173,7 +174,8 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   unsigned char* stage_base = smem;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accbar = empty + kStages;
+  uint64_t* fpready = empty + kStages;  // FP tile of the stage written (kFpWarps arrivals)
+  uint64_t* accbar = fpready + kStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accbar + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -187,6 +189,7 @@ __global__ void __launch_bounds__(kB2Threads, 1)
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
+      mbar_init(&fpready[s], kFpWarps);
     }
     mbar_init(accbar, 1);
     *abort_flag = 0;
@@ -203,30 +206,47 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
+  // ---- producer (warp 0, lane 0): TMA loads of stage k into buffer k % kStages,
+  // each once the MMAs that read the buffer's previous contents completed --------
   if (tid == 0) {
-    // ---- producer: TMA loads of stage k into buffer k % kStages -----------
-    // (one thread also issues the MMAs: producer runs kStages ahead)
-    const uint32_t idesc = idesc_i8(kTile, kTile);
     int issued = 0;
     bool ok = true;
-    auto load_stage = [&](int k) {
+    for (int k = 0; k < nk; ++k) {
       const int s = k % kStages;
+      if (k >= kStages &&
+          (*(volatile int*)abort_flag || !mbar_wait(&empty[s], (uint32_t)(((k / kStages) - 1) & 1)))) {
+        ok = false;
+        break;
+      }
       unsigned char* buf = stage_base + s * kStageBytes;
-      mbar_expect_tx(&full[s], kStageBytes);
+      mbar_expect_tx(&full[s], kTmaBytes);
       const int x0 = k * kKt;
-      // one 128-byte x 128-row box per operand, 128-byte swizzled
-      tma_load_2d(buf + 0 * kOpBytes, &maps.FP, x0, m0, &full[s]);
+      // one 128-byte x 128-row box per operand, 128-byte swizzled (FP: see below)
       tma_load_2d(buf + 1 * kOpBytes, &maps.P, x0, m0, &full[s]);
       tma_load_2d(buf + 2 * kOpBytes, &maps.F, x0, m0, &full[s]);
       tma_load_2d(buf + 3 * kOpBytes, &maps.P, x0, n0, &full[s]);
-    };
-    const int pre = nk < kStages ? nk : kStages;
-    for (int k = 0; k < pre; ++k) load_stage(k);
-    issued = pre;
-    for (int k = 0; k < nk && ok; ++k) {
+      issued = k + 1;
+    }
+    if (!ok) {
+      // no exit with copies in flight: wait (bounded) for every issued load
+      atomicExch(prm.err, 1);
+      *(volatile int*)abort_flag = 1;
+      for (int k = issued - kStages > 0 ? issued - kStages : 0; k < issued; ++k)
+        (void)mbar_wait(&full[k % kStages], (uint32_t)((k / kStages) & 1));
+    }
+  }
+
+  // ---- MMA issuer (warp 1, lane 0): stage k's 3 x 4 MMAs as soon as its operands
+  // (TMA) and its FP tile are in place; never waits on MMA completion, so the
+  // tensor pipe gets the stages back to back ----------------------------------
+  if (tid == 32) {
+    const uint32_t idesc = idesc_i8(kTile, kTile);
+    bool ok = true;
+    for (int k = 0; k < nk; ++k) {
       const int s = k % kStages;
       const uint32_t ph = (uint32_t)((k / kStages) & 1);
-      if (!mbar_wait(&full[s], ph)) {
+      if (*(volatile int*)abort_flag || !mbar_wait(&full[s], ph) ||
+          !mbar_wait(&fpready[s], ph)) {
         ok = false;
         break;
       }
@@ -246,32 +266,46 @@ __global__ void __launch_bounds__(kB2Threads, 1)
         mma_i8(tmem + 256, smem_desc_sw128(aF + off), bd, idesc, acc);
       }
       mma_commit(&empty[s]);  // stage s free once these MMAs complete
-      const int kn = k + kStages;
-      if (kn < nk) {
-        if (!mbar_wait(&empty[s], ph)) {
-          ok = false;
-          break;
-        }
-        load_stage(kn);
-        issued = kn + 1;
-      }
     }
-    if (ok) {
-      mma_commit(accbar);
-    } else {
-      // drain: wait (bounded) for every stage load still in flight, then abort
+    if (!ok) {
       atomicExch(prm.err, 1);
-      for (int k = 0; k < issued; ++k) {
-        const int s = k % kStages;
-        (void)mbar_wait(&full[s], (uint32_t)((k / kStages) & 1));
-      }
       *(volatile int*)abort_flag = 1;
-      mma_commit(accbar);  // still arrives (after any issued MMAs) so waiters wake
+    }
+    mma_commit(accbar);  // arrives after every issued MMA, so the epilogue wakes either way
+  }
+
+  // ---- FP = F & P of every stage, by warps 8..15 (idle until the epilogue) ---
+  // The three tiles have the same 128-byte swizzled layout, so the byte-wise AND
+  // of the F and P tiles is the FP tile. The stores are made visible to the
+  // tensor core's operand reads (async proxy) before the arrival the MMA thread
+  // waits on. The producer reloads a stage only after its MMAs completed, which
+  // needs this stage's FP first, so a stage's FP is never overwritten early.
+  if (warp >= 16 - kFpWarps) {
+    const int ft = tid - (16 - kFpWarps) * 32;
+    for (int k = 0; k < nk; ++k) {
+      if (*(volatile int*)abort_flag) break;
+      const int s = k % kStages;
+      if (!mbar_wait(&full[s], (uint32_t)((k / kStages) & 1))) {
+        atomicExch(prm.err, 1);
+        break;
+      }
+      unsigned char* buf = stage_base + s * kStageBytes;
+      const uint4* P4 = reinterpret_cast<const uint4*>(buf + 1 * kOpBytes);
+      const uint4* F4 = reinterpret_cast<const uint4*>(buf + 2 * kOpBytes);
+      uint4* FP4 = reinterpret_cast<uint4*>(buf);
+#pragma unroll
+      for (int c = ft; c < kOpBytes / 16; c += kFpWarps * 32) {
+        const uint4 f = F4[c], p = P4[c];
+        FP4[c] = make_uint4(f.x & p.x, f.y & p.y, f.z & p.z, f.w & p.w);
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if ((tid & 31) == 0) mbar_arrive(&fpready[s]);
     }
   }
 
   // ---- epilogue: 16 warps; lane quarter warp % 4, column quarter warp / 4 ---
-  bool ok_acc = tid == 0 ? mbar_wait(accbar, 0) : mbar_wait_sleep(accbar, 0, 200);
+  bool ok_acc = mbar_wait_sleep(accbar, 0, 200);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!ok_acc && tid == 0) atomicExch(prm.err, 1);
@@ -343,11 +377,12 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-static int make_map(CUtensorMap* map, const uint8_t* base, int rows, int Lpad) {
+static int make_map(CUtensorMap* map, const uint8_t* base, int rows, int64_t cols,
+                    int64_t stride) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return fail(TENEX_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
-  const cuuint64_t dims[2] = {(cuuint64_t)Lpad, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)Lpad};
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)stride};
   const cuuint32_t box[2] = {(cuuint32_t)kKt, (cuuint32_t)kTile};
   const cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
@@ -366,7 +401,7 @@ extern "C" size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t 
   if (n_vars < 1 || row_len <= lag) return 256;
   const int64_t L = row_len - lag;
   const int64_t Lpad = round_up(L, kKt);
-  return (size_t)(round_up(3 * (int64_t)n_vars * Lpad, 256) + round_up(3 * (int64_t)n_vars * 4, 256) +
+  return (size_t)(round_up((int64_t)n_vars * Lpad, 256) + round_up(3 * (int64_t)n_vars * 4, 256) +
                   256);
 }
 
@@ -393,19 +428,18 @@ extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_var
     return fail(TENEX_ERR_BADARG, "workspace must be 256-byte aligned");
   unsigned char* ws = reinterpret_cast<unsigned char*>(workspace);
   uint8_t* ops = ws;
-  int32_t* marg = reinterpret_cast<int32_t*>(ws + round_up(3 * (int64_t)n_vars * Lpad, 256));
-  int* err = reinterpret_cast<int*>(ws + round_up(3 * (int64_t)n_vars * Lpad, 256) +
+  int32_t* marg = reinterpret_cast<int32_t*>(ws + round_up((int64_t)n_vars * Lpad, 256));
+  int* err = reinterpret_cast<int*>(ws + round_up((int64_t)n_vars * Lpad, 256) +
                                     round_up(3 * (int64_t)n_vars * 4, 256));
   cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), stream);
   if (e != cudaSuccess) return check_cuda(e, "memset");
   b2_pack_kernel<<<n_vars, 256, 0, stream>>>(bins, ld, n_vars, (int)L, (int)lag, (int)Lpad, ops,
-                                             marg);
+                                             marg, err);
   int st = check_launch("b2_pack_kernel");
   if (st) return st;
   B2Maps maps;
-  if ((st = make_map(&maps.F, ops, n_vars, (int)Lpad))) return st;
-  if ((st = make_map(&maps.P, ops + (int64_t)n_vars * Lpad, n_vars, (int)Lpad))) return st;
-  if ((st = make_map(&maps.FP, ops + 2 * (int64_t)n_vars * Lpad, n_vars, (int)Lpad))) return st;
+  if ((st = make_map(&maps.F, ops, n_vars, Lpad, Lpad))) return st;
+  if ((st = make_map(&maps.P, bins, n_vars, L, ld))) return st;
   B2Params prm;
   prm.n = n_vars;
   prm.L = (int)L;
@@ -428,12 +462,13 @@ extern "C" int tenex_b2_status(const void* workspace, int n_vars, int64_t row_le
   const int64_t L = row_len - lag;
   const int64_t Lpad = round_up(L, kKt);
   const unsigned char* ws = reinterpret_cast<const unsigned char*>(workspace);
-  const int* err = reinterpret_cast<const int*>(ws + round_up(3 * (int64_t)n_vars * Lpad, 256) +
+  const int* err = reinterpret_cast<const int*>(ws + round_up((int64_t)n_vars * Lpad, 256) +
                                                 round_up(3 * (int64_t)n_vars * 4, 256));
   int h = 0;
   cudaError_t e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, as_stream(stream));
   if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
   if (e != cudaSuccess) return check_cuda(e, "tenex_b2_status");
+  if (h == 2) return fail(TENEX_ERR_BADDATA, "binary bins must be 0 or 1; results invalid");
   if (h) return fail(TENEX_ERR_TIMEOUT, "a tensor-core pipeline wait expired; results invalid");
   return TENEX_OK;
 }
