@@ -309,7 +309,8 @@ def run_ours(args) -> None:
                     "note": "compulsory bytes (bins read once + float32 outputs) / launch time; "
                             "peak = MEASURED_PEAKS.json hbm_gbs (of measured)"}
     cpu = cpu_baseline(*_coarsened_host(x, npv, limit)) if not args.no_cpu_baseline else None
-    sur = surrogate_leg(dev) if (world == 1 and not args.no_surrogate) else None
+    sur = (surrogate_leg(dev, with_cpu=not args.no_cpu_baseline)
+           if (world == 1 and not args.no_surrogate) else None)
     binl = binary_leg(dev) if (world == 1 and not args.no_surrogate) else None
     fdrl = fdr_leg(dev, out) if (world == 1 and not args.no_fdr and total == G * (G - 1)) else None
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
@@ -332,7 +333,7 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
-def surrogate_leg(dev, reps: int = 2) -> dict:
+def surrogate_leg(dev, reps: int = 2, with_cpu: bool = True) -> dict:
     """Wall seconds of NetWeaver's surrogate test on cfg5 (2,000 genes x 5,000 cells,
     100 block shuffles of length 50, seed 42, BH-FDR 0.05, parametric p): the full
     test against the learned null, each after one warm-up call, with the edge-set
@@ -365,6 +366,7 @@ def surrogate_leg(dev, reps: int = 2) -> dict:
 
     t_full, full = timed()
     t_lrn, lrn = timed(reps=5, null="learned")
+    cpu = surrogate_cpu_baseline(x, npv, 100, 50, 42, dev) if with_cpu else None
     e1 = set(map(tuple, full.grn.pairs.tolist()))
     e2 = set(map(tuple, lrn.grn.pairs.tolist()))
     inter = len(e1 & e2)
@@ -377,7 +379,33 @@ def surrogate_leg(dev, reps: int = 2) -> dict:
             "jaccard": inter / max(1, len(e1 | e2)), "precision": inter / max(1, len(e2)),
             "recall": inter / max(1, len(e1)),
             "verified_fraction": lrn.info.get("fallback_fraction"),
-            "band": lrn.info.get("band")}
+            "band": lrn.info.get("band"), "cpu_baseline": cpu}
+
+
+def surrogate_cpu_baseline(x, npv, S: int, bl: int, seed: int, dev, n_pairs: int = 100_000,
+                           n_shuffles: int = 5) -> dict:
+    """The CPU oracle on the surrogate workload: the first `n_shuffles` of the
+    test's own block shuffles (same permutations), `n_pairs` pair ids each, on all
+    host threads; the full test's CPU time extrapolated linearly in pairs x shuffles."""
+    from oracle import oracle as O
+    from tenex_b200.inference.surrogate_test import build_block_perm
+    n, T = x.shape[0], x.shape[1]
+    perms, blk, _ = build_block_perm(n, T, "block", bl, 0, n_shuffles, seed, dev)
+    perms = perms.cpu().numpy()
+    nthreads = os.cpu_count() or 1
+    total = n * (n - 1)
+    p0 = (total - n_pairs) // 2
+    dt = 0.0
+    for k in range(n_shuffles):
+        sh = O.block_shuffle(x, perms[k], blk)
+        t0 = time.time()
+        O.te_pairfree(sh, npv, 1, p0, n_pairs, threads=nthreads)
+        dt += time.time() - t0
+    rate = n_pairs * n_shuffles / dt
+    return {"value": rate, "unit": "pair-surrogate TEs/s", "cores": nthreads, "kind": "port",
+            "est_full_test_s": total * S / rate,
+            "sample": f"{n_shuffles} of the test's block shuffles x pair ids [{p0}, {p0 + n_pairs}) "
+                      f"({dt:.1f} s on {nthreads} threads; C oracle, float64 TE)"}
 
 
 def binary_leg(dev, reps: int = 5) -> dict:
