@@ -308,7 +308,8 @@ def run_ours(args) -> None:
                     "frac": (compulsory / (te_ms / 1e3) / 1e9 / hbm_peak) if hbm_peak else None,
                     "note": "compulsory bytes (bins read once + float32 outputs) / launch time; "
                             "peak = MEASURED_PEAKS.json hbm_gbs (of measured)"}
-    cpu = cpu_baseline(*_coarsened_host(x, npv, limit)) if not args.no_cpu_baseline else None
+    cpu = (cpu_baseline(*_coarsened_host(x, npv, limit))
+           if (world == 1 and not args.no_cpu_baseline) else None)   # rank 0 at N=1 only
     sur = (surrogate_leg(dev, with_cpu=not args.no_cpu_baseline)
            if (world == 1 and not args.no_surrogate) else None)
     binl = binary_leg(dev) if (world == 1 and not args.no_surrogate) else None
