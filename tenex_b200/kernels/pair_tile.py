@@ -20,7 +20,7 @@ from tenex_b200.kernels import device as D
 
 # Launch shapes the autotuner tries: (threads, ctas_per_sm, src_chunk)
 TUNE_SPACE = [(512, 2, 128), (1024, 1, 128), (512, 1, 128), (256, 2, 64), (1024, 1, 64),
-              (512, 2, 64), (512, 2, 256), (256, 4, 128), (256, 4, 256)]
+              (512, 2, 64), (512, 2, 256), (256, 4, 128), (256, 4, 256), (1024, 1, 256)]
 DEFAULT_CFG = dict(threads=512, ctas_per_sm=2, src_chunk=128)
 _tune_cache: dict[tuple, dict] = {}
 
@@ -31,10 +31,12 @@ def _npv_tensor(n_per_var, device) -> torch.Tensor:
 
 
 def autotune(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int = 1,
-             sample_pairs: int = 400_000, space=TUNE_SPACE) -> dict:
+             sample_pairs: int = 2_000_000, space=TUNE_SPACE) -> dict:
     """Times each launch shape on a contiguous slice of pair ids (whole targets
     from the middle of the range) and returns the fastest; cached per
-    (device, n, T, K, b_max, tau, bin-count histogram)."""
+    (device, n, T, K, b_max, tau, bin-count histogram). The slice is large
+    enough (2M pairs: ~20 ms per shape at 10k genes x 20k cells) that the end
+    of a launch, where few items remain, does not decide between item sizes."""
     dev = db.data.device
     npv_h = npv.cpu().numpy()
     key = (torch.cuda.get_device_name(dev), db.n, db.T, db.K, int(b_max), int(tau),
