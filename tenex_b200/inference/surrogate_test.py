@@ -164,6 +164,54 @@ def pair_statistics(observed_te: np.ndarray, sum_surr: np.ndarray, sum_sq_surr: 
     return mean_surr, std_surr, effective_te, p_values
 
 
+def pair_statistics_device(observed_te: torch.Tensor, sum_surr: torch.Tensor,
+                           sum_sq_surr: torch.Tensor, count_ge: torch.Tensor, n_surrogates: int,
+                           p_method: str):
+    """pair_statistics on device tensors, op for op: float64 mean and population
+    variance (sum_sq / S - (sum / S)^2, the square as one multiply), float32 mean,
+    std and effective TE, z in float32, p = erfc(z / sqrt 2) / 2 in float64. Every
+    step is a separate correctly rounded IEEE operation as in numpy; only erfc is
+    CUDA's instead of scipy's (both within ~1 ulp of double, so the float32 p
+    agrees except where a value sits on a float32 rounding boundary)."""
+    m64 = sum_surr / n_surrogates
+    mean_surr = m64.float()
+    var_surr = sum_sq_surr / n_surrogates - m64 * m64
+    std_surr = torch.sqrt(torch.clamp(var_surr, min=0.0)).float()
+    effective_te = observed_te - mean_surr
+    if p_method == "parametric":
+        z = effective_te / torch.clamp(std_surr, min=np.float32(1e-12).item())
+        p_values = (0.5 * torch.special.erfc(z.double() / np.sqrt(2.0))).float()
+    else:
+        p_values = ((1.0 + count_ge.double()) / (1.0 + n_surrogates)).float()
+    return mean_surr, std_surr, effective_te, p_values
+
+
+def tested_mask(n: int, variable_names, sources, device) -> torch.Tensor:
+    """(n, n) bool: the pairs BH runs over (the source-filtered pairs, or every
+    off-diagonal pair)."""
+    if sources is not None:
+        pb = build_pairs(np.asarray(variable_names), sources)
+        mask = torch.zeros((n, n), dtype=torch.bool, device=device)
+        mask[torch.as_tensor(pb[:, 0], device=device), torch.as_tensor(pb[:, 1], device=device)] = True
+        return mask
+    return ~torch.eye(n, dtype=torch.bool, device=device)
+
+
+def bh_edges_device(p: torch.Tensor, eff: torch.Tensor, tested: torch.Tensor, variable_names,
+                    fdr: float) -> GRN:
+    """bh_edges on device matrices: BH over p[tested] (row-major, float32), edges
+    with adjusted p < fdr and effective TE > 0; the same edges as bh_edges gives
+    for the same float32 values."""
+    adj = bh_fdr_gpu(p[tested], alpha=fdr)
+    sig = torch.zeros_like(tested)
+    sig[tested] = adj < fdr
+    sig &= eff > 0
+    idx = torch.nonzero(sig)
+    pairs = idx.cpu().numpy().astype(np.int64)
+    te = eff[idx[:, 0], idx[:, 1]].cpu().numpy()
+    return make_grn(np.asarray(variable_names), pairs, te)
+
+
 def bh_edges(p_values: np.ndarray, effective_te: np.ndarray, variable_names, sources, fdr: float,
              device) -> tuple[GRN, np.ndarray]:
     """BH-FDR over the tested pairs; edges with adjusted p < fdr and effective TE > 0.
@@ -247,17 +295,27 @@ class SurrogateTestMethod:
         # the binary path updates the whole matrix per surrogate (sub-millisecond each):
         # it stays on the first device
         if len(device_ids) == 1 or kernel_name == "GEMM-B2":
-            sum_surr, sum_sq_surr, count_ge = self.accumulate(
-                observed_te, dev, bin_data, n_per_var, int(b_max), kernel_name, tau,
-                n_surrogates, shuffle_method, block_length, seed, use_graph)
+            # sums stay on the device: statistics and BH there, one copy back
+            sums = self.accumulate(observed_te, dev, bin_data, n_per_var, int(b_max),
+                                   kernel_name, tau, n_surrogates, shuffle_method, block_length,
+                                   seed, use_graph, as_numpy=False)
+            obs_d = torch.as_tensor(observed_te).to(dev)
+            stats = pair_statistics_device(obs_d, *sums, n_surrogates, p_method)
+            diag = torch.arange(observed_te.shape[0], device=dev)
+            stats[3][diag, diag] = 1.0
+            grn = bh_edges_device(stats[3], stats[2],
+                                  tested_mask(observed_te.shape[0], variable_names,
+                                              kwargs.get("sources"), dev),
+                                  variable_names, fdr)
+            mean_surr, std_surr, effective_te, p_values = torch.stack(stats).cpu().numpy()
         else:
             sum_surr, sum_sq_surr, count_ge = self._accumulate_devices(
                 observed_te, device_ids, bin_data, n_per_var, int(b_max), kernel_name, tau,
                 n_surrogates, shuffle_method, block_length, seed, use_graph)
-        mean_surr, std_surr, effective_te, p_values = surrogate_statistics(
-            observed_te, sum_surr, sum_sq_surr, count_ge, n_surrogates, p_method)
-        grn, _ = bh_edges(p_values, effective_te, variable_names, kwargs.get("sources"), fdr,
-                          dev)
+            mean_surr, std_surr, effective_te, p_values = surrogate_statistics(
+                observed_te, sum_surr, sum_sq_surr, count_ge, n_surrogates, p_method)
+            grn, _ = bh_edges(p_values, effective_te, variable_names, kwargs.get("sources"), fdr,
+                              dev)
         _log.vprint(f"[TENEX] surrogate_test: {len(grn)} significant edges (FDR<{fdr})")
         return SurrogateTestResult(observed_te=observed_te, mean_surrogate_te=mean_surr,
                                    std_surrogate_te=std_surr, effective_te=effective_te,
@@ -297,7 +355,7 @@ class SurrogateTestMethod:
     @staticmethod
     def accumulate(observed_te, dev, bin_data, n_per_var, b_max, kernel_name, tau, n_surrogates,
                    shuffle_method, block_length, seed, use_graph=False, k_start=0,
-                   pair_offset=0, n_pairs=None, diag_count=True):
+                   pair_offset=0, n_pairs=None, diag_count=True, as_numpy=True):
         """float64 sum, sum of squares and int32 count_ge (numpy, (n, n)) over
         surrogates [k_start, k_start + n_surrogates), diagonal count included."""
         n_vars, T, K = bin_data.shape
@@ -316,8 +374,9 @@ class SurrogateTestMethod:
         perms, bl, _ = build_block_perm(n_vars, T, shuffle_method, block_length, k_start,
                                         k_start + n_surrogates, seed, dev)
         run_surrogates(acc, perms, bl, use_graph)
-        count = acc.cnt.cpu().numpy()
-        if diag_count:
-            diag = np.arange(n_vars)
-            count[diag, diag] += n_surrogates  # te_k >= observed holds on the diagonal (0 >= 0)
-        return acc.sum.cpu().numpy(), acc.sumsq.cpu().numpy(), count
+        if diag_count:  # te_k >= observed holds on the diagonal (0 >= 0)
+            diag = torch.arange(n_vars, device=acc.cnt.device)
+            acc.cnt[diag, diag] += n_surrogates
+        if not as_numpy:
+            return acc.sum, acc.sumsq, acc.cnt
+        return acc.sum.cpu().numpy(), acc.sumsq.cpu().numpy(), acc.cnt.cpu().numpy()

@@ -137,3 +137,25 @@ def test_surrogate_over_several_devices(cuda):
     assert np.allclose(one.mean_surrogate_te, two.mean_surrogate_te, rtol=1e-6, atol=1e-8)
     assert np.allclose(one.p_values, two.p_values, rtol=1e-4, atol=1e-6)
     assert np.array_equal(one.grn.pairs, two.grn.pairs)
+
+
+def test_device_statistics_match_numpy_expressions(cuda):
+    # the single-device test computes the statistics on the device with the same
+    # float64 / float32 expressions as the host path; erfc is the only library call
+    from tenex_b200.inference.surrogate_test import pair_statistics, pair_statistics_device
+    rng = np.random.default_rng(3)
+    n, S = 300, 100
+    te = (rng.gamma(2.0, 0.002, (S, n, n))).astype(np.float32)
+    obs = (rng.gamma(2.0, 0.002, (n, n)) + (rng.random((n, n)) < 0.02) * 0.01).astype(np.float32)
+    s1 = te.astype(np.float64).sum(0)
+    s2 = (te.astype(np.float64) ** 2).sum(0)
+    cnt = (te >= obs).sum(0).astype(np.int32)
+    for method in ("parametric", "mc"):
+        ref = pair_statistics(obs, s1, s2, cnt, S, method)
+        got = pair_statistics_device(*(torch.from_numpy(a).to(cuda) for a in (obs, s1, s2, cnt)),
+                                     S, method)
+        got = [g.cpu().numpy() for g in got]
+        for r, g in zip(ref[:3], got[:3]):
+            assert np.array_equal(r.view(np.uint32), g.view(np.uint32))
+        ulps = np.abs(ref[3].view(np.int32).astype(np.int64) - got[3].view(np.int32).astype(np.int64))
+        assert ulps.max() <= 1 and (ulps > 0).mean() < 1e-3, (method, ulps.max(), (ulps > 0).sum())
