@@ -41,8 +41,7 @@ constexpr int kKt = 128;       // bytes of K per pipeline stage (4 MMA K-steps o
 constexpr int kStages = 3;
 constexpr int kOpBytes = kKt * kTile;          // one operand tile per stage (16 KB)
 constexpr int kStageBytes = 4 * kOpBytes;      // FP, P, F (targets) + P (sources)
-constexpr int kTmaBytes = 3 * kOpBytes;        // P, F, P by TMA; FP = F & P made in smem
-constexpr int kFpWarps = 8;                    // warps 8..15 form FP during the main loop
+constexpr int kTmaBytes = kStageBytes;          // all four by TMA
 constexpr int kTmemCols = 512;
 
 struct B2Params {
@@ -78,11 +77,11 @@ __device__ __forceinline__ float cell_term(float c, float c1, float c2a, float c
   return c * __log2f(r);
 }
 
-// Pack: F[g, t] = x[g, t+lag] for t < L (0 beyond, up to Lpad), the lag-shifted
-// operand TMA cannot address (its copies start on 16-byte boundaries), plus the
-// per-gene counts nf, np, nfp (P = x[g, t] is read from the bins directly, FP =
-// F & P is formed in shared memory). One CTA per gene; each thread makes 16
-// bytes of F from two aligned 16-byte loads, with a scalar path for the row end.
+// Pack: F[g, t] = x[g, t+lag] (the lag-shifted operand TMA cannot address: its
+// copies start on 16-byte boundaries) and FP = F & P for t < L (0 beyond, up to
+// Lpad), plus the per-gene counts nf, np, nfp; P = x[g, t] is read from the bins
+// directly. One CTA per gene; each thread makes 16 bytes of F and FP from two
+// aligned 16-byte loads, with a scalar path for the row end.
 // Every bin must be 0 or 1 (the GEMM sums the raw bytes): a larger value sets
 // the error word to 2.
 __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L,
@@ -91,6 +90,7 @@ __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int
   const int g = blockIdx.x;
   const uint8_t* row = bins + (int64_t)g * ld;
   uint8_t* Fr = ops + (int64_t)g * Lpad;
+  uint8_t* FPr = ops + ((int64_t)n + g) * Lpad;
   int nf = 0, np = 0, nfp = 0;
   uint32_t high = 0;  // any bit above bit 0 of a byte: a bin other than 0/1
   const int sh = lag & 15;
@@ -130,6 +130,8 @@ __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int
       }
     }
     *reinterpret_cast<uint4*>(Fr + t) = make_uint4(f[0], f[1], f[2], f[3]);
+    *reinterpret_cast<uint4*>(FPr + t) =
+        make_uint4(f[0] & p[0], f[1] & p[1], f[2] & p[2], f[3] & p[3]);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       nf += __popc(f[k]);
@@ -158,10 +160,11 @@ __global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int
   if (high) atomicExch(err, 2);
 }
 
-// Tensor maps of the operands: F (packed, n x Lpad) and P (the bins themselves,
-// n x L with row stride ld; TMA fills columns >= L and rows >= n with zeros).
+// Tensor maps of the operands: F and FP (packed, n x Lpad) and P (the bins
+// themselves, n x L with row stride ld; TMA fills columns >= L and rows >= n
+// with zeros).
 struct B2Maps {
-  CUtensorMap F, P;
+  CUtensorMap F, P, FP;
 };
 
 constexpr int kB2Threads = 512;
@@ -174,8 +177,7 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   unsigned char* stage_base = smem;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* fpready = empty + kStages;  // FP tile of the stage written (kFpWarps arrivals)
-  uint64_t* accbar = fpready + kStages;
+  uint64_t* accbar = empty + kStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accbar + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -189,7 +191,6 @@ __global__ void __launch_bounds__(kB2Threads, 1)
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
-      mbar_init(&fpready[s], kFpWarps);
     }
     mbar_init(accbar, 1);
     *abort_flag = 0;
@@ -221,7 +222,8 @@ __global__ void __launch_bounds__(kB2Threads, 1)
       unsigned char* buf = stage_base + s * kStageBytes;
       mbar_expect_tx(&full[s], kTmaBytes);
       const int x0 = k * kKt;
-      // one 128-byte x 128-row box per operand, 128-byte swizzled (FP: see below)
+      // one 128-byte x 128-row box per operand, 128-byte swizzled
+      tma_load_2d(buf + 0 * kOpBytes, &maps.FP, x0, m0, &full[s]);
       tma_load_2d(buf + 1 * kOpBytes, &maps.P, x0, m0, &full[s]);
       tma_load_2d(buf + 2 * kOpBytes, &maps.F, x0, m0, &full[s]);
       tma_load_2d(buf + 3 * kOpBytes, &maps.P, x0, n0, &full[s]);
@@ -237,7 +239,7 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   }
 
   // ---- MMA issuer (warp 1, lane 0): stage k's 3 x 4 MMAs as soon as its operands
-  // (TMA) and its FP tile are in place; never waits on MMA completion, so the
+  // are in place; never waits on MMA completion, so the
   // tensor pipe gets the stages back to back ----------------------------------
   if (tid == 32) {
     const uint32_t idesc = idesc_i8(kTile, kTile);
@@ -245,8 +247,7 @@ __global__ void __launch_bounds__(kB2Threads, 1)
     for (int k = 0; k < nk; ++k) {
       const int s = k % kStages;
       const uint32_t ph = (uint32_t)((k / kStages) & 1);
-      if (*(volatile int*)abort_flag || !mbar_wait(&full[s], ph) ||
-          !mbar_wait(&fpready[s], ph)) {
+      if (*(volatile int*)abort_flag || !mbar_wait(&full[s], ph)) {
         ok = false;
         break;
       }
@@ -272,36 +273,6 @@ __global__ void __launch_bounds__(kB2Threads, 1)
       *(volatile int*)abort_flag = 1;
     }
     mma_commit(accbar);  // arrives after every issued MMA, so the epilogue wakes either way
-  }
-
-  // ---- FP = F & P of every stage, by warps 8..15 (idle until the epilogue) ---
-  // The three tiles have the same 128-byte swizzled layout, so the byte-wise AND
-  // of the F and P tiles is the FP tile. The stores are made visible to the
-  // tensor core's operand reads (async proxy) before the arrival the MMA thread
-  // waits on. The producer reloads a stage only after its MMAs completed, which
-  // needs this stage's FP first, so a stage's FP is never overwritten early.
-  if (warp >= 16 - kFpWarps) {
-    const int ft = tid - (16 - kFpWarps) * 32;
-    for (int k = 0; k < nk; ++k) {
-      if (*(volatile int*)abort_flag) break;
-      const int s = k % kStages;
-      if (!mbar_wait(&full[s], (uint32_t)((k / kStages) & 1))) {
-        atomicExch(prm.err, 1);
-        break;
-      }
-      unsigned char* buf = stage_base + s * kStageBytes;
-      const uint4* P4 = reinterpret_cast<const uint4*>(buf + 1 * kOpBytes);
-      const uint4* F4 = reinterpret_cast<const uint4*>(buf + 2 * kOpBytes);
-      uint4* FP4 = reinterpret_cast<uint4*>(buf);
-#pragma unroll
-      for (int c = ft; c < kOpBytes / 16; c += kFpWarps * 32) {
-        const uint4 f = F4[c], p = P4[c];
-        FP4[c] = make_uint4(f.x & p.x, f.y & p.y, f.z & p.z, f.w & p.w);
-      }
-      fence_proxy_async_smem();
-      __syncwarp();
-      if ((tid & 31) == 0) mbar_arrive(&fpready[s]);
-    }
   }
 
   // ---- epilogue: 16 warps; lane quarter warp % 4, column quarter warp / 4 ---
@@ -401,8 +372,8 @@ extern "C" size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t 
   if (n_vars < 1 || row_len <= lag) return 256;
   const int64_t L = row_len - lag;
   const int64_t Lpad = round_up(L, kKt);
-  return (size_t)(round_up((int64_t)n_vars * Lpad, 256) + round_up(3 * (int64_t)n_vars * 4, 256) +
-                  256);
+  return (size_t)(round_up(2 * (int64_t)n_vars * Lpad, 256) +
+                  round_up(3 * (int64_t)n_vars * 4, 256) + 256);
 }
 
 extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
@@ -428,8 +399,8 @@ extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_var
     return fail(TENEX_ERR_BADARG, "workspace must be 256-byte aligned");
   unsigned char* ws = reinterpret_cast<unsigned char*>(workspace);
   uint8_t* ops = ws;
-  int32_t* marg = reinterpret_cast<int32_t*>(ws + round_up((int64_t)n_vars * Lpad, 256));
-  int* err = reinterpret_cast<int*>(ws + round_up((int64_t)n_vars * Lpad, 256) +
+  int32_t* marg = reinterpret_cast<int32_t*>(ws + round_up(2 * (int64_t)n_vars * Lpad, 256));
+  int* err = reinterpret_cast<int*>(ws + round_up(2 * (int64_t)n_vars * Lpad, 256) +
                                     round_up(3 * (int64_t)n_vars * 4, 256));
   cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), stream);
   if (e != cudaSuccess) return check_cuda(e, "memset");
@@ -440,6 +411,7 @@ extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_var
   B2Maps maps;
   if ((st = make_map(&maps.F, ops, n_vars, Lpad, Lpad))) return st;
   if ((st = make_map(&maps.P, bins, n_vars, L, ld))) return st;
+  if ((st = make_map(&maps.FP, ops + (int64_t)n_vars * Lpad, n_vars, Lpad, Lpad))) return st;
   B2Params prm;
   prm.n = n_vars;
   prm.L = (int)L;
@@ -462,7 +434,7 @@ extern "C" int tenex_b2_status(const void* workspace, int n_vars, int64_t row_le
   const int64_t L = row_len - lag;
   const int64_t Lpad = round_up(L, kKt);
   const unsigned char* ws = reinterpret_cast<const unsigned char*>(workspace);
-  const int* err = reinterpret_cast<const int*>(ws + round_up((int64_t)n_vars * Lpad, 256) +
+  const int* err = reinterpret_cast<const int*>(ws + round_up(2 * (int64_t)n_vars * Lpad, 256) +
                                                 round_up(3 * (int64_t)n_vars * 4, 256));
   int h = 0;
   cudaError_t e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, as_stream(stream));
