@@ -238,11 +238,16 @@ __global__ void __launch_bounds__(kB2Threads, 1)
     }
   }
 
-  // ---- MMA issuer (warp 1, lane 0): stage k's 3 x 4 MMAs as soon as its operands
-  // are in place; never waits on MMA completion, so the
-  // tensor pipe gets the stages back to back ----------------------------------
+  // ---- MMA issuer (warp 1, lane 0): stage k's MMAs as soon as its operands are
+  // in place; never waits on MMA completion, so the tensor pipe gets the stages
+  // back to back. The source tile P_j is the A operand (M = 128 lanes = sources)
+  // and the target tiles are B: [FP_i; P_i] (adjacent in the stage, one N = 256
+  // MMA) and F_i (N = 128), so a K step reads P_j twice instead of three times
+  // (20 KB of shared memory instead of 24; shared-memory bandwidth bounds the
+  // main loop). TMEM columns 0-127 = C^T, 128-255 = D^T, 256-383 = E^T.
   if (tid == 32) {
-    const uint32_t idesc = idesc_i8(kTile, kTile);
+    const uint32_t idesc256 = idesc_i8(kTile, 2 * kTile);
+    const uint32_t idesc128 = idesc_i8(kTile, kTile);
     bool ok = true;
     for (int k = 0; k < nk; ++k) {
       const int s = k % kStages;
@@ -253,18 +258,16 @@ __global__ void __launch_bounds__(kB2Threads, 1)
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       unsigned char* buf = stage_base + s * kStageBytes;
-      const uint32_t aFP = smem_u32(buf + 0 * kOpBytes);
-      const uint32_t aP = smem_u32(buf + 1 * kOpBytes);
-      const uint32_t aF = smem_u32(buf + 2 * kOpBytes);
-      const uint32_t bP = smem_u32(buf + 3 * kOpBytes);
+      const uint32_t bFPP = smem_u32(buf + 0 * kOpBytes);  // FP_i rows, then P_i rows
+      const uint32_t bF = smem_u32(buf + 2 * kOpBytes);
+      const uint32_t aPj = smem_u32(buf + 3 * kOpBytes);
 #pragma unroll
       for (int kk = 0; kk < kKt / 32; ++kk) {
         const uint32_t off = kk * 32;  // 32-byte K step inside the 128-byte swizzle row
-        const uint64_t bd = smem_desc_sw128(bP + off);
+        const uint64_t ad = smem_desc_sw128(aPj + off);
         const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
-        mma_i8(tmem + 0, smem_desc_sw128(aFP + off), bd, idesc, acc);
-        mma_i8(tmem + 128, smem_desc_sw128(aP + off), bd, idesc, acc);
-        mma_i8(tmem + 256, smem_desc_sw128(aF + off), bd, idesc, acc);
+        mma_i8(tmem + 0, ad, smem_desc_sw128(bFPP + off), idesc256, acc);
+        mma_i8(tmem + 256, ad, smem_desc_sw128(bF + off), idesc128, acc);
       }
       mma_commit(&empty[s]);  // stage s free once these MMAs complete
     }
@@ -282,16 +285,9 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   if (!ok_acc && tid == 0) atomicExch(prm.err, 1);
   const bool run = ok_acc && (*(volatile int*)abort_flag == 0);
   const int lq = warp & 3, cq = warp >> 2;
-  const int i = m0 + lq * 32 + (tid & 31);  // target gene of this thread's TMEM lane
+  const int j = n0 + lq * 32 + (tid & 31);  // source gene of this thread's TMEM lane
   const float N = (float)prm.L;
-  float nf = 0.f, np_ = 0.f, nfp = 0.f;
-  if (i < prm.n) {
-    nf = (float)prm.marg[i];
-    np_ = (float)prm.marg[prm.n + i];
-    nfp = (float)prm.marg[2 * prm.n + i];
-  }
-  const float c1_1 = np_, c1_0 = N - np_;
-  const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
+  const float npj = j < prm.n ? (float)prm.marg[prm.n + j] : 0.f;
   const uint32_t lane_base = tmem + ((uint32_t)(lq * 32) << 16);
   for (int cb = cq * (kTile / 4); cb < (cq + 1) * (kTile / 4); cb += 16) {
     uint32_t rc[16], rd[16], re[16];
@@ -299,12 +295,15 @@ __global__ void __launch_bounds__(kB2Threads, 1)
     tmem_ld16(lane_base + 128 + cb, rd);
     tmem_ld16(lane_base + 256 + cb, re);
     tmem_wait_ld();
-    if (!run || i >= prm.n) continue;
+    if (!run || j >= prm.n) continue;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int j = n0 + cb + q;  // source gene
-      if (j >= prm.n || j == i) continue;
-      const float npj = (float)prm.marg[prm.n + j];
+      const int i = m0 + cb + q;  // target gene (the same for every lane: broadcast loads)
+      if (i >= prm.n || i == j) continue;
+      const float nf = (float)prm.marg[i], np_ = (float)prm.marg[prm.n + i];
+      const float nfp = (float)prm.marg[2 * prm.n + i];
+      const float c1_1 = np_, c1_0 = N - np_;
+      const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
       const float C = (float)rc[q], Dv = (float)rd[q], E = (float)re[q];
       const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
       float te = 0.f;
