@@ -4,7 +4,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from tenex_b200 import workloads as W
+from tenex_b200 import native, workloads as W
 from tenex_b200.kernels import device as D
 from tenex_b200.kernels.gemm_b2 import te_binary_matrix
 
@@ -42,3 +42,17 @@ def test_binary_tau2_constant_rows(cuda):
     m = _run(x, cuda, tau=2)
     ref = O.te_matrix(x.astype(np.int32), np.full(70, 2, np.int32), tau=2)
     assert np.max(np.abs(m - ref)) <= TOL
+
+
+def test_non_binary_bins_report_bad_data(cuda):
+    # the GEMM sums raw bytes, so a bin other than 0/1 must be reported by the status
+    # call, not silently counted; the context stays usable afterwards
+    rng = np.random.default_rng(2)
+    x = (rng.random((20, 300)) < 0.4).astype(np.int32)
+    x[7, 123] = 2
+    with pytest.raises(native.TenexError) as ei:
+        te_binary_matrix(D.pack_bins(x, cuda), 1)
+    assert ei.value.status == native.TENEX_ERR_BADDATA
+    x[7, 123] = 1
+    m = te_binary_matrix(D.pack_bins(x, cuda), 1).cpu().numpy()
+    assert np.max(np.abs(m - O.te_matrix(x, np.full(20, 2, np.int32)))) <= 1e-6
