@@ -6,22 +6,25 @@
 // per-gene marginals, then sum c*log2(c*c1/(c2a*c2b)) / N).
 //
 // B200 design:
-//   * pack kernel: one pass over the bins writes the three K-major int8
-//     operands F, P, FP (rows padded to a multiple of 128 bytes, zero filled)
-//     and the per-gene counts nf, np, nfp.
-//   * GEMM kernel: one CTA per 128 x 128 (target x source) output tile.
-//     TMA (cp.async.bulk.tensor.2d, no multicast) brings one 128-byte x
-//     128-row box of each of FP, P, F (targets) and P (sources) per stage into
-//     shared memory, 128-byte swizzled (the K-major SWIZZLE_128B layout the MMA
-//     descriptors name); one thread issues, per 32-byte
-//     K step, three tcgen05.mma.kind::i8 (FP x P^T -> C, P x P^T -> D,
-//     F x P^T -> E) into int32 accumulators in TMEM (3 x 128 columns). The
-//     counts are exact integers (int32, N < 2^31).
-//   * Epilogue: sixteen warps; warp w reads TMEM lanes 32*(w%4).. (one target row
-//     per lane) and a quarter of the 128 columns with tcgen05.ld, forms the 8
-//     cells and writes TE(src -> tgt) to out[src, tgt] (the other twelve warps
-//     only wait for the accumulators: four warps alone left the epilogue, not
-//     the MMAs, as the kernel's critical path).
+//   * pack kernel: one pass over the bins writes the lag-shifted K-major int8
+//     operand F and FP = F & P (rows padded to a multiple of 128 bytes, zero
+//     filled), the per-gene counts nf, np, nfp, and flags any bin other than
+//     0/1; P is the bins themselves (a tensor map with K extent L, TMA zero-fills
+//     beyond it).
+//   * GEMM kernel: one CTA per 128 x 128 (target x source) tile of the matrix.
+//     A producer warp brings, per stage, one 128-byte x 128-row box of FP, P, F
+//     (targets) and P (sources) by TMA (cp.async.bulk.tensor.2d, no multicast),
+//     128-byte swizzled (the K-major SWIZZLE_128B layout the MMA descriptors
+//     name); a separate MMA warp issues, per 32-byte K step, two
+//     tcgen05.mma.kind::i8 with the source tile as A (M = 128 lanes = sources):
+//     B = [FP; P] of the targets as one N = 256 MMA (C^T, D^T) and B = F at
+//     N = 128 (E^T), int32 accumulators in TMEM (384 columns). Shared-memory
+//     bandwidth (operand reads plus TMA writes) bounds the main loop, hence the
+//     source tile read twice per K step rather than three times. The counts are
+//     exact integers (int32, N < 2^31).
+//   * Epilogue: sixteen warps; warp w reads TMEM lanes 32*(w%4).. (one source
+//     per lane) and a quarter of the 128 target columns with tcgen05.ld, forms
+//     the 8 cells and writes TE(src -> tgt) to out[src, tgt].
 //   * Every mbarrier wait is bounded; on expiry the kernel records an error
 //     word, drains the copies it issued (bounded), frees TMEM and returns.
 #include <cuda.h>
