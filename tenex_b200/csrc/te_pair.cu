@@ -15,7 +15,11 @@
 //   * Shared memory after the target block is cut into histogram slots sized
 //     for the item (b_t^2 * b_s cells); a slot belongs to a group of G warps
 //     (G = 1: warp-private histograms for the common small pairs). Counters are
-//     32-bit when the slots fit, else 16-bit halves of a word (N < 65536).
+//     32-bit unless 32-bit slots would need groups of more than 4 warps, then
+//     16-bit halves of a word (N < 65536; two cells per word collide more
+//     often, so packing is the fallback, not the rule). Pairs whose histogram
+//     fits no shared-memory slot (coarsening off) run in a second instantiation
+//     on per-CTA slots in global memory.
 //   * Every sample is one predicated-free red.shared.add (16 samples per
 //     uint4 of source bins). Skipping the most frequent cells and deriving them
 //     by subtraction (fewer same-word collisions) was measured slower on every
@@ -24,8 +28,10 @@
 //   * The entropy pass reads each slot column once to form c2b, once more to
 //     form the terms (ratio c3 * (1/c2b) * (c1/c2a), lg2.approx; exact 0 where
 //     c3*c1 == c2a*c2b), and clears the slot for the next source.
-//   * Items are handed out by an atomic ticket in chunk-major order, so the
-//     CTAs resident at one moment share a small set of source rows in L2.
+//   * Items are handed out by an atomic ticket, targets in L2-sized blocks and
+//     chunk-major within a block, so the CTAs resident at one moment share a
+//     small set of source rows in L2. Sources are ordered by bin count, so one
+//     item's slots are sized for sources of similar b.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
