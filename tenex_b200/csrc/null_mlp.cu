@@ -145,9 +145,10 @@ __device__ __forceinline__ float g_poisson(float m, const float* __restrict__ ta
   return fmaf(f, tab[i + 1] - tab[i], tab[i]);
 }
 
-// q[g][b] = count of y_s = b over s < N, / N (b < 64; genes with b > 64 unused).
+// q[g][b] = count of y_s = b over s < N, / N, and cnt[g][b] the count itself
+// (b < 64; genes with b > 64 unused).
 __global__ void source_marginal_kernel(const uint8_t* __restrict__ bins, int64_t ld, int N,
-                                       float* __restrict__ q) {
+                                       float* __restrict__ q, int* __restrict__ cnt) {
   __shared__ int h[256];
   const int g = blockIdx.x;
   for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
@@ -155,16 +156,28 @@ __global__ void source_marginal_kernel(const uint8_t* __restrict__ bins, int64_t
   const uint8_t* row = bins + (int64_t)g * ld;
   for (int s = threadIdx.x; s < N; s += blockDim.x) atomicAdd(&h[row[s]], 1);
   __syncthreads();
-  if (threadIdx.x < kEiidMaxB) q[(int64_t)g * kEiidMaxB + threadIdx.x] = (float)h[threadIdx.x] / N;
+  if (threadIdx.x < kEiidMaxB) {
+    q[(int64_t)g * kEiidMaxB + threadIdx.x] = (float)h[threadIdx.x] / N;
+    cnt[(int64_t)g * kEiidMaxB + threadIdx.x] = h[threadIdx.x];
+  }
 }
 
 // One CTA per target: its non-zero n_a and n_x in shared memory, threads over
 // sources. out[src * n + tgt] = E_iid (NaN when b_t or b_s > 64).
+// TABLE: the target's sum over its state counts depends on the source bin only
+// through q = c / N, so the CTA first tabulates F(c) = sum_a g(n_a q) - sum_x
+// g(n_x q) for every count c in [0, N] (shared memory, N + 1 floats), with the
+// same operations in the same order as the per-pair loop, then each pair adds
+// F(c_b) over its source bins: the same floats, bitwise, in (N + 1) instead of
+// (sources x bins) evaluations of the state sum.
+template <bool TABLE>
 __global__ void __launch_bounds__(256) eiid_kernel(const uint8_t* __restrict__ bins, int64_t ld,
                                                    const int32_t* __restrict__ npv, int n, int N,
                                                    int lag, const float* __restrict__ q,
+                                                   const int* __restrict__ cnt,
                                                    const float* __restrict__ gtab,
                                                    float* __restrict__ out) {
+  extern __shared__ float Ftab[];  // TABLE: N + 1 entries
   __shared__ int hz[kEiidMaxB * kEiidMaxB];
   __shared__ int hx[kEiidMaxB];
   __shared__ float la[kEiidMaxB * kEiidMaxB + kEiidMaxB];
@@ -222,20 +235,41 @@ __global__ void __launch_bounds__(256) eiid_kernel(const uint8_t* __restrict__ b
   __syncthreads();
   const int kz = nz;
   const int kx = nx;
+  if (TABLE) {
+    for (int c = threadIdx.x; c <= N; c += blockDim.x) {
+      const float qb = (float)c / N;  // the source_marginal_kernel's q for count c
+      float part = 0.f;
+      if (qb > 0.f) {
+        for (int a = 0; a < kz; ++a) part += g_poisson(la[a] * qb, tab);
+        for (int a = 0; a < kx; ++a) part -= g_poisson(la[kz + a] * qb, tab);
+      }
+      Ftab[c] = part;
+    }
+    __syncthreads();
+  }
   for (int s = threadIdx.x; s < n; s += blockDim.x) {
     if (s == t) continue;
     const int bs = npv[s];
     float acc = nan;
     if (bs >= 1 && bs <= kEiidMaxB) {
       acc = 0.f;
-      const float* qs = q + (int64_t)s * kEiidMaxB;
-      for (int b = 0; b < bs; ++b) {
-        const float qb = qs[b];
-        if (qb <= 0.f) continue;
-        float part = 0.f;
-        for (int a = 0; a < kz; ++a) part += g_poisson(la[a] * qb, tab);
-        for (int a = 0; a < kx; ++a) part -= g_poisson(la[kz + a] * qb, tab);
-        acc += part;
+      if (TABLE) {
+        const int* cs = cnt + (int64_t)s * kEiidMaxB;
+        for (int b = 0; b < bs; ++b) {
+          const int c = cs[b];
+          if (c <= 0) continue;
+          acc += Ftab[c];
+        }
+      } else {
+        const float* qs = q + (int64_t)s * kEiidMaxB;
+        for (int b = 0; b < bs; ++b) {
+          const float qb = qs[b];
+          if (qb <= 0.f) continue;
+          float part = 0.f;
+          for (int a = 0; a < kz; ++a) part += g_poisson(la[a] * qb, tab);
+          for (int a = 0; a < kx; ++a) part -= g_poisson(la[kz + a] * qb, tab);
+          acc += part;
+        }
       }
     }
     out[(int64_t)s * n + t] = acc;
@@ -465,7 +499,9 @@ extern "C" int tenex_gene_features(const uint8_t* bins, int64_t ld, const int32_
 }
 
 extern "C" size_t tenex_eiid_workspace_bytes(int n_vars) {
-  return n_vars < 1 ? 0 : (size_t)n_vars * kEiidMaxB * sizeof(float) + kGTable * sizeof(float);
+  return n_vars < 1 ? 0
+                    : (size_t)n_vars * kEiidMaxB * (sizeof(float) + sizeof(int)) +
+                          kGTable * sizeof(float);
 }
 
 extern "C" int tenex_eiid_matrix(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
@@ -482,10 +518,29 @@ extern "C" int tenex_eiid_matrix(const uint8_t* bins, int64_t ld, const int32_t*
   cudaStream_t s = as_stream(stream);
   float* q = static_cast<float*>(workspace);
   float* tab = q + (size_t)n_vars * kEiidMaxB;
+  int* cnt = reinterpret_cast<int*>(tab + kGTable);
   const int N = (int)(row_len - lag);
   g_table_kernel<<<kGTable / 256, 256, 0, s>>>(tab);
-  source_marginal_kernel<<<n_vars, 256, 0, s>>>(bins, ld, N, q);
-  eiid_kernel<<<n_vars, 256, 0, s>>>(bins, ld, n_per_var, n_vars, N, (int)lag, q, tab, eiid);
+  source_marginal_kernel<<<n_vars, 256, 0, s>>>(bins, ld, N, q, cnt);
+  // the count table pays when it is smaller than the per-pair work it replaces
+  // (N + 1 entries against ~n sources x a few bins) and fits shared memory
+  DevAttr A;
+  int st = current_device_attr(&A);
+  if (st) return st;
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, eiid_kernel<true>);
+  const int64_t tab_bytes = ((int64_t)N + 1) * (int64_t)sizeof(float);
+  if ((int64_t)N + 1 <= 4 * (int64_t)n_vars && tab_bytes + (int64_t)fa.sharedSizeBytes <= A.smem_optin) {
+    cudaError_t e = cudaFuncSetAttribute(eiid_kernel<true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tab_bytes);
+    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+    eiid_kernel<true><<<n_vars, 256, (size_t)tab_bytes, s>>>(bins, ld, n_per_var, n_vars, N,
+                                                             (int)lag, q, cnt, tab, eiid);
+  } else {
+    eiid_kernel<false><<<n_vars, 256, 0, s>>>(bins, ld, n_per_var, n_vars, N, (int)lag, q, cnt,
+                                              tab, eiid);
+  }
   return check_launch("eiid kernels");
 }
 

@@ -95,3 +95,19 @@ def test_training_reduces_loss(cuda):
     h = rep["loss_history"]
     assert h[-1][1] < 0.5 * h[0][1]       # mean loss of steps 251-400 vs steps 1-250
     assert max(rep["val_mse"]) < 0.05
+
+
+def test_eiid_count_table_equals_pair_loop(cuda):
+    # E_iid of a pair depends only on its two genes: with 200 genes the kernel
+    # tabulates the target sums over counts (N + 1 <= 4 n), with 20 of the same genes
+    # it sums per pair; the two must agree bit for bit
+    x, npv, _ = W.cfg5_bins(n=200, T=500, seed=41)
+    sub = np.arange(0, 200, 10)
+    full = LN.eiid_matrix(D.pack_bins(x, cuda), torch.as_tensor(npv, dtype=torch.int32,
+                                                                 device=cuda), 1).cpu().numpy()
+    part = LN.eiid_matrix(D.pack_bins(x[sub], cuda),
+                          torch.as_tensor(npv[sub], dtype=torch.int32, device=cuda),
+                          1).cpu().numpy()
+    want = full[np.ix_(sub, sub)]
+    off = ~np.eye(len(sub), dtype=bool)
+    assert np.array_equal(part[off].view(np.uint32), want[off].view(np.uint32))
