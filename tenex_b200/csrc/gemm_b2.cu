@@ -83,84 +83,93 @@ __device__ __forceinline__ float cell_term(float c, float c1, float c2a, float c
 // Pack: F[g, t] = x[g, t+lag] (the lag-shifted operand TMA cannot address: its
 // copies start on 16-byte boundaries) and FP = F & P for t < L (0 beyond, up to
 // Lpad), plus the per-gene counts nf, np, nfp; P = x[g, t] is read from the bins
-// directly. One CTA per gene; each thread makes 16 bytes of F and FP from two
-// aligned 16-byte loads, with a scalar path for the row end.
+// directly. One warp per gene, kPackWarps genes per CTA, so the counts reduce
+// with shuffles alone (no CTA barrier). Each lane makes 16 bytes of F and FP
+// from two aligned 16-byte loads, two chunks per pass with all six loads issued
+// before the first store; a scalar path covers the row end.
 // Every bin must be 0 or 1 (the GEMM sums the raw bytes): a larger value sets
 // the error word to 2.
-__global__ void b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L,
-                               int lag, int Lpad, uint8_t* __restrict__ ops,
-                               int32_t* __restrict__ marg, int* __restrict__ err) {
-  const int g = blockIdx.x;
+constexpr int kPackWarps = 4;
+
+__global__ void __launch_bounds__(kPackWarps * 32)
+b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int lag, int Lpad,
+               uint8_t* __restrict__ ops, int32_t* __restrict__ marg, int* __restrict__ err) {
+  const int g = blockIdx.x * kPackWarps + (threadIdx.x >> 5);
+  if (g >= n) return;  // whole warps only: the shuffles below see full warps
+  const int lane = threadIdx.x & 31;
   const uint8_t* row = bins + (int64_t)g * ld;
   uint8_t* Fr = ops + (int64_t)g * Lpad;
   uint8_t* FPr = ops + ((int64_t)n + g) * Lpad;
   int nf = 0, np = 0, nfp = 0;
   uint32_t high = 0;  // any bit above bit 0 of a byte: a bin other than 0/1
   const int sh = lag & 15;
-  for (int t = threadIdx.x * 16; t < Lpad; t += blockDim.x * 16) {
-    uint32_t f[4], p[4];
-    const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;  // aligned start of F's window
-    if (t + 16 <= L && fa + 32 <= ld) {
-      const uint4 pv = *reinterpret_cast<const uint4*>(row + t);
-      const uint4 a = *reinterpret_cast<const uint4*>(row + fa);
-      const uint4 b = *reinterpret_cast<const uint4*>(row + fa + 16);
-      const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-      const uint32_t pw[4] = {pv.x, pv.y, pv.z, pv.w};
+  for (int t0 = lane * 16; t0 < Lpad; t0 += 2 * 32 * 16) {
+    uint4 pv[2], av[2], bv[2];
+    bool fast[2];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        // bytes sh + 4k .. sh + 4k + 3 of the 32-byte window
-        const int byte = sh + 4 * k;
-        const uint32_t lo = w[byte >> 2], hi = w[(byte >> 2) + 1];
-        const uint32_t fw = __funnelshift_r(lo, hi, (byte & 3) * 8);
-        high |= (fw | pw[k]) & 0xfefefefeu;
-        f[k] = fw;
-        p[k] = pw[k];
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        uint32_t fk = 0, pk = 0;
-        for (int j = 0; j < 4; ++j) {
-          const int tt = t + 4 * k + j;
-          if (tt < L) {
-            fk |= (uint32_t)row[tt + lag] << (8 * j);
-            pk |= (uint32_t)row[tt] << (8 * j);
-          }
-        }
-        high |= (fk | pk) & 0xfefefefeu;
-        f[k] = fk;
-        p[k] = pk;
+    for (int u = 0; u < 2; ++u) {
+      const int t = t0 + u * 32 * 16;
+      const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;  // aligned start of F's window
+      fast[u] = t + 16 <= L && fa + 32 <= ld;
+      if (fast[u]) {
+        pv[u] = *reinterpret_cast<const uint4*>(row + t);
+        av[u] = *reinterpret_cast<const uint4*>(row + fa);
+        bv[u] = *reinterpret_cast<const uint4*>(row + fa + 16);
       }
     }
-    *reinterpret_cast<uint4*>(Fr + t) = make_uint4(f[0], f[1], f[2], f[3]);
-    *reinterpret_cast<uint4*>(FPr + t) =
-        make_uint4(f[0] & p[0], f[1] & p[1], f[2] & p[2], f[3] & p[3]);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      nf += __popc(f[k]);
-      np += __popc(p[k]);
-      nfp += __popc(f[k] & p[k]);
+    for (int u = 0; u < 2; ++u) {
+      const int t = t0 + u * 32 * 16;
+      if (t >= Lpad) break;
+      uint32_t f[4], p[4];
+      if (fast[u]) {
+        const uint32_t w[8] = {av[u].x, av[u].y, av[u].z, av[u].w,
+                               bv[u].x, bv[u].y, bv[u].z, bv[u].w};
+        const uint32_t pw[4] = {pv[u].x, pv[u].y, pv[u].z, pv[u].w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          // bytes sh + 4k .. sh + 4k + 3 of the 32-byte window
+          const int byte = sh + 4 * k;
+          const uint32_t lo = w[byte >> 2], hi = w[(byte >> 2) + 1];
+          f[k] = __funnelshift_r(lo, hi, (byte & 3) * 8);
+          p[k] = pw[k];
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          uint32_t fk = 0, pk = 0;
+          for (int j = 0; j < 4; ++j) {
+            const int tt = t + 4 * k + j;
+            if (tt < L) {
+              fk |= (uint32_t)row[tt + lag] << (8 * j);
+              pk |= (uint32_t)row[tt] << (8 * j);
+            }
+          }
+          f[k] = fk;
+          p[k] = pk;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) high |= (f[k] | p[k]) & 0xfefefefeu;
+      *reinterpret_cast<uint4*>(Fr + t) = make_uint4(f[0], f[1], f[2], f[3]);
+      *reinterpret_cast<uint4*>(FPr + t) =
+          make_uint4(f[0] & p[0], f[1] & p[1], f[2] & p[2], f[3] & p[3]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        nf += __popc(f[k]);
+        np += __popc(p[k]);
+        nfp += __popc(f[k] & p[k]);
+      }
     }
   }
-  __shared__ int red[3][32];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     nf += __shfl_xor_sync(0xffffffffu, nf, o);
     np += __shfl_xor_sync(0xffffffffu, np, o);
     nfp += __shfl_xor_sync(0xffffffffu, nfp, o);
   }
-  if ((threadIdx.x & 31) == 0) {
-    red[0][threadIdx.x >> 5] = nf;
-    red[1][threadIdx.x >> 5] = np;
-    red[2][threadIdx.x >> 5] = nfp;
-  }
-  __syncthreads();
-  if (threadIdx.x < 3) {
-    int s = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
-    marg[(int64_t)threadIdx.x * n + g] = s;
-  }
-  if (high) atomicExch(err, 2);
+  if (lane < 3) marg[(int64_t)lane * n + g] = lane == 0 ? nf : (lane == 1 ? np : nfp);
+  if (__any_sync(0xffffffffu, high != 0) && lane == 0) atomicExch(err, 2);
 }
 
 // Tensor maps of the operands: F and FP (packed, n x Lpad) and P (the bins
@@ -406,8 +415,8 @@ extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_var
                                     round_up(3 * (int64_t)n_vars * 4, 256));
   cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), stream);
   if (e != cudaSuccess) return check_cuda(e, "memset");
-  b2_pack_kernel<<<n_vars, 256, 0, stream>>>(bins, ld, n_vars, (int)L, (int)lag, (int)Lpad, ops,
-                                             marg, err);
+  b2_pack_kernel<<<(n_vars + kPackWarps - 1) / kPackWarps, kPackWarps * 32, 0, stream>>>(
+      bins, ld, n_vars, (int)L, (int)lag, (int)Lpad, ops, marg, err);
   int st = check_launch("b2_pack_kernel");
   if (st) return st;
   B2Maps maps;

@@ -37,6 +37,8 @@ constexpr int kIn = 16, kH = 64, kOut = 2;
 constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kH * kIn, kOffW2 = kOffB1 + kH,
               kOffB2 = kOffW2 + kH * kH, kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kOut * kH,
               kParams = kOffB3 + kOut;
+static_assert(kOffW1 % 4 == 0 && kOffW2 % 4 == 0 && kIn % 4 == 0 && kH % 4 == 0,
+              "weight rows are read as float4");
 constexpr int kGeneFeat = 8;
 
 __device__ __forceinline__ float gelu(float x) {
@@ -292,27 +294,50 @@ __device__ __forceinline__ void pair_features(const float* __restrict__ gf, floa
   x[15] = t[2] + s[1];
 }
 
-// Forward of one sample with weights in shared memory (float). Returns the two
-// outputs; optionally stores z1 and z2 (pre-activations).
-__device__ __forceinline__ void mlp_forward_one(const float* __restrict__ w, const float* x,
+// Forward of one sample with weights in shared memory (float, 16-byte
+// aligned) and a transposed copy of W2 (w2t[i * kH + j] = W2[j][i]). Returns
+// the two outputs; optionally stores z1 and z2 (pre-activations). The outer
+// loop runs over the first hidden layer's units i; each g1[i] is added into all
+// kH second-layer sums at once (kH independent chains, kept in registers).
+// Every sum is still evaluated in the plain row order, b + w0*x0 + w1*x1 + ...
+// left to right, so the outputs do not depend on this loop structure. Weights
+// are read four at a time; all lanes read the same address (broadcast).
+__device__ __forceinline__ void mlp_forward_one(const float* __restrict__ w,
+                                                const float* __restrict__ w2t, const float* x,
                                                 float* z1s, float* z2s, float& o0, float& o1) {
-  float g1[kH];
-#pragma unroll 4
+  const float4* w4 = reinterpret_cast<const float4*>(w);
+  const float4* t4 = reinterpret_cast<const float4*>(w2t);
+  float a2[kH];
+#pragma unroll
+  for (int j = 0; j < kH; ++j) a2[j] = w[kOffB2 + j];
+#pragma unroll 1
   for (int i = 0; i < kH; ++i) {
     float a = w[kOffB1 + i];
 #pragma unroll
-    for (int f = 0; f < kIn; ++f) a = fmaf(w[kOffW1 + i * kIn + f], x[f], a);
+    for (int f = 0; f < kIn / 4; ++f) {
+      const float4 v = w4[(kOffW1 + i * kIn) / 4 + f];
+      a = fmaf(v.x, x[4 * f], a);
+      a = fmaf(v.y, x[4 * f + 1], a);
+      a = fmaf(v.z, x[4 * f + 2], a);
+      a = fmaf(v.w, x[4 * f + 3], a);
+    }
     if (z1s) z1s[i] = a;
-    g1[i] = gelu(a);
+    const float g = gelu(a);
+#pragma unroll
+    for (int j = 0; j < kH / 4; ++j) {
+      const float4 v = t4[(i * kH) / 4 + j];
+      a2[4 * j] = fmaf(v.x, g, a2[4 * j]);
+      a2[4 * j + 1] = fmaf(v.y, g, a2[4 * j + 1]);
+      a2[4 * j + 2] = fmaf(v.z, g, a2[4 * j + 2]);
+      a2[4 * j + 3] = fmaf(v.w, g, a2[4 * j + 3]);
+    }
   }
   o0 = w[kOffB3];
   o1 = w[kOffB3 + 1];
+#pragma unroll
   for (int j = 0; j < kH; ++j) {
-    float a = w[kOffB2 + j];
-#pragma unroll 8
-    for (int i = 0; i < kH; ++i) a = fmaf(w[kOffW2 + j * kH + i], g1[i], a);
-    if (z2s) z2s[j] = a;
-    const float g = gelu(a);
+    if (z2s) z2s[j] = a2[j];
+    const float g = gelu(a2[j]);
     o0 = fmaf(w[kOffW3 + j], g, o0);
     o1 = fmaf(w[kOffW3 + kH + j], g, o1);
   }
@@ -322,16 +347,26 @@ __device__ __forceinline__ void load_weights(const __nv_bfloat16* __restrict__ w
   for (int i = threadIdx.x; i < kParams; i += blockDim.x) ws[i] = __bfloat162float(wb[i]);
 }
 
+// w2t[i * kH + j] = W2[j][i], the layout mlp_forward_one reads.
+__device__ __forceinline__ void load_w2t(const __nv_bfloat16* __restrict__ wb, float* w2t) {
+  for (int k = threadIdx.x; k < kH * kH; k += blockDim.x) {
+    const int i = k / kH, j = k - i * kH;
+    w2t[k] = __bfloat162float(wb[kOffW2 + j * kH + i]);
+  }
+}
+
 // Inference over all pairs: mu_log/sigma_log matrices at [src, tgt] (diagonal
 // untouched), features standardised by (fmean, fstd); NaN features give NaN
 // outputs (the caller sends those pairs to the full surrogate test).
-__global__ void __launch_bounds__(128) null_predict_kernel(
+__global__ void __launch_bounds__(128, 4) null_predict_kernel(
     const float* __restrict__ gf, const float* __restrict__ eiid, int n, float log2bl,
     const __nv_bfloat16* __restrict__ wb, const float* __restrict__ fmean,
     const float* __restrict__ fstd, float* __restrict__ out0, float* __restrict__ out1) {
-  __shared__ float w[kParams];
+  __shared__ __align__(16) float w[kParams];
+  __shared__ __align__(16) float w2t[kH * kH];
   __shared__ float mu[kIn], sd[kIn];
   load_weights(wb, w);
+  load_w2t(wb, w2t);
   if (threadIdx.x < kIn) {
     mu[threadIdx.x] = fmean[threadIdx.x];
     sd[threadIdx.x] = fstd[threadIdx.x];
@@ -347,7 +382,7 @@ __global__ void __launch_bounds__(128) null_predict_kernel(
 #pragma unroll
     for (int f = 0; f < kIn; ++f) x[f] = (x[f] - mu[f]) / sd[f];
     float o0, o1;
-    mlp_forward_one(w, x, nullptr, nullptr, o0, o1);
+    mlp_forward_one(w, w2t, x, nullptr, nullptr, o0, o1);
     out0[m] = o0;
     out1[m] = o1;
   }
@@ -374,8 +409,10 @@ __global__ void __launch_bounds__(128) mlp_train_forward_kernel(
     const float* __restrict__ X, const float* __restrict__ Y, int B,
     const __nv_bfloat16* __restrict__ wb, float* __restrict__ z1, float* __restrict__ z2,
     float* __restrict__ dout, float* __restrict__ loss) {
-  __shared__ float w[kParams];
+  __shared__ __align__(16) float w[kParams];
+  __shared__ __align__(16) float w2t[kH * kH];
   load_weights(wb, w);
+  load_w2t(wb, w2t);
   __syncthreads();
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   float l = 0.f;
@@ -384,7 +421,7 @@ __global__ void __launch_bounds__(128) mlp_train_forward_kernel(
 #pragma unroll
     for (int f = 0; f < kIn; ++f) x[f] = X[(int64_t)b * kIn + f];
     float o0, o1;
-    mlp_forward_one(w, x, z1 + (int64_t)b * kH, z2 + (int64_t)b * kH, o0, o1);
+    mlp_forward_one(w, w2t, x, z1 + (int64_t)b * kH, z2 + (int64_t)b * kH, o0, o1);
     const float d0 = o0 - Y[2 * b], d1 = o1 - Y[2 * b + 1];
     dout[2 * b] = d0;
     dout[2 * b + 1] = d1;
@@ -400,7 +437,7 @@ __global__ void __launch_bounds__(128) mlp_train_forward_kernel(
 __global__ void __launch_bounds__(128) mlp_train_deltas_kernel(
     const __nv_bfloat16* __restrict__ wb, const float* __restrict__ dout, int B,
     float* __restrict__ z1, float* __restrict__ z2) {
-  __shared__ float w[kParams];
+  __shared__ __align__(16) float w[kParams];
   load_weights(wb, w);
   __syncthreads();
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
