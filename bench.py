@@ -334,7 +334,7 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
-def surrogate_leg(dev, reps: int = 2, with_cpu: bool = True) -> dict:
+def surrogate_leg(dev, reps: int = 3, with_cpu: bool = True) -> dict:
     """Wall seconds of NetWeaver's surrogate test on cfg5 (2,000 genes x 5,000 cells,
     100 block shuffles of length 50, seed 42, BH-FDR 0.05, parametric p): the full
     test against the learned null, each after one warm-up call, with the edge-set

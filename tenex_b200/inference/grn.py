@@ -46,6 +46,27 @@ def make_grn(variable_names: np.ndarray, pairs: np.ndarray, te: np.ndarray) -> G
                te=te.astype(np.float32), pairs=pairs)
 
 
+_SCAN_ROW = 4096
+
+
+def cummin_1d(x: torch.Tensor) -> torch.Tensor:
+    """Running minimum of a 1-D floating-point tensor, equal element for element
+    to x.cummin(0).values (min is exact; a NaN propagates to every later
+    element). A 1-D scan runs as a single row on the GPU; here the tensor is cut
+    into rows of _SCAN_ROW scanned in parallel, and each row is then lowered by
+    the running minimum of the rows before it (computed the same way)."""
+    m = x.numel()
+    if m <= _SCAN_ROW:
+        return x.cummin(0).values
+    rows = -(-m // _SCAN_ROW)
+    pad = rows * _SCAN_ROW - m
+    xp = torch.cat((x, x.new_full((pad,), float("inf")))) if pad else x
+    s = xp.view(rows, _SCAN_ROW).cummin(1).values
+    carry = cummin_1d(s[:, -1].contiguous())
+    s[1:] = torch.minimum(s[1:], carry[:-1, None])
+    return s.reshape(-1)[:m]
+
+
 def bh_fdr_gpu(pval: torch.Tensor, alpha: float) -> torch.Tensor:
     """Benjamini-Hochberg adjusted p-values (sort, p*m/rank, reverse cummin)."""
     m = pval.shape[0]
@@ -54,7 +75,7 @@ def bh_fdr_gpu(pval: torch.Tensor, alpha: float) -> torch.Tensor:
     sorted_pval, sort_idx = pval.sort()
     rank = torch.arange(1, m + 1, device=pval.device, dtype=pval.dtype)
     adjusted = (sorted_pval * m / rank).clamp(max=1.0)
-    adjusted = adjusted.flip(0).cummin(0).values.flip(0)
+    adjusted = cummin_1d(adjusted.flip(0)).flip(0)
     result = torch.empty_like(adjusted)
     result[sort_idx] = adjusted
     return result

@@ -523,22 +523,6 @@ def z_of_p(p: float, m: int, fdr: float) -> float:
 VERIFY_CFG = dict(threads=256, ctas_per_sm=4, src_chunk=128)
 
 
-def bh_edges_device(p: torch.Tensor, eff: torch.Tensor, tested: torch.Tensor, variable_names,
-                    fdr: float):
-    """bh_edges on device matrices: BH over p[tested] (row-major, float32), edges
-    with adjusted p < fdr and effective TE > 0; the same edges as bh_edges gives
-    for the same float32 values."""
-    from tenex_b200.inference.grn import bh_fdr_gpu, make_grn
-    adj = bh_fdr_gpu(p[tested], alpha=fdr)
-    sig = torch.zeros_like(tested)
-    sig[tested] = adj < fdr
-    sig &= eff > 0
-    idx = torch.nonzero(sig)
-    pairs = idx.cpu().numpy().astype(np.int64)
-    te = eff[idx[:, 0], idx[:, 1]].cpu().numpy()
-    return make_grn(np.asarray(variable_names), pairs, te)
-
-
 def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n_per_var, b_max,
                            kernel_name, tau, n_surrogates, shuffle_method, block_length, p_method,
                            fdr, seed, kwargs):
@@ -551,8 +535,8 @@ def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n
     rest keep the predicted null. BH is recomputed on the mixed p-values and the
     screen widened until z_FDR - band stops falling (at most max_rounds times)."""
     from tenex_b200.inference.grn import build_pairs
-    from tenex_b200.inference.surrogate_test import (SurrogateTestResult, build_block_perm,
-                                                     pair_statistics)
+    from tenex_b200.inference.surrogate_test import (SurrogateTestResult, bh_edges_device,
+                                                     build_block_perm, pair_statistics)
     t0 = time.time()
     model = kwargs.get("null_model")
     if model is None:
@@ -630,7 +614,7 @@ def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n
     eff_s[diag, diag] = obs_d[diag, diag]
     p32 = p_mix.float()
     grn = bh_edges_device(p32, eff_s, tested, variable_names, fdr)
-    host = torch.stack((p32, mean_s.float(), std_s.float(), eff_s.float())).cpu().numpy()
+    host = D.to_host(torch.stack((p32, mean_s.float(), std_s.float(), eff_s.float())))
     p_values, mean_np, std_np, effective = host[0], host[1], host[2], host[3]
     n_ver = int(verified.sum())
     info = {"n_fallback": n_ver, "fallback_fraction": n_ver / max(m_tested, 1),

@@ -307,7 +307,7 @@ class SurrogateTestMethod:
                                   tested_mask(observed_te.shape[0], variable_names,
                                               kwargs.get("sources"), dev),
                                   variable_names, fdr)
-            mean_surr, std_surr, effective_te, p_values = torch.stack(stats).cpu().numpy()
+            mean_surr, std_surr, effective_te, p_values = D.to_host(torch.stack(stats))
         else:
             sum_surr, sum_sq_surr, count_ge = self._accumulate_devices(
                 observed_te, device_ids, bin_data, n_per_var, int(b_max), kernel_name, tau,

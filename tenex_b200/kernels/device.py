@@ -38,6 +38,20 @@ class DeviceBins:
         return self.data[:, :self.row_len].reshape(self.n, self.T, self.K).contiguous()
 
 
+def to_host(t: torch.Tensor) -> np.ndarray:
+    """numpy copy of a device tensor, made through page-locked memory from torch's
+    caching host allocator: a copy into fresh pageable memory runs at a few GB/s
+    (the destination's pages are first touched during the copy), a copy into
+    reused page-locked memory near the link rate. The array keeps its block
+    alive; once the array is released the block goes back to the allocator's
+    cache and the next copy of that size reuses it."""
+    if t.device.type != "cuda":
+        return t.numpy()
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t)
+    return h.numpy()
+
+
 def padded_ld(row_len: int) -> int:
     return (row_len + ROW_ALIGN - 1) // ROW_ALIGN * ROW_ALIGN
 

@@ -83,3 +83,25 @@ def test_fdr_method_registered_and_cuda_only():
         m.infer(np.zeros((3, 3), np.float32), np.array(["a", "b", "c"]), torch.device("cpu"))
     with pytest.raises(NotImplementedError):
         get_method("clr")
+
+
+@pytest.mark.parametrize("m", [1, 4096, 4097, 50_000, 4096 * 4096 + 17])
+def test_blocked_cummin_equals_sequential(m):
+    """BH's reverse running minimum is computed in rows of 4096 plus a carry pass;
+    it must equal the one-row scan element for element, ties and NaN included."""
+    from tenex_b200.inference.grn import bh_fdr_gpu, cummin_1d
+    g = torch.Generator().manual_seed(m)
+    for dt in (torch.float32, torch.float64):
+        x = torch.rand(m, generator=g, dtype=dt)
+        x[::5] = x[::5].round(decimals=2)
+        assert torch.equal(cummin_1d(x), x.cummin(0).values)
+        if m > 2:
+            x[m // 3] = float("nan")
+            a, b = cummin_1d(x), x.cummin(0).values
+            assert torch.equal(a.isnan(), b.isnan())
+            assert torch.equal(a[~a.isnan()], b[~b.isnan()])
+    if m > 100_000:
+        return
+    p = torch.rand(m, generator=g, dtype=torch.float64) ** 4
+    ref = F.bh_adjust(p.numpy())
+    assert np.allclose(bh_fdr_gpu(p, 0.05).numpy(), ref, rtol=1e-12, atol=0)
