@@ -19,6 +19,7 @@ import torch
 
 from tenex_b200 import _log, native
 from tenex_b200.inference.grn import bh_fdr_gpu, build_pairs, make_grn
+from tenex_b200.kernels import device as D
 
 
 def fdr_threshold_gpu(te: torch.Tensor, pairs: torch.Tensor, fdr: float):
@@ -61,16 +62,21 @@ def _offdiag(M: torch.Tensor):
     return te, _LazyPairs(n, M.device)
 
 
-def threshold_pairs(te: torch.Tensor, pairs: torch.Tensor, fdr: float = 0.01, links: int = 0):
-    """Top-`links` or FDR thresholding (tenex/inference/__init__.py:155-170);
-    returns numpy (te_cut, pairs_cut)."""
+def threshold_pairs_device(te: torch.Tensor, pairs, fdr: float = 0.01, links: int = 0):
+    """Top-`links` or FDR thresholding (tenex/inference/__init__.py:155-170) on
+    the device; returns device tensors (te_cut, pairs_cut)."""
     if links > 0:
         k = min(links, len(te))
         _, idx = te.topk(k)
         idx = idx[te[idx].argsort(descending=True)]
-        return te[idx].cpu().numpy(), pairs[idx].cpu().numpy()
-    te_c, p_c = fdr_threshold_gpu(te, pairs, fdr)
-    return te_c.cpu().numpy(), p_c.cpu().numpy()
+        return te[idx], pairs[idx]
+    return fdr_threshold_gpu(te, pairs, fdr)
+
+
+def threshold_pairs(te: torch.Tensor, pairs: torch.Tensor, fdr: float = 0.01, links: int = 0):
+    """threshold_pairs_device with numpy results (te_cut, pairs_cut)."""
+    te_c, p_c = threshold_pairs_device(te, pairs, fdr, links)
+    return D.to_host(te_c), D.to_host(p_c)
 
 
 def dpi_trim_matrix(arr: torch.Tensor, mediator: torch.Tensor | None = None,
@@ -149,14 +155,15 @@ def dpi_trim(n: int, variable_names, pairs: np.ndarray, te_values: np.ndarray,
     (sparse when its work is the smaller); both give the same edges."""
     if method not in ("auto", "dense", "sparse"):
         raise ValueError(f"method must be 'auto', 'dense' or 'sparse' (got {method!r})")
-    pairs = np.asarray(pairs)
     arr = torch.zeros((n, n), dtype=torch.float32, device=device)
     if len(pairs):
-        p = torch.as_tensor(pairs, dtype=torch.long, device=device)
-        arr[p[:, 0], p[:, 1]] = torch.as_tensor(np.asarray(te_values, np.float32), device=device)
+        p = torch.as_tensor(pairs, device=device).long()
+        arr[p[:, 0], p[:, 1]] = torch.as_tensor(te_values, device=device).float()
     mediator = arr.sum(dim=1) > 0
     if not bool(mediator.any()):
-        return make_grn(variable_names, pairs, np.asarray(te_values))
+        host = [D.to_host(x) if isinstance(x, torch.Tensor) else np.asarray(x)
+                for x in (pairs, te_values)]
+        return make_grn(variable_names, host[0], host[1])
     # a batch is active when one of its nonzero columns is a mediator
     row_active = ((arr != 0) & mediator[None, :]).any(dim=1)
     nb = (n + batch_size - 1) // batch_size
@@ -172,8 +179,8 @@ def dpi_trim(n: int, variable_names, pairs: np.ndarray, te_values: np.ndarray,
     if rows.numel() == 0:
         return make_grn(variable_names, np.empty((0, 2), dtype=np.int32),
                         np.empty(0, dtype=np.float32))
-    kept = torch.stack((rows, cols), dim=1).cpu().numpy()
-    return make_grn(variable_names, kept, vals.cpu().numpy())
+    kept = D.to_host(torch.stack((rows, cols), dim=1))
+    return make_grn(variable_names, kept, D.to_host(vals))
 
 
 class FDRMethod:
@@ -197,7 +204,7 @@ class FDRMethod:
                                f"{device}")
         variable_names = np.asarray(variable_names)
         te_matrix = np.asarray(te_matrix, dtype=np.float32)
-        M = torch.as_tensor(te_matrix).to(device)
+        M = D.to_device(te_matrix, device)
         if sources is None:
             # build_pairs' all-pairs order is the row-major off-diagonal order of
             # M[src, tgt]: select it on the device instead of materialising the
@@ -207,12 +214,12 @@ class FDRMethod:
             pairs_np = build_pairs(variable_names, sources)
             pairs_t = torch.from_numpy(np.ascontiguousarray(pairs_np)).to(device, dtype=torch.long)
             te_t = M[pairs_t[:, 0], pairs_t[:, 1]]
-        te_cut, pairs_cut = threshold_pairs(te_t, pairs_t, fdr=fdr, links=links)
-        grn = make_grn(variable_names, pairs_cut, te_cut)
+        te_d, pairs_d = threshold_pairs_device(te_t, pairs_t, fdr=fdr, links=links)
+        grn = make_grn(variable_names, D.to_host(pairs_d), D.to_host(te_d))
         _log.vprint(f"[TENEX] inference(fdr): {len(grn)} links after thresholding")
         if not is_trimming:
             return grn
-        trimmed = dpi_trim(te_matrix.shape[0], variable_names, pairs_cut, te_cut, device,
+        trimmed = dpi_trim(te_matrix.shape[0], variable_names, pairs_d, te_d, device,
                            batch_size=batch_size, trim_threshold=trim_threshold,
                            method=dpi_method)
         _log.vprint(f"[TENEX] inference(fdr): {len(trimmed)} links after trimming")

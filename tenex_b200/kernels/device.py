@@ -8,6 +8,8 @@ is stored as row[t*K + k] (row_len = T*K) and TE uses lag = tau*K.
 from __future__ import annotations
 
 import ctypes
+import os
+import threading
 from dataclasses import dataclass
 
 import numpy as np
@@ -38,18 +40,112 @@ class DeviceBins:
         return self.data[:, :self.row_len].reshape(self.n, self.T, self.K).contiguous()
 
 
+_copy_pool = None
+_copy_workers = max(1, min(8, os.cpu_count() or 1))
+_copy_pool_lock = threading.Lock()
+_STAGE_BYTES = 32 << 20        # one staging chunk of the host -> device copy
+_DIRECT_BYTES = 16 << 20       # smaller arrays take the plain pageable copy (to device)
+_DIRECT_HOST_BYTES = 4 << 20   # and below this, the plain copy back
+
+
+def _pool():
+    global _copy_pool
+    with _copy_pool_lock:
+        if _copy_pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            _copy_pool = ThreadPoolExecutor(max_workers=_copy_workers,
+                                            thread_name_prefix="tenex-h2d")
+        return _copy_pool
+
+
+def to_device(a, device) -> torch.Tensor:
+    """Device copy of a host array (numpy or CPU tensor), same shape and dtype.
+    A large array goes through two page-locked staging chunks: host threads fill
+    chunk i + 1 (numpy copies run without the GIL) while the DMA engine moves
+    chunk i, which runs several times faster than one pageable copy (the driver
+    stages a pageable copy through its own buffer with one host thread). A
+    page-locked tensor is copied directly. The source is no longer read once
+    this returns (except a page-locked source, read by the DMA in stream order);
+    the device copy is ordered on the current stream."""
+    if isinstance(a, torch.Tensor):
+        if a.device.type == "cuda" or (torch.cuda.is_available() and a.is_pinned()):
+            return a.to(device)             # already DMA-able: one direct copy
+        a = a.numpy()
+    a = np.ascontiguousarray(a)
+    device = torch.device(device)
+    if device.type != "cuda" or a.nbytes < _DIRECT_BYTES or a.dtype == object:
+        return torch.as_tensor(a).to(device)
+    flat = a.reshape(-1)
+    proto = torch.from_numpy(flat[:1].copy())
+    out = torch.empty(flat.size, dtype=proto.dtype, device=device)
+    per = max(1, _STAGE_BYTES // a.itemsize)
+    bufs = [torch.empty(per, dtype=proto.dtype, pin_memory=True) for _ in range(2)]
+    done = [None, None]
+    pool = _pool()
+    workers = _copy_workers
+    with torch.cuda.device(device):
+        stream = torch.cuda.current_stream()
+        for i, off in enumerate(range(0, flat.size, per)):
+            k = min(per, flat.size - off)
+            j = i & 1
+            if done[j] is not None:
+                done[j].synchronize()        # the DMA that last read this chunk is over
+            dst = bufs[j].numpy()
+            step = -(-k // workers)
+            cuts = [(c, min(c + step, k)) for c in range(0, k, step)]
+            list(pool.map(lambda r: np.copyto(dst[r[0]:r[1]], flat[off + r[0]:off + r[1]]),
+                          cuts))
+            out[off:off + k].copy_(bufs[j][:k], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            done[j] = ev
+    return out.view(a.shape)
+
+
 def to_host(t: torch.Tensor) -> np.ndarray:
-    """numpy copy of a device tensor, made through page-locked memory from torch's
-    caching host allocator: a copy into fresh pageable memory runs at a few GB/s
-    (the destination's pages are first touched during the copy), a copy into
-    reused page-locked memory near the link rate. The array keeps its block
-    alive; once the array is released the block goes back to the allocator's
-    cache and the next copy of that size reuses it."""
+    """numpy copy of a device tensor. A large tensor comes back through two
+    page-locked staging chunks: the DMA engine fills chunk i + 1 while host
+    threads copy chunk i out into an ordinary numpy array. One pageable copy
+    runs at a few GB/s (the driver's own staging with one host thread, and the
+    destination's pages first touched inside the copy); the staging chunks come
+    from torch's caching host allocator and are released before this returns,
+    so no page-locked memory outlives the call."""
     if t.device.type != "cuda":
         return t.numpy()
-    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-    h.copy_(t)
-    return h.numpy()
+    t = t.contiguous()
+    nbytes = t.numel() * t.element_size()
+    if nbytes < _DIRECT_HOST_BYTES:
+        return t.cpu().numpy()
+    flat = t.view(-1)
+    numel = flat.numel()
+    out = np.empty(numel, dtype=torch.empty(0, dtype=t.dtype).numpy().dtype)
+    per = max(1, _STAGE_BYTES // t.element_size())
+    bufs = [torch.empty(per, dtype=t.dtype, pin_memory=True) for _ in range(2)]
+    offs = list(range(0, numel, per))
+    done = [None, None]
+    pool = _pool()
+    with torch.cuda.device(t.device):
+        stream = torch.cuda.current_stream()
+
+        def issue(i):
+            off = offs[i]
+            k = min(per, numel - off)
+            bufs[i & 1][:k].copy_(flat[off:off + k], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            done[i & 1] = ev
+
+        issue(0)
+        for i, off in enumerate(offs):
+            if i + 1 < len(offs):
+                issue(i + 1)       # its buffer's previous chunk was copied out last pass
+            done[i & 1].synchronize()
+            k = min(per, numel - off)
+            src = bufs[i & 1].numpy()
+            step = -(-k // _copy_workers)
+            list(pool.map(lambda c: np.copyto(out[off + c:off + min(c + step, k)],
+                                              src[c:min(c + step, k)]), range(0, k, step)))
+    return out.reshape(tuple(t.shape))
 
 
 def padded_ld(row_len: int) -> int:
@@ -78,7 +174,8 @@ def pack_bins(bin_arrs, device, b_max: int | None = None) -> DeviceBins:
     if b_max is not None and b_max > 255:
         raise ValueError(f"b_max={b_max} does not fit the uint8 bin layout")
     db = empty_bins(n, T, K, device)
-    src = t.reshape(n, T * K).to(device=device)
+    src = t.reshape(n, T * K)
+    src = to_device(src, device) if src.device.type == "cpu" else src.to(device=device)
     if src.dtype != torch.uint8:
         src = src.to(torch.int32).clamp_(0, 255).to(torch.uint8)
     db.data[:, :T * K].copy_(src)

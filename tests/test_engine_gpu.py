@@ -195,3 +195,47 @@ def test_compute_over_several_devices(cuda):
     d = TransferEntropyEngine(xb, nb).compute(accelerator="gpu", devices=[0, 0],
                                               binarization="nonzero").matrix
     assert np.array_equal(c, d)
+
+
+@pytest.mark.parametrize("dtype,shape", [(np.float32, (2500, 2500)), (np.uint8, (3, 20_000_011)),
+                                         (np.int16, (4097, 4099)), (np.float64, (7,)),
+                                         (np.int64, (9_000_001,))])
+def test_staged_host_copy_equals_plain_copy(cuda, dtype, shape):
+    """to_device (page-locked staging chunks filled by host threads) gives the
+    same tensor as a plain copy: sizes below, at and across chunk boundaries,
+    several dtypes, and a non-contiguous source."""
+    rng = np.random.default_rng(7)
+    if np.issubdtype(dtype, np.integer):
+        info = np.iinfo(dtype)
+        a = rng.integers(info.min, info.max, size=shape, dtype=dtype, endpoint=True)
+    else:
+        a = (rng.standard_normal(shape) * 100).astype(dtype)
+    t = D.to_device(a, cuda)
+    assert t.dtype == torch.as_tensor(a).dtype and tuple(t.shape) == a.shape
+    assert torch.equal(t.cpu(), torch.as_tensor(a))
+    if a.ndim == 2:
+        b = a.T                                           # non-contiguous view
+        assert torch.equal(D.to_device(b, cuda).cpu(), torch.as_tensor(np.ascontiguousarray(b)))
+    src = torch.as_tensor(a)
+    assert torch.equal(D.to_device(src, cuda).cpu(), src)
+
+
+@pytest.mark.parametrize("dtype,shape", [(torch.float32, (4000, 4000)), (torch.int64, (9_000_001,)),
+                                         (torch.bool, (3, 30_000_001)), (torch.uint8, (5_000_000,)),
+                                         (torch.float64, (1000, 3))])
+def test_staged_device_copy_back_equals_plain(cuda, dtype, shape):
+    """to_host (DMA into two page-locked chunks, host threads copying out) gives
+    the array a plain .cpu().numpy() gives: sizes below, at and across the
+    32 MB chunks, several dtypes, a non-contiguous source."""
+    g = torch.Generator(device=cuda).manual_seed(11)
+    if dtype == torch.bool:
+        t = torch.rand(shape, generator=g, device=cuda) > 0.5
+    elif dtype.is_floating_point:
+        t = torch.randn(shape, generator=g, device=cuda, dtype=dtype)
+    else:
+        t = torch.randint(0, 200, shape, generator=g, device=cuda, dtype=dtype)
+    h = D.to_host(t)
+    ref = t.cpu().numpy()
+    assert h.dtype == ref.dtype and h.shape == ref.shape and np.array_equal(h, ref)
+    if t.dim() == 2:
+        assert np.array_equal(D.to_host(t.t()), t.t().cpu().numpy())

@@ -39,3 +39,13 @@ def test_batch_size_hooks_and_multi_device_contracts():
         k.compute_matrix_multi_gpu(cpu_bins, 4, 1, [0])
     with pytest.raises(ValueError):
         get_kernel("GEMM-B2").compute_matrix_multi_gpu(cpu_bins, 4, 1, [])
+
+
+def test_host_copy_helpers_without_cuda():
+    """to_device / to_host keep shape, dtype and values on a CPU target (the
+    staging path is CUDA-only and is covered by the GPU tests)."""
+    from tenex_b200.kernels import device as D
+    a = np.arange(24, dtype=np.int16).reshape(4, 6)
+    t = D.to_device(a, "cpu")
+    assert t.dtype == torch.int16 and torch.equal(t, torch.as_tensor(a))
+    assert np.array_equal(D.to_host(t), a)
