@@ -59,7 +59,7 @@ class GEMMB2Kernel(TEKernel):
         if db.K != 1:
             raise ValueError(f"GEMM-B2 kernel only supports K=1, got K={db.K}")
         m = te_binary_matrix(db, tau)
-        return m.t().contiguous().cpu().numpy()  # reference orientation: [i, j] = TE(j -> i)
+        return D.to_host(m.t())  # reference orientation: [i, j] = TE(j -> i)
 
     def compute_single_gpu(self, bin_arrs, pairs, b_max, n_per_var, tau, batch_size, device,
                            **kwargs) -> np.ndarray:

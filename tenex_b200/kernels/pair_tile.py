@@ -105,7 +105,7 @@ class PairTileKernel(TEKernel):
             raise ValueError(f"bin_arrs has {db.n} variables, n_vars={n_vars}")
         te = self.compute_pairfree_device(db, n_per_var, b_max, tau, pair_offset,
                                           n_pairs_local)
-        return te.cpu().numpy()
+        return D.to_host(te)
 
     def compute_pairfree_cross(self, bin_arrs, n_per_var, n_tgt: int, n_src: int, tau: int,
                                device, pair_offset: int = 0,
@@ -124,7 +124,7 @@ class PairTileKernel(TEKernel):
                              f"outside [0, {total})")
         out = torch.empty(n_pairs_local, dtype=torch.float32, device=dev)
         if n_pairs_local == 0:
-            return out.cpu().numpy()
+            return D.to_host(out)
         b_max = int(torch.as_tensor(n_per_var).max())
         db = D.pack_bins(bin_arrs, dev, b_max)
         npv = _npv_tensor(n_per_var, dev)
@@ -139,7 +139,7 @@ class PairTileKernel(TEKernel):
                     items.numel() - 1, out.data_ptr(), ws.data_ptr(), ws.numel(),
                     D._cfg(self.cfg), s)
         native.call("tenex_workspace_status", ws.data_ptr(), s)
-        return out.cpu().numpy()
+        return D.to_host(out)
 
     def compute_single_gpu(self, bin_arrs, pairs, b_max, n_per_var, tau, batch_size, device,
                            **kwargs) -> np.ndarray:

@@ -43,7 +43,7 @@ def fsbwl_bins(x, kp: float = 0.5, device=None) -> tuple[torch.Tensor, torch.Ten
     dev = _device(device)
     xt = torch.as_tensor(np.ascontiguousarray(x, dtype=np.float32)) if not isinstance(
         x, torch.Tensor) else x.to(torch.float32)
-    xt = xt.to(dev).contiguous()
+    xt = (D.to_device(xt, dev) if xt.device.type == "cpu" else xt.to(dev)).contiguous()
     n, T = (int(s) for s in xt.shape)
     bins = torch.empty((n, T), dtype=torch.int32, device=dev)
     nb = torch.empty(n, dtype=torch.int32, device=dev)
@@ -60,18 +60,16 @@ def remap_bins(raw, K: int = 1, device=None) -> tuple[D.DeviceBins, torch.Tensor
     if t.dim() == 3:
         K = int(t.shape[2])
         t = t.reshape(t.shape[0], -1)
+    if t.dtype.is_floating_point or t.dtype == torch.uint16:
+        t = t.to(torch.int32)             # on the host: same conversion as before upload
+    # integers go up in their own width (staged copy) and are widened on the device
+    t = D.to_device(t, dev) if t.device.type == "cpu" else t.to(dev)
     if t.dtype == torch.uint8:
         in_bytes = 1
-    elif t.dtype in (torch.int16, torch.uint16):
-        t = t.to(torch.int32)
-        in_bytes = 4
-    elif t.dtype == torch.int8:
-        t = t.to(torch.int32)
-        in_bytes = 4
     else:
         t = t.to(torch.int32)
         in_bytes = 4
-    t = t.to(dev).contiguous()
+    t = t.contiguous()
     n, row = (int(s) for s in t.shape)
     if row % K:
         raise ValueError(f"row length {row} is not a multiple of K={K}")

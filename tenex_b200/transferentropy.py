@@ -263,7 +263,7 @@ class TransferEntropyEngine:
             else:
                 m = kobj.compute_matrix_device(db, tau)  # [src, tgt] = TE(src -> tgt)
                 mark(5)
-                self._result_matrix = m.cpu().numpy()
+                self._result_matrix = D.to_host(m)
             self._finish(info, db, npv, b_max, ev, stream, t0, "matrix")
             return self._wrap_result()
 
@@ -288,7 +288,7 @@ class TransferEntropyEngine:
                 te = te_pair_list(work, npv_w, b_max_w, tau, pairs,
                                   cfg=getattr(kobj, "cfg", None))
                 mark(6)
-                te_h = te.cpu().numpy()
+                te_h = D.to_host(te)
             rm = np.zeros((n_vars, n_vars), dtype=np.float32)
             rm[pairs[:, 0], pairs[:, 1]] = te_h
             self._result_matrix = rm.T.copy()
@@ -302,14 +302,14 @@ class TransferEntropyEngine:
                 m = kobj.compute_pairfree_device(work, npv_w, b_max_w, tau, matrix=True,
                                                  autotune_shape=autotune)
                 mark(6)
-                self._result_matrix = m.cpu().numpy()
+                self._result_matrix = D.to_host(m)
         self._finish(info, work, npv_w, b_max_w, ev, stream, t0, "pair")
         return self._wrap_result()
 
     @staticmethod
     def _host_bins(db: D.DeviceBins) -> np.ndarray:
         """(n, T, K) host copy of device bins (the padding dropped)."""
-        return db.data[:, :db.row_len].cpu().numpy().reshape(db.n, db.T, db.K)
+        return D.to_host(db.data[:, :db.row_len]).reshape(db.n, db.T, db.K)
 
     @staticmethod
     def _pairfree_multi_device(kobj, work: D.DeviceBins, npv: torch.Tensor, b_max: int,
@@ -334,7 +334,7 @@ class TransferEntropyEngine:
             db = D.DeviceBins(host.to(dev), n, work.T, work.K)
             m = kobj.compute_pairfree_device(db, npv_h.to(dev), b_max, tau, p0, p1 - p0,
                                              matrix=True, autotune_shape=autotune)
-            return m.cpu().numpy()
+            return D.to_host(m)
 
         with ThreadPoolExecutor(max_workers=len(device_ids)) as ex:
             parts = [p for p in ex.map(run, range(len(device_ids))) if p is not None]
@@ -363,7 +363,10 @@ class TransferEntropyEngine:
                 timings["assemble"] = sec(6, 7)
             info["timings"] = timings
         self._last_run_info = info
-        self._last_bin_arrs = (db.unpadded().cpu().numpy().astype(compact_dtype(b_max)))
+        # the compact dtype is applied on the device (bins are < 256, so the values
+        # are unchanged), then one staged copy
+        dt = torch.from_numpy(np.empty(0, dtype=compact_dtype(b_max))).dtype
+        self._last_bin_arrs = D.to_host(db.unpadded().to(dt))
         self._last_n_per_var = npv.cpu().numpy()
         elapsed = time.time() - t0
         _log.vprint(f"[TENEX] done -- {elapsed:.3f}s "
