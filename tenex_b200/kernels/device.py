@@ -58,6 +58,18 @@ def _pool():
         return _copy_pool
 
 
+def all_finite(a: np.ndarray) -> bool:
+    """np.isfinite(a).all() for a large C-contiguous array, checked in 4M-element
+    slabs on the host copy threads (ufuncs run without the GIL)."""
+    a = np.asarray(a)
+    if a.size < (1 << 23) or not a.flags.c_contiguous:
+        return bool(np.isfinite(a).all())
+    flat = a.reshape(-1)
+    step = 1 << 22
+    return all(_pool().map(lambda c: bool(np.isfinite(flat[c:c + step]).all()),
+                           range(0, flat.size, step)))
+
+
 def to_device(a, device) -> torch.Tensor:
     """Device copy of a host array (numpy or CPU tensor), same shape and dtype.
     A large array goes through two page-locked staging chunks: host threads fill

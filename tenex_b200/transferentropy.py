@@ -50,7 +50,7 @@ class TransferEntropyEngine:
         if self._data.ndim != 2 or self._data.size == 0:
             raise ValueError(f"data must be a non-empty 2-D array of shape (n_vars, T); "
                              f"got shape {self._data.shape}")
-        if not np.isfinite(self._data).all():
+        if not D.all_finite(self._data):
             raise ValueError("data contains NaN or infinite values")
         if self._variable_names.ndim != 1:
             raise ValueError(f"variable_names must be 1-D; got shape "

@@ -49,3 +49,14 @@ def test_host_copy_helpers_without_cuda():
     t = D.to_device(a, "cpu")
     assert t.dtype == torch.int16 and torch.equal(t, torch.as_tensor(a))
     assert np.array_equal(D.to_host(t), a)
+
+
+def test_all_finite_matches_numpy():
+    from tenex_b200.kernels import device as D
+    x = np.random.default_rng(3).standard_normal((700, 20_000)).astype(np.float32)
+    assert D.all_finite(x)
+    for bad in (np.nan, np.inf, -np.inf):
+        y = x.copy()
+        y[699, 19_998] = bad
+        assert not D.all_finite(y) and not np.isfinite(y).all()
+    assert not D.all_finite(y[:, ::2]) and D.all_finite(x[:, ::2])  # non-contiguous
