@@ -291,6 +291,7 @@ def run_ours(args) -> None:
     N = C - TAU
     incr = (p1 - p0) * N                                   # histogram increments per launch
     peak_atomic = max(native.probe_smem_atomics(0, 8192) for _ in range(3))
+    peak_scatter = max(native.probe_smem_atomics(2, 8192) for _ in range(3))
     achieved = incr / (te_ms / 1e3)
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs")
@@ -302,6 +303,11 @@ def run_ours(args) -> None:
                         "launch time (CUDA events); peak = conflict-free shared-memory atomicAdd "
                         "rate measured live by tenex_probe_smem_atomics (mode 0) on this GPU "
                         "(MEASURED_PEAKS.json has no shared-memory-atomic figure)",
+                "scatter_peak": peak_scatter / 1e9,
+                "frac_of_scatter": achieved / peak_scatter,
+                "scatter_note": "second denominator, for context: the same probe with each lane "
+                                "adding into a random word of a 16 KB histogram (mode 2), the "
+                                "access pattern of a histogram of random cells",
                 "te_kernel_ms": te_ms}
     roofline_hbm = {"bound": "hbm", "achieved": compulsory / (te_ms / 1e3) / 1e9,
                     "peak": hbm_peak, "unit": "GB/s",
