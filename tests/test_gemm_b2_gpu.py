@@ -56,3 +56,25 @@ def test_non_binary_bins_report_bad_data(cuda):
     x[7, 123] = 1
     m = te_binary_matrix(D.pack_bins(x, cuda), 1).cpu().numpy()
     assert np.max(np.abs(m - O.te_matrix(x, np.full(20, 2, np.int32)))) <= 1e-6
+
+
+def test_binary_full_size_sampled_and_deterministic(cuda):
+    """2,000 genes x 5,000 cells of binary Markov bins with 20 planted lag-1
+    pairs, the whole matrix in one pack + GEMM launch pair: 50,000 random pairs
+    and every planted pair within 1e-6 of the float64 oracle, zero diagonal, a
+    second run bitwise equal."""
+    x, planted = W.cfg2_binary()
+    n = x.shape[0]
+    m = _run(x, cuda)                                   # [src, tgt]
+    rng = np.random.default_rng(21)
+    src = rng.integers(0, n, 50_000)
+    tgt = rng.integers(0, n, 50_000)
+    pl = np.asarray(planted, dtype=np.int64).reshape(-1, 2)
+    src = np.concatenate([src, pl[:, 0]])
+    tgt = np.concatenate([tgt, pl[:, 1]])
+    keep = src != tgt
+    src, tgt = src[keep], tgt[keep]
+    ref = O.te_pairs(x.astype(np.int32), np.full(n, 2, np.int32), np.stack([tgt, src], axis=1))
+    assert np.max(np.abs(m[src, tgt].astype(np.float64) - ref)) <= TOL
+    assert np.all(np.diag(m) == 0)
+    assert np.array_equal(m.view(np.uint32), _run(x, cuda).view(np.uint32))

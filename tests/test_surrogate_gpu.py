@@ -159,3 +159,43 @@ def test_device_statistics_match_numpy_expressions(cuda):
             assert np.array_equal(r.view(np.uint32), g.view(np.uint32))
         ulps = np.abs(ref[3].view(np.int32).astype(np.int64) - got[3].view(np.int32).astype(np.int64))
         assert ulps.max() <= 1 and (ulps > 0).mean() < 1e-3, (method, ulps.max(), (ulps > 0).sum())
+
+
+def test_full_size_surrogates_sampled_against_oracle(cuda):
+    """2,000 genes x 5,000 cells (b ~ U{2..16} Markov), 100 block shuffles of
+    length 50 with the reference's seeds (42 + k): the device sums, sums of
+    squares and counts of 1,500 sampled pairs against the float64 oracle run on
+    the same permutations (float32 TE widened to float64, as the reference's
+    loop accumulates)."""
+    x, npv, _ = W.cfg5_bins()
+    n, T = x.shape
+    bmax = int(npv.max())
+    db = D.pack_bins(x, cuda)
+    obs = D.te_pairfree(db, torch.as_tensor(npv, device=cuda), bmax, matrix=True).cpu().numpy()
+    S, bl = 100, 50
+    perms, eff_bl, _ = build_block_perm(n, T, "block", bl, 0, S, 42, cuda)
+    acc = _acc(x, npv, bmax, obs, cuda)
+    run_surrogates(acc, perms, eff_bl)
+    rng = np.random.default_rng(46)
+    src = rng.integers(0, n, 1500)
+    tgt = rng.integers(0, n, 1500)
+    keep = src != tgt
+    src, tgt = src[keep], tgt[keep]
+    pairs_ts = np.stack([tgt, src], axis=1)
+    obs_ref = O.te_pairs(x, npv, pairs_ts).astype(np.float32)
+    assert np.max(np.abs(obs[src, tgt] - obs_ref)) <= TOL
+    s = np.zeros(len(src))
+    ss = np.zeros(len(src))
+    c = np.zeros(len(src), np.int64)
+    ph = perms.cpu().numpy()
+    for k in range(S):
+        te = O.te_pairs(O.block_shuffle(x, ph[k], eff_bl), npv, pairs_ts).astype(np.float32)
+        t64 = te.astype(np.float64)
+        s += t64
+        ss += t64 * t64
+        c += te >= obs_ref
+    assert np.max(np.abs(acc.sum.cpu().numpy()[src, tgt] - s)) <= S * TOL
+    assert np.max(np.abs(acc.sumsq.cpu().numpy()[src, tgt] - ss)) <= S * TOL
+    cg = acc.cnt.cpu().numpy()[src, tgt]
+    assert np.mean(cg != c) <= 1e-2           # ties within 1e-6 may flip a comparison
+    assert np.max(np.abs(cg - c)) <= 2
