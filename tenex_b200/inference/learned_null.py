@@ -441,7 +441,8 @@ def fallback_surrogates_batched(db: D.DeviceBins, npv: torch.Tensor, b_max: int,
     g is gene k * n + g) and every listed pair is listed once per copy, so one
     tenex_te_pairs launch covers S_chunk surrogates with full-GPU occupancy instead
     of S launches of a few thousand small work items. The per-surrogate TEs are
-    then added into the statistics in surrogate order (float64)."""
+    then reduced over the surrogate axis in float64 (a sum of float32 values;
+    the order of the additions changes the result by float64 rounding at most)."""
     dev = db.data.device
     n, S = db.n, perms.shape[0]
     sp, items = _pair_items(pairs_ts)
@@ -481,11 +482,10 @@ def fallback_surrogates_batched(db: D.DeviceBins, npv: torch.Tensor, b_max: int,
                     native.stream_ptr())
         native.call("tenex_workspace_status", ws.data_ptr(), native.stream_ptr())
         te = te.view(kk, P)
-        for j in range(kk):                                   # surrogate order
-            t = te[j].double()
-            s1 += t
-            s2 += t * t
-            c += (te[j] >= obs_p).to(torch.int32)
+        t64 = te.double()
+        s1 += t64.sum(dim=0)
+        s2 += (t64 * t64).sum(dim=0)
+        c += (te >= obs_p[None, :]).sum(dim=0, dtype=torch.int32)
         del big, pairs_big, items_big, ws, te
     ssum[src_d, tgt_d] = s1
     ssq[src_d, tgt_d] = s2
