@@ -177,6 +177,14 @@ int tenex_block_shuffle(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T,
                         const int32_t* perm, int n_blocks, int block_length,
                         uint8_t* out, int64_t out_ld, void* stream);
 
+/* n_copies block shuffles of the same bins in one launch (the learned null's
+ * verification pass): copy s uses perms + s*n_vars*n_blocks and writes the
+ * (n_vars, out_ld) rows at out + s*out_copy_stride. The outputs must not
+ * overlap the input or each other; T*K < 2^31. */
+int tenex_block_shuffle_many(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T, int K,
+                             const int32_t* perms, int n_copies, int n_blocks, int block_length,
+                             uint8_t* out, int64_t out_ld, int64_t out_copy_stride, void* stream);
+
 /* FSBW-L discretisation, bit-identical to the reference's numpy path
  * (bin_fsbw_l_numpy, tenex/preprocess.py:61-88, then clamp(min=0) of :680):
  * x float32 (n_vars, T) row stride ldx; bins int32 (n_vars, T) row stride ldb;

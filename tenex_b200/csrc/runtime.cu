@@ -59,31 +59,47 @@ int current_device_attr(DevAttr* out) {
 }
 
 // out[g, t*K+k] = in[g, (perm[g, t/bl]*bl + t%bl)*K + k] for t < n_blocks*bl; tail copied.
-// Grid: (ceil(T*K / 256 / 4), n_vars); each thread moves 4 consecutive bytes.
+// With blK = bl*K bytes per block, byte i < head of a row maps to
+// perm[g, i / blK] * blK + i % blK. Grid: (ceil(T*K / 4096), n_vars, copies); each
+// thread gathers 16 consecutive output bytes (one 32-bit division, then a running
+// block offset) and writes them as one 16-byte store when the row holds all 16
+// (rows start on 16-byte boundaries, checked by the launcher), bytewise at the row
+// end. row < 2^31 (checked). Copy s reads perm + s * perm_stride and writes
+// out + s * out_stride.
 __global__ void block_shuffle_kernel(const uint8_t* __restrict__ in, int64_t in_ld, int n,
-                                     int64_t T, int K, const int32_t* __restrict__ perm,
-                                     int n_blocks, int bl, uint8_t* __restrict__ out,
-                                     int64_t out_ld) {
+                                     uint32_t row, uint32_t blK, uint32_t head,
+                                     const int32_t* __restrict__ perm, int64_t perm_stride,
+                                     int n_blocks, uint8_t* __restrict__ out, int64_t out_ld,
+                                     int64_t out_stride) {
   const int g = blockIdx.y;
-  const int64_t row = T * K;
-  const int64_t head = (int64_t)n_blocks * bl * K;
   const uint8_t* src = in + (int64_t)g * in_ld;
-  uint8_t* dst = out + (int64_t)g * out_ld;
-  const int32_t* pg = perm + (int64_t)g * n_blocks;
-  const int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  uint8_t* dst = out + (int64_t)blockIdx.z * out_stride + (int64_t)g * out_ld;
+  const int32_t* pg = perm + (int64_t)blockIdx.z * perm_stride + (int64_t)g * n_blocks;
+  const uint32_t i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 16u;
+  if (i0 >= row) return;
+  uint32_t b = i0 / blK, off = i0 - b * blK;
+  uint32_t w[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    const int64_t i = i0 + u;
-    if (i >= row) break;
-    int64_t j = i;
-    if (i < head) {
-      const int64_t t = i / K, k = i - t * K;
-      const int64_t b = t / bl, off = t - b * bl;
-      int pb = pg[b];
-      if ((unsigned)pb >= (unsigned)n_blocks) pb = (int)b;  // out-of-range entry: identity
-      j = ((int64_t)pb * bl + off) * K + k;
+  for (uint32_t u = 0; u < 16u; ++u) {
+    const uint32_t i = i0 + u;
+    if (i < row) {
+      uint32_t j = i;
+      if (i < head) {
+        uint32_t pb = (uint32_t)pg[b];
+        if (pb >= (uint32_t)n_blocks) pb = b;  // out-of-range entry: identity
+        j = pb * blK + off;
+      }
+      w[u >> 2] |= (uint32_t)src[j] << (8u * (u & 3u));
     }
-    dst[i] = src[j];
+    if (++off == blK) {
+      off = 0;
+      ++b;
+    }
+  }
+  if (i0 + 16u <= row) {
+    *reinterpret_cast<uint4*>(dst + i0) = make_uint4(w[0], w[1], w[2], w[3]);
+  } else {
+    for (uint32_t u = 0; i0 + u < row; ++u) dst[i0 + u] = (uint8_t)(w[u >> 2] >> (8u * (u & 3u)));
   }
 }
 
@@ -159,24 +175,44 @@ extern "C" int tenex_device_query(int device, tenex_dev_info* info) {
   return TENEX_OK;
 }
 
-extern "C" int tenex_block_shuffle(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T, int K,
-                                   const int32_t* perm, int n_blocks, int block_length,
-                                   uint8_t* out, int64_t out_ld, void* stream) {
-  if (!in || !out || !perm) return fail(TENEX_ERR_BADARG, "in, out and perm must be non-NULL");
+extern "C" int tenex_block_shuffle_many(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T,
+                                        int K, const int32_t* perms, int n_copies, int n_blocks,
+                                        int block_length, uint8_t* out, int64_t out_ld,
+                                        int64_t out_copy_stride, void* stream) {
+  if (!in || !out || !perms) return fail(TENEX_ERR_BADARG, "in, out and perms must be non-NULL");
   if (n_vars < 1 || T < 1 || K < 1) return fail(TENEX_ERR_BADARG, "empty bins");
+  if (n_copies < 1) return fail(TENEX_ERR_BADARG, "n_copies must be >= 1");
   if (block_length < 1 || n_blocks < 1 || (int64_t)n_blocks * block_length > T)
     return fail(TENEX_ERR_BADARG, "need n_blocks*block_length <= T (n_blocks=%d, bl=%d, T=%lld)",
                 n_blocks, block_length, (long long)T);
   if (in_ld < T * K || out_ld < T * K)
     return fail(TENEX_ERR_BADARG, "row strides must be >= T*K");
-  if (in == out) return fail(TENEX_ERR_BADARG, "block shuffle cannot run in place");
+  const int64_t copy_bytes = (int64_t)(n_vars - 1) * out_ld + T * K;
+  if (n_copies > 1 && out_copy_stride < copy_bytes)
+    return fail(TENEX_ERR_BADARG, "copies overlap (out_copy_stride %lld < %lld)",
+                (long long)out_copy_stride, (long long)copy_bytes);
+  const uint8_t* in_end = in + (int64_t)(n_vars - 1) * in_ld + T * K;
+  const uint8_t* out_end = out + (int64_t)(n_copies - 1) * out_copy_stride + copy_bytes;
+  if (in < out_end && out < in_end) return fail(TENEX_ERR_BADARG, "block shuffle cannot run in place");
+  if ((reinterpret_cast<uintptr_t>(out) & 15) || (out_ld & 15) || (n_copies > 1 && (out_copy_stride & 15)))
+    return fail(TENEX_ERR_BADARG, "out, out_ld and out_copy_stride must be 16-byte aligned");
   const int64_t row = T * K;
-  const int64_t gx = (row + 1023) / 1024;
-  if (gx > 0x7fffffff || n_vars > 65535)
-    return fail(TENEX_ERR_UNSUPPORTED, "grid too large (row=%lld, n_vars=%d)", (long long)row,
-                n_vars);
-  dim3 grid((unsigned)gx, (unsigned)n_vars);
-  block_shuffle_kernel<<<grid, 256, 0, as_stream(stream)>>>(in, in_ld, n_vars, T, K, perm,
-                                                             n_blocks, block_length, out, out_ld);
+  if (row > 0x7fffffff - 4096)
+    return fail(TENEX_ERR_UNSUPPORTED, "row of %lld bytes", (long long)row);
+  const int64_t gx = (row + 4095) / 4096;
+  if (n_vars > 65535 || n_copies > 65535)
+    return fail(TENEX_ERR_UNSUPPORTED, "grid too large (n_vars=%d, copies=%d)", n_vars, n_copies);
+  dim3 grid((unsigned)gx, (unsigned)n_vars, (unsigned)n_copies);
+  block_shuffle_kernel<<<grid, 256, 0, as_stream(stream)>>>(
+      in, in_ld, n_vars, (uint32_t)row, (uint32_t)(block_length * K),
+      (uint32_t)((int64_t)n_blocks * block_length * K), perms, (int64_t)n_vars * n_blocks,
+      n_blocks, out, out_ld, out_copy_stride);
   return check_launch("block_shuffle_kernel");
+}
+
+extern "C" int tenex_block_shuffle(const uint8_t* in, int64_t in_ld, int n_vars, int64_t T, int K,
+                                   const int32_t* perm, int n_blocks, int block_length,
+                                   uint8_t* out, int64_t out_ld, void* stream) {
+  return tenex_block_shuffle_many(in, in_ld, n_vars, T, K, perm, 1, n_blocks, block_length, out,
+                                  out_ld, 0, stream);
 }

@@ -466,9 +466,7 @@ def fallback_surrogates_batched(db: D.DeviceBins, npv: torch.Tensor, b_max: int,
     for k0 in range(0, S, chunk):
         kk = min(chunk, S - k0)
         big = D.empty_bins(kk * n, db.T, db.K, dev)
-        for j in range(kk):
-            D.block_shuffle(db, perms[k0 + j], bl,
-                            out=D.DeviceBins(big.data[j * n:(j + 1) * n], n, db.T, db.K))
+        D.block_shuffle_many(db, perms[k0:k0 + kk], bl, big)
         off = torch.arange(kk, device=dev, dtype=torch.int64)
         pairs_big = (sp_d[None, :, :] + (off * n)[:, None, None]).reshape(-1, 2).contiguous()
         items_big = torch.cat([(it_d[:-1][None, :] + (off * P)[:, None]).reshape(-1),

@@ -277,3 +277,17 @@ def block_shuffle(db: DeviceBins, perm: torch.Tensor, block_length: int,
                 perm.data_ptr(), int(perm.shape[1]), int(block_length), out.data.data_ptr(),
                 out.ld, native.stream_ptr())
     return out
+
+
+def block_shuffle_many(db: DeviceBins, perms: torch.Tensor, block_length: int,
+                       out: DeviceBins) -> DeviceBins:
+    """S block shuffles in one launch: perms (S, n, n_blocks) int32; shuffled
+    copy s goes to rows [s*n, (s+1)*n) of out (S*n rows)."""
+    S, n, nb = (int(v) for v in perms.shape)
+    if n != db.n or out.n < S * n or out.ld != db.ld or out.row_len != db.row_len:
+        raise ValueError("block_shuffle_many: out must hold S copies of the bins' layout")
+    perms = perms.to(dtype=torch.int32).contiguous()
+    native.call("tenex_block_shuffle_many", db.data.data_ptr(), db.ld, n, db.T, db.K,
+                perms.data_ptr(), S, nb, int(block_length), out.data.data_ptr(), out.ld,
+                n * out.ld, native.stream_ptr())
+    return out

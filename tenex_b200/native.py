@@ -72,6 +72,7 @@ _SIGS = {
     "tenex_surrogate_accumulate": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _P, _P, _P, _P, _S,
                                    ctypes.POINTER(TeConfig), _P],
     "tenex_block_shuffle": [_P, _L, _I, _L, _I, _P, _I, _I, _P, _L, _P],
+    "tenex_block_shuffle_many": [_P, _L, _I, _L, _I, _P, _I, _I, _I, _P, _L, _L, _P],
     "tenex_stats_accumulate": [_P, _P, _P, _P, _P, _I, _P],
     "tenex_surrogate_accumulate_pairs": [_P, _L, _P, _I, _I, _L, _L, _P, _L, _P, _L, _P, _P, _P,
                                          _P, _P, _S, ctypes.POINTER(TeConfig), _P],

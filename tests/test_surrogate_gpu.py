@@ -199,3 +199,24 @@ def test_full_size_surrogates_sampled_against_oracle(cuda):
     cg = acc.cnt.cpu().numpy()[src, tgt]
     assert np.mean(cg != c) <= 1e-2           # ties within 1e-6 may flip a comparison
     assert np.max(np.abs(cg - c)) <= 2
+
+
+@pytest.mark.parametrize("T,K,bl", [(600, 1, 50), (601, 2, 7), (97, 1, 1), (1000, 3, 333)])
+def test_block_shuffles_bitexact_single_and_batched(cuda, T, K, bl):
+    """tenex_block_shuffle and tenex_block_shuffle_many (several copies in one
+    launch) against the oracle's shuffle: every copy bit-exact, the tail after
+    the last whole block unchanged."""
+    rng = np.random.default_rng(T + K + bl)
+    n, S = 37, 5
+    x = rng.integers(0, 200, (n, T, K)).astype(np.uint8)
+    nb = T // bl
+    perms = np.stack([np.argsort(rng.random((n, nb)), axis=1) for _ in range(S)]).astype(np.int32)
+    db = D.pack_bins(x, cuda)
+    big = D.empty_bins(S * n, T, K, cuda)
+    D.block_shuffle_many(db, torch.as_tensor(perms, device=cuda), bl, big)
+    got = big.unpadded().cpu().numpy()
+    for s in range(S):
+        ref = O.block_shuffle(x, perms[s], bl)
+        assert np.array_equal(got[s * n:(s + 1) * n], ref)
+        one = D.block_shuffle(db, torch.as_tensor(perms[s], device=cuda), bl)
+        assert np.array_equal(one.unpadded().cpu().numpy(), ref)
