@@ -162,3 +162,29 @@ def test_fdr_source_filter_and_no_mediator(cuda):
     p = np.array([[0, 1], [2, 3]])
     g = dpi_trim(4, names[:4], p, np.array([-0.5, -0.25], np.float32), cuda)
     assert np.array_equal(g.pairs, p)
+
+
+def test_fdr_full_size_threshold_and_dpi_forms_agree(cuda, full_size_multibin):
+    """The FDR method's steps on the 10,000-gene TE matrix (99,990,000 pairs):
+    BH-FDR 0.01 on the device keeps the pairs at the top of the TE ranking (p
+    falls as TE rises), and the sparse and dense DPI kernels give the same
+    trimmed network bit for bit (about 2 million kept edges)."""
+    from tenex_b200.inference.fdr import _offdiag, threshold_pairs_device
+    M = full_size_multibin["matrix"]
+    n = M.shape[0]
+    te_t, pairs_t = _offdiag(M)
+    te_d, pairs_d = threshold_pairs_device(te_t, pairs_t, fdr=0.01)
+    kept = te_d.numel()
+    assert 0 < kept < te_t.numel()
+    at_or_above = int((te_t >= te_d.min()).sum())
+    assert kept <= at_or_above <= kept + 2      # ulp-level wiggles of erfc at the cut at most
+    A = torch.zeros((n, n), dtype=torch.float32, device=cuda)
+    A[pairs_d[:, 0], pairs_d[:, 1]] = te_d
+    med = A.sum(dim=1) > 0
+    dense = dpi_trim_matrix(A, med, None, 0.0)
+    r, c = torch.nonzero(dense, as_tuple=True)
+    rs, cs, vs = dpi_trim_sparse(A, med, None, 0.0)
+    assert torch.equal(rs, r) and torch.equal(cs, c)
+    assert torch.equal(vs.view(torch.int32), dense[r, c].view(torch.int32))
+    assert 0 < r.numel() < kept
+    assert torch.all(A[r, c] == dense[r, c])           # trimming only removes edges

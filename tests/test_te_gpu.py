@@ -237,26 +237,19 @@ def test_skewed_bins_dominant_value_derivation(cuda):
     assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
 
 
-def test_full_size_all_pairs_sampled_parity_and_determinism(cuda):
+def test_full_size_all_pairs_sampled_parity_and_determinism(cuda, full_size_multibin):
     """The full 10,000-gene x 20,000-cell workload (95% of genes b ~ U{2..16},
     5% b ~ U{64..256} coarsened to 38 bins; all 99,990,000 ordered pairs in one
     launch, matrix output): 4,000 random pairs plus 300 pairs on each side of
     three coarsened genes against the float64 C oracle within 1e-6, and a second
     launch bitwise equal to the first."""
-    from tenex_b200 import workloads as W
-    from tenex_b200.kernels.adaptive_smem import AdaptiveSMEMKernel
-    x, npv = W.cfg4_bins(10000, 20000, seed=1004)
-    cb, cnpv, bmax = O.coarsen(x, npv, 38)
-    cb = np.ascontiguousarray(cb, dtype=np.uint8)
+    fs = full_size_multibin
+    cb, cnpv, m1 = fs["bins"], fs["npv"], fs["matrix"]
     n = cb.shape[0]
-    db = D.pack_bins(cb, cuda)
-    npv_t = torch.as_tensor(cnpv, dtype=torch.int32, device=cuda)
-    k = AdaptiveSMEMKernel()
-    m1 = k.compute_pairfree_device(db, npv_t, int(bmax), 1, matrix=True)   # [src, tgt]
     rng = np.random.default_rng(44)
     src = rng.integers(0, n, 4000)
     tgt = rng.integers(0, n, 4000)
-    heavy = np.flatnonzero(np.asarray(npv) > 38)[:3]
+    heavy = np.flatnonzero(fs["npv_raw"] > 38)[:3]
     assert len(heavy) == 3
     for h in heavy:
         other = rng.integers(0, n, 300)
@@ -268,7 +261,7 @@ def test_full_size_all_pairs_sampled_parity_and_determinism(cuda):
     got = m1[torch.as_tensor(src, device=cuda), torch.as_tensor(tgt, device=cuda)].double()
     assert np.max(np.abs(got.cpu().numpy() - ref)) <= TOL
     assert np.all(np.diag(m1[:4, :4].cpu().numpy()) == 0)
-    m2 = k.compute_pairfree_device(db, npv_t, int(bmax), 1, matrix=True)
+    m2 = fs["kernel"].compute_pairfree_device(fs["db"], fs["npv_t"], fs["b_max"], 1, matrix=True)
     assert torch.equal(m1.view(torch.int32), m2.view(torch.int32))
 
 
