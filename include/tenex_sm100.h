@@ -58,8 +58,9 @@ typedef struct {
 } tenex_dev_info;
 
 /* Launch shape of the persistent histogram kernels (0 fields, or a NULL config,
- * = defaults: 512 threads, 2 CTAs per SM, 128 sources per item; fewer CTAs per
- * SM when the largest pair's histogram does not fit). */
+ * = defaults: 2 CTAs x 512 threads per SM, 512 sources per item; when the
+ * largest pair's histogram does not fit two CTAs per SM, one CTA per SM, of
+ * 1024 threads if neither threads nor ctas_per_sm was given). */
 typedef struct {
   int threads;      /* threads per CTA: 128, 256, 512 or 1024          */
   int ctas_per_sm;  /* resident CTAs per SM (grid = sm_count * this)    */

@@ -18,10 +18,16 @@ from tenex_b200 import native
 from tenex_b200.kernels import TEKernel
 from tenex_b200.kernels import device as D
 
-# Launch shapes the autotuner tries: (threads, ctas_per_sm, src_chunk)
-TUNE_SPACE = [(512, 2, 128), (1024, 1, 128), (512, 1, 128), (256, 2, 64), (1024, 1, 64),
-              (512, 2, 64), (512, 2, 256), (256, 4, 128), (256, 4, 256), (1024, 1, 256)]
-DEFAULT_CFG = dict(threads=512, ctas_per_sm=2, src_chunk=128)
+# Launch shapes the autotuner tries: (threads, ctas_per_sm, src_chunk); 0 = the
+# library's choice (2 x 512 threads, or 1 x 1024 when the largest histogram needs
+# a whole SM's shared memory)
+TUNE_SPACE = [(0, 0, 512), (1024, 1, 512), (512, 2, 512), (512, 2, 256), (1024, 1, 256),
+              (256, 4, 128), (256, 4, 256), (512, 2, 128), (1024, 1, 128), (256, 2, 64)]
+# Without autotuning the library picks the shape; 512 sources per item. Measured
+# (ms per all-pairs launch): 10,000 x 20,000 (b_max 38) 989 vs 1097 for the old
+# 2 x 512 / 128 default; 5,000 x 10,000 (b_max 32) 256.0 vs 258.8; 2,000 x 5,000
+# (b_max 16) 11.37 vs 11.78 (11.14 for the best tuned shape).
+DEFAULT_CFG = dict(threads=0, ctas_per_sm=0, src_chunk=512)
 _tune_cache: dict[tuple, dict] = {}
 
 
@@ -31,12 +37,14 @@ def _npv_tensor(n_per_var, device) -> torch.Tensor:
 
 
 def autotune(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int = 1,
-             sample_pairs: int = 2_000_000, space=TUNE_SPACE) -> dict:
+             sample_pairs: int = 6_000_000, space=TUNE_SPACE) -> dict:
     """Times each launch shape on a contiguous slice of pair ids (whole targets
     from the middle of the range) and returns the fastest; cached per
     (device, n, T, K, b_max, tau, bin-count histogram). The slice is large
-    enough (2M pairs: ~20 ms per shape at 10k genes x 20k cells) that the end
-    of a launch, where few items remain, does not decide between item sizes."""
+    enough (6M pairs: ~60 ms per shape at 10k genes x 20k cells, ~80 items of
+    512 sources per SM) that the end of a launch, where few items remain, does
+    not decide between item sizes; a 2M-pair slice picked 128 sources per item,
+    3% slower than 512 on the full launch."""
     dev = db.data.device
     npv_h = npv.cpu().numpy()
     key = (torch.cuda.get_device_name(dev), db.n, db.T, db.K, int(b_max), int(tau),
