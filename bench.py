@@ -221,9 +221,15 @@ def run_ours(args) -> None:
         db0, npv0, bmax0 = step()
         kern.cfg = autotune(db0, npv0, bmax0, TAU)
         del db0, npv0
+    bmax_run = None
     for _ in range(args.warmup):
-        step()
+        _, _, bmax_run = step()
+    if bmax_run is None:
+        _, _, bmax_run = step()
     torch.cuda.synchronize(dev)
+    # the shape the library resolves for this launch (0 fields of the requested
+    # config = its defaults)
+    launch_resolved = native.te_launch_shape(C, TAU, int(bmax_run), kern.cfg)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -330,7 +336,7 @@ def run_ours(args) -> None:
                        "genes": G, "cells": C, "tau": TAU,
                        "pairs": total, "step": "remap + coarsen + all-pairs TE matrix",
                        "parallelism": f"pair-range x{world}", "l2": "inputs (200 MB) > L2",
-                       "launch": kern.cfg},
+                       "launch": kern.cfg, "launch_resolved": launch_resolved},
             "gpu_launches": 6 * args.steps,  # remap, coarsen x2, prepass, order, TE tile
             "roofline": roofline, "roofline_hbm": roofline_hbm,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "surrogate": sur,

@@ -76,10 +76,19 @@ int tenex_last_error(char* buf, size_t len);
 int tenex_device_query(int device, tenex_dev_info* info);
 
 /* Bytes of device workspace the TE / surrogate entry points need: a 256-byte
- * header (work ticket, validation words) plus each gene's bin marginal
- * (n_vars * b_max int32), most frequent bin (n_vars int32) and the source
- * processing order (n_vars int32). */
+ * header (work tickets, validation words) plus the source processing order
+ * (n_vars int32, genes sorted by bin count), rounded up to 256 bytes. With
+ * coarsening off, pairs whose histogram fits no shared-memory slot also need
+ * global-memory slots: the call reports the size it needs when these are
+ * missing. */
 size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len, int b_max);
+
+/* The launch shape the histogram kernels would use on the current device for
+ * rows of row_len samples at this lag and b_max, with cfg as given (NULL or 0
+ * fields: the defaults above): threads per CTA, CTAs per SM, dynamic shared
+ * memory per CTA and sources per item. Same planner as the launches. */
+int tenex_te_launch_shape(int64_t row_len, int64_t lag, int b_max, const tenex_te_config* cfg,
+                          int* threads, int* ctas_per_sm, int* smem_bytes, int* src_chunk);
 
 /* Reads back the data-validation word a previous TE call left in the
  * workspace (synchronises `stream`). Returns TENEX_ERR_BADDATA if any bin value

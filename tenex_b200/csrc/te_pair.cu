@@ -701,6 +701,37 @@ static int64_t gmem_bytes(int b_max, int N, int zbytes, const DevAttr& A) {
 
 using namespace tenex;
 
+// Launch shape the histogram kernels would use on the current device for series
+// of row_len samples at this lag and b_max, with cfg as given (NULL or 0 fields:
+// the defaults): threads per CTA, CTAs per SM, dynamic shared memory per CTA and
+// sources per item. Computed by the same planner as the launches.
+extern "C" int tenex_te_launch_shape(int64_t row_len, int64_t lag, int b_max,
+                                     const tenex_te_config* cfg, int* threads, int* ctas_per_sm,
+                                     int* smem_bytes, int* src_chunk) {
+  if (!threads || !ctas_per_sm || !smem_bytes || !src_chunk)
+    return fail(TENEX_ERR_BADARG, "output pointers must be non-NULL");
+  if (lag < 1 || row_len <= lag) return fail(TENEX_ERR_BADARG, "need 1 <= lag < row_len");
+  if (row_len - lag >= ((int64_t)1 << 24))
+    return fail(TENEX_ERR_UNSUPPORTED, "N = %lld samples per pair", (long long)(row_len - lag));
+  if (b_max < 1 || b_max > 255) return fail(TENEX_ERR_BADARG, "b_max must be in 1..255");
+  DevAttr A;
+  int st = current_device_attr(&A);
+  if (st) return st;
+  TeParams P{};
+  P.N = (int)(row_len - lag);
+  P.bmax = b_max;
+  P.zbytes = b_max <= 16 ? 1 : 2;
+  const int64_t hb = P.N < 65536 ? (b_max + 1) / 2 : b_max;
+  const int64_t worst_slot = round_up((int64_t)b_max * b_max * hb, 4) * 4;
+  TeLaunch L{};
+  if ((st = plan_te_launch(P, cfg, A, &L, worst_slot))) return st;
+  *threads = L.threads;
+  *ctas_per_sm = L.grid / A.sm_count;
+  *smem_bytes = L.smem;
+  *src_chunk = (cfg && cfg->src_chunk) ? cfg->src_chunk : 512;
+  return TENEX_OK;
+}
+
 extern "C" size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len, int b_max) {
   if (n_vars < 1 || b_max < 1) return sizeof(WsHeader);
   size_t total = (size_t)ws_total(n_vars, b_max);

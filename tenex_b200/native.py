@@ -60,6 +60,7 @@ _SIGS = {
     "tenex_last_error": [ctypes.c_char_p, _S],
     "tenex_device_query": [_I, ctypes.POINTER(DevInfo)],
     "tenex_te_workspace_bytes": [_I, _L, _I],
+    "tenex_te_launch_shape": [_L, _L, _I, _P, _P, _P, _P, _P],
     "tenex_workspace_status": [_P, _P],
     "tenex_te_pairfree": [_P, _L, _P, _I, _I, _L, _L, _L, _L, _P, _I, _L, _P, _S,
                           ctypes.POINTER(TeConfig), _P],
@@ -212,6 +213,19 @@ def probe_tc_int8(iters: int = 100_000) -> float:
     ms = ctypes.c_float()
     call("tenex_probe_tc_int8", int(iters), ctypes.byref(ops), ctypes.byref(ms), stream_ptr())
     return ops.value / (ms.value * 1e-3)
+
+
+def te_launch_shape(row_len: int, lag: int, b_max: int, cfg: dict | None = None) -> dict:
+    """The launch shape the histogram kernels resolve on the current device for
+    this series length, lag, b_max and requested config (0 / None = defaults)."""
+    c = cfg or {}
+    tc = te_config(c.get("threads", 0), c.get("ctas_per_sm", 0), c.get("src_chunk", 0),
+                   c.get("smem_bytes", 0))
+    out = [ctypes.c_int() for _ in range(4)]
+    call("tenex_te_launch_shape", int(row_len), int(lag), int(b_max), ctypes.byref(tc),
+         *[ctypes.byref(v) for v in out])
+    return dict(threads=out[0].value, ctas_per_sm=out[1].value, smem_bytes=out[2].value,
+                src_chunk=out[3].value)
 
 
 def probe_minmax(iters: int = 20_000) -> float:

@@ -288,3 +288,19 @@ def test_full_size_multibin_b32_sampled_parity(cuda):
     pf = D.te_pairfree(db, npv_t, bmax)                          # target-major pair-free ids
     pid = tgt * (n - 1) + src - (src > tgt)
     assert torch.equal(pf[torch.as_tensor(pid, device=cuda)].cpu(), got.float().cpu())
+
+
+def test_launch_shape_query(cuda):
+    """tenex_te_launch_shape reports the planner's choice: 2 x 512 threads with
+    512 sources per item by default, 1 x 1024 when the largest histogram (38
+    bins at 19,999 samples) needs a whole SM's shared memory, and an explicit
+    config as given."""
+    small = native.te_launch_shape(5000, 1, 16)
+    assert (small["threads"], small["ctas_per_sm"], small["src_chunk"]) == (512, 2, 512)
+    big = native.te_launch_shape(20000, 1, 38)
+    assert (big["threads"], big["ctas_per_sm"]) == (1024, 1)
+    fixed = native.te_launch_shape(20000, 1, 38, dict(threads=512, ctas_per_sm=2, src_chunk=64))
+    assert (fixed["threads"], fixed["ctas_per_sm"], fixed["src_chunk"]) == (512, 1, 64)
+    assert 0 < big["smem_bytes"] <= native.device_info(0).smem_optin
+    with pytest.raises(native.TenexError):
+        native.te_launch_shape(10, 10, 4)
