@@ -271,6 +271,10 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
     }
     const uint32_t bs = (uint32_t)P.npv[src];
     if (P.overflow && slot_fits(bt, bs, N, slot_region) == GMEM) continue;  // other launch's
+    // surrogate statistics: the observed TE is loaded now, so its latency hides
+    // behind the histogram pass instead of stalling the epilogue
+    float obs_m = 0.f;
+    if (P.out_mode == kOutStats && lane_g == 0) obs_m = __ldg(P.obs + (int64_t)src * P.n + tgt);
     const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
     const uint8_t* srow = P.bins + (int64_t)src * P.ld;
     uint64_t slot_addr;
@@ -357,11 +361,13 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
       } else if (P.out_mode == kOutMatrix) {
         P.out[(int64_t)src * P.out_ld + tgt] = te;
       } else {
+        // one addend per cell per launch: reductions without a return value
+        // (no load-to-store stall) give the same float64 sums as += would
         const int64_t m = (int64_t)src * P.n + tgt;
         const double td = (double)te;
-        P.sum[m] += td;
-        P.sumsq[m] += td * td;
-        P.cnt_ge[m] += (te >= P.obs[m]) ? 1 : 0;
+        atomicAdd(P.sum + m, td);
+        atomicAdd(P.sumsq + m, td * td);
+        if (te >= obs_m) atomicAdd(P.cnt_ge + m, 1);
       }
     }
     group_sync(G, g, gthreads);
