@@ -1,5 +1,5 @@
-// probes.cu — microbenchmarks that measure the roofline denominators the TE
-// kernels are judged against (no vendor figure exists for them):
+// probes.cu — microbenchmarks that measure the roofline denominators of the TE
+// kernels' reported fractions (no vendor figure exists for them):
 //   mode 0: conflict-free shared-memory atomicAdd (int32): lane l of every warp
 //           updates a word in bank l; all SMs, 1024 threads per CTA.
 //   mode 1: the same with 16-bit halves (increment 1 or 1<<16), the TE kernel's
