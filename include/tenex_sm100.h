@@ -77,10 +77,11 @@ int tenex_device_query(int device, tenex_dev_info* info);
 
 /* Bytes of device workspace the TE / surrogate entry points need: a 256-byte
  * header (work tickets, validation words) plus the source processing order
- * (n_vars int32, genes sorted by bin count), rounded up to 256 bytes. With
- * coarsening off, pairs whose histogram fits no shared-memory slot also need
- * global-memory slots: the call reports the size it needs when these are
- * missing. */
+ * (n_vars int32, genes sorted by bin count), rounded up to 256 bytes; plus, when
+ * pairs with b up to b_max would not fit a shared-memory slot on the current
+ * device (coarsening off), the global-memory histogram slots of the overflow
+ * launch. A workspace without them makes such a call fail with the size it
+ * needs. */
 size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len, int b_max);
 
 /* The launch shape the histogram kernels would use on the current device for
