@@ -1,12 +1,13 @@
-"""Multi-lag combine of the surrogate test against the reference's own output
-(tests/golden/multilag.npz, made by tenex.pipeline.Pipeline._combine_surrogate_multi_lag)."""
+"""Multi-lag merge of the surrogate test against the reference's own output
+(tests/golden/multilag.npz, made by tenex.pipeline.Pipeline._combine_surrogate_multi_lag),
+and the Pipeline's argument checks."""
 import numpy as np
 import pytest
 import torch
 
 from tenex_b200.inference.grn import make_grn
 from tenex_b200.inference.surrogate_test import SurrogateTestResult
-from tenex_b200.pipeline import Pipeline
+from tenex_b200.pipeline import Pipeline, merge_lag_results
 
 
 def _results(g):
@@ -27,8 +28,7 @@ def _results(g):
 def test_combine_matches_reference(golden, combine):
     g = golden("multilag.npz")
     res, names = _results(g)
-    r = Pipeline._combine_surrogate_multi_lag(res, list(g["taus"]), combine, names,
-                                              torch.device("cpu"))
+    r = merge_lag_results(res, list(g["taus"]), combine, names, torch.device("cpu"))
     for f in ("observed_te", "mean_surrogate_te", "std_surrogate_te", "effective_te",
               "p_values"):
         assert np.array_equal(getattr(r, f), g[f"{combine}_{f}"]), f
@@ -41,14 +41,17 @@ def test_combine_errors(golden):
     for r in res:
         r.p_values = np.ones_like(r.p_values)
     with pytest.raises(ValueError, match="weighted_sum"):
-        Pipeline._combine_surrogate_multi_lag(res, [1, 2, 3], "weighted_sum", names,
-                                              torch.device("cpu"))
+        merge_lag_results(res, [1, 2, 3], "weighted_sum", names, torch.device("cpu"))
+    with pytest.raises(ValueError, match="lag_combine"):
+        merge_lag_results(res, [1, 2, 3], "mean", names, torch.device("cpu"))
     p = Pipeline()
-    with pytest.raises(ValueError, match="non-empty"):
-        p._infer_multi_lag([], "max")
-    with pytest.raises(ValueError, match="combine"):
-        p._infer_multi_lag([1], "mean")
+    with pytest.raises(ValueError, match="at least one lag"):
+        p.infer("surrogate_test", taus=[])
+    with pytest.raises(ValueError, match="lag_combine"):
+        p.infer("surrogate_test", taus=[1], lag_combine="mean")
     with pytest.raises(NotImplementedError):
-        p._infer_multi_lag([1], "max", inference_method="clr")
-    with pytest.raises(ValueError, match="no engine"):
+        p.infer("clr", taus=[1])
+    with pytest.raises(ValueError, match="no data"):
         p.run()
+    with pytest.raises(ValueError, match="variable_names"):
+        p.run(data=np.zeros((3, 10), np.float32))

@@ -101,7 +101,7 @@ def test_pipeline_multi_lag_surrogate(cuda):
     # per-lag run must equal NetWeaver's single-lag run on the same engine output
     from tenex_b200 import TransferEntropyEngine
     from tenex_b200.inference import NetWeaver
-    from tenex_b200.pipeline import Pipeline
+    from tenex_b200.pipeline import Pipeline, merge_lag_results
     x, _ = W.cfg1_expression(n=30, T=400, seed=5, n_planted=3)
     names = np.array([f"g{i}" for i in range(30)])
     kw = dict(n_surrogates=8, block_length=10, fdr=0.05, seed=3)
@@ -112,7 +112,7 @@ def test_pipeline_multi_lag_surrogate(cuda):
         for tau in (1, 2):
             te = TransferEntropyEngine(x, names).compute(tau=tau)
             singles.append(NetWeaver(te, fdr=0.05).infer("surrogate_test", device=cuda, **kw))
-        ref = Pipeline._combine_surrogate_multi_lag(singles, [1, 2], combine, names, cuda)
+        ref = merge_lag_results(singles, [1, 2], combine, names, cuda)
         assert np.array_equal(multi.p_values, ref.p_values)
         assert np.array_equal(multi.effective_te, ref.effective_te)
         assert np.array_equal(multi.grn.pairs, ref.grn.pairs)
