@@ -5,17 +5,22 @@ without any exchange on the data path. The reference splits the pair-id range
 [0, n(n-1)) into contiguous chunks of ceil(n(n-1) / n_gpus)
 (tenex/transferentropy.py:376-379, 424-428) and runs one thread per GPU; here
 each rank is its own process (torchrun, NCCL over NVLink), computes its chunk
-with the single-GPU kernels, and the chunks are combined by one collective:
+with the single-GPU kernels, and the chunks are assembled by one collective:
 
   * bins + n_per_var: broadcast once from rank 0 (broadcast_bins);
-  * TE matrix: each rank fills its pairs of a zeroed (n, n) float32 matrix and
-    an all-reduce SUM assembles it (the supports are disjoint, and x + 0 is
-    exact, so the result is bit-identical to one GPU computing every pair);
-  * surrogate statistics: the same all-reduce over the float64 sum / sum of
-    squares and the int32 count_ge of each rank's pairs.
+  * results: each rank's chunk is a contiguous run of pair-free ids (target-
+    major), so its values form one contiguous vector; an all-gather of the
+    equal-sized (padded) chunks gives every rank the whole pair-free vector,
+    which becomes the (n, n) [src, tgt] matrix with one on-device transpose.
+    Each rank receives (world - 1) / world of the n(n-1) values: ~400 MB for
+    the float32 TE of 10,000 genes (an all-reduce of zero-filled n x n
+    matrices would move twice that). Values are copied, not summed, so the
+    result is bit-identical to one GPU computing every pair;
+  * surrogate statistics: the same all-gather of each rank's chunk of the
+    float64 sum / sum of squares and the int32 count_ge.
 
 No kernel here waits on another rank's memory; the only cross-GPU traffic is
-the NCCL broadcast and all-reduce.
+the NCCL broadcast and all-gather.
 """
 from __future__ import annotations
 
@@ -71,30 +76,79 @@ def broadcast_bins(bins: torch.Tensor | None, n_per_var: torch.Tensor | None, de
     return b, npv
 
 
-def combine_disjoint(*tensors: torch.Tensor, group=None) -> None:
-    """In-place all-reduce SUM of per-rank results whose non-zero entries are
-    disjoint across ranks (exact for float and integer types)."""
-    world, _ = world_and_rank(group)
+def pairfree_ids_to_cells(n: int, p0: int, p1: int, device) -> tuple[torch.Tensor, torch.Tensor]:
+    """(src, tgt) of pair-free ids [p0, p1): p = tgt * (n - 1) + src_local,
+    src = src_local + (src_local >= tgt)."""
+    p = torch.arange(p0, p1, dtype=torch.int64, device=device)
+    tgt = torch.div(p, n - 1, rounding_mode="floor")
+    sl = p - tgt * (n - 1)
+    return sl + (sl >= tgt).to(torch.int64), tgt
+
+
+def pairfree_to_matrix(pf: torch.Tensor, n: int) -> torch.Tensor:
+    """(n, n) [src, tgt] matrix (zero diagonal) from the full pair-free vector
+    (n(n-1) values in target-major order), on pf's device. Target-major, the
+    off-diagonal cells of row t are its sources in increasing order, and the
+    n(n-1) off-diagonal cells of a row-major (n, n) matrix are exactly the cells
+    after flat position 0 cut into n - 1 rows of n + 1 (the diagonal is the last
+    of each), so the vector drops into place with one strided copy; the matrix
+    is its transpose."""
+    mt = torch.zeros((n, n), dtype=pf.dtype, device=pf.device)
+    if n > 1:
+        mt.view(-1)[1:].view(n - 1, n + 1)[:, :n].copy_(pf[:n * (n - 1)].view(n - 1, n))
+    return mt.t().contiguous()
+
+
+def gather_pairfree(local: torch.Tensor, n_pairs: int, group=None) -> torch.Tensor:
+    """Every rank's contiguous chunk (pair_range) of a per-pair vector, all-gathered
+    into the full (n_pairs,) vector on every rank. `local` holds this rank's
+    p1 - p0 values."""
+    world, rank = world_and_rank(group)
+    p0, p1 = pair_range(n_pairs, rank, world)
+    if local.numel() != p1 - p0:
+        raise ValueError(f"rank {rank} holds {local.numel()} values for pair ids [{p0}, {p1})")
+    if world == 1:
+        return local
+    chunk = pair_range(n_pairs, 0, world)[1]
+    send = torch.zeros(chunk, dtype=local.dtype, device=local.device)
+    send[:p1 - p0] = local
+    full = torch.empty(chunk * world, dtype=local.dtype, device=local.device)
+    dist.all_gather_into_tensor(full, send, group=group)
+    return full[:n_pairs]
+
+
+def assemble_matrices(*mats: torch.Tensor, group=None) -> None:
+    """In place: (n, n) [src, tgt] matrices of which each rank filled only the
+    cells of its own pair chunk become the full matrices on every rank (one
+    all-gather of each rank's chunk per matrix; diagonals are left as they are)."""
+    world, rank = world_and_rank(group)
     if world == 1:
         return
-    for t in tensors:
-        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    for m in mats:
+        n = int(m.shape[0])
+        total = n * (n - 1)
+        src, tgt = pairfree_ids_to_cells(n, *pair_range(total, rank, world), m.device)
+        full = gather_pairfree(m[src, tgt].contiguous(), total, group)
+        diag = torch.diagonal(m).clone()
+        m.copy_(pairfree_to_matrix(full, n))
+        torch.diagonal(m).copy_(diag)
 
 
 def te_matrix_sharded(kernel, db, n_per_var: torch.Tensor, b_max: int, tau: int,
                       group=None) -> torch.Tensor:
     """(n, n) float32 TE matrix [src, tgt] on every rank: this rank's pair chunk
-    from `kernel.compute_pairfree_device`, then combine_disjoint."""
+    as a pair-free vector from `kernel.compute_pairfree_device`, then one
+    all-gather and the on-device transpose."""
     world, rank = world_and_rank(group)
     n = int(db.n)
-    p0, p1 = pair_range(n * (n - 1), rank, world)
+    total = n * (n - 1)
+    p0, p1 = pair_range(total, rank, world)
     dev = db.data.device
-    out = torch.zeros((n, n), dtype=torch.float32, device=dev)
+    local = torch.empty(p1 - p0, dtype=torch.float32, device=dev)
     if p1 > p0:
-        kernel.compute_pairfree_device(db, n_per_var, b_max, tau, p0, p1 - p0, matrix=True,
-                                       out=out)
-    combine_disjoint(out, group=group)
-    return out
+        kernel.compute_pairfree_device(db, n_per_var, b_max, tau, p0, p1 - p0, matrix=False,
+                                       out=local)
+    return pairfree_to_matrix(gather_pairfree(local, total, group), n)
 
 
 def surrogate_sharded(db, n_per_var: torch.Tensor, b_max: int, tau: int, observed: torch.Tensor,
@@ -109,7 +163,7 @@ def surrogate_sharded(db, n_per_var: torch.Tensor, b_max: int, tau: int, observe
     acc = SurrogateAccumulator(db, n_per_var, b_max, tau, observed, False, cfg, p0, p1 - p0)
     if p1 > p0:
         run_surrogates(acc, perms, block_length, use_graph)
-    combine_disjoint(acc.sum, acc.sumsq, acc.cnt, group=group)
+    assemble_matrices(acc.sum, acc.sumsq, acc.cnt, group=group)
     return acc.sum, acc.sumsq, acc.cnt
 
 

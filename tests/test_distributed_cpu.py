@@ -3,7 +3,7 @@
 The per-rank TE of a pair chunk comes from an oracle-backed stand-in kernel
 defined here (the GPU kernel cannot run without a GPU); what is under test is
 the split of the pair-id range, the bins broadcast and the exact assembly of
-disjoint per-rank results."""
+the per-rank chunks by all-gather (bit-identical to one rank computing all)."""
 import os
 import socket
 
@@ -37,7 +37,8 @@ class _OracleKernel:
 
     def compute_pairfree_device(self, db, npv, b_max, tau, pair_offset, n_pairs, matrix, out):
         vals = O.te_pairfree(db.bins, npv.numpy(), tau, pair_offset, n_pairs).astype(np.float32)
-        out += torch.from_numpy(TD.pairfree_chunk_to_matrix(vals, db.n, pair_offset))
+        assert not matrix and out.numel() == n_pairs
+        out.copy_(torch.from_numpy(vals))
         self.calls.append((pair_offset, n_pairs))
         return out
 
@@ -84,7 +85,7 @@ def _worker(rank, world, port, out_dir):
             if r == rank:
                 s += torch.from_numpy(mm)
                 c += torch.from_numpy((mm > 5e-4).astype(np.int32))
-        TD.combine_disjoint(s, c)
+        TD.assemble_matrices(s, c)
         assert np.array_equal(s.numpy(), full_s) and np.array_equal(c.numpy(), full_c)
         with open(os.path.join(out_dir, f"ok{rank}"), "w") as f:
             f.write("ok")
@@ -119,3 +120,12 @@ def test_chunk_to_matrix_layout():
     vals = np.arange(n * (n - 1), dtype=np.float32) + 1
     m = TD.pairfree_chunk_to_matrix(vals, n, 0)
     assert np.array_equal(m, O.pairfree_to_matrix(vals, n).astype(np.float32))
+
+
+@pytest.mark.parametrize("n", [2, 3, 7, 40])
+def test_pairfree_to_matrix_on_device_layout(n):
+    vals = torch.arange(n * (n - 1), dtype=torch.float32) + 1
+    m = TD.pairfree_to_matrix(vals, n)
+    assert np.array_equal(m.numpy(), O.pairfree_to_matrix(vals.numpy(), n).astype(np.float32))
+    src, tgt = TD.pairfree_ids_to_cells(n, 0, n * (n - 1), "cpu")
+    assert torch.equal(m[src, tgt], vals)
