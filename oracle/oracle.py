@@ -81,7 +81,8 @@ def _flat_bins(bins) -> tuple[np.ndarray, int, int]:
     if b.ndim == 2:
         b = b[:, :, None]
     n, T, K = b.shape
-    return np.ascontiguousarray(b.reshape(n, T * K).astype(np.int32)), T * K, K
+    # int32 C-contiguous input is used as it is (no per-call copy of large bins)
+    return np.ascontiguousarray(b.reshape(n, T * K), dtype=np.int32), T * K, K
 
 
 # ---------------------------------------------------------------- preprocess
