@@ -14,6 +14,9 @@
 //   tenex_coarsen      new = old * limit / n_per_var for genes above the limit
 //                      (tenex/preprocess.py:462-551; coarsen_bins_cuda of
 //                      tenex/csrc/adaptive_smem.cu:557-592).
+//   tenex_coarsen_narrow  the same rule from uint16 bins (genes with more than
+//                      256 distinct values, int16 in the reference,
+//                      tenex/preprocess.py:335-354,520-536) into uint8 rows.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -71,8 +74,10 @@ __device__ float leaf_sumsq(const float* a, int n, float mean) {
   return res;
 }
 
-// Enumerates the leaves of pairwise_sum(0, n) left to right (serial, lane 0).
-__device__ int enum_leaves(int n, int* starts, int* lens) {
+// Enumerates, left to right, the nodes of the pairwise_sum(0, n) tree that hold
+// at most `cap` samples and have no such ancestor (cap = 128: the leaves).
+// Serial, one thread.
+__device__ int enum_nodes(int n, int cap, int* starts, int* lens) {
   int so[64], sl[64];
   int sp = 0, nl = 0;
   so[sp] = 0;
@@ -81,7 +86,7 @@ __device__ int enum_leaves(int n, int* starts, int* lens) {
   while (sp > 0) {
     --sp;
     const int o = so[sp], l = sl[sp];
-    if (l <= 128) {
+    if (l <= cap) {
       starts[nl] = o;
       lens[nl] = l;
       ++nl;
@@ -99,8 +104,9 @@ __device__ int enum_leaves(int n, int* starts, int* lens) {
   return nl;
 }
 
-// Combines leaf sums in the order pairwise_sum(a, n2) + pairwise_sum(a+n2, n-n2).
-__device__ float combine_leaves(int n, const float* leaf) {
+// Combines the sums of those nodes in the order of
+// pairwise_sum(a, n2) + pairwise_sum(a + n2, n - n2).
+__device__ float combine_nodes(int n, int cap, const float* node) {
   // explicit post-order walk: frames (len, state); values on a separate stack
   int fl[64], fs[64];
   float val[64];
@@ -110,8 +116,8 @@ __device__ float combine_leaves(int n, const float* leaf) {
   sp = 1;
   while (sp > 0) {
     const int l = fl[sp - 1];
-    if (l <= 128) {
-      val[vp++] = leaf[k++];
+    if (l <= cap) {
+      val[vp++] = node[k++];
       --sp;
       continue;
     }
@@ -137,20 +143,60 @@ __device__ float combine_leaves(int n, const float* leaf) {
   return val[0];
 }
 
+// Rows longer than kSuperLen are summed as a tree of "super nodes" of at most
+// kSuperLen samples (every subtree's sum is independent of where it sits), each
+// super node leaf by leaf in shared memory.
+constexpr int kSuperLen = kMaxLeaves * 56;  // leaves of a super node: >= 57 samples each
+constexpr int kMaxSuper = 1024;             // super nodes hold >= kSuperLen/2 - 8 samples
+constexpr int64_t kMaxPairwiseLen = (int64_t)(kMaxSuper - 1) * (kSuperLen / 2 - 8);
+
+struct PairwiseScratch {
+  int lstart[kMaxLeaves];
+  int llen[kMaxLeaves];
+  float lsum[kMaxLeaves];
+  int sstart[kMaxSuper];
+  int slen[kMaxSuper];
+  float ssum[kMaxSuper];
+  int nl, ns;
+  float result;
+};
+
+// numpy's float32 pairwise sum of row[0, T) (SQ: of the squared deviations
+// (row[i] - mean)^2 that np.var sums), bit for bit; all CTA threads call it,
+// the result is returned to all of them.
+template <bool SQ>
+__device__ float row_pairwise_sum(const float* row, int T, float mean, PairwiseScratch& S) {
+  const int tid = threadIdx.x;
+  if (tid == 0) S.ns = enum_nodes(T, kSuperLen, S.sstart, S.slen);
+  __syncthreads();
+  const int ns = S.ns;
+  for (int k = 0; k < ns; ++k) {
+    const int o = S.sstart[k], l = S.slen[k];
+    if (tid == 0) S.nl = enum_nodes(l, 128, S.lstart, S.llen);
+    __syncthreads();
+    const int nl = S.nl;
+    for (int j = tid; j < nl; j += blockDim.x)
+      S.lsum[j] = SQ ? leaf_sumsq(row + o + S.lstart[j], S.llen[j], mean)
+                     : leaf_sum(row + o + S.lstart[j], S.llen[j]);
+    __syncthreads();
+    if (tid == 0) S.ssum[k] = combine_nodes(l, 128, S.lsum);
+    __syncthreads();
+  }
+  if (tid == 0) S.result = combine_nodes(T, kSuperLen, S.ssum);
+  __syncthreads();
+  return S.result;
+}
+
 // One CTA (128 threads) per gene.
 __global__ void fsbwl_kernel(const float* __restrict__ x, int64_t ldx, int T, float kp,
                              int32_t* __restrict__ bins, int64_t ldb,
                              int32_t* __restrict__ n_bins) {
-  __shared__ int lstart[kMaxLeaves];
-  __shared__ int llen[kMaxLeaves];
-  __shared__ float lsum[kMaxLeaves];
-  __shared__ float sh_mean, sh_sd, sh_mn, sh_mx;
-  __shared__ int sh_nl;
+  __shared__ PairwiseScratch S;
+  __shared__ float sh_sd, sh_mn, sh_mx;
   __shared__ float wmin[32], wmax[32];
   const int g = blockIdx.x;
   const float* row = x + (int64_t)g * ldx;
   const int tid = threadIdx.x;
-  if (tid == 0) sh_nl = enum_leaves(T, lstart, llen);
   // min / max
   float mn = 3.402823466e38f, mx = -3.402823466e38f;
   for (int t = tid; t < T; t += blockDim.x) {
@@ -167,10 +213,7 @@ __global__ void fsbwl_kernel(const float* __restrict__ x, int64_t ldx, int T, fl
     wmin[tid >> 5] = mn;
     wmax[tid >> 5] = mx;
   }
-  __syncthreads();
-  const int nl = sh_nl;
-  for (int k = tid; k < nl; k += blockDim.x) lsum[k] = leaf_sum(row + lstart[k], llen[k]);
-  __syncthreads();
+  const float s = row_pairwise_sum<false>(row, T, 0.f, S);
   if (tid == 0) {
     float a = wmin[0], b = wmax[0];
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
@@ -179,15 +222,10 @@ __global__ void fsbwl_kernel(const float* __restrict__ x, int64_t ldx, int T, fl
     }
     sh_mn = a;
     sh_mx = b;
-    const float s = combine_leaves(T, lsum);
-    sh_mean = __double2float_rn(__ddiv_rn((double)s, (double)T));
   }
-  __syncthreads();
-  const float mean = sh_mean;
-  for (int k = tid; k < nl; k += blockDim.x) lsum[k] = leaf_sumsq(row + lstart[k], llen[k], mean);
-  __syncthreads();
+  const float mean = __double2float_rn(__ddiv_rn((double)s, (double)T));
+  const float ss = row_pairwise_sum<true>(row, T, mean, S);
   if (tid == 0) {
-    const float ss = combine_leaves(T, lsum);
     const double cnt = T - 1 > 0 ? (double)(T - 1) : 0.0;
     const float var = __double2float_rn(__ddiv_rn((double)ss, cnt));
     float sd = __fsqrt_rn(var);
@@ -284,6 +322,23 @@ __global__ void coarsen_kernel(uint8_t* __restrict__ bins, int64_t ld, int64_t r
     row[i] = (uint8_t)(((int)row[i] * limit) / b);
 }
 
+// Coarsening of uint16 rows into uint8 rows (bins of genes with more than 256
+// distinct values): new = old * limit / b above the limit, else a plain copy;
+// grid (chunks, genes). Every output value is below min(b, limit) <= 255.
+__global__ void coarsen_narrow_kernel(const uint16_t* __restrict__ in, int64_t ldi,
+                                      int64_t row_len, const int32_t* __restrict__ npv,
+                                      int limit, uint8_t* __restrict__ out, int64_t ldo) {
+  const int g = blockIdx.y;
+  const int b = npv[g];
+  const uint16_t* row = in + (int64_t)g * ldi;
+  uint8_t* orow = out + (int64_t)g * ldo;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < row_len;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int v = row[i];
+    orow[i] = (uint8_t)(b > limit ? (v * limit) / b : v);
+  }
+}
+
 // Binarisation 1[x > thr_g] into uint8 padded rows, one CTA per gene.
 // mode 0: thr = 0 (nonzero); 1: thr = float32 mean with numpy's pairwise sum and
 // float64 division (np.mean on float32 rows); 2: thr = thr_in[g].
@@ -291,22 +346,14 @@ __global__ void coarsen_kernel(uint8_t* __restrict__ bins, int64_t ld, int64_t r
 __global__ void binarize_kernel(const float* __restrict__ x, int64_t ldx, int T, int mode,
                                 const float* __restrict__ thr_in, uint8_t* __restrict__ out,
                                 int64_t ldo, int32_t* __restrict__ npv) {
-  __shared__ int lstart[kMaxLeaves];
-  __shared__ int llen[kMaxLeaves];
-  __shared__ float lsum[kMaxLeaves];
+  __shared__ PairwiseScratch S;
   __shared__ float sh_thr;
-  __shared__ int sh_nl;
   const int g = blockIdx.x;
   const float* row = x + (int64_t)g * ldx;
   const int tid = threadIdx.x;
   if (mode == 1) {
-    if (tid == 0) sh_nl = enum_leaves(T, lstart, llen);
-    __syncthreads();
-    const int nl = sh_nl;
-    for (int k = tid; k < nl; k += blockDim.x) lsum[k] = leaf_sum(row + lstart[k], llen[k]);
-    __syncthreads();
-    if (tid == 0)
-      sh_thr = __double2float_rn(__ddiv_rn((double)combine_leaves(T, lsum), (double)T));
+    const float s = row_pairwise_sum<false>(row, T, 0.f, S);
+    if (tid == 0) sh_thr = __double2float_rn(__ddiv_rn((double)s, (double)T));
   } else if (tid == 0) {
     sh_thr = mode == 0 ? 0.f : thr_in[g];
   }
@@ -340,10 +387,9 @@ extern "C" int tenex_fsbwl_bins(const float* x, int64_t ldx, int n_vars, int T, 
   if (!x || !bins || !n_bins) return fail(TENEX_ERR_BADARG, "x, bins, n_bins must be non-NULL");
   if (n_vars < 1 || T < 1) return fail(TENEX_ERR_BADARG, "empty expression matrix");
   if (ldx < T || ldb < T) return fail(TENEX_ERR_BADARG, "row strides must be >= T");
-  // leaves of the pairwise tree hold >= 57 samples once n > 128
-  if ((int64_t)T > (int64_t)kMaxLeaves * 56)
-    return fail(TENEX_ERR_UNSUPPORTED, "T=%d exceeds the discretiser's %d-sample limit", T,
-                kMaxLeaves * 56);
+  if ((int64_t)T > kMaxPairwiseLen)
+    return fail(TENEX_ERR_UNSUPPORTED, "T=%d exceeds the discretiser's %lld-sample limit", T,
+                (long long)kMaxPairwiseLen);
   fsbwl_kernel<<<n_vars, 128, 0, as_stream(stream)>>>(x, ldx, T, kp, bins, ldb, n_bins);
   return check_launch("fsbwl_kernel");
 }
@@ -403,6 +449,26 @@ extern "C" int tenex_coarsen(uint8_t* bins, int64_t ld, int n_vars, int64_t row_
   return check_launch("coarsen_npv_kernel");
 }
 
+extern "C" int tenex_coarsen_narrow(const uint16_t* in, int64_t ldi, int n_vars, int64_t row_len,
+                                    int32_t* n_per_var, int limit, uint8_t* out, int64_t ldo,
+                                    void* stream) {
+  if (!in || !out || !n_per_var)
+    return fail(TENEX_ERR_BADARG, "in, out and n_per_var must be non-NULL");
+  if (limit < 1 || limit > 255) return fail(TENEX_ERR_BADARG, "limit must be in [1, 255]");
+  if (n_vars < 1 || row_len < 1) return fail(TENEX_ERR_BADARG, "empty bins");
+  if (ldi < row_len || ldo < row_len) return fail(TENEX_ERR_BADARG, "row strides < row_len");
+  if (n_vars > 65535) return fail(TENEX_ERR_UNSUPPORTED, "n_vars > 65535");
+  cudaStream_t s = as_stream(stream);
+  const int64_t chunks64 = (row_len + 4095) / 4096;
+  const unsigned chunks = (unsigned)(chunks64 < 1024 ? chunks64 : 1024);
+  coarsen_narrow_kernel<<<dim3(chunks, n_vars), 256, 0, s>>>(in, ldi, row_len, n_per_var, limit,
+                                                             out, ldo);
+  int st = check_launch("coarsen_narrow_kernel");
+  if (st) return st;
+  coarsen_npv_kernel<<<(n_vars + 255) / 256, 256, 0, s>>>(n_per_var, n_vars, limit);
+  return check_launch("coarsen_npv_kernel");
+}
+
 extern "C" int tenex_binarize(const float* x, int64_t ldx, int n_vars, int T, int mode,
                               const float* thresholds, uint8_t* out, int64_t ldo,
                               int32_t* n_per_var, void* stream) {
@@ -411,7 +477,7 @@ extern "C" int tenex_binarize(const float* x, int64_t ldx, int n_vars, int T, in
   if (ldx < T || ldo < T) return fail(TENEX_ERR_BADARG, "row strides must be >= T");
   if (mode < 0 || mode > 2) return fail(TENEX_ERR_BADARG, "mode must be 0, 1 or 2");
   if (mode == 2 && !thresholds) return fail(TENEX_ERR_BADARG, "mode 2 needs thresholds");
-  if (mode == 1 && (int64_t)T > (int64_t)kMaxLeaves * 56)
+  if (mode == 1 && (int64_t)T > kMaxPairwiseLen)
     return fail(TENEX_ERR_UNSUPPORTED, "T=%d too long for the mean binariser", T);
   binarize_kernel<<<n_vars, 128, 0, as_stream(stream)>>>(x, ldx, T, mode, thresholds, out, ldo,
                                                          n_per_var);

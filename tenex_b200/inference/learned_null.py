@@ -108,7 +108,7 @@ class NullModel:
 def gene_features(db: D.DeviceBins, npv: torch.Tensor, tau: int) -> torch.Tensor:
     """(n, 8) float32 per-gene features on the device."""
     feat = torch.empty((db.n, GENE_FEAT), dtype=torch.float32, device=db.data.device)
-    native.call("tenex_gene_features", db.data.data_ptr(), db.ld, npv.data_ptr(), db.n,
+    native.call("tenex_gene_features", db.ptr(), db.ld, npv.data_ptr(), db.n,
                 db.row_len, tau * db.K, feat.data_ptr(), native.stream_ptr())
     return feat
 
@@ -119,7 +119,7 @@ def eiid_matrix(db: D.DeviceBins, npv: torch.Tensor, tau: int) -> torch.Tensor:
     out = torch.empty((db.n, db.n), dtype=torch.float32, device=dev)
     ws = torch.empty(int(native.lib().tenex_eiid_workspace_bytes(db.n)), dtype=torch.uint8,
                      device=dev)
-    native.call("tenex_eiid_matrix", db.data.data_ptr(), db.ld, npv.data_ptr(), db.n,
+    native.call("tenex_eiid_matrix", db.ptr(), db.ld, npv.data_ptr(), db.n,
                 db.row_len, tau * db.K, out.data_ptr(), ws.data_ptr(), ws.numel(),
                 native.stream_ptr())
     return out
@@ -410,7 +410,7 @@ def fallback_surrogates(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: in
 
     def one(k):
         D.block_shuffle(db, perms[k], bl, out=shuf)
-        native.call("tenex_surrogate_accumulate_pairs", shuf.data.data_ptr(), shuf.ld,
+        native.call("tenex_surrogate_accumulate_pairs", shuf.ptr(), shuf.ld,
                     npv.data_ptr(), int(b_max), n, shuf.row_len, tau * db.K, pairs_d.data_ptr(),
                     sp.shape[0], items_d.data_ptr(), items.shape[0] - 1, obs.data_ptr(),
                     ssum.data_ptr(), ssq.data_ptr(), cnt.data_ptr(), ws.data_ptr(), ws.numel(),
@@ -474,7 +474,7 @@ def fallback_surrogates_batched(db: D.DeviceBins, npv: torch.Tensor, b_max: int,
         npv_big = npv.to(torch.int32).repeat(kk).contiguous()
         ws = D.workspace(dev, kk * n, db.row_len, b_max)
         te = torch.empty(kk * P, dtype=torch.float32, device=dev)
-        native.call("tenex_te_pairs", big.data.data_ptr(), big.ld, npv_big.data_ptr(), int(b_max),
+        native.call("tenex_te_pairs", big.ptr(), big.ld, npv_big.data_ptr(), int(b_max),
                     kk * n, big.row_len, lag, pairs_big.data_ptr(), kk * P, items_big.data_ptr(),
                     items_big.numel() - 1, te.data_ptr(), ws.data_ptr(), ws.numel(), D._cfg(cfg),
                     native.stream_ptr())

@@ -94,7 +94,7 @@ class SurrogateAccumulator:
         s = native.stream_ptr()
         if self.binary:
             n = self.db.n
-            native.call("tenex_te_binary_matrix", self.shuf.data.data_ptr(), self.shuf.ld, n,
+            native.call("tenex_te_binary_matrix", self.shuf.ptr(), self.shuf.ld, n,
                         self.shuf.row_len, self.tau * self.db.K, self.tmp.data_ptr(), n,
                         self.b2ws.data_ptr(), self.b2ws.numel(), s)
             native.call("tenex_stats_accumulate", self.tmp.data_ptr(), self.obs.data_ptr(),

@@ -22,7 +22,7 @@ ROW_ALIGN = 64
 
 @dataclass
 class DeviceBins:
-    data: torch.Tensor   # (n, ld) uint8, CUDA
+    data: torch.Tensor   # (n, ld) uint8, CUDA (uint16 "wide" bins: genes with > 256 bins)
     n: int
     T: int
     K: int
@@ -33,7 +33,22 @@ class DeviceBins:
 
     @property
     def ld(self) -> int:
+        """Row stride in elements (bytes for the uint8 layout)."""
         return int(self.data.shape[1])
+
+    @property
+    def wide(self) -> bool:
+        """uint16 bins: some gene has more than 256 distinct values. Only the
+        coarsening step reads them; it writes the uint8 layout the TE kernels use."""
+        return self.data.dtype != torch.uint8
+
+    def ptr(self) -> int:
+        """Device address of the uint8 rows the TE kernels read."""
+        if self.wide:
+            raise ValueError("these bins hold genes with more than 256 distinct values (uint16); "
+                             "the TE kernels read uint8 bins: coarsen them first "
+                             "(AdaptiveSMEMKernel.prepare / preprocess.coarsen_bins)")
+        return self.data.data_ptr()
 
     def unpadded(self) -> torch.Tensor:
         """(n, T, K) view-free copy of the bins (uint8)."""
@@ -164,15 +179,18 @@ def padded_ld(row_len: int) -> int:
     return (row_len + ROW_ALIGN - 1) // ROW_ALIGN * ROW_ALIGN
 
 
-def empty_bins(n: int, T: int, K: int, device) -> DeviceBins:
-    data = torch.zeros((n, padded_ld(T * K)), dtype=torch.uint8, device=device)
+def empty_bins(n: int, T: int, K: int, device, wide: bool = False) -> DeviceBins:
+    data = torch.zeros((n, padded_ld(T * K)), dtype=torch.uint16 if wide else torch.uint8,
+                       device=device)
     return DeviceBins(data, n, T, K)
 
 
 def pack_bins(bin_arrs, device, b_max: int | None = None) -> DeviceBins:
     """Copies (n, T) / (n, T, K) integer bins into the padded uint8 layout.
 
-    Bin values must fit uint8 (the shared-memory kernels handle b <= 255).
+    Bin values must fit uint8 (the shared-memory kernels handle b <= 255): larger
+    values raise ValueError (dense-remap such bins with preprocess.remap_bins,
+    which keeps them as uint16 until coarsened).
     """
     if isinstance(bin_arrs, DeviceBins):
         return bin_arrs
@@ -189,7 +207,11 @@ def pack_bins(bin_arrs, device, b_max: int | None = None) -> DeviceBins:
     src = t.reshape(n, T * K)
     src = to_device(src, device) if src.device.type == "cpu" else src.to(device=device)
     if src.dtype != torch.uint8:
-        src = src.to(torch.int32).clamp_(0, 255).to(torch.uint8)
+        src = src.to(torch.int32)
+        if src.numel() and int(src.max()) > 255:
+            raise ValueError("bin values above 255 do not fit the uint8 bin layout; remap them "
+                             "with tenex_b200.preprocess.remap_bins and coarsen them first")
+        src = src.clamp_(0, 255).to(torch.uint8)
     db.data[:, :T * K].copy_(src)
     return db
 
@@ -236,12 +258,12 @@ def te_pairfree(db: DeviceBins, n_per_var: torch.Tensor, b_max: int, tau: int = 
     s = native.stream_ptr()
     lag = tau * db.K
     if counts is not None:
-        native.call("tenex_te_pairfree_counts", db.data.data_ptr(), db.ld, npv.data_ptr(),
+        native.call("tenex_te_pairfree_counts", db.ptr(), db.ld, npv.data_ptr(),
                     int(b_max), n, db.row_len, lag, int(pair_offset), int(n_pairs),
                     out.data_ptr(), counts.data_ptr(), int(counts_stride), ws.data_ptr(),
                     ws.numel(), _cfg(cfg), s)
     else:
-        native.call("tenex_te_pairfree", db.data.data_ptr(), db.ld, npv.data_ptr(), int(b_max),
+        native.call("tenex_te_pairfree", db.ptr(), db.ld, npv.data_ptr(), int(b_max),
                     n, db.row_len, lag, int(pair_offset), int(n_pairs), out.data_ptr(),
                     native.OUT_MATRIX if matrix else native.OUT_PAIRFREE,
                     n if matrix else 0, ws.data_ptr(), ws.numel(), _cfg(cfg), s)
@@ -261,7 +283,7 @@ def surrogate_accumulate(db: DeviceBins, n_per_var: torch.Tensor, b_max: int, ta
         n_pairs = n * (n - 1) - pair_offset
     if ws is None:
         ws = workspace(db.data.device, n, db.row_len, b_max)
-    native.call("tenex_surrogate_accumulate", db.data.data_ptr(), db.ld,
+    native.call("tenex_surrogate_accumulate", db.ptr(), db.ld,
                 n_per_var.data_ptr(), int(b_max), n, db.row_len, tau * db.K, int(pair_offset),
                 int(n_pairs), observed.data_ptr(), ssum.data_ptr(), ssq.data_ptr(),
                 cnt.data_ptr(), ws.data_ptr(), ws.numel(), _cfg(cfg), native.stream_ptr())
@@ -273,7 +295,7 @@ def block_shuffle(db: DeviceBins, perm: torch.Tensor, block_length: int,
     if out is None:
         out = empty_bins(db.n, db.T, db.K, db.data.device)
     perm = perm.to(dtype=torch.int32).contiguous()
-    native.call("tenex_block_shuffle", db.data.data_ptr(), db.ld, db.n, db.T, db.K,
+    native.call("tenex_block_shuffle", db.ptr(), db.ld, db.n, db.T, db.K,
                 perm.data_ptr(), int(perm.shape[1]), int(block_length), out.data.data_ptr(),
                 out.ld, native.stream_ptr())
     return out
@@ -287,7 +309,7 @@ def block_shuffle_many(db: DeviceBins, perms: torch.Tensor, block_length: int,
     if n != db.n or out.n < S * n or out.ld != db.ld or out.row_len != db.row_len:
         raise ValueError("block_shuffle_many: out must hold S copies of the bins' layout")
     perms = perms.to(dtype=torch.int32).contiguous()
-    native.call("tenex_block_shuffle_many", db.data.data_ptr(), db.ld, n, db.T, db.K,
+    native.call("tenex_block_shuffle_many", db.ptr(), db.ld, n, db.T, db.K,
                 perms.data_ptr(), S, nb, int(block_length), out.data.data_ptr(), out.ld,
                 n * out.ld, native.stream_ptr())
     return out

@@ -27,7 +27,7 @@ def te_binary_matrix(db: D.DeviceBins, tau: int = 1, out: torch.Tensor | None = 
     nb = int(native.lib().tenex_b2_workspace_bytes(n, db.row_len, lag))
     ws = torch.empty(nb, dtype=torch.uint8, device=dev)
     s = native.stream_ptr()
-    native.call("tenex_te_binary_matrix", db.data.data_ptr(), db.ld, n, db.row_len, lag,
+    native.call("tenex_te_binary_matrix", db.ptr(), db.ld, n, db.row_len, lag,
                 out.data_ptr(), n, ws.data_ptr(), nb, s)
     if check:
         native.call("tenex_b2_status", ws.data_ptr(), n, db.row_len, lag, s)

@@ -50,7 +50,7 @@ def te_pair_list(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int, pair
     ws = D.workspace(dev, db.n, db.row_len, b_max)
     s = native.stream_ptr()
     tmp = torch.empty(P, dtype=torch.float32, device=dev)
-    native.call("tenex_te_pairs", db.data.data_ptr(), db.ld, npv.data_ptr(), int(b_max), db.n,
+    native.call("tenex_te_pairs", db.ptr(), db.ld, npv.data_ptr(), int(b_max), db.n,
                 db.row_len, tau * db.K, pairs_d.data_ptr(), P, items_d.data_ptr(),
                 items.shape[0] - 1, tmp.data_ptr(), ws.data_ptr(), ws.numel(), D._cfg(cfg), s)
     if check_data:

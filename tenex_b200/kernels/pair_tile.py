@@ -142,7 +142,7 @@ class PairTileKernel(TEKernel):
         items = torch.from_numpy(item_table(tgt.cpu().numpy(), 128)).to(dev)
         ws = D.workspace(dev, db.n, db.row_len, b_max)
         s = native.stream_ptr()
-        native.call("tenex_te_pairs", db.data.data_ptr(), db.ld, npv.data_ptr(), b_max, db.n,
+        native.call("tenex_te_pairs", db.ptr(), db.ld, npv.data_ptr(), b_max, db.n,
                     db.row_len, tau * db.K, pairs.data_ptr(), n_pairs_local, items.data_ptr(),
                     items.numel() - 1, out.data_ptr(), ws.data_ptr(), ws.numel(),
                     D._cfg(self.cfg), s)

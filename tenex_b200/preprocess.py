@@ -5,10 +5,12 @@ Mirrors tenex/preprocess.py of the reference:
   remap_bins()      :401-459
   coarsen_bins()    :462-551
   compact_dtype()   :335-354  (the dtype the reference stores bins in; here the
-                               device layout is always uint8 padded rows and this
-                               only decides the dtype handed back to callers)
+                               device layout is uint8 padded rows, uint16 for
+                               genes of more than 256 distinct bins until they are
+                               coarsened, and this only decides the dtype handed
+                               back to callers)
 All work runs in libtenex_sm100.so kernels; bins stay on the device as
-DeviceBins (uint8, rows padded to 64 bytes).
+DeviceBins (uint8 or uint16, rows padded to 64 elements).
 """
 from __future__ import annotations
 
@@ -54,7 +56,9 @@ def fsbwl_bins(x, kp: float = 0.5, device=None) -> tuple[torch.Tensor, torch.Ten
 
 def remap_bins(raw, K: int = 1, device=None) -> tuple[D.DeviceBins, torch.Tensor, int]:
     """Dense per-gene relabelling of integer bins (n, T[, K]) into the padded
-    uint8 device layout. Returns (DeviceBins, n_per_var int32, b_max)."""
+    device layout: uint8, or uint16 when a gene has more than 256 distinct
+    values (coarsen_bins narrows those). Returns (DeviceBins, n_per_var int32,
+    b_max)."""
     dev = _device(device)
     t = raw if isinstance(raw, torch.Tensor) else torch.as_tensor(np.asarray(raw))
     if t.dim() == 3:
@@ -73,17 +77,23 @@ def remap_bins(raw, K: int = 1, device=None) -> tuple[D.DeviceBins, torch.Tensor
     n, row = (int(s) for s in t.shape)
     if row % K:
         raise ValueError(f"row length {row} is not a multiple of K={K}")
-    db = D.empty_bins(n, row // K, K, dev)
     npv = torch.empty(n, dtype=torch.int32, device=dev)
     err = torch.zeros(1, dtype=torch.int32, device=dev)
-    native.call("tenex_remap_dense", t.data_ptr(), in_bytes, row, n, row, db.data.data_ptr(), 1,
-                db.ld, npv.data_ptr(), err.data_ptr(), native.stream_ptr())
-    e = int(err.item())
-    if e == 1:
-        raise ValueError("a gene's raw bins span more than 8192 values; cannot remap")
-    if e == 2:
-        raise ValueError("a gene has more than 256 distinct bins; the uint8 layout cannot hold "
-                         "them (coarsen first)")
+    db = None
+    for wide in (False, True):
+        # uint8 rows; a gene with more than 256 distinct values keeps uint16 rows
+        # (the reference's int16 bins, tenex/preprocess.py:335-354) until the
+        # coarsening step narrows them
+        db = D.empty_bins(n, row // K, K, dev, wide=wide)
+        err.zero_()
+        native.call("tenex_remap_dense", t.data_ptr(), in_bytes, row, n, row,
+                    db.data.data_ptr(), 2 if wide else 1, db.ld, npv.data_ptr(), err.data_ptr(),
+                    native.stream_ptr())
+        e = int(err.item())
+        if e == 1:
+            raise ValueError("a gene's raw bins span more than 8192 values; cannot remap")
+        if e == 0:
+            break
     b_max = int(npv.max().item())
     return db, npv, b_max
 
@@ -108,9 +118,16 @@ def discretize(arr, method: str = "FSBW-L", kp: float = 0.5, device=None,
 
 
 def coarsen_bins(db: D.DeviceBins, n_per_var: torch.Tensor, smem_bin_limit: int):
-    """In-place coarsening new = old * limit // n_per_var for genes above the
-    limit; returns (db, n_per_var, new b_max)."""
+    """Coarsening new = old * limit // n_per_var for genes above the limit, in
+    place on uint8 bins; uint16 bins (genes with more than 256 distinct values)
+    are coarsened into new uint8 bins. Returns (db, n_per_var, new b_max)."""
     npv = n_per_var.to(device=db.data.device, dtype=torch.int32).contiguous()
+    if db.wide:
+        out = D.empty_bins(db.n, db.T, db.K, db.data.device)
+        native.call("tenex_coarsen_narrow", db.data.data_ptr(), db.ld, db.n, db.row_len,
+                    npv.data_ptr(), int(smem_bin_limit), out.data.data_ptr(), out.ld,
+                    native.stream_ptr())
+        return out, npv, int(npv.max().item())
     native.call("tenex_coarsen", db.data.data_ptr(), db.ld, db.n, db.row_len, npv.data_ptr(),
                 int(smem_bin_limit), native.stream_ptr())
     return db, npv, int(npv.max().item())

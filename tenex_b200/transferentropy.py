@@ -247,7 +247,8 @@ class TransferEntropyEngine:
                 "binning_method": binning_method if binarization is None else binarization,
                 "binarization": binarization, "kp": kp, "b_max_before_coarsen": b_max,
                 "b_max": b_max, "kernel": kobj.name, "smem_optin": smem_optin,
-                "smem_bytes": smem_bytes, "source_filter": source_filter, "bin_dtype": "uint8",
+                "smem_bytes": smem_bytes, "source_filter": source_filter,
+                "bin_dtype": "uint16" if db.wide else "uint8",
                 "bin_bytes": db.data.numel()}
         _log.vprint(f"[TENEX] data: {n_vars} x {T}, K={K}, b_max={b_max}, kernel={kobj.name}")
         mark(3)

@@ -23,8 +23,11 @@ product to the reference's own CPU code paths:
                         DPI trimming (_trim) on CPU tensors, for a synthetic TE matrix
                         with planted direct and indirect edges
 
-`python tests/golden/make_golden.py /path/to/reference multilag` (or `fdr`) writes
-only that one.
+  coarsen_wide.npz      tenex.preprocess.remap_bins + _compact_dtype (int16) +
+                        coarsen_bins on genes with 257, 300 and 1000 distinct bins
+
+`python tests/golden/make_golden.py /path/to/reference multilag` (or `fdr`, `wide`)
+writes only that one.
 """
 from __future__ import annotations
 
@@ -142,6 +145,33 @@ def main(ref: str) -> None:
     print("golden fixtures written to", HERE)
 
 
+def wide(ref: str) -> None:
+    """Genes with more than 256 distinct bins: the reference remaps them into
+    int32, stores them as int16 (_compact_dtype) and coarsens the int16 bins to
+    the B200 shared-memory limit (38) in coarsen_bins."""
+    sys.path.insert(0, ref)
+    os.environ.setdefault("TENEX_CPU_ONLY", "1")
+    import torch
+    from tenex.preprocess import _compact_dtype, coarsen_bins, remap_bins
+    rng = np.random.default_rng(256)
+    n, T = 40, 4000
+    nb = rng.integers(2, 30, n)
+    nb[3], nb[17], nb[30] = 300, 1000, 257
+    raw = np.stack([rng.choice(np.arange(0, 3 * v, 3), T) for v in nb]).astype(np.int32)
+    for g in range(n):          # every value present, shuffled into the series
+        raw[g, rng.permutation(T)[:nb[g]]] = np.arange(0, 3 * nb[g], 3)
+    rem, npv, bmax = remap_bins(torch.from_numpy(raw[:, :, None].copy()))
+    rem16 = _compact_dtype(rem, bmax)
+    assert rem16.dtype == torch.int16
+    remapped = rem16.numpy()[:, :, 0].copy()           # coarsen_bins works in place
+    out, out_npv, out_bmax = coarsen_bins(rem16, npv.clone(), 38)
+    np.savez_compressed(os.path.join(HERE, "coarsen_wide.npz"), raw=raw,
+                        remapped=remapped, n_per_var=npv.numpy(), b_max=bmax,
+                        limit=38, out=out.numpy()[:, :, 0].astype(np.int32),
+                        out_dtype=str(out.dtype), out_npv=out_npv.numpy(), out_bmax=out_bmax)
+    print("coarsen_wide.npz written to", HERE)
+
+
 def multilag(ref: str) -> None:
     """The reference's multi-lag combine on synthetic per-lag surrogate results."""
     sys.path.insert(0, ref)
@@ -241,13 +271,18 @@ def fdr(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    ref_dir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py REFERENCE_SOURCE_TREE [multilag|fdr|wide]")
+    ref_dir = sys.argv[1]
     only = sys.argv[2] if len(sys.argv) > 2 else None
     if only == "multilag":
         multilag(ref_dir)
     elif only == "fdr":
         fdr(ref_dir)
+    elif only == "wide":
+        wide(ref_dir)
     else:
         main(ref_dir)
         multilag(ref_dir)
         fdr(ref_dir)
+        wide(ref_dir)

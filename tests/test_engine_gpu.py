@@ -27,7 +27,7 @@ def test_engine_cfg1_golden(cuda, golden):
 
 
 @pytest.mark.parametrize("n,T", [(7, 1), (9, 7), (33, 128), (31, 129), (40, 1000), (12, 5003),
-                                 (6, 20001)])
+                                 (6, 20001), (3, 114689), (3, 300007)])
 def test_fsbwl_bitexact_vs_numpy(cuda, n, T):
     rng = np.random.default_rng(n * T)
     x = np.log1p(rng.lognormal(0, 1, (n, T)) * (rng.random((n, T)) > 0.6)).astype(np.float32)
@@ -36,6 +36,21 @@ def test_fsbwl_bitexact_vs_numpy(cuda, n, T):
     rb, rnb = O.fsbwl(x, 0.5)
     assert np.array_equal(nb.cpu().numpy(), rnb)
     assert np.array_equal(bins.cpu().numpy(), rb)
+
+
+def test_compute_on_series_longer_than_shared_memory(cuda):
+    """compute(accelerator="gpu") on 6 genes x 150,000 cells: FSBW-L over rows
+    longer than one shared-memory pass of the pairwise sum, and TE launches whose
+    target states are staged in tiles. Bins equal the oracle's, TE within 1e-6."""
+    x, _ = W.cfg1_expression(n=6, T=150_000, seed=12, n_planted=2)
+    names = np.array([f"g{i}" for i in range(6)])
+    res = TransferEntropyEngine(x, names).compute(accelerator="gpu")
+    rb, _ = O.fsbwl(x, 0.5)
+    bins, npv, bmax = O.remap(rb)
+    if bmax > 38:                                    # the B200 coarsening limit
+        bins, npv, bmax = O.coarsen(bins, npv, 38)
+    assert np.array_equal(res.bin_arrs[:, :, 0].astype(np.int32), bins)
+    assert np.max(np.abs(res.matrix - O.te_matrix(bins, npv))) <= TOL
 
 
 def test_remap_and_discretize_match_reference(cuda, golden):
@@ -58,6 +73,34 @@ def test_coarsen_matches_reference(cuda, golden):
     assert np.array_equal(db.unpadded()[:, :, 0].cpu().numpy().astype(np.int32), g["out"])
     assert np.array_equal(npv.cpu().numpy(), g["out_npv"])
     assert bmax == int(g["out_bmax"])
+
+
+def test_genes_with_more_than_256_bins(cuda, golden):
+    """Genes of 257, 300 and 1000 distinct bins (the reference keeps them as int16
+    until coarsened): remap_bins keeps uint16 rows, AdaptiveSMEMKernel.prepare
+    coarsens them to the B200 limit (38) into uint8 rows equal to the reference's
+    coarsen_bins output, and the TE of all pairs is within 1e-6 of the oracle on
+    those bins. The uint16 bins themselves are refused by the TE kernels."""
+    from tenex_b200.preprocess import remap_bins
+    g = golden("coarsen_wide.npz")
+    db, npv, bmax = remap_bins(g["raw"], 1, cuda)
+    assert db.wide and bmax == int(g["b_max"]) == 1000
+    assert np.array_equal(db.unpadded()[:, :, 0].cpu().numpy().astype(np.int32), g["remapped"])
+    assert np.array_equal(npv.cpu().numpy(), g["n_per_var"])
+    k = AdaptiveSMEMKernel()
+    with pytest.raises(ValueError, match="256"):
+        k.compute_pairfree_device(db, npv, bmax, 1)
+    with pytest.raises(ValueError, match="256"):
+        k.prepare(db, npv.clone(), bmax, tau=1, use_coarsening=False, smem_optin=232448)
+    db2, npv2, bmax2 = k.prepare(db, npv.clone(), bmax, tau=1, smem_optin=232448)
+    assert not db2.wide and bmax2 == int(g["out_bmax"]) == 38
+    assert np.array_equal(db2.unpadded()[:, :, 0].cpu().numpy().astype(np.int32), g["out"])
+    assert np.array_equal(npv2.cpu().numpy(), g["out_npv"])
+    te = k.compute_pairfree_device(db2, npv2, bmax2, 1).cpu().numpy()
+    assert np.max(np.abs(te - O.te_pairfree(g["out"], g["out_npv"]))) <= TOL
+    # the plugin's host entry takes the raw int32 bins the same way once remapped
+    with pytest.raises(ValueError, match="255"):
+        D.pack_bins(g["raw"], cuda)
 
 
 def test_adaptive_prepare_and_heavy_genes(cuda):

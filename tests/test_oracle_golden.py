@@ -51,6 +51,20 @@ def test_coarsen_matches_reference(golden):
     assert bmax == int(g["out_bmax"])
 
 
+def test_remap_and_coarsen_of_wide_bins_match_reference(golden):
+    """Genes of 257, 300 and 1000 distinct bins: the reference's int32 remap,
+    int16 storage and coarsening to 38 bins."""
+    g = golden("coarsen_wide.npz")
+    rem, npv, bmax = O.remap(g["raw"])
+    assert np.array_equal(rem, g["remapped"])
+    assert np.array_equal(npv, g["n_per_var"])
+    assert bmax == int(g["b_max"]) == 1000
+    out, onpv, obmax = O.coarsen(rem, npv, int(g["limit"]))
+    assert np.array_equal(out, g["out"])
+    assert np.array_equal(onpv, g["out_npv"])
+    assert obmax == int(g["out_bmax"])
+
+
 def test_smem_bin_limit_rule(golden):
     g = golden("smem_limit.npz")
     for s, lim in zip(g["smem"], g["limit"]):
