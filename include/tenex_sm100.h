@@ -66,6 +66,10 @@ typedef struct {
   int ctas_per_sm;  /* resident CTAs per SM (grid = sm_count * this)    */
   int src_chunk;    /* sources per work item (one target per item)     */
   int smem_bytes;   /* dynamic shared memory per CTA (0 = fill the SM)  */
+  int lane_cells;   /* histograms of at most this many cells (b_t^2 * b_s) use
+                       lane-private tables, one copy per lane (conflict-free
+                       shared-memory reductions); 0 = the library's rule
+                       (about N / 18 cells), -1 = never */
 } tenex_te_config;
 
 int tenex_abi_version(void);
@@ -126,11 +130,18 @@ int tenex_te_pairfree_counts(const uint8_t* bins, int64_t ld, const int32_t* n_p
  * device memory. (No counterpart in the reference.) Its scratch is a fixed
  * 4 MiB area inside the library's device image, so n_vars * 4 plus about
  * 512 bytes must fit in 4 MiB (TENEX_ERR_UNSUPPORTED otherwise; up to about
- * 1,048,000 genes). The area's address is looked up by the
- * first call on each device (make that call before any stream capture); every
+ * 1,048,000 genes). Bins whose largest histograms do not fit shared memory
+ * (coarsening off) need global-memory slots the area cannot hold: such calls
+ * return TENEX_ERR_UNSUPPORTED before launching anything (use tenex_te_pairfree).
+ * The area's address is looked up by the first call on each device (make that
+ * call before any stream capture) and kept for the life of the process, so a
+ * device reset (cudaDeviceReset) after that first call is not supported; every
  * call reuses and re-initialises the same area, so calls that overlap on the
  * GPU race and must not be issued. status: optional device int32 that receives
- * the validation word (0 = inputs valid, else no TE was computed); NULL skips it.
+ * the call's outcome, written on `stream`: 0 = inputs valid and every pair
+ * computed (also for an empty range), 1 = a bin value >= its gene's n_per_var
+ * or n_per_var outside [1, b_max] (no TE computed), 3 = a work item's histogram
+ * did not fit shared memory (its pairs not computed); NULL skips it.
  * Allocates nothing: no cudaMalloc, cudaFree or allocating library call. */
 int tenex_te_pairfree_static(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
                              int b_max, int n_vars, int64_t row_len, int64_t lag,
@@ -217,6 +228,16 @@ int tenex_remap_dense(const void* raw, int in_bytes, int64_t ldr, int n_vars, in
  * genes with n_per_var > limit get bin*limit/n_per_var and n_per_var = limit. */
 int tenex_coarsen(uint8_t* bins, int64_t ld, int n_vars, int64_t row_len, int32_t* n_per_var,
                   int limit, void* stream);
+
+/* Coarsening of uint16 padded rows (genes with more than 256 distinct bins,
+ * which the reference keeps as int16 until coarsened: tenex/preprocess.py:335-354
+ * and the int16 branch of coarsen_bins, :520-536) into uint8 padded rows `out`:
+ * genes with n_per_var > limit get bin*limit/n_per_var and n_per_var = limit,
+ * the others are copied (their values are below n_per_var <= limit <= 255).
+ * ldi in uint16 elements, ldo in bytes; in and out must not overlap. */
+int tenex_coarsen_narrow(const uint16_t* in, int64_t ldi, int n_vars, int64_t row_len,
+                         int32_t* n_per_var, int limit, uint8_t* out, int64_t ldo,
+                         void* stream);
 
 /* Binarisation 1[x > thr_g] (tenex/binarize.py:225-295; kernels of
  * tenex/csrc/binarize_cuda.cu:14-56): mode 0 nonzero (thr 0), 1 mean (numpy

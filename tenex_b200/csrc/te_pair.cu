@@ -12,22 +12,34 @@
 //     target's joint state z[s] = x[s+lag]*b_t + x[s] into shared memory once
 //     per item (u8 when b_t <= 16, else u16) with the target-only marginals
 //     c2a (= row sums of c3 over yt) and c1, so sources never re-read it.
-//   * Shared memory after the target block is cut into histogram slots sized
-//     for the item (b_t^2 * b_s cells); a slot belongs to a group of G warps
-//     (G = 1: warp-private histograms for the common small pairs). Counters are
-//     32-bit unless 32-bit slots would need groups of more than 4 warps, then
-//     16-bit halves of a word (N < 65536; two cells per word collide more
-//     often, so packing is the fallback, not the rule). Pairs whose histogram
-//     fits no shared-memory slot (coarsening off) run in a second instantiation
-//     on per-CTA slots in global memory.
-//   * Every sample is one predicated-free red.shared.add (16 samples per
-//     uint4 of source bins). Skipping the most frequent cells and deriving them
-//     by subtraction (fewer same-word collisions) was measured slower on every
-//     workload, binary ones included: the derivation passes cost more than the
-//     collisions they avoid.
-//   * The entropy pass reads each slot column once to form c2b, once more to
-//     form the terms (ratio c3 * (1/c2b) * (c1/c2a), lg2.approx; exact 0 where
-//     c3*c1 == c2a*c2b), and clears the slot for the next source.
+//     Series too long for that are staged in tiles of samples, the CTA's groups
+//     walking the tiles together.
+//   * Shared memory after the target block holds the histograms of the item's
+//     pairs, in one of two layouts chosen per item:
+//       - lane-private tables (small histograms, b_t^2 * b_s up to a cell
+//         limit): 32 copies of the histogram, cell c of lane l at word
+//         c*32 + l, so the 32 lanes of a warp always hit 32 different banks
+//         (one shared-memory wavefront per warp-wide reduction instead of ~3.1
+//         for random cells). The copies are summed after each source (eight
+//         conflict-free 16-byte reads per lane per 32 cells); they are never
+//         cleared within an item: the per-source counts are the difference of
+//         two consecutive sums (modulo 2^32, exact);
+//       - shared slots (larger histograms): one slot per group of G warps
+//         (G = 1: warp-private). Counters are 32-bit unless 32-bit slots would
+//         need groups of more than 4 warps, then 16-bit halves of a word
+//         (N < 65536; two cells per word collide more often, so packing is the
+//         fallback, not the rule).
+//     Pairs whose histogram fits no shared-memory slot (coarsening off) run in a
+//     second instantiation on per-CTA slots in global memory.
+//   * Every sample is one red.shared.add (16 samples per uint4 of source bins).
+//     The hardware merges lanes that add to the same word, so the cost of a
+//     warp-wide reduction is the largest number of distinct words in one bank;
+//     warp-level aggregation of equal cells would not lower it.
+//   * The entropy pass reads each column once to form c2b, once more to form
+//     the terms (ratio c3 * (1/c2b) * (c1/c2a), lg2.approx; exact 0 where
+//     c3*c1 == c2a*c2b) and clears shared slots for the next source. Series of
+//     2^24 samples or more take a float64 pass (float32 holds the counts exactly
+//     only below 2^24).
 //   * Items are handed out by an atomic ticket, targets in L2-sized blocks and
 //     chunk-major within a block, so the CTAs resident at one moment share a
 //     small set of source rows in L2. Sources are ordered by bin count, so one
@@ -50,8 +62,11 @@ struct TeParams {
   int64_t ld;
   const int32_t* npv;
   int n;
-  int N;          // samples per pair (row_len - lag), < 2^24
+  int N;          // samples per pair (row_len - lag), < 2^31
   int lag;
+  int ztile;      // samples of the target staged at a time (N: the whole series)
+  int big;        // N >= 2^24: float64 entropy pass
+  int lane_cells; // lane-private tables for items of at most this many cells (0: never)
   int64_t p0, p1;  // pair-free id range [p0, p1)
   int t_first;
   int n_targets;
@@ -95,35 +110,34 @@ __host__ __device__ inline int64_t ws_total(int n, int bmax) {
   return round_up(ws_order_off(n, bmax) + (int64_t)n * 4, 256);
 }
 
-#ifdef TENEX_PHASE_TIMERS
-#define PHASE_MARK(var) const long long var = clock64()
-#define PHASE_ADD(k, a, b) \
-  if (lane_g == 0) atomicAdd(&P.ws->phase_cycles[k], (unsigned long long)((b) - (a)))
-#else
-#define PHASE_MARK(var)
-#define PHASE_ADD(k, a, b)
-#endif
-
 namespace {
 
 constexpr int kMaxWarps = 32;
+
+// Histogram layouts (see the file comment).
+enum { kSlot32 = 0, kSlot16 = 1, kGmem = 2, kLane32 = 3 };
 
 struct SmemLayout {
   int z_off, c2a_off, c1_off, q_off, red_off, misc_off, slot_off;
 };
 
-__host__ __device__ inline SmemLayout smem_layout(int N, int zbytes, int bmax) {
+// ztile: samples staged at a time (the z region holds ztile entries of zbytes).
+__host__ __device__ inline SmemLayout smem_layout(int ztile, int zbytes, int bmax) {
   SmemLayout L;
   int off = 0;
   L.misc_off = off;  off += 64;                               // int misc[16]
   L.red_off = off;   off += kMaxWarps * 8;                    // double red[32]
-  L.c1_off = off;    off += (int)round_up((int64_t)bmax * 4, 16);
-  L.c2a_off = off;   off += (int)round_up((int64_t)bmax * bmax * 4, 16);
-  L.q_off = off;     off += (int)round_up((int64_t)bmax * bmax * 8, 16);  // {c1/c2a, c2a}
-  L.z_off = off;     off += (int)round_up((int64_t)N * zbytes, 16);
+  L.c1_off = off;    off += (int)round_up((int64_t)bmax * 4, 16);          // int c1[bt]
+  L.c2a_off = off;   off += (int)round_up((int64_t)bmax * bmax * 4, 16);   // int c2a[bt^2]
+  L.q_off = off;     off += (int)round_up((int64_t)bmax * bmax * 8, 16);   // {c1/c2a, c2a}
+  L.z_off = off;     off += (int)round_up((int64_t)ztile * zbytes, 16);
   L.slot_off = (int)round_up(off, 128);
   return L;
 }
+
+// Words of one lane-private table with cells_pad cells: 32 copies, the summed
+// counts of the previous source and the difference (this source's counts).
+__host__ __device__ inline int64_t lane_table_words(int64_t cells_pad) { return cells_pad * 34; }
 
 // Slot cell (z, y): PACK16 -> 16-bit half (y & 1) of word z*hb + (y >> 1),
 // else word z*bs + y.
@@ -137,28 +151,30 @@ __device__ __forceinline__ uint32_t cell_get(const uint32_t* slot, uint32_t z, u
   return slot[z * bs + y];
 }
 
-// Counts one sample: one reduction per sample (inline PTX, no return value);
-// PACK16 adds 1 or 1 << 16 to the word holding the cell's 16-bit half. base is
-// the slot's address: the 32-bit shared window address, or (GMEM, the
+// Counts one sample: one reduction per sample (inline PTX, no return value).
+// kSlot16 adds 1 or 1 << 16 to the word holding the cell's 16-bit half; kLane32
+// adds to the lane's copy (base already holds the lane's offset). base is the
+// table's address: the 32-bit shared window address, or (kGmem, the
 // global-memory overflow slot) the global address.
-template <bool PACK16, bool GMEM>
+template <int MODE>
 __device__ __forceinline__ void hist_add(uint64_t base, uint32_t z, uint32_t y, uint32_t bs,
                                          uint32_t hb) {
-  uint32_t off, inc;
-  if (PACK16) {
+  uint32_t off, inc = 1u;
+  if (MODE == kSlot16) {
     off = (z * hb + (y >> 1)) << 2;
     inc = (y & 1u) * 0xffffu + 1u;
+  } else if (MODE == kLane32) {
+    off = (z * bs + y) << 7;
   } else {
     off = (z * bs + y) << 2;
-    inc = 1u;
   }
-  if (GMEM)
+  if (MODE == kGmem)
     asm volatile("red.global.add.u32 [%0], %1;" ::"l"(base + off), "r"(inc) : "memory");
   else
     asm volatile("red.shared.add.u32 [%0], %1;" ::"r"((uint32_t)base + off), "r"(inc) : "memory");
 }
 
-template <bool PACK16, bool GMEM>
+template <int MODE>
 __device__ __forceinline__ void hist16_z8(uint64_t slot, uint4 yv, uint4 zv, uint32_t bs,
                                           uint32_t hb) {
   const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
@@ -169,12 +185,12 @@ __device__ __forceinline__ void hist16_z8(uint64_t slot, uint4 yv, uint4 zv, uin
     for (int b = 0; b < 4; ++b) {
       const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
       const uint32_t z = __byte_perm(zs[w], 0, 0x4440 + b);
-      hist_add<PACK16, GMEM>(slot, z, y, bs, hb);
+      hist_add<MODE>(slot, z, y, bs, hb);
     }
   }
 }
 
-template <bool PACK16, bool GMEM>
+template <int MODE>
 __device__ __forceinline__ void hist16_z16(uint64_t slot, uint4 yv, uint4 za, uint4 zb,
                                            uint32_t bs, uint32_t hb) {
   const uint32_t ys[4] = {yv.x, yv.y, yv.z, yv.w};
@@ -186,17 +202,18 @@ __device__ __forceinline__ void hist16_z16(uint64_t slot, uint4 yv, uint4 za, ui
       const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
       const uint32_t zw = zs[(w * 4 + b) >> 1];
       const uint32_t z = (b & 1) ? (zw >> 16) : (zw & 0xffffu);
-      hist_add<PACK16, GMEM>(slot, z, y, bs, hb);
+      hist_add<MODE>(slot, z, y, bs, hb);
     }
   }
 }
 
-// Histogram of one source against the staged target (all group lanes).
-template <bool PACK16, bool GMEM>
+// Histogram of one source against the staged target over n samples (all group
+// lanes): zsm[i] is the target state of sample i of srow (both 16-byte aligned).
+template <int MODE>
 __device__ __forceinline__ void hist_source(uint64_t slot32, const unsigned char* zsm, bool z8,
-                                            const uint8_t* srow, int N, int lane_g,
+                                            const uint8_t* srow, int n, int lane_g,
                                             int gthreads, uint32_t bs, uint32_t hb) {
-  const int nvec = N >> 4;
+  const int nvec = n >> 4;
   const uint4* yv = reinterpret_cast<const uint4*>(srow);
   const uint4* zv = reinterpret_cast<const uint4*>(zsm);
   int v = lane_g;
@@ -207,12 +224,12 @@ __device__ __forceinline__ void hist_source(uint64_t slot32, const unsigned char
         const int vn = v + gthreads;
         uint4 ynext = ycur;
         if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
-        hist16_z8<PACK16, GMEM>(slot32, ycur, zv[v], bs, hb);
+        hist16_z8<MODE>(slot32, ycur, zv[v], bs, hb);
         ycur = ynext;
       }
     }
-    for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
-      hist_add<PACK16, GMEM>(slot32, zsm[s], srow[s], bs, hb);
+    for (int s = (nvec << 4) + lane_g; s < n; s += gthreads)
+      hist_add<MODE>(slot32, zsm[s], srow[s], bs, hb);
   } else {
     const uint16_t* z16 = reinterpret_cast<const uint16_t*>(zsm);
     if (v < nvec) {
@@ -221,12 +238,12 @@ __device__ __forceinline__ void hist_source(uint64_t slot32, const unsigned char
         const int vn = v + gthreads;
         uint4 ynext = ycur;
         if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
-        hist16_z16<PACK16, GMEM>(slot32, ycur, zv[2 * v], zv[2 * v + 1], bs, hb);
+        hist16_z16<MODE>(slot32, ycur, zv[2 * v], zv[2 * v + 1], bs, hb);
         ycur = ynext;
       }
     }
-    for (int s = (nvec << 4) + lane_g; s < N; s += gthreads)
-      hist_add<PACK16, GMEM>(slot32, z16[s], srow[s], bs, hb);
+    for (int s = (nvec << 4) + lane_g; s < n; s += gthreads)
+      hist_add<MODE>(slot32, z16[s], srow[s], bs, hb);
   }
 }
 
@@ -245,136 +262,303 @@ __host__ __device__ inline bool slot_fits(int64_t bt, int64_t bs, int N, int64_t
   return N < 65536 && w16 * 4 <= slot_region;
 }
 
-// One group's pass over its sources of the current item. GMEM: the global-memory
-// overflow launch (one slot per CTA in the workspace, only pairs that do not fit
-// shared memory); otherwise only pairs that fit.
-template <bool PACK16, bool GMEM>
-__device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, int G, int g,
-                                            int n_groups, int lane_g, int tid, int warp,
-                                            int tgt, int64_t lo, int64_t base, int n_src,
-                                            int bt, const unsigned char* zsm, bool z8,
-                                            const float* c1s, const float2* qa, double* red,
-                                            int slot_region) {
+// Lane-private tables: sums the 32 copies of 32 consecutive cells per warp
+// iteration (lane l: cell cb*32 + l, its 16-byte chunk ((l + j) & 7) in step j,
+// so every quarter-warp reads eight different bank quads), and writes this
+// source's counts D = sum - (previous sum) and the new sum Pv.
+__device__ __forceinline__ void lane_fold(const uint32_t* T, uint32_t* D, uint32_t* Pv, int ncb,
+                                          int w_g, int G, int lane) {
+  for (int cb = w_g; cb < ncb; cb += G) {
+    const int cell = cb * 32 + lane;
+    const uint32_t* row = T + (int64_t)cell * 32;
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint4 v = *reinterpret_cast<const uint4*>(row + (((lane + j) & 7) << 2));
+      s += (v.x + v.y) + (v.z + v.w);
+    }
+    const uint32_t prev = Pv[cell];
+    Pv[cell] = s;
+    D[cell] = s - prev;
+  }
+}
+
+// Per-lane part of sum c3 * log2(c3 * c1 / (c2a * c2b)) over the pair's cells.
+// Cell (z = xt1*bt + xt, y) is tab[z * stride + y] (PACK16: the 16-bit half
+// (y & 1) of word z * stride + (y >> 1), stride = hb). Columns (xt, y) are
+// spread over the group's lanes; CLEAR zeroes every word after reading it.
+// term = c3 * log2(c3 * c1 / (c2a * c2b)), the ratio formed as
+// c3 * (1/c2b) * (c1/c2a) (one reciprocal per column, c1/c2a staged per target)
+// except where c3 * c1 == c2a * c2b, whose term is exactly 0 as in the
+// reference's formula (constant or duplicated sources give TE = 0, not a
+// rounding residue). Empty cells take log2(1) = 0 (no branch).
+template <bool PACK16, bool CLEAR>
+__device__ __forceinline__ float entropy_cols(uint32_t* tab, int bt, int bs, int stride,
+                                              const int* c1i, const float2* qa, int lane_g,
+                                              int gthreads) {
+  float acc = 0.f;
+  const int ncy = PACK16 ? stride : bs;
+  const int ncols = bt * ncy;
+  for (int col = lane_g; col < ncols; col += gthreads) {
+    const int j = col / ncy;
+    const int wk = col - j * ncy;
+    uint32_t s = 0;
+    for (int i = 0; i < bt; ++i) s += tab[(i * bt + j) * stride + wk];
+    if (s == 0u) continue;
+    const float c1j = (float)c1i[j];
+    if (PACK16) {
+      const float blo = (float)(s & 0xffffu), bhi = (float)(s >> 16);
+      const float inv_lo = __frcp_rn(blo), inv_hi = __frcp_rn(bhi);
+      for (int i = 0; i < bt; ++i) {
+        const int idx = (i * bt + j) * stride + wk;
+        const uint32_t w = tab[idx];
+        if (CLEAR) tab[idx] = 0u;
+        const float2 q = qa[i * bt + j];  // {c1/c2a, c2a}
+        const float clo = (float)(w & 0xffffu), chi = (float)(w >> 16);
+        const bool elo = clo == 0.f || clo * c1j == q.y * blo;
+        const bool ehi = chi == 0.f || chi * c1j == q.y * bhi;
+        const float rlo = elo ? 1.f : clo * inv_lo * q.x;
+        const float rhi = ehi ? 1.f : chi * inv_hi * q.x;
+        acc = fmaf(clo, __log2f(rlo), acc);
+        acc = fmaf(chi, __log2f(rhi), acc);
+      }
+    } else {
+      const float b = (float)s;
+      const float inv = __frcp_rn(b);
+      for (int i = 0; i < bt; ++i) {
+        const int idx = (i * bt + j) * stride + wk;
+        const uint32_t w = tab[idx];
+        if (CLEAR) tab[idx] = 0u;
+        const float2 q = qa[i * bt + j];
+        const float c = (float)w;
+        const bool e = w == 0u || c * c1j == q.y * b;
+        const float r = e ? 1.f : c * inv * q.x;
+        acc = fmaf(c, __log2f(r), acc);
+      }
+    }
+  }
+  return acc;
+}
+
+// Same sum for series of 2^24 samples or more, in float64 from the integer
+// counts (32-bit counters only; the zero-term test on exact 64-bit products).
+template <bool CLEAR>
+__device__ double entropy_cols_f64(uint32_t* tab, int bt, int bs, int stride, const int* c1i,
+                                   const int* c2ai, int lane_g, int gthreads) {
+  double acc = 0.0;
+  const int ncols = bt * bs;
+  for (int col = lane_g; col < ncols; col += gthreads) {
+    const int j = col / bs;
+    const int y = col - j * bs;
+    uint64_t s = 0;
+    for (int i = 0; i < bt; ++i) s += tab[(i * bt + j) * stride + y];
+    if (s == 0u) continue;
+    const uint64_t c1j = (uint64_t)(uint32_t)c1i[j];
+    for (int i = 0; i < bt; ++i) {
+      const int idx = (i * bt + j) * stride + y;
+      const uint64_t c = tab[idx];
+      if (CLEAR) tab[idx] = 0u;
+      const uint64_t c2a = (uint64_t)(uint32_t)c2ai[i * bt + j];
+      if (c == 0u || c * c1j == c2a * s) continue;
+      acc += (double)c * log2(((double)c * (double)c1j) / ((double)c2a * (double)s));
+    }
+  }
+  return acc;
+}
+
+// Everything a group needs about the current item.
+struct ItemCtx {
+  int tgt;
+  int64_t lo, base;
+  int n_src;
+  int bt;
+  int BS;             // the item's largest source bin count (table stride, kLane32)
+  bool z8;
+  const unsigned char* zsm;
+  const int* c1i;
+  const int* c2ai;
+  const float2* qa;
+  double* red;
+  int slot_region;    // shared-memory slot region (overflow split rule)
+  int ncb;            // kLane32: 32-cell blocks of the table
+  int cells_pad;      // kLane32: padded cells per table
+};
+
+// Source r of the item for this launch: its id and pair id, or false if the
+// pair is not this launch's (the target itself, outside [p0, p1), or, with an
+// overflow launch, on the other launch's side of the shared-memory fit rule).
+template <int MODE>
+__device__ __forceinline__ bool pair_of(const TeParams& P, const ItemCtx& it, int r, int* src_o,
+                                        int64_t* p_o) {
+  int64_t p;
+  int src;
+  if (P.pairs) {
+    p = it.lo + r;
+    src = (int)P.pairs[2 * p + 1];
+  } else {
+    src = P.order[it.lo + r];
+    p = it.base + (src < it.tgt ? src : src - 1);
+    if (src == it.tgt || p < P.p0 || p >= P.p1) return false;
+  }
+  if (P.overflow && slot_fits(it.bt, P.npv[src], P.N, it.slot_region) == (MODE == kGmem))
+    return false;
+  *src_o = src;
+  *p_o = p;
+  return true;
+}
+
+// After the histogram of source src (pair id p) is complete in the group's
+// table: optional raw-count export, the entropy pass and the output.
+template <int MODE>
+__device__ __forceinline__ void finish_pair(const TeParams& P, const ItemCtx& it, uint32_t* slot,
+                                            int G, int g, int lane_g, int tid, int warp, int src,
+                                            int64_t p, float obs_m) {
+  const int gthreads = G * 32;
+  const int bt = it.bt;
+  const int bt2 = bt * bt;
+  const int bs = P.npv[src];
+  constexpr bool PACK16 = MODE == kSlot16;
+  constexpr bool LANE = MODE == kLane32;
+  const int hb = PACK16 ? (bs + 1) >> 1 : bs;
+  group_sync(G, g, gthreads);
+  uint32_t* tab = slot;  // counts read by the entropy pass
+  int stride = PACK16 ? hb : bs;
+  if (LANE) {
+    uint32_t* D = slot + (int64_t)32 * it.cells_pad;
+    lane_fold(slot, D, D + it.cells_pad, it.ncb, lane_g >> 5, G, tid & 31);
+    group_sync(G, g, gthreads);
+    tab = D;
+    stride = it.BS;
+  }
+
+  // -- optional raw-count export (parity checks only) --------------------
+  if (P.counts_dbg != nullptr) {
+    int32_t* cd = P.counts_dbg + (p - P.p0) * P.counts_stride;
+    const int ncell = bt2 * bs;
+    for (int c = lane_g; c < ncell; c += gthreads) {
+      const int z = c / bs, y = c - z * bs;
+      cd[c] = (int32_t)(PACK16 ? cell_get<true>(tab, z, y, bs, hb) : tab[z * stride + y]);
+    }
+    group_sync(G, g, gthreads);
+  }
+
+  // -- entropy pass (shared slots are cleared for the next source) ---------
+  double tot;
+  if (P.big) {
+    tot = dev::warp_sum(entropy_cols_f64<!LANE>(tab, bt, bs, stride, it.c1i, it.c2ai, lane_g,
+                                                gthreads));
+  } else {
+    tot = dev::warp_sum((double)entropy_cols<PACK16, !LANE>(tab, bt, bs, stride, it.c1i, it.qa,
+                                                            lane_g, gthreads));
+  }
+  if (G > 1) {
+    if ((tid & 31) == 0) it.red[warp] = tot;
+    dev::named_bar(1 + g, gthreads);
+    if (lane_g == 0) {
+      tot = 0.0;
+      for (int w = 0; w < G; ++w) tot += it.red[g * G + w];
+    }
+  }
+  if (lane_g == 0) {
+    const float te = (float)(tot / (double)P.N);
+    if (P.out_mode == kOutPairfree) {
+      P.out[p - P.p0] = te;
+    } else if (P.out_mode == kOutMatrix) {
+      P.out[(int64_t)src * P.out_ld + it.tgt] = te;
+    } else {
+      // one addend per cell per launch: reductions without a return value
+      // (no load-to-store stall) give the same float64 sums as += would
+      const int64_t m = (int64_t)src * P.n + it.tgt;
+      const double td = (double)te;
+      atomicAdd(P.sum + m, td);
+      atomicAdd(P.sumsq + m, td * td);
+      if (te >= obs_m) atomicAdd(P.cnt_ge + m, 1);
+    }
+  }
+  group_sync(G, g, gthreads);
+}
+
+// Address of the group's table for hist_add.
+template <int MODE>
+__device__ __forceinline__ uint64_t table_addr(uint32_t* slot, int tid) {
+  uint64_t a;
+  if (MODE == kGmem) asm("cvta.to.global.u64 %0, %1;" : "=l"(a) : "l"(slot));
+  else a = (uint64_t)__cvta_generic_to_shared(slot);
+  if (MODE == kLane32) a += (uint64_t)((tid & 31) * 4);
+  return a;
+}
+
+// Stages target states of samples [s0, s0 + n) into zsm (all CTA threads);
+// COUNT also adds them to the c2a counts.
+template <bool COUNT>
+__device__ __forceinline__ void stage_z(const uint8_t* trow, int lag, int bt, bool z8, int s0,
+                                        int n, unsigned char* zsm, int* c2ai, int tid,
+                                        int nthreads) {
+  if (z8) {
+    for (int s = tid; s < n; s += nthreads) {
+      const uint32_t z = (uint32_t)trow[s0 + s + lag] * bt + trow[s0 + s];
+      zsm[s] = (unsigned char)z;
+      if (COUNT) atomicAdd(&c2ai[z], 1);
+    }
+  } else {
+    uint16_t* z16 = reinterpret_cast<uint16_t*>(zsm);
+    for (int s = tid; s < n; s += nthreads) {
+      const uint32_t z = (uint32_t)trow[s0 + s + lag] * bt + trow[s0 + s];
+      z16[s] = (uint16_t)z;
+      if (COUNT) atomicAdd(&c2ai[z], 1);
+    }
+  }
+}
+
+// One group's pass over its sources of the current item. Whole series staged
+// (ztile == N): each group walks its sources on its own. Tiled: the CTA's
+// groups take one source each per round and walk the sample tiles together.
+template <int MODE>
+__device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it, uint32_t* slot,
+                                            unsigned char* zsm, int G, int g, int n_groups,
+                                            int lane_g, int tid, int warp, int nthreads) {
   const int gthreads = G * 32;
   const int N = P.N;
-  const int bt2 = bt * bt;
-  for (int r = g; r < n_src; r += n_groups) {
-    int64_t p;
-    int src;
-    if (P.pairs) {
-      p = lo + r;
-      src = (int)P.pairs[2 * p + 1];
-    } else {
-      src = P.order[lo + r];
-      p = base + (src < tgt ? src : src - 1);
-      if (src == tgt || p < P.p0 || p >= P.p1) continue;  // group-uniform skip
+  constexpr bool PACK16 = MODE == kSlot16;
+  const uint64_t slot_addr = table_addr<MODE>(slot, tid);
+  if (P.ztile >= N) {
+    for (int r = g; r < it.n_src; r += n_groups) {
+      int src;
+      int64_t p;
+      if (!pair_of<MODE>(P, it, r, &src, &p)) continue;  // group-uniform skip
+      // surrogate statistics: the observed TE is loaded now, so its latency hides
+      // behind the histogram pass instead of stalling the epilogue
+      float obs_m = 0.f;
+      if (P.out_mode == kOutStats && lane_g == 0) obs_m = __ldg(P.obs + (int64_t)src * P.n + it.tgt);
+      const uint32_t bs = (uint32_t)P.npv[src];
+      const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
+      const uint32_t stride = MODE == kLane32 ? (uint32_t)it.BS : bs;
+      hist_source<MODE>(slot_addr, it.zsm, it.z8, P.bins + (int64_t)src * P.ld, N, lane_g,
+                        gthreads, stride, hb);
+      finish_pair<MODE>(P, it, slot, G, g, lane_g, tid, warp, src, p, obs_m);
     }
-    const uint32_t bs = (uint32_t)P.npv[src];
-    if (P.overflow && slot_fits(bt, bs, N, slot_region) == GMEM) continue;  // other launch's
-    // surrogate statistics: the observed TE is loaded now, so its latency hides
-    // behind the histogram pass instead of stalling the epilogue
+    return;
+  }
+  const uint8_t* trow = P.bins + (int64_t)it.tgt * P.ld;
+  for (int r0 = 0; r0 < it.n_src; r0 += n_groups) {
+    int src = 0;
+    int64_t p = 0;
+    const bool act = r0 + g < it.n_src && pair_of<MODE>(P, it, r0 + g, &src, &p);
     float obs_m = 0.f;
-    if (P.out_mode == kOutStats && lane_g == 0) obs_m = __ldg(P.obs + (int64_t)src * P.n + tgt);
+    if (act && P.out_mode == kOutStats && lane_g == 0)
+      obs_m = __ldg(P.obs + (int64_t)src * P.n + it.tgt);
+    const uint32_t bs = act ? (uint32_t)P.npv[src] : 1u;
     const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
+    const uint32_t stride = MODE == kLane32 ? (uint32_t)it.BS : bs;
     const uint8_t* srow = P.bins + (int64_t)src * P.ld;
-    uint64_t slot_addr;
-    if (GMEM) asm("cvta.to.global.u64 %0, %1;" : "=l"(slot_addr) : "l"(slot));
-    else slot_addr = (uint64_t)__cvta_generic_to_shared(slot);
-    PHASE_MARK(t0);
-
-    // -- histogram of every sample -----------------------------------------
-    hist_source<PACK16, GMEM>(slot_addr, zsm, z8, srow, N, lane_g, gthreads, bs, hb);
-    group_sync(G, g, gthreads);
-    PHASE_MARK(t1);
-    PHASE_MARK(t2);
-
-    // -- optional raw-count export (parity checks only) --------------------
-    if (P.counts_dbg != nullptr) {
-      int32_t* cd = P.counts_dbg + (p - P.p0) * P.counts_stride;
-      const int ncell = bt2 * (int)bs;
-      for (int c = lane_g; c < ncell; c += gthreads) {
-        const int z = c / (int)bs, y = c - z * (int)bs;
-        cd[c] = (int32_t)cell_get<PACK16>(slot, z, y, bs, hb);
-      }
-      group_sync(G, g, gthreads);
+    for (int s0 = 0; s0 < N; s0 += P.ztile) {
+      const int n = min(P.ztile, N - s0);
+      __syncthreads();  // every group is done with the previous tile
+      stage_z<false>(trow, P.lag, it.bt, it.z8, s0, n, zsm, nullptr, tid, nthreads);
+      __syncthreads();
+      if (act) hist_source<MODE>(slot_addr, zsm, it.z8, srow + s0, n, lane_g, gthreads, stride, hb);
     }
-
-    // -- entropy pass: column (xt=j, word wk) over xt1=i, clearing the slot --
-    // term = c3 * log2(c3 * c1 / (c2a * c2b)). The ratio is formed as
-    // c3 * (1/c2b) * (c1/c2a) (one reciprocal per column, c1/c2a staged per
-    // target) except where c3 * c1 == c2a * c2b, whose term is exactly 0 as in
-    // the reference's formula (constant or duplicated sources give TE = 0, not a
-    // rounding residue). Empty cells take log2(1) = 0 (no branch).
-    float acc = 0.f;
-    const int ncols = bt * (int)hb;
-    for (int col = lane_g; col < ncols; col += gthreads) {
-      const int j = col / (int)hb;
-      const int wk = col - j * (int)hb;
-      uint32_t s = 0;
-      for (int i = 0; i < bt; ++i) s += slot[(i * bt + j) * hb + wk];
-      if (s == 0u) continue;
-      const float c1j = c1s[j];
-      if (PACK16) {
-        const float blo = (float)(s & 0xffffu), bhi = (float)(s >> 16);
-        const float inv_lo = __frcp_rn(blo), inv_hi = __frcp_rn(bhi);
-        for (int i = 0; i < bt; ++i) {
-          const int idx = (i * bt + j) * hb + wk;
-          const uint32_t w = slot[idx];
-          slot[idx] = 0u;
-          const float2 q = qa[i * bt + j];  // {c1/c2a, c2a}
-          const float clo = (float)(w & 0xffffu), chi = (float)(w >> 16);
-          const bool elo = clo == 0.f || clo * c1j == q.y * blo;
-          const bool ehi = chi == 0.f || chi * c1j == q.y * bhi;
-          const float rlo = elo ? 1.f : clo * inv_lo * q.x;
-          const float rhi = ehi ? 1.f : chi * inv_hi * q.x;
-          acc = fmaf(clo, __log2f(rlo), acc);
-          acc = fmaf(chi, __log2f(rhi), acc);
-        }
-      } else {
-        const float b = (float)s;
-        const float inv = __frcp_rn(b);
-        for (int i = 0; i < bt; ++i) {
-          const int idx = (i * bt + j) * hb + wk;
-          const uint32_t w = slot[idx];
-          slot[idx] = 0u;
-          const float2 q = qa[i * bt + j];
-          const float c = (float)w;
-          const bool e = w == 0u || c * c1j == q.y * b;
-          const float r = e ? 1.f : c * inv * q.x;
-          acc = fmaf(c, __log2f(r), acc);
-        }
-      }
-    }
-    double tot = dev::warp_sum((double)acc);
-    if (G > 1) {
-      if ((tid & 31) == 0) red[warp] = tot;
-      dev::named_bar(1 + g, gthreads);
-      if (lane_g == 0) {
-        tot = 0.0;
-        for (int w = 0; w < G; ++w) tot += red[g * G + w];
-      }
-    }
-    if (lane_g == 0) {
-      const float te = (float)(tot / (double)N);
-      if (P.out_mode == kOutPairfree) {
-        P.out[p - P.p0] = te;
-      } else if (P.out_mode == kOutMatrix) {
-        P.out[(int64_t)src * P.out_ld + tgt] = te;
-      } else {
-        // one addend per cell per launch: reductions without a return value
-        // (no load-to-store stall) give the same float64 sums as += would
-        const int64_t m = (int64_t)src * P.n + tgt;
-        const double td = (double)te;
-        atomicAdd(P.sum + m, td);
-        atomicAdd(P.sumsq + m, td * td);
-        if (te >= obs_m) atomicAdd(P.cnt_ge + m, 1);
-      }
-    }
-    group_sync(G, g, gthreads);
-    PHASE_MARK(t3);
-    PHASE_ADD(0, t0, t1);
-    PHASE_ADD(1, t1, t2);
-    PHASE_ADD(2, t2, t3);
+    if (act) finish_pair<MODE>(P, it, slot, G, g, lane_g, tid, warp, src, p, obs_m);
   }
 }
 
@@ -385,13 +569,12 @@ __device__ __forceinline__ void run_sources(const TeParams& P, uint32_t* slot, i
 template <bool GMEM>
 __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const SmemLayout SL = smem_layout(P.N, P.zbytes, P.bmax);
+  const SmemLayout SL = smem_layout(P.ztile, P.zbytes, P.bmax);
   int* misc = reinterpret_cast<int*>(smem + SL.misc_off);
   double* red = reinterpret_cast<double*>(smem + SL.red_off);
-  float* c1s = reinterpret_cast<float*>(smem + SL.c1_off);
-  float* c2as = reinterpret_cast<float*>(smem + SL.c2a_off);
+  int* c1i = reinterpret_cast<int*>(smem + SL.c1_off);
+  int* c2ai = reinterpret_cast<int*>(smem + SL.c2a_off);
   float2* qa = reinterpret_cast<float2*>(smem + SL.q_off);
-  int* c2a_cnt = reinterpret_cast<int*>(smem + SL.c2a_off);
   unsigned char* zsm = smem + SL.z_off;
   uint32_t* slots = reinterpret_cast<uint32_t*>(smem + SL.slot_off);
   const int slot_region = P.smem_bytes - SL.slot_off;
@@ -402,6 +585,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   const int n_warps = nthreads >> 5;
   const int nm1 = P.n - 1;
   const int N = P.N;
+  const bool tiled = P.ztile < N;
 
   if (*(volatile int*)&P.ws->bad_data != 0) return;  // validation failed: do nothing
   uint32_t* gslot = GMEM ? P.gslots + (int64_t)blockIdx.x * P.gslot_words : nullptr;
@@ -493,7 +677,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     if (P.overflow && !__syncthreads_or(mine)) continue;  // no pair of this launch (uniform)
     my_max = dev::warp_max(my_max);
     if ((tid & 31) == 0) reinterpret_cast<unsigned*>(red)[warp] = my_max;
-    for (int i = tid; i < bt2; i += nthreads) c2a_cnt[i] = 0;
+    for (int i = tid; i < bt2; i += nthreads) c2ai[i] = 0;
     __syncthreads();
     if (tid < 32) {
       unsigned v = tid < n_warps ? reinterpret_cast<unsigned*>(red)[tid] : 1u;
@@ -501,42 +685,44 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       if (tid == 0) misc[1] = (int)v;
     }
 
-    // ---- stage the target: z[s] = x[s+lag]*bt + x[s], and c2a counts ------
+    // ---- the target: z[s] = x[s+lag]*bt + x[s] staged (whole series) and the
+    // c2a counts (tiled series: counted here, staged tile by tile later) ------
     const uint8_t* trow = P.bins + (int64_t)tgt * P.ld;
     const bool z8 = bt <= 16;
-    if (z8) {
-      for (int s = tid; s < N; s += nthreads) {
-        uint32_t z = (uint32_t)trow[s + P.lag] * bt + trow[s];
-        zsm[s] = (unsigned char)z;
-        atomicAdd(&c2a_cnt[z], 1);
-      }
+    if (!tiled) {
+      stage_z<true>(trow, P.lag, bt, z8, 0, N, zsm, c2ai, tid, nthreads);
     } else {
-      uint16_t* z16 = reinterpret_cast<uint16_t*>(zsm);
-      for (int s = tid; s < N; s += nthreads) {
-        uint32_t z = (uint32_t)trow[s + P.lag] * bt + trow[s];
-        z16[s] = (uint16_t)z;
-        atomicAdd(&c2a_cnt[z], 1);
-      }
+      for (int s = tid; s < N; s += nthreads)
+        atomicAdd(&c2ai[(uint32_t)trow[s + P.lag] * bt + trow[s]], 1);
     }
     __syncthreads();
     const int bsmax = misc[1];
-    for (int i = tid; i < bt2; i += nthreads) c2as[i] = (float)c2a_cnt[i];
-    __syncthreads();
     for (int j = tid; j < bt; j += nthreads) {
-      float s = 0.f;
-      for (int i = 0; i < bt; ++i) s += c2as[i * bt + j];
-      c1s[j] = s;
+      int s = 0;
+      for (int i = 0; i < bt; ++i) s += c2ai[i * bt + j];
+      c1i[j] = s;
     }
 
-    // ---- carve slots: 32-bit counters when groups of <= 4 warps fit --------
-    // (the overflow launch: the whole CTA on one 32-bit slot in global memory)
+    // ---- table layout of this item ---------------------------------------
+    // lane-private tables for small histograms (after the target block, which
+    // takes ztile bytes when b_t <= 16); else shared slots: 32-bit counters
+    // when groups of <= 4 warps fit (the overflow launch: the whole CTA on one
+    // 32-bit slot in global memory)
+    const int cells = bt2 * bsmax;
+    const int cells_pad = (int)round_up(cells, 32);
+    const int lane_off =
+        (int)round_up((int64_t)SL.z_off + (int64_t)P.ztile * (z8 ? 1 : 2), 128);
+    const int fitl = GMEM || cells > P.lane_cells
+                         ? 0
+                         : (int)((P.smem_bytes - lane_off) / (lane_table_words(cells_pad) * 4));
+    const bool lane = fitl >= 1;
     const int words32 = (int)round_up((int64_t)bt2 * bsmax, 4);
     const int words16 = (int)round_up((int64_t)bt2 * ((bsmax + 1) >> 1), 4);
     const int fit32 = GMEM ? 1 : slot_region / (words32 * 4);
     const int fit16 = GMEM ? 0 : slot_region / (words16 * 4);
-    const bool pack16 = !GMEM && (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
-    const int fit = pack16 ? fit16 : fit32;
-    const int slot_words = pack16 ? words16 : words32;
+    const bool pack16 = !lane && !GMEM && (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
+    const int fit = lane ? fitl : (pack16 ? fit16 : fit32);
+    const int slot_words = lane ? (int)lane_table_words(cells_pad) : (pack16 ? words16 : words32);
     if (fit < 1) {
       if (tid == 0) atomicExch(&P.ws->bad_item, 1);
       __syncthreads();
@@ -548,25 +734,42 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     const int n_groups = n_warps / G;
     const int g = warp / G;
     const int lane_g = tid - g * G * 32;
-    uint32_t* slot = GMEM ? gslot : slots + (int64_t)g * slot_words;
+    uint32_t* tbase =
+        lane ? reinterpret_cast<uint32_t*>(smem + lane_off) : slots;
+    uint32_t* slot = GMEM ? gslot : tbase + (int64_t)g * slot_words;
     if (!GMEM)
-      for (int i = tid; i < n_groups * slot_words; i += nthreads) slots[i] = 0u;
+      for (int i = tid; i < n_groups * slot_words; i += nthreads) tbase[i] = 0u;
     __syncthreads();
     for (int z = tid; z < bt2; z += nthreads) {
-      const float c2a = c2as[z];
-      qa[z] = make_float2(c2a > 0.f ? __fdiv_rn(c1s[z % bt], c2a) : 0.f, c2a);
+      const float c2a = (float)c2ai[z];
+      qa[z] = make_float2(c2a > 0.f ? __fdiv_rn((float)c1i[z % bt], c2a) : 0.f, c2a);
     }
     __syncthreads();
 
+    ItemCtx it;
+    it.tgt = tgt;
+    it.lo = lo;
+    it.base = base;
+    it.n_src = n_src;
+    it.bt = bt;
+    it.BS = bsmax;
+    it.z8 = z8;
+    it.zsm = zsm;
+    it.c1i = c1i;
+    it.c2ai = c2ai;
+    it.qa = qa;
+    it.red = red;
+    it.slot_region = slot_region;
+    it.ncb = cells_pad / 32;
+    it.cells_pad = cells_pad;
     if (GMEM)
-      run_sources<false, true>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src,
-                               bt, zsm, z8, c1s, qa, red, slot_region);
+      run_sources<kGmem>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
+    else if (lane)
+      run_sources<kLane32>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
     else if (pack16)
-      run_sources<true, false>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src,
-                               bt, zsm, z8, c1s, qa, red, slot_region);
+      run_sources<kSlot16>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
     else
-      run_sources<false, false>(P, slot, G, g, n_groups, lane_g, tid, warp, tgt, lo, base, n_src,
-                                bt, zsm, z8, c1s, qa, red, slot_region);
+      run_sources<kSlot32>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
     __syncthreads();
   }
 }
@@ -647,6 +850,21 @@ struct TeLaunch {
   int threads, grid, smem;
 };
 
+// Samples of the target staged in shared memory at a time: the whole series
+// when its states take at most 64 KB (10,000-20,000 samples of u16 states, any
+// series up to 65,536 samples of u8 states), else tiles of 32 KB, which leave
+// the histograms room for every bin count the coarsening limit allows.
+static int z_tile(int N, int zbytes) {
+  if ((int64_t)N * zbytes <= 65536) return N;
+  return 32768 / zbytes;
+}
+
+// Default cell limit of the lane-private tables for series of N samples: about
+// where a table's per-source summation (one wavefront per cell) costs what its
+// conflict-free reductions save over shared slots (~2.1 wavefronts per 32
+// samples).
+static int default_lane_cells(int N) { return N / 18; }
+
 static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const DevAttr& A,
                           TeLaunch* L, int64_t max_slot_bytes) {
   // Default shape: 2 CTAs x 512 threads per SM. When the largest histogram needs
@@ -666,7 +884,7 @@ static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const D
   if (fixed > A.smem_optin)
     return fail(TENEX_ERR_BADARG, "smem_bytes=%d exceeds the device opt-in %d", fixed,
                 A.smem_optin);
-  const SmemLayout SL = smem_layout(P.N, P.zbytes, P.bmax);
+  const SmemLayout SL = smem_layout(P.ztile, P.zbytes, P.bmax);
   int smem = 0;
   // With shared memory sized automatically, fewer CTAs per SM are used when the
   // largest pair's histogram would not fit (e.g. 38-bin genes need ~110 KB).
@@ -681,8 +899,9 @@ static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const D
   if (auto_shape && cps == 1) threads = std::min(1024, A.max_threads_per_sm);
   if ((int64_t)SL.slot_off + 1024 > smem)
     return fail(TENEX_ERR_UNSUPPORTED,
-                "the staged target (%d B of shared memory for N = %d samples) leaves no room "
-                "for histograms in %d B; shorten the series", SL.slot_off, P.N, smem);
+                "the target block (%d B of shared memory: marginals for b_max = %d and %d "
+                "staged samples) leaves no room for histograms in %d B; coarsen the bins",
+                SL.slot_off, P.bmax, P.ztile, smem);
   L->threads = threads;
   L->smem = smem;
   L->grid = A.sm_count * cps;
@@ -697,7 +916,7 @@ static int64_t gmem_slot_count(int b_max, const DevAttr& A) {
   return std::max<int64_t>(1, std::min<int64_t>(A.sm_count, ((int64_t)1 << 30) / (words * 4)));
 }
 static int64_t gmem_bytes(int b_max, int N, int zbytes, const DevAttr& A) {
-  const SmemLayout SL = smem_layout(N, zbytes, b_max);
+  const SmemLayout SL = smem_layout(z_tile(N, zbytes), zbytes, b_max);
   const int smem = std::min(A.smem_per_sm - 1024, A.smem_optin) / 16 * 16;
   if (slot_fits(b_max, b_max, N, (int64_t)smem - SL.slot_off)) return 0;
   return round_up(gmem_slot_count(b_max, A) * (int64_t)b_max * b_max * b_max * 4, 256);
@@ -717,8 +936,9 @@ extern "C" int tenex_te_launch_shape(int64_t row_len, int64_t lag, int b_max,
   if (!threads || !ctas_per_sm || !smem_bytes || !src_chunk)
     return fail(TENEX_ERR_BADARG, "output pointers must be non-NULL");
   if (lag < 1 || row_len <= lag) return fail(TENEX_ERR_BADARG, "need 1 <= lag < row_len");
-  if (row_len - lag >= ((int64_t)1 << 24))
-    return fail(TENEX_ERR_UNSUPPORTED, "N = %lld samples per pair", (long long)(row_len - lag));
+  if (row_len >= ((int64_t)1 << 31))
+    return fail(TENEX_ERR_UNSUPPORTED, "row_len = %lld samples (must be < 2^31)",
+                (long long)row_len);
   if (b_max < 1 || b_max > 255) return fail(TENEX_ERR_BADARG, "b_max must be in 1..255");
   DevAttr A;
   int st = current_device_attr(&A);
@@ -727,6 +947,7 @@ extern "C" int tenex_te_launch_shape(int64_t row_len, int64_t lag, int b_max,
   P.N = (int)(row_len - lag);
   P.bmax = b_max;
   P.zbytes = b_max <= 16 ? 1 : 2;
+  P.ztile = z_tile(P.N, P.zbytes);
   const int64_t hb = P.N < 65536 ? (b_max + 1) / 2 : b_max;
   const int64_t worst_slot = round_up((int64_t)b_max * b_max * hb, 4) * 4;
   TeLaunch L{};
@@ -742,7 +963,7 @@ extern "C" size_t tenex_te_workspace_bytes(int n_vars, int64_t row_len, int b_ma
   if (n_vars < 1 || b_max < 1) return sizeof(WsHeader);
   size_t total = (size_t)ws_total(n_vars, b_max);
   DevAttr A;
-  if (row_len > 1 && row_len < ((int64_t)1 << 24) && current_device_attr(&A) == TENEX_OK)
+  if (row_len > 1 && row_len < ((int64_t)1 << 31) && current_device_attr(&A) == TENEX_OK)
     total += (size_t)gmem_bytes(b_max, (int)row_len, b_max <= 16 ? 1 : 2, A);
   return total;
 }
@@ -785,10 +1006,9 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   if (lag < 1 || row_len <= lag)
     return fail(TENEX_ERR_BADARG, "need 1 <= lag < row_len (lag=%lld, row_len=%lld)",
                 (long long)lag, (long long)row_len);
-  if (row_len - lag >= ((int64_t)1 << 24))
-    return fail(TENEX_ERR_UNSUPPORTED,
-                "N=%lld samples: float32 marginals are exact only below 2^24",
-                (long long)(row_len - lag));
+  if (row_len >= ((int64_t)1 << 31))
+    return fail(TENEX_ERR_UNSUPPORTED, "row_len=%lld: series must be shorter than 2^31",
+                (long long)row_len);
   if (ld < row_len || (ld % 16) != 0 || (reinterpret_cast<uintptr_t>(bins) % 16) != 0)
     return fail(TENEX_ERR_BADARG,
                 "bins rows must be 16-byte aligned with ld %% 16 == 0 and ld >= row_len "
@@ -852,6 +1072,12 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
                 (long long)P.n_items);
   P.bmax = b_max;
   P.zbytes = b_max <= 16 ? 1 : 2;
+  P.ztile = z_tile(P.N, P.zbytes);
+  P.big = P.N >= (1 << 24) ? 1 : 0;
+  {
+    const int lc = cfg ? cfg->lane_cells : 0;
+    P.lane_cells = lc < 0 ? 0 : (lc > 0 ? lc : default_lane_cells(P.N));
+  }
   P.out_mode = out_mode;
   P.out = out;
   P.out_ld = out_ld;
@@ -874,7 +1100,7 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   if (st) return st;
   P.smem_bytes = L.smem;
   // pairs whose histogram does not fit shared memory: global-memory overflow launch
-  const SmemLayout SLh = smem_layout(P.N, P.zbytes, P.bmax);
+  const SmemLayout SLh = smem_layout(P.ztile, P.zbytes, P.bmax);
   const bool overflow = !slot_fits(b_max, b_max, P.N, (int64_t)L.smem - SLh.slot_off);
   int64_t n_gslots = 0;
   if (overflow) {
@@ -1024,6 +1250,15 @@ int static_scratch(void** out) {
 }  // namespace
 }  // namespace tenex
 
+// Status word of a static-scratch call: 0 = inputs valid and every pair
+// computed; 1 = a bin value >= its gene's n_per_var or n_per_var outside
+// [1, b_max] (no TE computed); 3 = a work item's histogram did not fit shared
+// memory (its pairs were not computed).
+__global__ void static_status_kernel(const WsHeader* h, int32_t* status) {
+  const int bad = h->bad_data;
+  *status = bad != 0 ? bad : (h->bad_item != 0 ? 3 : 0);
+}
+
 extern "C" int tenex_te_pairfree_static(const uint8_t* bins, int64_t ld, const int32_t* n_per_var,
                                         int b_max, int n_vars, int64_t row_len, int64_t lag,
                                         int64_t pair_offset, int64_t n_pairs, float* out,
@@ -1038,13 +1273,32 @@ extern "C" int tenex_te_pairfree_static(const uint8_t* bins, int64_t ld, const i
                 "%zu bytes (about 4*n_vars + 512 must fit). Use tenex_te_pairfree "
                 "with a workspace instead.",
                 n_vars, b_max, (long long)need, kStaticScratchBytes);
+  if (lag >= 1 && row_len > lag && row_len < ((int64_t)1 << 31)) {
+    // pairs too large for shared memory (coarsening off) need global-memory
+    // histogram slots, far beyond the built-in area
+    DevAttr A;
+    const int st0 = current_device_attr(&A);
+    if (st0) return st0;
+    const int64_t ov = gmem_bytes(b_max, (int)(row_len - lag), b_max <= 16 ? 1 : 2, A);
+    if (ov > 0)
+      return fail(TENEX_ERR_UNSUPPORTED,
+                  "b_max=%d: pairs whose histogram does not fit shared memory need %lld bytes "
+                  "of global-memory histogram slots, which the built-in %zu-byte scratch area "
+                  "cannot hold; coarsen the bins, or call tenex_te_pairfree with a workspace of "
+                  "tenex_te_workspace_bytes() bytes",
+                  b_max, (long long)(need + ov), kStaticScratchBytes);
+  }
   void* ws = nullptr;
   int st = static_scratch(&ws);
   if (st) return st;
   st = tenex_te_pairfree(bins, ld, n_per_var, b_max, n_vars, row_len, lag, pair_offset, n_pairs,
                          out, out_mode, out_ld, ws, kStaticScratchBytes, cfg, stream);
   if (st || !status) return st;
-  cudaError_t e = cudaMemcpyAsync(status, static_cast<unsigned char*>(ws) + offsetof(WsHeader, bad_data),
-                                  sizeof(int32_t), cudaMemcpyDeviceToDevice, as_stream(stream));
-  return check_cuda(e, "status copy");
+  if (n_pairs == 0) {  // nothing ran: the area still holds an earlier call's words
+    return check_cuda(cudaMemsetAsync(status, 0, sizeof(int32_t), as_stream(stream)),
+                      "status reset");
+  }
+  static_status_kernel<<<1, 1, 0, as_stream(stream)>>>(reinterpret_cast<const WsHeader*>(ws),
+                                                       status);
+  return check_launch("static_status_kernel");
 }

@@ -73,4 +73,4 @@ def test_launch_shape_argument_checks():
     assert _status("tenex_te_launch_shape", 5, 5, 8, None, *refs) == bad         # lag >= row
     assert _status("tenex_te_launch_shape", 100, 1, 0, None, *refs) == bad       # b_max 0
     assert _status("tenex_te_launch_shape", 100, 1, 256, None, *refs) == bad     # b_max 256
-    assert _status("tenex_te_launch_shape", (1 << 24) + 1, 1, 8, None, *refs) == unsup
+    assert _status("tenex_te_launch_shape", 1 << 31, 1, 8, None, *refs) == unsup  # >= 2^31

@@ -41,15 +41,15 @@ def _regular(db, npv_t, bmax, dev):
     return out
 
 
-def _static(db, npv_t, bmax, dev):
+def _static(db, npv_t, bmax, dev, n_pairs=None, expect=0):
     n = db.n
     out = torch.zeros((n, n), dtype=torch.float32, device=dev)
     status = torch.full((1,), -1, dtype=torch.int32, device=dev)
     native.call("tenex_te_pairfree_static", db.data.data_ptr(), db.ld, npv_t.data_ptr(), bmax, n,
-                db.row_len, 1, 0, n * (n - 1), out.data_ptr(), native.OUT_MATRIX, n,
-                status.data_ptr(), None, native.stream_ptr())
+                db.row_len, 1, 0, n * (n - 1) if n_pairs is None else n_pairs, out.data_ptr(),
+                native.OUT_MATRIX, n, status.data_ptr(), None, native.stream_ptr())
     torch.cuda.synchronize(dev)
-    assert int(status.item()) == 0
+    assert int(status.item()) == expect
     return out
 
 
@@ -70,3 +70,32 @@ def test_static_scratch_rejects_oversized_problem(cuda):
                                                None, 0, 0, None, None, None)
     assert st == native.TENEX_ERR_UNSUPPORTED
     assert "scratch" in native.last_error()
+
+
+def test_static_status_after_invalid_and_empty_calls(cuda):
+    """The status word reports each call's own outcome: invalid bins (a bin value
+    >= its gene's n_per_var, caught by the device-side check without a fault)
+    give 1 and leave the output untouched; an empty pair range right after gives
+    0, not the previous call's word; a valid call after both matches the
+    oracle with status 0 (no flag of the failed call survives in the shared area)."""
+    bins, npv, bmax = _case(3, 20, 700, 9)
+    db = D.pack_bins(bins, cuda)
+    bad = np.asarray(npv, np.int32).copy()
+    bad[4] = max(1, int(bad[4]) - 1)
+    bad_t = torch.as_tensor(bad, dtype=torch.int32, device=cuda)
+    out = _static(db, bad_t, bmax, cuda, expect=1)
+    assert not bool(out.any())
+    _static(db, bad_t, bmax, cuda, n_pairs=0, expect=0)
+    npv_t = torch.as_tensor(npv, dtype=torch.int32, device=cuda)
+    good = _static(db, npv_t, bmax, cuda).cpu().numpy()
+    assert np.max(np.abs(good - O.te_matrix(bins, npv))) <= TOL
+
+
+def test_static_scratch_refuses_global_memory_overflow(cuda):
+    """Bins whose largest histograms need global-memory slots (coarsening off:
+    120 bins at 70,000 samples) are refused before any launch, with a message
+    that names the workspace entry point."""
+    st = native.lib().tenex_te_pairfree_static(None, 70016, None, 120, 4, 70000, 1, 0, 12,
+                                               None, 0, 0, None, None, None)
+    assert st == native.TENEX_ERR_UNSUPPORTED
+    assert "tenex_te_pairfree" in native.last_error()
