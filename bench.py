@@ -121,21 +121,40 @@ def profile_traffic():
     return None
 
 
-def cpu_baseline(bins, npv, b_max_c, seconds: float = 12.0, chunk: int = 20_000) -> dict:
-    """The CPU oracle on consecutive pair-id chunks until `seconds` elapsed."""
+def sample_pairs(n: int, count: int, seed: int) -> np.ndarray:
+    """A seed-fixed uniform sample (with replacement, then deduplicated and
+    sorted) of `count` ordered pairs of n genes as [target, source] rows."""
+    rng = np.random.default_rng(seed)
+    ids = np.unique(rng.integers(0, n * (n - 1), count, dtype=np.int64))
+    tgt = ids // (n - 1)
+    sl = ids - tgt * (n - 1)
+    return np.stack([tgt, sl + (sl >= tgt)], axis=1)
+
+
+def cpu_oracle_rate(bins, npv, seconds: float, seed: int, sample: int = 100_000,
+                    min_samples: int = 1) -> dict:
+    """The CPU oracle (C, exact integer counts, float64 TE, every host thread) on
+    seed-fixed uniform samples of `sample` ordered pairs, one sample after another
+    until `seconds` have elapsed (at least `min_samples`). The bins are converted
+    to the oracle's int32 rows once, outside the timed calls. Both the GPU arm's
+    cpu_baseline and the --impl reference arm time the CPU path through here."""
     from oracle import oracle as O
+    b = np.asarray(bins)
+    n = b.shape[0]
+    flat = np.ascontiguousarray(b.reshape(n, -1), dtype=np.int32)
+    npv = np.asarray(npv, np.int32)
     nthreads = os.cpu_count() or 1
-    done, t0 = 0, time.time()
-    n = bins.shape[0]
-    total = n * (n - 1)
-    while time.time() - t0 < seconds and done < total:
-        c = min(chunk, total - done)
-        O.te_pairfree(bins, npv, TAU, done, c, threads=nthreads)
-        done += c
-    dt = time.time() - t0
-    return {"value": done / dt, "unit": "pairs/s", "cores": nthreads, "kind": "port",
-            "sample": f"pair ids [0, {done}) of the same coarsened cfg4 bins "
-                      f"({dt:.1f} s on {nthreads} threads; C oracle, exact counts, float64 TE)"}
+    done, busy, k = 0, 0.0, 0
+    while k < min_samples or busy < seconds:
+        pairs = sample_pairs(n, sample, seed + k)
+        t0 = time.perf_counter()
+        O.te_pairs(flat, npv, pairs, TAU, threads=nthreads)
+        busy += time.perf_counter() - t0
+        done += len(pairs)
+        k += 1
+    return {"value": done / busy, "unit": "pairs/s", "cores": nthreads, "kind": "port",
+            "sample": f"{k} seed-fixed uniform samples of {sample} ordered pairs ({done} pairs, "
+                      f"{busy:.1f} s on {nthreads} threads; C oracle: exact counts, float64 TE)"}
 
 
 def run_reference(args) -> None:
@@ -145,23 +164,23 @@ def run_reference(args) -> None:
     from oracle import oracle as O
     x, npv = make_bins()
     cb, cnpv, bmax = O.coarsen(x, npv, 38)
-    nthreads = os.cpu_count() or 1
+    flat = np.ascontiguousarray(cb, dtype=np.int32)
     sample = args.ref_pairs
     for w in range(args.warmup):
-        O.te_pairfree(cb, cnpv, TAU, 0, min(sample, 20_000), threads=nthreads)
-    t0 = time.time()
-    for k in range(args.steps):
-        O.te_pairfree(cb, cnpv, TAU, (k * sample) % (N_GENES * (N_GENES - 1) - sample), sample,
-                      threads=nthreads)
-    dt = time.time() - t0
-    v = args.steps * sample / dt
+        cpu_oracle_rate(flat, cnpv, 0.0, seed=900 + w, sample=min(sample, 20_000))
+    rates = [cpu_oracle_rate(flat, cnpv, 0.0, seed=1000 + k, sample=sample)
+             for k in range(args.steps)]
+    busy = sum(sample / r["value"] for r in rates)
+    v = args.steps * sample / busy
     line = {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": busy / args.steps * 1e3,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "pairs_per_step": sample, "tau": TAU},
-            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": nthreads, "kind": "port",
-                             "sample": f"{sample} consecutive pair ids per step, C oracle"},
+            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": rates[0]["cores"],
+                             "kind": "port",
+                             "sample": f"per step a seed-fixed uniform sample of {sample} ordered "
+                                       f"pairs of the coarsened bins, C oracle"},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -219,8 +238,10 @@ def run_ours(args) -> None:
         kern.cfg = dict(threads=th, ctas_per_sm=cps, src_chunk=w)
     else:
         db0, npv0, bmax0 = step()
-        kern.cfg = autotune(db0, npv0, bmax0, TAU)
+        kern.cfg = dict(autotune(db0, npv0, bmax0, TAU))
         del db0, npv0
+    if args.lane_cells is not None:
+        kern.cfg["lane_cells"] = args.lane_cells
     bmax_run = None
     for _ in range(args.warmup):
         _, _, bmax_run = step()
@@ -320,11 +341,19 @@ def run_ours(args) -> None:
                     "frac": (compulsory / (te_ms / 1e3) / 1e9 / hbm_peak) if hbm_peak else None,
                     "note": "compulsory bytes (bins read once + float32 outputs) / launch time; "
                             "peak = MEASURED_PEAKS.json hbm_gbs (of measured)"}
-    cpu = (cpu_baseline(*_coarsened_host(x, npv, limit))
-           if (world == 1 and not args.no_cpu_baseline) else None)   # rank 0 at N=1 only
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:                      # rank 0 at N=1 only
+        cb, cnpv, _ = _coarsened_host(x, npv, limit)
+        cpu = cpu_oracle_rate(cb, cnpv, 10.0, seed=1000)
     sur = (surrogate_leg(dev, with_cpu=not args.no_cpu_baseline)
            if (world == 1 and not args.no_surrogate) else None)
     binl = binary_leg(dev) if (world == 1 and not args.no_surrogate) else None
+    c3 = (cfg3_leg(dev, peak_atomic, with_cpu=not args.no_cpu_baseline)
+          if (world == 1 and not args.no_configs) else None)
+    c1 = (cfg1_leg(dev, peak_atomic, with_cpu=not args.no_cpu_baseline)
+          if (world == 1 and not args.no_configs) else None)
+    refg = (reference_gpu_leg(dev) if (world == 1 and not args.no_reference_gpu
+                                        and total == G * (G - 1)) else None)
     fdrl = fdr_leg(dev, out) if (world == 1 and not args.no_fdr and total == G * (G - 1)) else None
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -340,10 +369,145 @@ def run_ours(args) -> None:
             "gpu_launches": 6 * args.steps,  # remap, coarsen x2, prepass, order, TE tile
             "roofline": roofline, "roofline_hbm": roofline_hbm,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "surrogate": sur,
-            "binary_path": binl, "fdr": fdrl}
+            "binary_path": binl, "fdr": fdrl, "cfg3": c3, "cfg1": c1,
+            "reference_gpu": refg}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def _te_device_ms(kern, db, npv_t, bmax, reps: int = 3) -> float:
+    """Median device time (CUDA events on the launching stream) of one all-pairs
+    TE matrix launch from resident bins, after two warm-up launches."""
+    import torch
+    out = torch.zeros((db.n, db.n), dtype=torch.float32, device=db.data.device)
+    for _ in range(2):
+        kern.compute_pairfree_device(db, npv_t, bmax, TAU, matrix=True, out=out)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(reps)]
+    s = torch.cuda.current_stream()
+    for a, b in ev:
+        a.record(s)
+        kern.compute_pairfree_device(db, npv_t, bmax, TAU, matrix=True, out=out)
+        b.record(s)
+    torch.cuda.synchronize()
+    return statistics.median(a.elapsed_time(b) for a, b in ev)
+
+
+def _smem_roofline(pairs: int, N: int, ms: float, peak: float) -> dict:
+    achieved = pairs * N / (ms / 1e3)
+    return {"bound": "smem_atomic", "achieved": achieved / 1e9, "peak": peak / 1e9,
+            "unit": "Gincr/s", "frac": achieved / peak,
+            "note": "pairs x (T - tau) histogram increments / device time of the TE launch; "
+                    "peak = conflict-free shared-memory atomic probe (tenex_probe_smem_atomics "
+                    "mode 0) measured live"}
+
+
+def cfg3_leg(dev, peak: float, with_cpu: bool = True) -> dict:
+    """5,000 genes x 10,000 cells, b ~ U{2..32} (Full-SMEM, all 24,995,000 pairs
+    in one persistent launch): device time from resident bins against the
+    shared-memory atomic probe, end to end through FullSMEMKernel from pinned host
+    bins to a pinned host matrix, and the CPU oracle on a uniform pair sample."""
+    import torch
+
+    from tenex_b200 import workloads as W
+    from tenex_b200.kernels import device as D
+    from tenex_b200.kernels.full_smem import FullSMEMKernel
+    x, npv = W.cfg3_bins()
+    bins = np.ascontiguousarray(x, dtype=np.uint8)
+    n, T = bins.shape
+    bmax = int(npv.max())
+    kern = FullSMEMKernel()
+    db = D.pack_bins(bins, dev)
+    npv_t = torch.as_tensor(npv, dtype=torch.int32, device=dev)
+    ms = _te_device_ms(kern, db, npv_t, bmax)
+    pairs = n * (n - 1)
+    # end to end: pinned host bins -> padded device rows -> TE matrix -> pinned host matrix
+    x_pin = torch.from_numpy(bins).pin_memory()
+    out_pin = torch.empty((n, n), dtype=torch.float32).pin_memory()
+    npv_pin = torch.from_numpy(np.asarray(npv, np.int32)).pin_memory()
+    s = torch.cuda.current_stream()
+
+    def e2e_step():
+        d = D.empty_bins(n, T, 1, dev)
+        d.data[:, :T].copy_(x_pin, non_blocking=True)
+        nd = npv_pin.to(dev, non_blocking=True)
+        m = kern.compute_pairfree_device(d, nd, bmax, TAU, matrix=True)
+        out_pin.copy_(m, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(2):
+        e2e_step()
+    b.record(s)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b) / 2
+    return {"workload": "cfg3: 5000 genes x 10000 cells, b~U{2..32} Dirichlet(1), 5% AR lag-1 "
+                        "(Full-SMEM, all 24,995,000 ordered pairs)",
+            "pairs_per_s": pairs / (ms / 1e3), "ms": ms,
+            "roofline": _smem_roofline(pairs, T - TAU, ms, peak),
+            "e2e": {"value": pairs / (e2e_ms / 1e3), "unit": "pairs/s",
+                    "h2d_bytes_per_step": int(bins.nbytes + npv_pin.numel() * 4),
+                    "d2h_bytes_per_step": int(n * n * 4),
+                    "path": "FullSMEMKernel: pinned host bins -> padded device rows -> "
+                            "compute_pairfree_device -> pinned host matrix"},
+            "cpu_baseline": cpu_oracle_rate(bins, npv, 5.0, seed=3000) if with_cpu else None}
+
+
+def cfg1_leg(dev, peak: float, with_cpu: bool = True, reps: int = 5) -> dict:
+    """100 genes x 1,000 cells of expression (float32 log1p of zero-inflated NB
+    counts) through TransferEntropyEngine.compute(accelerator="gpu"): wall seconds
+    of the whole call (host matrix in, host TE matrix out: FSBW-L, remap, kernel
+    choice, all 9,900 pairs) with a new engine per call, the TE launch's device
+    time, and the CPU oracle on the same path (FSBW-L, remap, all pairs)."""
+    import torch
+
+    from tenex_b200 import TransferEntropyEngine, workloads as W
+    from tenex_b200.kernels import device as D
+    from tenex_b200.kernels.full_smem import FullSMEMKernel
+    from oracle import oracle as O
+    x, _ = W.cfg1_expression()
+    n, T = x.shape
+    names = np.array([f"g{i}" for i in range(n)])
+    ts, res = [], None
+    for _ in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = TransferEntropyEngine(x, names).compute(accelerator="gpu", devices=[dev.index or 0])
+        ts.append(time.perf_counter() - t0)
+    wall = statistics.median(ts[1:])
+    bins = res.bin_arrs[:, :, 0].astype(np.uint8)
+    npv = res.n_per_var
+    db = D.pack_bins(bins, dev)
+    ms = _te_device_ms(FullSMEMKernel(), db, torch.as_tensor(npv, device=dev), int(npv.max()))
+    pairs = n * (n - 1)
+    cpu = None
+    if with_cpu:
+        nthreads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        k = 0
+        while k < 3 or time.perf_counter() - t0 < 2.0:
+            rb, _ = O.fsbwl(x, 0.5)
+            cb, cnpv, _ = O.remap(rb)
+            O.te_pairfree(cb, cnpv, TAU, threads=nthreads)
+            k += 1
+        dt = (time.perf_counter() - t0) / k
+        cpu = {"value": pairs / dt, "unit": "pairs/s", "cores": nthreads, "kind": "port",
+               "sample": f"the whole 9,900-pair matrix from the float32 data (FSBW-L, remap, "
+                         f"TE), {k} runs, {dt * 1e3:.1f} ms each; C oracle"}
+    return {"workload": "cfg1: 100 genes x 1000 cells expression, FSBW-L, Full-SMEM "
+                        "(9,900 ordered pairs)",
+            "metric": "TransferEntropyEngine.compute(accelerator='gpu') wall seconds from the "
+                      "host matrix (median of %d after a warm-up call)" % reps,
+            "seconds": wall, "pairs_per_s": pairs / wall, "te_kernel_ms": ms,
+            "roofline": _smem_roofline(pairs, T - TAU, ms, peak),
+            "e2e": {"value": pairs / wall, "unit": "pairs/s", "h2d_bytes_per_step": int(x.nbytes),
+                    "d2h_bytes_per_step": int(n * n * 4),
+                    "path": "TransferEntropyEngine(x, names).compute(accelerator='gpu')"},
+            "kernel": res.kernel, "cpu_baseline": cpu}
 
 
 def surrogate_leg(dev, reps: int = 3, with_cpu: bool = True) -> dict:
@@ -525,6 +689,128 @@ def fdr_leg(dev, mat, reps: int = 2) -> dict:
                                  "time; peak = tenex_probe_minmax measured live"}}
 
 
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def _reference_gpu_worker(path: str) -> None:
+    """Runs in a separate process with only the installed reference importable
+    (nothing of this repository is imported): times the reference's own GPU
+    wrappers on the workloads saved in `path` and prints one JSON object.
+    Device time = CUDA events around the wrapper call (the wrappers also copy
+    their float32 result to the host, which is included)."""
+    import torch
+    sys.path.insert(0, REF_DIR)
+    import tenex
+    from tenex.kernels.adaptive_smem import compute_te_adaptive_smem_pairfree
+    from tenex.kernels.full_smem import compute_te_smem_pairfree
+    from tenex.kernels.gemm_b2 import compute_te_gemm_b2
+    dev = torch.device("cuda", 0)
+    d = np.load(path)
+
+    def timed(fn, reps=2):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return min(ts)
+
+    out = {"reference": os.path.dirname(tenex.__file__)}
+    # cfg4 slice: Adaptive-SMEM pair-free on the coarsened bins (int8)
+    b4 = torch.from_numpy(d["cfg4_bins"].astype(np.int8)[:, :, None]).to(dev)
+    n4 = torch.from_numpy(d["cfg4_npv"].astype(np.int32)).to(dev)
+    n = b4.shape[0]
+    p0, cnt = int(d["cfg4_p0"]), int(d["cfg4_pairs"])
+    ms = timed(lambda: compute_te_adaptive_smem_pairfree(b4, n4, n, 1, p0, cnt))
+    out["cfg4"] = {"entry": "tenex.kernels.adaptive_smem.compute_te_adaptive_smem_pairfree",
+                   "pairs": cnt, "ms": ms, "pairs_per_s": cnt / (ms / 1e3),
+                   "sample": f"pair ids [{p0}, {p0 + cnt}) of the coarsened 10,000 x 20,000 bins"}
+    del b4, n4
+    # cfg3: Full-SMEM pair-free, all pairs (int32 bins as its wrapper expects)
+    b3 = torch.from_numpy(d["cfg3_bins"].astype(np.int32)[:, :, None]).to(dev)
+    n3 = b3.shape[0]
+    bm3 = int(d["cfg3_npv"].max())
+    ms = timed(lambda: compute_te_smem_pairfree(b3, bm3, n3, 1), reps=1)
+    out["cfg3"] = {"entry": "tenex.kernels.full_smem.compute_te_smem_pairfree",
+                   "pairs": n3 * (n3 - 1), "ms": ms, "pairs_per_s": n3 * (n3 - 1) / (ms / 1e3)}
+    del b3
+    # cfg2: GEMM-B2 (torch.mm + Triton epilogue)
+    x2 = d["cfg2_bins"].astype(np.int32)
+    n2 = x2.shape[0]
+    ms = timed(lambda: compute_te_gemm_b2(x2, tau=1, device=dev), reps=3)
+    out["cfg2"] = {"entry": "tenex.kernels.gemm_b2.compute_te_gemm_b2 (torch.mm + Triton)",
+                   "pairs": n2 * (n2 - 1), "ms": ms, "pairs_per_s": n2 * (n2 - 1) / (ms / 1e3),
+                   "note": "from host bins to a host matrix, as the wrapper is called"}
+    # cfg5: SurrogateTestMethod.infer, 100 block shuffles on the GPU
+    from tenex.inference.surrogate_test import SurrogateTestMethod
+    x5 = d["cfg5_bins"].astype(np.int32)
+    npv5 = d["cfg5_npv"].astype(np.int32)
+    obs = d["cfg5_obs"]
+    names = np.array([f"g{i}" for i in range(x5.shape[0])])
+    kw = dict(bin_data=x5[:, :, None], n_per_var=npv5, b_max=int(npv5.max()), kernel="Full-SMEM",
+              tau=1, n_surrogates=100, block_length=50, fdr=0.05, seed=42)
+    m = SurrogateTestMethod()
+    m.infer(obs, names, dev, **dict(kw, n_surrogates=2))       # warm-up (compile, load)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = m.infer(obs, names, dev, **kw)
+    torch.cuda.synchronize()
+    out["cfg5"] = {"entry": "tenex.inference.surrogate_test.SurrogateTestMethod.infer "
+                            "(kernel='Full-SMEM', 100 block shuffles)",
+                   "seconds": time.perf_counter() - t0, "n_edges": int(len(r.grn))}
+    print(json.dumps(out), flush=True)
+
+
+def reference_gpu_leg(dev, timeout_s: int = 900) -> dict | None:
+    """The reference's own CUDA kernels timed on this GPU (context, not the
+    driver's reference arm): cfg4 on a 4M-pair slice, cfg3 and cfg2 whole, the
+    cfg5 surrogate test whole, each through the reference's Python wrapper, in a
+    child process that imports only the reference installed under baseline/_ref."""
+    import subprocess
+    import tempfile
+
+    import torch
+
+    from tenex_b200 import workloads as W
+    from tenex_b200.kernels import device as D
+    from tenex_b200.kernels.full_smem import FullSMEMKernel
+    from oracle import oracle as O
+    if not os.path.isdir(os.path.join(REF_DIR, "tenex")):
+        return {"unavailable": "the reference is not installed under baseline/_ref"}
+    x4, npv4 = make_bins()
+    cb, cnpv, _ = O.coarsen(x4, npv4, 38)
+    n4 = cb.shape[0]
+    x3, npv3 = W.cfg3_bins()
+    x2, _ = W.cfg2_binary()
+    x5, npv5, _ = W.cfg5_bins(seed=1005)
+    obs = FullSMEMKernel().compute_pairfree_device(
+        D.pack_bins(x5, dev), torch.as_tensor(npv5, device=dev), int(npv5.max()), 1,
+        matrix=True).cpu().numpy()
+    mid = (n4 * (n4 - 1) // 2) // (n4 - 1) * (n4 - 1)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "ref_gpu_inputs.npz")
+        np.savez(path, cfg4_bins=cb.astype(np.uint8), cfg4_npv=cnpv, cfg4_p0=mid,
+                 cfg4_pairs=4_000_000, cfg3_bins=x3, cfg3_npv=npv3, cfg2_bins=x2,
+                 cfg5_bins=x5, cfg5_npv=npv5, cfg5_obs=obs)
+        env = dict(os.environ, PYTHONPATH=REF_DIR)
+        try:
+            r = subprocess.run([sys.executable, os.path.abspath(__file__),
+                                "--reference-gpu-worker", path], capture_output=True, text=True,
+                               timeout=timeout_s, env=env, cwd=tmp)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": f"the reference's GPU run exceeded {timeout_s} s"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"unavailable": f"reference GPU worker exit {r.returncode}: "
+                               f"{(r.stderr or r.stdout)[-400:]}"}
+    return json.loads(lines[-1])
+
+
 def _coarsened_host(x, npv, limit):
     from oracle import oracle as O
     cb, cnpv, bmax = O.coarsen(x, npv, limit)
@@ -542,20 +828,42 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--no-fdr", action="store_true")
-    ap.add_argument("--only", choices=["binary", "surrogate", "fdr"], default=None,
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the cfg1 / cfg3 objects of the line")
+    ap.add_argument("--only", choices=["binary", "surrogate", "fdr", "cfg1", "cfg3",
+                                       "reference_gpu"],
+                    default=None,
                     help="run one side leg alone and print its JSON object (profiling)")
     ap.add_argument("--genes", type=int, default=N_GENES)
     ap.add_argument("--cells", type=int, default=N_CELLS)
     ap.add_argument("--pairs", type=int, default=None)
     ap.add_argument("--launch", default=None)
+    ap.add_argument("--reference-gpu-worker", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference_gpu object (the reference's CUDA kernels)")
+    ap.add_argument("--lane-cells", type=int, default=None,
+                    help="cell limit of the lane-private histogram tables (-1: none)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.reference_gpu_worker:
+        _reference_gpu_worker(args.reference_gpu_worker)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.only == "binary":
         import torch
         print(json.dumps(binary_leg(torch.device("cuda", 0))), flush=True)
+    elif args.only == "reference_gpu":
+        import torch
+        print(json.dumps(reference_gpu_leg(torch.device("cuda", 0))), flush=True)
+    elif args.only in ("cfg1", "cfg3"):
+        import torch
+
+        from tenex_b200 import native
+        dev = torch.device("cuda", 0)
+        peak = max(native.probe_smem_atomics(0, 8192) for _ in range(3))
+        leg = cfg1_leg if args.only == "cfg1" else cfg3_leg
+        print(json.dumps(leg(dev, peak, with_cpu=not args.no_cpu_baseline)), flush=True)
     elif args.only == "surrogate":
         import torch
         print(json.dumps(surrogate_leg(torch.device("cuda", 0))), flush=True)
