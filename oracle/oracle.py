@@ -7,6 +7,9 @@ Contents (reference file:line relative to the reference project):
   fsbwl(x, kp)                 tenex/preprocess.py:61-88 + :680 clamp
   remap(bins)                  tenex/preprocess.py:401-459
   coarsen(bins, npv, limit)    tenex/preprocess.py:462-551
+  binarize(x, method, q)       tenex/binarize.py:45-150 with the default numpy backend
+                               (1[x > thr]; median = np.median, quantile = np.quantile
+                               "linear" (Hyndman-Fan type 7), restated from a sort)
   counts(bins, lag, t, s, npv) tenex/kernels/scatter_add.py:63-90
   te_pairfree / te_pairs       tenex/csrc/full_smem.cu:113-141 in float64
   te_matrix                    pair-free output assembled as
@@ -127,6 +130,45 @@ def smem_bin_limit(smem_optin: int, warps: int = 32) -> int:
     while B > 2 and (B ** 3 + 2 * B ** 2 + B + warps) * 4 > smem_optin:
         B -= 1
     return B
+
+
+def binarize_thresholds(x: np.ndarray, method: str, q: float = 0.5) -> np.ndarray:
+    """Per-row thresholds of the reference's numpy binarizers, restated from a
+    sorted copy: median -> the middle value, or (a + b) / 2 of the two middle
+    values with a + b in float32 (np.median's mean); quantile -> numpy's linear
+    method, virtual index (T - 1) q in float64, lerp of the neighbours a, b with
+    diff = b - a in float32 and gamma in float64: a + diff * gamma, or
+    b - diff * (1 - gamma) when gamma >= 0.5, in float64. mean -> float32
+    pairwise mean as np.mean; nonzero -> 0."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    n, T = x.shape
+    if method == "nonzero":
+        return np.zeros(n, np.float32)
+    if method == "mean":
+        return x.mean(axis=1)
+    s = np.sort(x, axis=1)
+    if method == "median":
+        h = T // 2
+        if T % 2:
+            return s[:, h].copy()
+        return ((s[:, h - 1] + s[:, h]).astype(np.float64) / 2).astype(np.float32)
+    vi = (T - 1) * float(q)
+    if vi >= T - 1:
+        return s[:, T - 1].astype(np.float64)
+    lo = int(np.floor(vi))
+    g = vi - lo
+    a, b = s[:, lo], s[:, lo + 1]
+    diff = (b - a).astype(np.float64)
+    if g >= 0.5:
+        return b.astype(np.float64) - diff * (1.0 - g)
+    return a.astype(np.float64) + diff * g
+
+
+def binarize(x: np.ndarray, method: str, q: float = 0.5) -> np.ndarray:
+    """uint8 1[x > thr] per row (the comparison in the threshold's precision)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    thr = binarize_thresholds(x, method, 0.5 if method == "median" else q)
+    return (x > thr[:, None]).astype(np.uint8)
 
 
 # ---------------------------------------------------------------- counts / TE

@@ -25,8 +25,10 @@ product to the reference's own CPU code paths:
 
   coarsen_wide.npz      tenex.preprocess.remap_bins + _compact_dtype (int16) +
                         coarsen_bins on genes with 257, 300 and 1000 distinct bins
+  binarize.npz          tenex.binarize.binarize (numpy backend): median, quantile
+                        q = 0.7 / 0.25, mean and nonzero at T = 400 and 401
 
-`python tests/golden/make_golden.py /path/to/reference multilag` (or `fdr`, `wide`)
+`python tests/golden/make_golden.py /path/to/reference multilag` (or `fdr`, `wide`, `binarize`)
 writes only that one.
 """
 from __future__ import annotations
@@ -172,6 +174,30 @@ def wide(ref: str) -> None:
     print("coarsen_wide.npz written to", HERE)
 
 
+def binarized(ref: str) -> None:
+    """tenex.binarize.binarize with its default numpy backend (np.median and
+    np.quantile thresholds) on expression matrices with many ties (zeros), at an
+    even and an odd number of time points."""
+    sys.path.insert(0, ref)
+    sys.path.insert(0, REPO)
+    os.environ.setdefault("TENEX_CPU_ONLY", "1")
+    import torch
+    from tenex.binarize import binarize
+    from tenex_b200 import workloads as W
+    out = {}
+    for T in (400, 401):
+        x, _ = W.cfg1_expression(n=50, T=T, seed=8)
+        out[f"x{T}"] = x
+        for tag, method, params in (("median", "median", {}), ("q70", "quantile", {"q": 0.7}),
+                                    ("q25", "quantile", {"q": 0.25}),
+                                    ("mean", "mean", {}), ("nonzero", "nonzero", {})):
+            b, _, _, npv = binarize(x, method=method, device=torch.device("cpu"), **params)
+            out[f"{tag}{T}"] = b.numpy()[:, :, 0].astype(np.uint8)
+            out[f"{tag}{T}_npv"] = npv.numpy()
+    np.savez_compressed(os.path.join(HERE, "binarize.npz"), **out)
+    print("binarize.npz written to", HERE)
+
+
 def multilag(ref: str) -> None:
     """The reference's multi-lag combine on synthetic per-lag surrogate results."""
     sys.path.insert(0, ref)
@@ -272,7 +298,7 @@ def fdr(ref: str) -> None:
 
 if __name__ == "__main__":
     if len(sys.argv) < 2:
-        sys.exit("usage: make_golden.py REFERENCE_SOURCE_TREE [multilag|fdr|wide]")
+        sys.exit("usage: make_golden.py REFERENCE_SOURCE_TREE [multilag|fdr|wide|binarize]")
     ref_dir = sys.argv[1]
     only = sys.argv[2] if len(sys.argv) > 2 else None
     if only == "multilag":
@@ -281,8 +307,11 @@ if __name__ == "__main__":
         fdr(ref_dir)
     elif only == "wide":
         wide(ref_dir)
+    elif only == "binarize":
+        binarized(ref_dir)
     else:
         main(ref_dir)
         multilag(ref_dir)
         fdr(ref_dir)
         wide(ref_dir)
+        binarized(ref_dir)

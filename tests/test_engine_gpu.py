@@ -133,20 +133,24 @@ def test_adaptive_no_coarsening_uses_overflow(cuda):
                   smem_optin=232448)
 
 
-@pytest.mark.parametrize("method", ["nonzero", "mean", "median", "quantile"])
-def test_binarization_routes_to_gemm_b2(cuda, method):
-    x, _ = W.cfg1_expression(n=50, T=400, seed=3)
-    names = np.array([f"g{i}" for i in range(50)])
-    res = TransferEntropyEngine(x, names).compute(accelerator="gpu", binarization=method,
-                                                  binarization_kwargs={"q": 0.7}
-                                                  if method == "quantile" else None)
+@pytest.mark.parametrize("T", [400, 401])
+@pytest.mark.parametrize("method,q,tag", [("nonzero", None, "nonzero"), ("mean", None, "mean"),
+                                          ("median", None, "median"), ("quantile", 0.7, "q70"),
+                                          ("quantile", 0.25, "q25")])
+def test_binarization_routes_to_gemm_b2(cuda, golden, method, q, tag, T):
+    """Bins bit-equal to the reference's binarize (numpy backend, its default) on
+    expression data with many ties, at an even and an odd series length; the
+    binary matrix goes through GEMM-B2 and matches the oracle."""
+    g = golden("binarize.npz")
+    x = g[f"x{T}"]
+    names = np.array([f"g{i}" for i in range(x.shape[0])])
+    res = TransferEntropyEngine(x, names).compute(
+        accelerator="gpu", binarization=method,
+        binarization_kwargs={"q": q} if q is not None else None)
     assert res.kernel == "GEMM-B2"
-    b = res.bin_arrs[:, :, 0].astype(np.int32)
-    if method == "nonzero":
-        assert np.array_equal(b, (x > 0).astype(np.int32))
-    elif method == "mean":
-        assert np.array_equal(b, (x > x.mean(axis=1, keepdims=True)).astype(np.int32))
-    ref = O.te_matrix(b, np.full(50, 2, np.int32))
+    b = res.bin_arrs[:, :, 0].astype(np.uint8)
+    assert np.array_equal(b, g[f"{tag}{T}"])
+    ref = O.te_matrix(b, np.full(x.shape[0], 2, np.int32))
     assert np.max(np.abs(res.matrix - ref)) <= TOL
 
 

@@ -90,3 +90,13 @@ def test_surrogate_stats_match_reference_loop(golden):
     std = np.sqrt(np.maximum(ss / S - (s / S) ** 2, 0.0)).astype(np.float32)
     assert np.max(np.abs(mean - g["mean"])) < 1e-6
     assert np.max(np.abs(std - g["std"])) < 2e-6
+
+
+def test_binarize_thresholds_match_reference_numpy_backend(golden):
+    g = golden("binarize.npz")
+    for T in (400, 401):
+        x = g[f"x{T}"]
+        for tag, method, q in (("median", "median", 0.5), ("q70", "quantile", 0.7),
+                               ("q25", "quantile", 0.25), ("mean", "mean", 0.5),
+                               ("nonzero", "nonzero", 0.5)):
+            assert np.array_equal(O.binarize(x, method, q), g[f"{tag}{T}"]), (tag, T)
