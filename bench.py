@@ -587,8 +587,9 @@ def surrogate_cpu_baseline(x, npv, S: int, bl: int, seed: int, dev, n_pairs: int
 
 def binary_leg(dev, reps: int = 5) -> dict:
     """cfg2 binary path (2,000 genes x 5,000 cells, GEMM-B2 on tcgen05): device time of
-    one full TE matrix (pack kernel + INT8 GEMM with the TE epilogue), against the
-    live INT8 tensor-pipe probe."""
+    one full TE matrix (pack kernel + GEMM with the TE epilogue) for the default
+    4-bit operand form (kind::mxf4) against the live 4-bit tensor-pipe probe, and
+    the int8 form (kind::i8) against the live INT8 probe."""
     import torch
 
     from tenex_b200 import native, workloads as W
@@ -598,29 +599,37 @@ def binary_leg(dev, reps: int = 5) -> dict:
     n, T = x.shape
     db = D.pack_bins(x, dev)
     out = torch.zeros((n, n), dtype=torch.float32, device=dev)
-    for _ in range(3):
-        te_binary_matrix(db, 1, out=out)
-    torch.cuda.synchronize(dev)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(reps)]
-    for a, b in ev:
-        a.record()
-        te_binary_matrix(db, 1, out=out, check=False)
-        b.record()
-    torch.cuda.synchronize(dev)
-    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
     L = T - 1
-    Lpad = -(-L // 128) * 128
     tiles = -(-n // 128)
-    ops = 6.0 * (tiles * 128) ** 2 * Lpad          # 3 int8 GEMMs of (n x Lpad) x (Lpad x n)
-    peak = max(native.probe_tc_int8(100_000) for _ in range(2))
+    forms = {}
+    for form, kpad, probe in (("fp4", 256, native.probe_tc_fp4), ("int8", 128, native.probe_tc_int8)):
+        for _ in range(3):
+            te_binary_matrix(db, 1, out=out, operands=form)
+        torch.cuda.synchronize(dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(reps)]
+        for a, b in ev:
+            a.record()
+            te_binary_matrix(db, 1, out=out, check=False, operands=form)
+            b.record()
+        torch.cuda.synchronize(dev)
+        ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+        Lpad = -(-L // kpad) * kpad
+        ops = 6.0 * (tiles * 128) ** 2 * Lpad      # 3 GEMMs of (n x Lpad) x (Lpad x n)
+        peak = max(probe(100_000) for _ in range(2))
+        forms[form] = {"ms": ms, "pairs_per_s": n * (n - 1) / (ms / 1e3),
+                       "roofline": {"bound": "tensor", "achieved": ops / (ms / 1e3) / 1e12,
+                                    "peak": peak / 1e12,
+                                    "unit": "TOP/s (%s)" % ("e2m1" if form == "fp4" else "int8"),
+                                    "frac": ops / (ms / 1e3) / peak,
+                                    "note": "achieved = 6*n_pad^2*L_pad ops (C, D, E) / device "
+                                            "time of pack + GEMM; peak = the live %s probe"
+                                            % ("tenex_probe_tc_fp4" if form == "fp4"
+                                               else "tenex_probe_tc_int8")}}
+    d = forms["fp4"]
     return {"workload": "cfg2: 2000 genes x 5000 cells, binary Markov bins, GEMM-B2",
-            "pairs_per_s": n * (n - 1) / (ms / 1e3), "ms": ms,
-            "roofline": {"bound": "tensor", "achieved": ops / (ms / 1e3) / 1e12,
-                         "peak": peak / 1e12, "unit": "TOP/s (int8)",
-                         "frac": ops / (ms / 1e3) / peak,
-                         "note": "achieved = 6*n_pad^2*L_pad int8 ops (C, D, E) / device time of "
-                                 "pack + GEMM; peak = tenex_probe_tc_int8 measured live"}}
+            "pairs_per_s": d["pairs_per_s"], "ms": d["ms"], "operands": "fp4 (kind::mxf4)",
+            "roofline": d["roofline"], "int8_form": forms["int8"]}
 
 
 def fdr_leg(dev, mat, reps: int = 2) -> dict:

@@ -257,6 +257,13 @@ size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t lag);
 int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
                            int64_t lag, float* out, int64_t out_ld, void* workspace,
                            size_t workspace_bytes, void* stream);
+/* Same with the operand form chosen: kind 1 = int8 operands (tcgen05 kind::i8,
+ * int32 sums), 2 = packed 4-bit operands (kind::mxf4: the 0/1 values as E2M1,
+ * two per byte, unit block scales, float32 sums, exact below 2^24), 0 = the
+ * default (2). Both give the same counts and TE. */
+int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
+                                int64_t lag, float* out, int64_t out_ld, void* workspace,
+                                size_t workspace_bytes, int kind, void* stream);
 /* Error word of the last tenex_te_binary_matrix call on this workspace
  * (synchronises `stream`): TENEX_ERR_BADDATA if a bin was not 0 or 1,
  * TENEX_ERR_TIMEOUT if a pipeline wait expired. */
@@ -335,6 +342,10 @@ int tenex_probe_smem_atomics(int mode, int iters, int64_t* increments, float* ms
  * into TMEM; returns the operation count (2*M*N*K per MMA) and the milliseconds.
  * Synchronises `stream`; TENEX_ERR_TIMEOUT if the bounded completion wait expired. */
 int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stream);
+/* Roofline probe (no reference counterpart): dense 4-bit (kind::mxf4, packed E2M1
+ * with unit UE8M0 block scales) tensor-pipe rate, M=128, N=256, K=64 per MMA, the
+ * denominator of the 4-bit GEMM-B2 form; same conventions as tenex_probe_tc_int8. */
+int tenex_probe_tc_fp4(int iters, double* ops, float* ms, void* stream);
 /* Roofline probe (no reference counterpart): FP32 min/max issue rate, the bound of
  * tenex_dpi_trim. Every thread of 2 CTAs x 1024 threads per SM runs `iters` steps
  * of 8 independent chains (two min.f32 and one three-input max.f32 each); returns

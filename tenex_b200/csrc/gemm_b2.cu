@@ -172,15 +172,111 @@ b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int l
   if (__any_sync(0xffffffffu, high != 0) && lane == 0) atomicExch(err, 2);
 }
 
+// 4-bit form of the pack: F, FP and P as packed E2M1 values (1.0 = 0x2, 0.0 =
+// 0x0; sample 2k in the low nibble of byte k, 2k + 1 in the high one), rows of
+// Lpad / 2 bytes (Lpad a multiple of 256: whole 128-byte TMA boxes), the same
+// per-gene counts and the same 0/1 check. Each lane makes 16 bytes of each
+// operand from 32 samples: two aligned 16-byte loads of P and a 48-byte aligned
+// window of F.
+__device__ __forceinline__ uint32_t e2m1_nibbles(uint32_t w) {
+  // four 0/1 bytes b0..b3 -> 16 bits: 2*b0 | 2*b1 << 4 | 2*b2 << 8 | 2*b3 << 12
+  const uint32_t t = (w | (w >> 4)) & 0x00ff00ffu;
+  return __byte_perm(t, 0, 0x4420) << 1;
+}
+
+__global__ void __launch_bounds__(kPackWarps * 32)
+b2_pack4_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int lag, int Lpad,
+                uint8_t* __restrict__ ops, int32_t* __restrict__ marg, int* __restrict__ err) {
+  const int g = blockIdx.x * kPackWarps + (threadIdx.x >> 5);
+  if (g >= n) return;  // whole warps only: the shuffles below see full warps
+  const int lane = threadIdx.x & 31;
+  const int64_t rowb = Lpad / 2;
+  const uint8_t* row = bins + (int64_t)g * ld;
+  uint8_t* Fr = ops + (int64_t)g * rowb;
+  uint8_t* FPr = ops + ((int64_t)n + g) * rowb;
+  uint8_t* Pr = ops + (2 * (int64_t)n + g) * rowb;
+  int nf = 0, np = 0, nfp = 0;
+  uint32_t high = 0;
+  for (int t = lane * 32; t < Lpad; t += 32 * 32) {
+    uint32_t f[8], p[8];
+    const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;
+    if (t + 32 <= L && fa + 48 <= ld) {
+      const uint4 p0 = *reinterpret_cast<const uint4*>(row + t);
+      const uint4 p1 = *reinterpret_cast<const uint4*>(row + t + 16);
+      const uint4 a0 = *reinterpret_cast<const uint4*>(row + fa);
+      const uint4 a1 = *reinterpret_cast<const uint4*>(row + fa + 16);
+      const uint4 a2 = *reinterpret_cast<const uint4*>(row + fa + 32);
+      const uint32_t w[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
+                              a2.x, a2.y, a2.z, a2.w};
+      const uint32_t pw[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+      const int sh = (int)((t + lag) - fa);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int byte = sh + 4 * k;
+        f[k] = __funnelshift_r(w[byte >> 2], w[(byte >> 2) + 1], (byte & 3) * 8);
+        p[k] = pw[k];
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        uint32_t fk = 0, pk = 0;
+        for (int j = 0; j < 4; ++j) {
+          const int tt = t + 4 * k + j;
+          if (tt < L) {
+            fk |= (uint32_t)row[tt + lag] << (8 * j);
+            pk |= (uint32_t)row[tt] << (8 * j);
+          }
+        }
+        f[k] = fk;
+        p[k] = pk;
+      }
+    }
+    uint32_t of[4], ofp[4], op[4];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      high |= (f[k] | p[k]) & 0xfefefefeu;
+      nf += __popc(f[k]);
+      np += __popc(p[k]);
+      nfp += __popc(f[k] & p[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      of[k] = e2m1_nibbles(f[2 * k]) | (e2m1_nibbles(f[2 * k + 1]) << 16);
+      ofp[k] = e2m1_nibbles(f[2 * k] & p[2 * k]) | (e2m1_nibbles(f[2 * k + 1] & p[2 * k + 1]) << 16);
+      op[k] = e2m1_nibbles(p[2 * k]) | (e2m1_nibbles(p[2 * k + 1]) << 16);
+    }
+    *reinterpret_cast<uint4*>(Fr + t / 2) = make_uint4(of[0], of[1], of[2], of[3]);
+    *reinterpret_cast<uint4*>(FPr + t / 2) = make_uint4(ofp[0], ofp[1], ofp[2], ofp[3]);
+    *reinterpret_cast<uint4*>(Pr + t / 2) = make_uint4(op[0], op[1], op[2], op[3]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    nf += __shfl_xor_sync(0xffffffffu, nf, o);
+    np += __shfl_xor_sync(0xffffffffu, np, o);
+    nfp += __shfl_xor_sync(0xffffffffu, nfp, o);
+  }
+  if (lane < 3) marg[(int64_t)lane * n + g] = lane == 0 ? nf : (lane == 1 ? np : nfp);
+  if (__any_sync(0xffffffffu, high != 0) && lane == 0) atomicExch(err, 2);
+}
+
 // Tensor maps of the operands: F and FP (packed, n x Lpad) and P (the bins
 // themselves, n x L with row stride ld; TMA fills columns >= L and rows >= n
-// with zeros).
+// with zeros). The 4-bit form has all three packed (rows of Lpad / 2 bytes).
 struct B2Maps {
   CUtensorMap F, P, FP;
 };
 
 constexpr int kB2Threads = 512;
+// 4-bit form: TMEM columns of the UE8M0 scale factors (all 1.0), after the
+// three 128-column accumulators: A (sources, M = 128) at kSfaCol, B (targets,
+// up to N = 256) at kSfbCol; 8 columns each hold every layout those take.
+constexpr uint32_t kSfaCol = 384, kSfbCol = 392;
 
+// FP4 = false: kind::i8 MMAs on the int8 operands (K = 32 per MMA), int32 sums.
+// FP4 = true: kind::mxf4 MMAs on the packed E2M1 operands (K = 64 per MMA, two
+// samples per byte: half the shared-memory bytes per multiply), unit block
+// scales, float32 sums (exact integers below 2^24).
+template <bool FP4>
 __global__ void __launch_bounds__(kB2Threads, 1)
     b2_gemm_kernel(const __grid_constant__ B2Maps maps, B2Params prm) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -197,7 +293,7 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   const int warp = tid >> 5;
   const int m0 = blockIdx.y * kTile;  // targets
   const int n0 = blockIdx.x * kTile;  // sources
-  const int nk = prm.Lpad / kKt;
+  const int nk = (FP4 ? prm.Lpad / 2 : prm.Lpad) / kKt;  // 128-byte K stages
 
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -218,6 +314,17 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
+  if (FP4) {
+    // unit scale factors (UE8M0 127 = 1.0 in every byte) for the MMAs to read
+    if (warp < 4) {
+      const uint32_t lanes = (uint32_t)(warp * 32) << 16;
+      tmem_st8(tmem + lanes + kSfaCol, 0x7f7f7f7fu);
+      tmem_st8(tmem + lanes + kSfbCol, 0x7f7f7f7fu);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
 
   // ---- producer (warp 0, lane 0): TMA loads of stage k into buffer k % kStages,
   // each once the MMAs that read the buffer's previous contents completed --------
@@ -258,8 +365,8 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   // (20 KB of shared memory instead of 24; shared-memory bandwidth bounds the
   // main loop). TMEM columns 0-127 = C^T, 128-255 = D^T, 256-383 = E^T.
   if (tid == 32) {
-    const uint32_t idesc256 = idesc_i8(kTile, 2 * kTile);
-    const uint32_t idesc128 = idesc_i8(kTile, kTile);
+    const uint32_t idesc256 = FP4 ? idesc_mxf4(kTile, 2 * kTile) : idesc_i8(kTile, 2 * kTile);
+    const uint32_t idesc128 = FP4 ? idesc_mxf4(kTile, kTile) : idesc_i8(kTile, kTile);
     bool ok = true;
     for (int k = 0; k < nk; ++k) {
       const int s = k % kStages;
@@ -278,8 +385,15 @@ __global__ void __launch_bounds__(kB2Threads, 1)
         const uint32_t off = kk * 32;  // 32-byte K step inside the 128-byte swizzle row
         const uint64_t ad = smem_desc_sw128(aPj + off);
         const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
-        mma_i8(tmem + 0, ad, smem_desc_sw128(bFPP + off), idesc256, acc);
-        mma_i8(tmem + 256, ad, smem_desc_sw128(bF + off), idesc128, acc);
+        if (FP4) {
+          mma_mxf4(tmem + 0, ad, smem_desc_sw128(bFPP + off), idesc256, acc, tmem + kSfaCol,
+                   tmem + kSfbCol);
+          mma_mxf4(tmem + 256, ad, smem_desc_sw128(bF + off), idesc128, acc, tmem + kSfaCol,
+                   tmem + kSfbCol);
+        } else {
+          mma_i8(tmem + 0, ad, smem_desc_sw128(bFPP + off), idesc256, acc);
+          mma_i8(tmem + 256, ad, smem_desc_sw128(bF + off), idesc128, acc);
+        }
       }
       mma_commit(&empty[s]);  // stage s free once these MMAs complete
     }
@@ -316,7 +430,9 @@ __global__ void __launch_bounds__(kB2Threads, 1)
       const float nfp = (float)prm.marg[2 * prm.n + i];
       const float c1_1 = np_, c1_0 = N - np_;
       const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
-      const float C = (float)rc[q], Dv = (float)rd[q], E = (float)re[q];
+      const float C = FP4 ? __uint_as_float(rc[q]) : (float)rc[q];
+      const float Dv = FP4 ? __uint_as_float(rd[q]) : (float)rd[q];
+      const float E = FP4 ? __uint_as_float(re[q]) : (float)re[q];
       const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
       float te = 0.f;
       te += cell_term(C, c1_1, c2a11, c2b11);                                   // [1,1,1]
@@ -379,17 +495,25 @@ static int make_map(CUtensorMap* map, const uint8_t* base, int rows, int64_t col
 
 using namespace tenex;
 
-extern "C" size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t lag) {
-  if (n_vars < 1 || row_len <= lag) return 256;
-  const int64_t L = row_len - lag;
-  const int64_t Lpad = round_up(L, kKt);
-  return (size_t)(round_up(2 * (int64_t)n_vars * Lpad, 256) +
-                  round_up(3 * (int64_t)n_vars * 4, 256) + 256);
+// Workspace: the packed operands (the larger of the two forms: int8 F and FP,
+// n x round_up(L, 128) bytes each; 4-bit F, FP and P, n x round_up(L, 256) / 2
+// bytes each), then the per-gene counts (3 x n int32), then the error word.
+static int64_t b2_ops_bytes(int n, int64_t L) {
+  const int64_t i8 = 2 * (int64_t)n * round_up(L, kKt);
+  const int64_t f4 = 3 * (int64_t)n * (round_up(L, 2 * kKt) / 2);
+  return round_up(i8 > f4 ? i8 : f4, 256);
 }
 
-extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
-                                      int64_t lag, float* out, int64_t out_ld, void* workspace,
-                                      size_t workspace_bytes, void* stream_) {
+extern "C" size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t lag) {
+  if (n_vars < 1 || row_len <= lag) return 256;
+  return (size_t)(b2_ops_bytes(n_vars, row_len - lag) + round_up(3 * (int64_t)n_vars * 4, 256) +
+                  256);
+}
+
+extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int n_vars,
+                                           int64_t row_len, int64_t lag, float* out,
+                                           int64_t out_ld, void* workspace,
+                                           size_t workspace_bytes, int kind, void* stream_) {
   cudaStream_t stream = as_stream(stream_);
   if (!bins || !out || !workspace) return fail(TENEX_ERR_BADARG, "bins, out, workspace non-NULL");
   if (n_vars < 2) return fail(TENEX_ERR_BADARG, "n_vars must be >= 2");
@@ -399,30 +523,46 @@ extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_var
   if ((ld & 15) || (reinterpret_cast<uintptr_t>(bins) & 15))
     return fail(TENEX_ERR_BADARG, "bins and ld must be 16-byte aligned");
   if (out_ld < n_vars) return fail(TENEX_ERR_BADARG, "out_ld must be >= n_vars");
+  if (kind < 0 || kind > 2)
+    return fail(TENEX_ERR_BADARG, "kind must be 0 (default), 1 (int8) or 2 (4-bit)");
+  const bool fp4 = kind != 1;
   const int64_t L = row_len - lag;
   if (L >= ((int64_t)1 << 24))
     return fail(TENEX_ERR_UNSUPPORTED, "L=%lld: float32 cell counts are exact only below 2^24",
                 (long long)L);
-  const int64_t Lpad = round_up(L, kKt);
+  const int64_t Lpad = round_up(L, fp4 ? 2 * kKt : kKt);
   if ((int64_t)workspace_bytes < (int64_t)tenex_b2_workspace_bytes(n_vars, row_len, lag))
     return fail(TENEX_ERR_OOM, "workspace too small (tenex_b2_workspace_bytes)");
   if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
     return fail(TENEX_ERR_BADARG, "workspace must be 256-byte aligned");
   unsigned char* ws = reinterpret_cast<unsigned char*>(workspace);
   uint8_t* ops = ws;
-  int32_t* marg = reinterpret_cast<int32_t*>(ws + round_up(2 * (int64_t)n_vars * Lpad, 256));
-  int* err = reinterpret_cast<int*>(ws + round_up(2 * (int64_t)n_vars * Lpad, 256) +
-                                    round_up(3 * (int64_t)n_vars * 4, 256));
+  const int64_t ob = b2_ops_bytes(n_vars, L);
+  int32_t* marg = reinterpret_cast<int32_t*>(ws + ob);
+  int* err = reinterpret_cast<int*>(ws + ob + round_up(3 * (int64_t)n_vars * 4, 256));
   cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), stream);
   if (e != cudaSuccess) return check_cuda(e, "memset");
-  b2_pack_kernel<<<(n_vars + kPackWarps - 1) / kPackWarps, kPackWarps * 32, 0, stream>>>(
-      bins, ld, n_vars, (int)L, (int)lag, (int)Lpad, ops, marg, err);
+  const int pack_grid = (n_vars + kPackWarps - 1) / kPackWarps;
+  if (fp4)
+    b2_pack4_kernel<<<pack_grid, kPackWarps * 32, 0, stream>>>(bins, ld, n_vars, (int)L,
+                                                                (int)lag, (int)Lpad, ops, marg,
+                                                                err);
+  else
+    b2_pack_kernel<<<pack_grid, kPackWarps * 32, 0, stream>>>(bins, ld, n_vars, (int)L, (int)lag,
+                                                               (int)Lpad, ops, marg, err);
   int st = check_launch("b2_pack_kernel");
   if (st) return st;
   B2Maps maps;
-  if ((st = make_map(&maps.F, ops, n_vars, Lpad, Lpad))) return st;
-  if ((st = make_map(&maps.P, bins, n_vars, L, ld))) return st;
-  if ((st = make_map(&maps.FP, ops + (int64_t)n_vars * Lpad, n_vars, Lpad, Lpad))) return st;
+  if (fp4) {
+    const int64_t rb = Lpad / 2;
+    if ((st = make_map(&maps.F, ops, n_vars, rb, rb))) return st;
+    if ((st = make_map(&maps.FP, ops + (int64_t)n_vars * rb, n_vars, rb, rb))) return st;
+    if ((st = make_map(&maps.P, ops + 2 * (int64_t)n_vars * rb, n_vars, rb, rb))) return st;
+  } else {
+    if ((st = make_map(&maps.F, ops, n_vars, Lpad, Lpad))) return st;
+    if ((st = make_map(&maps.P, bins, n_vars, L, ld))) return st;
+    if ((st = make_map(&maps.FP, ops + (int64_t)n_vars * Lpad, n_vars, Lpad, Lpad))) return st;
+  }
   B2Params prm;
   prm.n = n_vars;
   prm.L = (int)L;
@@ -432,20 +572,34 @@ extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_var
   prm.out_ld = out_ld;
   prm.err = err;
   const int smem = kStages * kStageBytes + 1024 + 256;
-  e = cudaFuncSetAttribute(b2_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
   const unsigned tiles = (unsigned)((n_vars + kTile - 1) / kTile);
-  b2_gemm_kernel<<<dim3(tiles, tiles), kB2Threads, smem, stream>>>(maps, prm);
+  if (fp4) {
+    e = cudaFuncSetAttribute(b2_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
+    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+    b2_gemm_kernel<true><<<dim3(tiles, tiles), kB2Threads, smem, stream>>>(maps, prm);
+  } else {
+    e = cudaFuncSetAttribute(b2_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
+    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+    b2_gemm_kernel<false><<<dim3(tiles, tiles), kB2Threads, smem, stream>>>(maps, prm);
+  }
   return check_launch("b2_gemm_kernel");
+}
+
+extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
+                                      int64_t lag, float* out, int64_t out_ld, void* workspace,
+                                      size_t workspace_bytes, void* stream) {
+  return tenex_te_binary_matrix_kind(bins, ld, n_vars, row_len, lag, out, out_ld, workspace,
+                                     workspace_bytes, 0, stream);
 }
 
 extern "C" int tenex_b2_status(const void* workspace, int n_vars, int64_t row_len, int64_t lag,
                                void* stream) {
   if (!workspace) return fail(TENEX_ERR_BADARG, "workspace is NULL");
   const int64_t L = row_len - lag;
-  const int64_t Lpad = round_up(L, kKt);
   const unsigned char* ws = reinterpret_cast<const unsigned char*>(workspace);
-  const int* err = reinterpret_cast<const int*>(ws + round_up(2 * (int64_t)n_vars * Lpad, 256) +
+  const int* err = reinterpret_cast<const int*>(ws + b2_ops_bytes(n_vars, L) +
                                                 round_up(3 * (int64_t)n_vars * 4, 256));
   int h = 0;
   cudaError_t e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, as_stream(stream));

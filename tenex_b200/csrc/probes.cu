@@ -17,7 +17,9 @@
 // back-to-back tcgen05.mma.cta_group::1.kind::i8 of M = 128, N = 256, K = 32 from
 // fixed shared-memory operands into two alternating int32 TMEM accumulators
 // (512 columns), commits to an mbarrier and waits for it (bounded); nothing is
-// loaded from global memory, so this is the issue-limited MMA rate.
+// loaded from global memory, so this is the issue-limited MMA rate. The FP4
+// variant issues kind::mxf4 (packed E2M1, K = 64, unit block scales): the rate of
+// the 4-bit GEMM-B2 form.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -62,7 +64,11 @@ __global__ void __launch_bounds__(1024, 1) smem_atomic_probe(int mode, int iters
 constexpr int kProbeM = 128, kProbeN = 256, kProbeK = 32;
 constexpr int kProbeSmem = 120 * 1024;  // > half of an SM's shared memory: one CTA per SM
 
-__global__ void __launch_bounds__(128, 1) tc_int8_probe(int iters, int* err) {
+// FP4 = true: the same with tcgen05.mma.kind::mxf4 (packed E2M1, M = 128, N = 256,
+// K = 64 from the same 32-byte operand rows) and unit UE8M0 block scales in TMEM,
+// one float32 accumulator (256 columns) plus the scale columns.
+template <bool FP4>
+__global__ void __launch_bounds__(128, 1) tc_probe(int iters, int* err) {
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)sm_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* a = sm;                                  // 128 rows x 32 B: 2 planes of 2 KB
@@ -87,12 +93,26 @@ __global__ void __launch_bounds__(128, 1) tc_int8_probe(int iters, int* err) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
+  constexpr uint32_t kSf = 256;  // FP4: scale-factor columns (8 each for A and B)
+  if (FP4) {
+    tmem_st8(tmem + ((uint32_t)(tid & ~31) << 16) + kSf, 0x7f7f7f7fu);       // 4 warps
+    tmem_st8(tmem + ((uint32_t)(tid & ~31) << 16) + kSf + 8, 0x7f7f7f7fu);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
   if (tid == 0) {
-    const uint32_t idesc = idesc_i8(kProbeM, kProbeN);
     const uint64_t ad = smem_desc(smem_u32(a), kProbeM * 16, 128);
     const uint64_t bd = smem_desc(smem_u32(b), kProbeN * 16, 128);
-    for (int it = 0; it < iters; ++it)
-      mma_i8(tmem + (uint32_t)((it & 1) * kProbeN), ad, bd, idesc, it >= 2 ? 1u : 0u);
+    if (FP4) {
+      const uint32_t idesc = idesc_mxf4(kProbeM, kProbeN);
+      for (int it = 0; it < iters; ++it)
+        mma_mxf4(tmem, ad, bd, idesc, it >= 1 ? 1u : 0u, tmem + kSf, tmem + kSf + 8);
+    } else {
+      const uint32_t idesc = idesc_i8(kProbeM, kProbeN);
+      for (int it = 0; it < iters; ++it)
+        mma_i8(tmem + (uint32_t)((it & 1) * kProbeN), ad, bd, idesc, it >= 2 ? 1u : 0u);
+    }
     mma_commit(bar);
     if (!mbar_wait(bar, 0)) atomicExch(err, 1);
   }
@@ -107,7 +127,8 @@ __global__ void __launch_bounds__(128, 1) tc_int8_probe(int iters, int* err) {
 
 using namespace tenex;
 
-extern "C" int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stream_) {
+template <bool FP4>
+static int probe_tc(int iters, double* ops, float* ms, void* stream_) {
   if (iters < 1 || !ops || !ms) return fail(TENEX_ERR_BADARG, "iters >= 1, outputs non-NULL");
   DevAttr A;
   int st = current_device_attr(&A);
@@ -117,7 +138,7 @@ extern "C" int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stre
   cudaError_t e = cudaMallocAsync(&err, sizeof(int), s);
   if (e != cudaSuccess) return check_cuda(e, "cudaMallocAsync");
   cudaMemsetAsync(err, 0, sizeof(int), s);
-  e = cudaFuncSetAttribute(tc_int8_probe, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(tc_probe<FP4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            kProbeSmem + 1024);
   if (e != cudaSuccess) {
     cudaFreeAsync(err, s);
@@ -126,11 +147,11 @@ extern "C" int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stre
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  tc_int8_probe<<<A.sm_count, 128, kProbeSmem + 1024, s>>>(iters < 64 ? iters : 64, err);
+  tc_probe<FP4><<<A.sm_count, 128, kProbeSmem + 1024, s>>>(iters < 64 ? iters : 64, err);
   cudaEventRecord(e0, s);
-  tc_int8_probe<<<A.sm_count, 128, kProbeSmem + 1024, s>>>(iters, err);
+  tc_probe<FP4><<<A.sm_count, 128, kProbeSmem + 1024, s>>>(iters, err);
   cudaEventRecord(e1, s);
-  st = check_launch("tc_int8_probe");
+  st = check_launch("tc_probe");
   e = cudaEventSynchronize(e1);
   if (!st && e != cudaSuccess) st = check_cuda(e, "cudaEventSynchronize");
   float t = 0.f;
@@ -144,8 +165,16 @@ extern "C" int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stre
   if (st) return st;
   if (h) return fail(TENEX_ERR_TIMEOUT, "tensor-pipe probe: commit wait expired");
   *ms = t;
-  *ops = 2.0 * kProbeM * kProbeN * kProbeK * (double)iters * A.sm_count;
+  *ops = 2.0 * kProbeM * kProbeN * (FP4 ? 2 * kProbeK : kProbeK) * (double)iters * A.sm_count;
   return TENEX_OK;
+}
+
+extern "C" int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stream) {
+  return probe_tc<false>(iters, ops, ms, stream);
+}
+
+extern "C" int tenex_probe_tc_fp4(int iters, double* ops, float* ms, void* stream) {
+  return probe_tc<true>(iters, ops, ms, stream);
 }
 
 extern "C" int tenex_probe_smem_atomics(int mode, int iters, int64_t* increments, float* ms,

@@ -110,6 +110,40 @@ __device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t
       : "memory");
 }
 
+// Instruction descriptor, kind::mxf4 with block scales: A and B E2M1 (format 1
+// at bits 7-9 and 10-12), K-major, N >> 3 at bit 17, UE8M0 scales (bit 23),
+// M >> 4 at bit 24, scale-factor byte ids 0 (bits 4-5, 29-30), dense K = 64.
+__host__ __device__ constexpr uint32_t idesc_mxf4(int M, int N) {
+  return (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | (1u << 23) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+// D += A * B with A, B packed E2M1 (two per byte, K = 64 per MMA = 32 bytes of a
+// K-major row) and one UE8M0 scale per 32 elements read from TMEM at sfa / sfb;
+// float32 accumulators.
+__device__ __forceinline__ void mma_mxf4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate, uint32_t sfa,
+                                         uint32_t sfb) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], "
+      "p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(sfa), "r"(sfb)
+      : "memory");
+}
+
+// Stores v into 8 consecutive TMEM columns starting at taddr for the 32 lanes of
+// the calling warp's lane quarter (taddr's lane field = 32 * (warp % 4)).
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, uint32_t v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(
+          taddr),
+      "r"(v)
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 // Plain arrival (release at CTA scope) on a shared-memory mbarrier.
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");

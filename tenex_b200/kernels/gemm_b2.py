@@ -2,9 +2,10 @@
 
 Reference: tenex/kernels/gemm_b2.py (GEMMB2Kernel :565-596, compute_te_gemm_b2
 :307-425). Same name, supports() predicate and compute_matrix() contract
-([i, j] = TE(j -> i), diagonal 0); the counts come from tcgen05 INT8 MMAs with
-int32 accumulators (exact), the 8-cell TE from the TMEM epilogue of the same
-kernel (gemm_b2.cu).
+([i, j] = TE(j -> i), diagonal 0); the counts come from tcgen05 MMAs over the
+0/1 operands, packed as 4-bit E2M1 values (kind::mxf4, float32 sums) or as int8
+(kind::i8, int32 sums), both exact, and the 8-cell TE from the TMEM epilogue of
+the same kernel (gemm_b2.cu).
 """
 from __future__ import annotations
 
@@ -16,9 +17,14 @@ from tenex_b200.kernels import TEKernel
 from tenex_b200.kernels import device as D
 
 
+OPERANDS = {"default": 0, "int8": 1, "fp4": 2}
+
+
 def te_binary_matrix(db: D.DeviceBins, tau: int = 1, out: torch.Tensor | None = None,
-                     check: bool = True) -> torch.Tensor:
-    """(n, n) float32 device matrix with [src, tgt] = TE(src -> tgt), diagonal 0."""
+                     check: bool = True, operands: str = "default") -> torch.Tensor:
+    """(n, n) float32 device matrix with [src, tgt] = TE(src -> tgt), diagonal 0.
+    operands: "int8" (kind::i8 MMAs), "fp4" (the 0/1 values as packed E2M1,
+    kind::mxf4) or "default" (fp4); the counts and TE are the same."""
     dev = db.data.device
     n = db.n
     lag = tau * db.K
@@ -27,8 +33,8 @@ def te_binary_matrix(db: D.DeviceBins, tau: int = 1, out: torch.Tensor | None = 
     nb = int(native.lib().tenex_b2_workspace_bytes(n, db.row_len, lag))
     ws = torch.empty(nb, dtype=torch.uint8, device=dev)
     s = native.stream_ptr()
-    native.call("tenex_te_binary_matrix", db.ptr(), db.ld, n, db.row_len, lag,
-                out.data_ptr(), n, ws.data_ptr(), nb, s)
+    native.call("tenex_te_binary_matrix_kind", db.ptr(), db.ld, n, db.row_len, lag,
+                out.data_ptr(), n, ws.data_ptr(), nb, OPERANDS[operands], s)
     if check:
         native.call("tenex_b2_status", ws.data_ptr(), n, db.row_len, lag, s)
     return out

@@ -85,6 +85,7 @@ _SIGS = {
     "tenex_binarize": [_P, _L, _I, _I, _I, _P, _P, _L, _P, _P],
     "tenex_b2_workspace_bytes": [_I, _L, _L],
     "tenex_te_binary_matrix": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _P],
+    "tenex_te_binary_matrix_kind": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _I, _P],
     "tenex_b2_status": [_P, _I, _L, _L, _P],
     "tenex_dpi_trim": [_P, _L, _I, _P, _P, ctypes.c_float, _P, _L, _P],
     "tenex_dpi_trim_sparse": [_P, _P, _P, _I, _P, _P, ctypes.c_float, _P, _P],
@@ -103,6 +104,8 @@ _SIGS = {
                                  ctypes.POINTER(ctypes.c_float), _P],
     "tenex_probe_tc_int8": [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float),
                             _P],
+    "tenex_probe_tc_fp4": [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float),
+                           _P],
     "tenex_probe_minmax": [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float),
                            _P],
 }
@@ -229,6 +232,14 @@ def te_launch_shape(row_len: int, lag: int, b_max: int, cfg: dict | None = None)
          *[ctypes.byref(v) for v in out])
     return dict(threads=out[0].value, ctas_per_sm=out[1].value, smem_bytes=out[2].value,
                 src_chunk=out[3].value)
+
+
+def probe_tc_fp4(iters: int = 100_000) -> float:
+    """Measured dense 4-bit (kind::mxf4) tensor-pipe operations per second over all SMs."""
+    ops = ctypes.c_double()
+    ms = ctypes.c_float()
+    call("tenex_probe_tc_fp4", int(iters), ctypes.byref(ops), ctypes.byref(ms), stream_ptr())
+    return ops.value / (ms.value * 1e-3)
 
 
 def probe_minmax(iters: int = 20_000) -> float:

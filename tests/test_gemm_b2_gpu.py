@@ -12,49 +12,53 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-6
 
 
-def _run(x, cuda, tau=1):
+def _run(x, cuda, tau=1, operands="default"):
     db = D.pack_bins(x, cuda)
-    m = te_binary_matrix(db, tau).cpu().numpy()
+    m = te_binary_matrix(db, tau, operands=operands).cpu().numpy()
     torch.cuda.synchronize()
     return m
 
 
-@pytest.mark.parametrize("n,T", [(5, 40), (130, 300), (257, 1100)])
-def test_binary_matrix_matches_oracle(cuda, n, T):
+@pytest.mark.parametrize("operands", ["int8", "fp4"])
+@pytest.mark.parametrize("n,T", [(5, 40), (130, 300), (257, 1100), (129, 257), (200, 513)])
+def test_binary_matrix_matches_oracle(cuda, n, T, operands):
     x, _ = W.cfg2_binary(n=n, T=T, seed=n + T, n_planted=min(3, n // 2))
-    m = _run(x, cuda)
+    m = _run(x, cuda, operands=operands)
     ref = O.te_matrix(x.astype(np.int32), np.full(n, 2, np.int32))
     assert np.all(np.diag(m) == 0)
     assert np.max(np.abs(m - ref)) <= TOL
 
 
-def test_binary_matches_reference_fixture(cuda, golden):
+@pytest.mark.parametrize("operands", ["int8", "fp4"])
+def test_binary_matches_reference_fixture(cuda, golden, operands):
     g = golden("gemm_b2.npz")
-    m = _run(g["bins"], cuda)
+    m = _run(g["bins"], cuda, operands=operands)
     assert np.max(np.abs(m - g["te_ij_j_to_i"].T)) <= TOL
 
 
-def test_binary_tau2_constant_rows(cuda):
+@pytest.mark.parametrize("operands", ["int8", "fp4"])
+def test_binary_tau2_constant_rows(cuda, operands):
     rng = np.random.default_rng(2)
     x = (rng.random((70, 500)) < 0.3).astype(np.uint8)
     x[3] = 0
     x[4] = 1
-    m = _run(x, cuda, tau=2)
+    m = _run(x, cuda, tau=2, operands=operands)
     ref = O.te_matrix(x.astype(np.int32), np.full(70, 2, np.int32), tau=2)
     assert np.max(np.abs(m - ref)) <= TOL
 
 
-def test_non_binary_bins_report_bad_data(cuda):
+@pytest.mark.parametrize("operands", ["int8", "fp4"])
+def test_non_binary_bins_report_bad_data(cuda, operands):
     # the GEMM sums raw bytes, so a bin other than 0/1 must be reported by the status
     # call, not silently counted; the context stays usable afterwards
     rng = np.random.default_rng(2)
     x = (rng.random((20, 300)) < 0.4).astype(np.int32)
     x[7, 123] = 2
     with pytest.raises(native.TenexError) as ei:
-        te_binary_matrix(D.pack_bins(x, cuda), 1)
+        te_binary_matrix(D.pack_bins(x, cuda), 1, operands=operands)
     assert ei.value.status == native.TENEX_ERR_BADDATA
     x[7, 123] = 1
-    m = te_binary_matrix(D.pack_bins(x, cuda), 1).cpu().numpy()
+    m = te_binary_matrix(D.pack_bins(x, cuda), 1, operands=operands).cpu().numpy()
     assert np.max(np.abs(m - O.te_matrix(x, np.full(20, 2, np.int32)))) <= 1e-6
 
 
@@ -78,3 +82,6 @@ def test_binary_full_size_sampled_and_deterministic(cuda):
     assert np.max(np.abs(m[src, tgt].astype(np.float64) - ref)) <= TOL
     assert np.all(np.diag(m) == 0)
     assert np.array_equal(m.view(np.uint32), _run(x, cuda).view(np.uint32))
+    # the int8 and 4-bit operand forms give the same exact counts, so the same bits
+    assert np.array_equal(m.view(np.uint32), _run(x, cuda, operands="int8").view(np.uint32))
+    assert np.array_equal(m.view(np.uint32), _run(x, cuda, operands="fp4").view(np.uint32))
