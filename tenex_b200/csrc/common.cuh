@@ -36,15 +36,13 @@ __host__ __device__ inline int64_t round_up(int64_t x, int64_t m) { return (x + 
 //   [0]   uint32 work ticket of the persistent kernel
 //   [4]   int32  data-validation word (nonzero = bad bin / n_per_var)
 //   [8]   int32  unsupported-item word (nonzero = an item's histogram did not fit)
-//   [64]  uint64 phase_cycles[8] (filled only by builds with TENEX_PHASE_TIMERS)
+//   [12]  uint32 work ticket of the global-memory overflow launch
 struct WsHeader {
   unsigned int ticket;
   int bad_data;
   int bad_item;
-  unsigned int ov_ticket;  // work ticket of the global-memory overflow launch
-  int pad[12];
-  unsigned long long phase_cycles[8];
-  int pad2[32];
+  unsigned int ov_ticket;
+  int pad[60];
 };
 static_assert(sizeof(WsHeader) == 256, "workspace header is 256 bytes");
 
