@@ -240,8 +240,6 @@ def run_ours(args) -> None:
         db0, npv0, bmax0 = step()
         kern.cfg = dict(autotune(db0, npv0, bmax0, TAU))
         del db0, npv0
-    if args.lane_cells is not None:
-        kern.cfg["lane_cells"] = args.lane_cells
     bmax_run = None
     for _ in range(args.warmup):
         _, _, bmax_run = step()
@@ -850,8 +848,6 @@ def main():
     ap.add_argument("--reference-gpu-worker", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the reference_gpu object (the reference's CUDA kernels)")
-    ap.add_argument("--lane-cells", type=int, default=None,
-                    help="cell limit of the lane-private histogram tables (-1: none)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -66,10 +66,6 @@ typedef struct {
   int ctas_per_sm;  /* resident CTAs per SM (grid = sm_count * this)    */
   int src_chunk;    /* sources per work item (one target per item)     */
   int smem_bytes;   /* dynamic shared memory per CTA (0 = fill the SM)  */
-  int lane_cells;   /* histograms of at most this many cells (b_t^2 * b_s) use
-                       lane-private tables, one copy per lane (conflict-free
-                       shared-memory reductions); 0 = the library's rule
-                       (about N / 18 cells), -1 = never */
 } tenex_te_config;
 
 int tenex_abi_version(void);

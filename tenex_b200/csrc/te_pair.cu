@@ -14,23 +14,14 @@
 //     c2a (= row sums of c3 over yt) and c1, so sources never re-read it.
 //     Series too long for that are staged in tiles of samples, the CTA's groups
 //     walking the tiles together.
-//   * Shared memory after the target block holds the histograms of the item's
-//     pairs, in one of two layouts chosen per item:
-//       - lane-private tables (small histograms, b_t^2 * b_s up to a cell
-//         limit): 32 copies of the histogram, cell c of lane l at word
-//         c*32 + l, so the 32 lanes of a warp always hit 32 different banks
-//         (one shared-memory wavefront per warp-wide reduction instead of ~3.1
-//         for random cells). The copies are summed after each source (eight
-//         conflict-free 16-byte reads per lane per 32 cells); they are never
-//         cleared within an item: the per-source counts are the difference of
-//         two consecutive sums (modulo 2^32, exact);
-//       - shared slots (larger histograms): one slot per group of G warps
-//         (G = 1: warp-private). Counters are 32-bit unless 32-bit slots would
-//         need groups of more than 4 warps, then 16-bit halves of a word
-//         (N < 65536; two cells per word collide more often, so packing is the
-//         fallback, not the rule).
-//     Pairs whose histogram fits no shared-memory slot (coarsening off) run in a
-//     second instantiation on per-CTA slots in global memory.
+//   * Shared memory after the target block is cut into histogram slots sized
+//     for the item (b_t^2 * b_s cells); a slot belongs to a group of G warps
+//     (G = 1: warp-private histograms for the common small pairs). Counters are
+//     32-bit unless 32-bit slots would need groups of more than 4 warps, then
+//     16-bit halves of a word (N < 65536; two cells per word collide more
+//     often, so packing is the fallback, not the rule). Pairs whose histogram
+//     fits no shared-memory slot (coarsening off) run in a second
+//     instantiation on per-CTA slots in global memory.
 //   * Every sample is one red.shared.add (16 samples per uint4 of source bins).
 //     The hardware merges lanes that add to the same word, so the cost of a
 //     warp-wide reduction is the largest number of distinct words in one bank;
@@ -66,7 +57,6 @@ struct TeParams {
   int lag;
   int ztile;      // samples of the target staged at a time (N: the whole series)
   int big;        // N >= 2^24: float64 entropy pass
-  int lane_cells; // lane-private tables for items of at most this many cells (0: never)
   int64_t p0, p1;  // pair-free id range [p0, p1)
   int t_first;
   int n_targets;
@@ -115,7 +105,7 @@ namespace {
 constexpr int kMaxWarps = 32;
 
 // Histogram layouts (see the file comment).
-enum { kSlot32 = 0, kSlot16 = 1, kGmem = 2, kLane32 = 3 };
+enum { kSlot32 = 0, kSlot16 = 1, kGmem = 2 };
 
 struct SmemLayout {
   int z_off, c2a_off, c1_off, q_off, red_off, misc_off, slot_off;
@@ -135,10 +125,6 @@ __host__ __device__ inline SmemLayout smem_layout(int ztile, int zbytes, int bma
   return L;
 }
 
-// Words of one lane-private table with cells_pad cells: 32 copies, the summed
-// counts of the previous source and the difference (this source's counts).
-__host__ __device__ inline int64_t lane_table_words(int64_t cells_pad) { return cells_pad * 34; }
-
 // Slot cell (z, y): PACK16 -> 16-bit half (y & 1) of word z*hb + (y >> 1),
 // else word z*bs + y.
 template <bool PACK16>
@@ -152,9 +138,8 @@ __device__ __forceinline__ uint32_t cell_get(const uint32_t* slot, uint32_t z, u
 }
 
 // Counts one sample: one reduction per sample (inline PTX, no return value).
-// kSlot16 adds 1 or 1 << 16 to the word holding the cell's 16-bit half; kLane32
-// adds to the lane's copy (base already holds the lane's offset). base is the
-// table's address: the 32-bit shared window address, or (kGmem, the
+// kSlot16 adds 1 or 1 << 16 to the word holding the cell's 16-bit half. base is
+// the slot's address: the 32-bit shared window address, or (kGmem, the
 // global-memory overflow slot) the global address.
 template <int MODE>
 __device__ __forceinline__ void hist_add(uint64_t base, uint32_t z, uint32_t y, uint32_t bs,
@@ -163,8 +148,6 @@ __device__ __forceinline__ void hist_add(uint64_t base, uint32_t z, uint32_t y, 
   if (MODE == kSlot16) {
     off = (z * hb + (y >> 1)) << 2;
     inc = (y & 1u) * 0xffffu + 1u;
-  } else if (MODE == kLane32) {
-    off = (z * bs + y) << 7;
   } else {
     off = (z * bs + y) << 2;
   }
@@ -262,27 +245,6 @@ __host__ __device__ inline bool slot_fits(int64_t bt, int64_t bs, int N, int64_t
   return N < 65536 && w16 * 4 <= slot_region;
 }
 
-// Lane-private tables: sums the 32 copies of 32 consecutive cells per warp
-// iteration (lane l: cell cb*32 + l, its 16-byte chunk ((l + j) & 7) in step j,
-// so every quarter-warp reads eight different bank quads), and writes this
-// source's counts D = sum - (previous sum) and the new sum Pv.
-__device__ __forceinline__ void lane_fold(const uint32_t* T, uint32_t* D, uint32_t* Pv, int ncb,
-                                          int w_g, int G, int lane) {
-  for (int cb = w_g; cb < ncb; cb += G) {
-    const int cell = cb * 32 + lane;
-    const uint32_t* row = T + (int64_t)cell * 32;
-    uint32_t s = 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const uint4 v = *reinterpret_cast<const uint4*>(row + (((lane + j) & 7) << 2));
-      s += (v.x + v.y) + (v.z + v.w);
-    }
-    const uint32_t prev = Pv[cell];
-    Pv[cell] = s;
-    D[cell] = s - prev;
-  }
-}
-
 // Per-lane part of sum c3 * log2(c3 * c1 / (c2a * c2b)) over the pair's cells.
 // Cell (z = xt1*bt + xt, y) is tab[z * stride + y] (PACK16: the 16-bit half
 // (y & 1) of word z * stride + (y >> 1), stride = hb). Columns (xt, y) are
@@ -372,7 +334,6 @@ struct ItemCtx {
   int64_t lo, base;
   int n_src;
   int bt;
-  int BS;             // the item's largest source bin count (table stride, kLane32)
   bool z8;
   const unsigned char* zsm;
   const int* c1i;
@@ -380,8 +341,6 @@ struct ItemCtx {
   const float2* qa;
   double* red;
   int slot_region;    // shared-memory slot region (overflow split rule)
-  int ncb;            // kLane32: 32-cell blocks of the table
-  int cells_pad;      // kLane32: padded cells per table
 };
 
 // Source r of the item for this launch: its id and pair id, or false if the
@@ -418,18 +377,10 @@ __device__ __forceinline__ void finish_pair(const TeParams& P, const ItemCtx& it
   const int bt2 = bt * bt;
   const int bs = P.npv[src];
   constexpr bool PACK16 = MODE == kSlot16;
-  constexpr bool LANE = MODE == kLane32;
   const int hb = PACK16 ? (bs + 1) >> 1 : bs;
   group_sync(G, g, gthreads);
   uint32_t* tab = slot;  // counts read by the entropy pass
-  int stride = PACK16 ? hb : bs;
-  if (LANE) {
-    uint32_t* D = slot + (int64_t)32 * it.cells_pad;
-    lane_fold(slot, D, D + it.cells_pad, it.ncb, lane_g >> 5, G, tid & 31);
-    group_sync(G, g, gthreads);
-    tab = D;
-    stride = it.BS;
-  }
+  const int stride = PACK16 ? hb : bs;
 
   // -- optional raw-count export (parity checks only) --------------------
   if (P.counts_dbg != nullptr) {
@@ -445,10 +396,10 @@ __device__ __forceinline__ void finish_pair(const TeParams& P, const ItemCtx& it
   // -- entropy pass (shared slots are cleared for the next source) ---------
   double tot;
   if (P.big) {
-    tot = dev::warp_sum(entropy_cols_f64<!LANE>(tab, bt, bs, stride, it.c1i, it.c2ai, lane_g,
+    tot = dev::warp_sum(entropy_cols_f64<true>(tab, bt, bs, stride, it.c1i, it.c2ai, lane_g,
                                                 gthreads));
   } else {
-    tot = dev::warp_sum((double)entropy_cols<PACK16, !LANE>(tab, bt, bs, stride, it.c1i, it.qa,
+    tot = dev::warp_sum((double)entropy_cols<PACK16, true>(tab, bt, bs, stride, it.c1i, it.qa,
                                                             lane_g, gthreads));
   }
   if (G > 1) {
@@ -484,7 +435,6 @@ __device__ __forceinline__ uint64_t table_addr(uint32_t* slot, int tid) {
   uint64_t a;
   if (MODE == kGmem) asm("cvta.to.global.u64 %0, %1;" : "=l"(a) : "l"(slot));
   else a = (uint64_t)__cvta_generic_to_shared(slot);
-  if (MODE == kLane32) a += (uint64_t)((tid & 31) * 4);
   return a;
 }
 
@@ -532,9 +482,8 @@ __device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it
       if (P.out_mode == kOutStats && lane_g == 0) obs_m = __ldg(P.obs + (int64_t)src * P.n + it.tgt);
       const uint32_t bs = (uint32_t)P.npv[src];
       const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
-      const uint32_t stride = MODE == kLane32 ? (uint32_t)it.BS : bs;
       hist_source<MODE>(slot_addr, it.zsm, it.z8, P.bins + (int64_t)src * P.ld, N, lane_g,
-                        gthreads, stride, hb);
+                        gthreads, bs, hb);
       finish_pair<MODE>(P, it, slot, G, g, lane_g, tid, warp, src, p, obs_m);
     }
     return;
@@ -549,14 +498,13 @@ __device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it
       obs_m = __ldg(P.obs + (int64_t)src * P.n + it.tgt);
     const uint32_t bs = act ? (uint32_t)P.npv[src] : 1u;
     const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
-    const uint32_t stride = MODE == kLane32 ? (uint32_t)it.BS : bs;
     const uint8_t* srow = P.bins + (int64_t)src * P.ld;
     for (int s0 = 0; s0 < N; s0 += P.ztile) {
       const int n = min(P.ztile, N - s0);
       __syncthreads();  // every group is done with the previous tile
       stage_z<false>(trow, P.lag, it.bt, it.z8, s0, n, zsm, nullptr, tid, nthreads);
       __syncthreads();
-      if (act) hist_source<MODE>(slot_addr, zsm, it.z8, srow + s0, n, lane_g, gthreads, stride, hb);
+      if (act) hist_source<MODE>(slot_addr, zsm, it.z8, srow + s0, n, lane_g, gthreads, bs, hb);
     }
     if (act) finish_pair<MODE>(P, it, slot, G, g, lane_g, tid, warp, src, p, obs_m);
   }
@@ -703,26 +651,15 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       c1i[j] = s;
     }
 
-    // ---- table layout of this item ---------------------------------------
-    // lane-private tables for small histograms (after the target block, which
-    // takes ztile bytes when b_t <= 16); else shared slots: 32-bit counters
-    // when groups of <= 4 warps fit (the overflow launch: the whole CTA on one
-    // 32-bit slot in global memory)
-    const int cells = bt2 * bsmax;
-    const int cells_pad = (int)round_up(cells, 32);
-    const int lane_off =
-        (int)round_up((int64_t)SL.z_off + (int64_t)P.ztile * (z8 ? 1 : 2), 128);
-    const int fitl = GMEM || cells > P.lane_cells
-                         ? 0
-                         : (int)((P.smem_bytes - lane_off) / (lane_table_words(cells_pad) * 4));
-    const bool lane = fitl >= 1;
+    // ---- carve slots: 32-bit counters when groups of <= 4 warps fit --------
+    // (the overflow launch: the whole CTA on one 32-bit slot in global memory)
     const int words32 = (int)round_up((int64_t)bt2 * bsmax, 4);
     const int words16 = (int)round_up((int64_t)bt2 * ((bsmax + 1) >> 1), 4);
     const int fit32 = GMEM ? 1 : slot_region / (words32 * 4);
     const int fit16 = GMEM ? 0 : slot_region / (words16 * 4);
-    const bool pack16 = !lane && !GMEM && (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
-    const int fit = lane ? fitl : (pack16 ? fit16 : fit32);
-    const int slot_words = lane ? (int)lane_table_words(cells_pad) : (pack16 ? words16 : words32);
+    const bool pack16 = !GMEM && (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
+    const int fit = pack16 ? fit16 : fit32;
+    const int slot_words = pack16 ? words16 : words32;
     if (fit < 1) {
       if (tid == 0) atomicExch(&P.ws->bad_item, 1);
       __syncthreads();
@@ -734,11 +671,9 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     const int n_groups = n_warps / G;
     const int g = warp / G;
     const int lane_g = tid - g * G * 32;
-    uint32_t* tbase =
-        lane ? reinterpret_cast<uint32_t*>(smem + lane_off) : slots;
-    uint32_t* slot = GMEM ? gslot : tbase + (int64_t)g * slot_words;
+    uint32_t* slot = GMEM ? gslot : slots + (int64_t)g * slot_words;
     if (!GMEM)
-      for (int i = tid; i < n_groups * slot_words; i += nthreads) tbase[i] = 0u;
+      for (int i = tid; i < n_groups * slot_words; i += nthreads) slots[i] = 0u;
     __syncthreads();
     for (int z = tid; z < bt2; z += nthreads) {
       const float c2a = (float)c2ai[z];
@@ -752,7 +687,6 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     it.base = base;
     it.n_src = n_src;
     it.bt = bt;
-    it.BS = bsmax;
     it.z8 = z8;
     it.zsm = zsm;
     it.c1i = c1i;
@@ -760,12 +694,8 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     it.qa = qa;
     it.red = red;
     it.slot_region = slot_region;
-    it.ncb = cells_pad / 32;
-    it.cells_pad = cells_pad;
     if (GMEM)
       run_sources<kGmem>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
-    else if (lane)
-      run_sources<kLane32>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
     else if (pack16)
       run_sources<kSlot16>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
     else
@@ -858,12 +788,6 @@ static int z_tile(int N, int zbytes) {
   if ((int64_t)N * zbytes <= 65536) return N;
   return 32768 / zbytes;
 }
-
-// Default cell limit of the lane-private tables for series of N samples: about
-// where a table's per-source summation (one wavefront per cell) costs what its
-// conflict-free reductions save over shared slots (~2.1 wavefronts per 32
-// samples).
-static int default_lane_cells(int N) { return N / 18; }
 
 static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const DevAttr& A,
                           TeLaunch* L, int64_t max_slot_bytes) {
@@ -1074,10 +998,6 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   P.zbytes = b_max <= 16 ? 1 : 2;
   P.ztile = z_tile(P.N, P.zbytes);
   P.big = P.N >= (1 << 24) ? 1 : 0;
-  {
-    const int lc = cfg ? cfg->lane_cells : 0;
-    P.lane_cells = lc < 0 ? 0 : (lc > 0 ? lc : default_lane_cells(P.N));
-  }
   P.out_mode = out_mode;
   P.out = out;
   P.out_ld = out_ld;

@@ -46,8 +46,7 @@ class DevInfo(ctypes.Structure):
 
 class TeConfig(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
-                ("src_chunk", ctypes.c_int), ("smem_bytes", ctypes.c_int),
-                ("lane_cells", ctypes.c_int)]
+                ("src_chunk", ctypes.c_int), ("smem_bytes", ctypes.c_int)]
 
 
 _P = ctypes.c_void_p
@@ -199,9 +198,8 @@ def device_info(device: int | None = None) -> DevInfo:
     return info
 
 
-def te_config(threads=0, ctas_per_sm=0, src_chunk=0, smem_bytes=0, lane_cells=0) -> TeConfig:
-    return TeConfig(int(threads), int(ctas_per_sm), int(src_chunk), int(smem_bytes),
-                    int(lane_cells))
+def te_config(threads=0, ctas_per_sm=0, src_chunk=0, smem_bytes=0) -> TeConfig:
+    return TeConfig(int(threads), int(ctas_per_sm), int(src_chunk), int(smem_bytes))
 
 
 def probe_smem_atomics(mode: int = 0, iters: int = 4096) -> float:
@@ -226,7 +224,7 @@ def te_launch_shape(row_len: int, lag: int, b_max: int, cfg: dict | None = None)
     this series length, lag, b_max and requested config (0 / None = defaults)."""
     c = cfg or {}
     tc = te_config(c.get("threads", 0), c.get("ctas_per_sm", 0), c.get("src_chunk", 0),
-                   c.get("smem_bytes", 0), c.get("lane_cells", 0))
+                   c.get("smem_bytes", 0))
     out = [ctypes.c_int() for _ in range(4)]
     call("tenex_te_launch_shape", int(row_len), int(lag), int(b_max), ctypes.byref(tc),
          *[ctypes.byref(v) for v in out])
