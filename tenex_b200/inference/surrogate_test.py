@@ -267,6 +267,17 @@ class SurrogateTestMethod:
             raise ValueError(f"p_method must be 'parametric' or 'mc' (got {p_method!r})")
         if null not in ("full", "learned"):
             raise ValueError(f"null must be 'full' or 'learned' (got {null!r})")
+        # fused= picks the reference's per-pair fused kernel (float32 running sums,
+        # the default below L = 1500) or its loop path (float64 sums). This build has
+        # one path for both: a full TE launch per surrogate whose epilogue adds into
+        # float64 sums, i.e. the loop path's accumulation for every L. The argument is
+        # validated as the reference validates it.
+        fused = kwargs.get("fused")
+        if fused not in (None, True, False):
+            raise ValueError(f"fused must be None, True or False (got {fused!r})")
+        if fused is True and kernel_name not in ("Full-SMEM", "Adaptive-SMEM"):
+            raise ValueError(f"fused=True requested but kernel {kernel_name!r} has no fused "
+                             f"variant (supported: 'Full-SMEM', 'Adaptive-SMEM')")
         bin_data = np.asarray(bin_data)
         if bin_data.ndim == 2:
             bin_data = bin_data[..., None]

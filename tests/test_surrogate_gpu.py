@@ -94,6 +94,15 @@ def test_netweaver_surrogate_end_to_end(cuda):
         NetWeaver(res).infer("surrogate_test", device=cuda, n_surrogates=1)
     with pytest.raises(NotImplementedError):
         NetWeaver(res).infer("trace", device=cuda)
+    # fused=: accepted for the kernels the reference has a fused variant of (the same
+    # float64 accumulation runs either way), refused for the others as the reference does
+    for fused in (True, False, None):
+        sf = NetWeaver(res, fdr=0.05).infer("surrogate_test", device=cuda, n_surrogates=8,
+                                            block_length=20, seed=5, fused=fused)
+        assert np.array_equal(sf.p_values, st.p_values)
+    with pytest.raises(ValueError, match="fused"):
+        NetWeaver(res).infer("surrogate_test", device=cuda, n_surrogates=8, kernel="GEMM-B2",
+                             fused=True)
 
 
 def test_pipeline_multi_lag_surrogate(cuda):
