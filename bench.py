@@ -14,18 +14,28 @@ the B200 shared-memory limit (38, the reference rule) and the full TE matrix
 Profiling options (not the headline run): --genes / --cells shrink the
 workload, --pairs times only the first pair ids, --launch T,C,W fixes the
 launch shape (threads, CTAs per SM, sources per work item) instead of running
-the autotuner, --no-e2e, --no-cpu-baseline and --no-surrogate skip those legs.
-The line's "surrogate" object times NetWeaver's surrogate test on cfg5 (full
-100-shuffle test against the learned null, wall seconds, edge agreement), and
-"binary_path" the cfg2 GEMM-B2 matrix against the measured INT8 tensor peak
-(both skipped by --no-surrogate).
+the autotuner, --no-e2e, --no-cpu-baseline, --no-surrogate, --no-fdr,
+--no-configs and --no-reference-gpu skip those legs; --only NAME prints one leg.
+Side objects of the line:
+  surrogate      NetWeaver's surrogate test on cfg5 (full 100-shuffle test and
+                 the learned null, wall seconds, edge agreement)
+  binary_path    the cfg2 GEMM-B2 matrix, 4-bit and int8 operand forms, each
+                 against its live tensor-pipe probe
+  fdr            NetWeaver's default FDR method on the cfg4 matrix
+  cfg3, cfg1     the other TE configs: device time and roofline, end to end,
+                 and the CPU oracle on the same workload
+  reference_gpu  the reference's own CUDA wrappers (installed under
+                 baseline/_ref) on the same GPU, in a child process that imports
+                 nothing of this repository (context, not the reference arm)
+The CPU figures (cpu_baseline objects and --impl reference) all come from one
+routine: the C oracle on seed-fixed uniform samples of 100,000 ordered pairs.
 
 N > 1 (torchrun, one process per GPU): the pair-id range is split into
 contiguous chunks of ceil(pairs / N), the reference's split (no data-path
 collective); total work is fixed (strong scaling); time is the max over ranks.
 --impl reference: rank 0 times the CPU oracle (a C restatement of the
-reference's counting and TE formula, all host threads) on a bounded sample of
-the same pairs.
+reference's counting and TE formula, all host threads) on uniform samples of
+100,000 pairs of the same coarsened bins, one sample per step.
 """
 from __future__ import annotations
 
