@@ -29,7 +29,9 @@ entropy sum, whose reduction order follows the launch's warp grouping). BH is
 then recomputed over the mixed p-values and the screen is
 widened while z_FDR - band keeps falling. Called edges are therefore always
 verified by the full test; the band only decides how many true edges could be
-missed (pairs whose predicted z falls more than `band` below z_FDR).
+missed (pairs whose predicted z falls more than `band` below z_FDR). When more
+than half of the pairs cannot be scored (data unlike the training set: other
+series lengths, block lengths or bin statistics), the full test runs instead.
 """
 from __future__ import annotations
 
@@ -561,6 +563,22 @@ def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n
     else:
         tested = ~torch.eye(n, dtype=torch.bool, device=dev)
     valid = torch.isfinite(z_d) & in_range[None, :] & in_range[:, None]
+    m_tested = int(tested.sum())
+    n_unscored = int((tested & ~valid).sum())
+    if n_unscored > float(kwargs.get("full_test_fraction", 0.5)) * max(m_tested, 1):
+        # data unlike the training set: most pairs would go to the full test anyway,
+        # so run the full test itself (its exact statistics, without the screen's
+        # per-pair bookkeeping)
+        full_kw = {k: v for k, v in kwargs.items() if k != "null"}
+        res = method.infer(observed_te, variable_names, dev, **full_kw)
+        res.null_model = "learned"
+        res.info = {"n_fallback": m_tested, "fallback_fraction": 1.0, "n_invalid": n_unscored,
+                    "delegated_to_full_test": True, "band": band, "rounds": 0,
+                    "seconds_predict": time.time() - t0, "seconds_total": time.time() - t0,
+                    "n_out_of_range_genes": int((~in_range).sum().item())}
+        _log.vprint(f"[TENEX] learned null: {n_unscored} of {m_tested} pairs outside the "
+                    f"model's training range; ran the full surrogate test")
+        return res
     p_mix = 0.5 * torch.special.erfc(z_d.double() / np.sqrt(2.0))
     p_mix = torch.where(valid, p_mix, torch.ones_like(p_mix))
     mean_s = mu_d.clone()
@@ -568,7 +586,6 @@ def learned_surrogate_test(method, observed_te, variable_names, dev, bin_data, n
     eff_s = obs_d - mean_s
     count = torch.zeros((n, n), dtype=torch.int32, device=dev)
     verified = torch.zeros((n, n), dtype=torch.bool, device=dev)
-    m_tested = int(tested.sum())
     t_pred = time.time() - t0
     perms = None
     rounds, z_cuts, t_verify = 0, [], 0.0

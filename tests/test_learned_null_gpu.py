@@ -131,3 +131,5 @@ def test_learned_null_away_from_its_training_data(cuda, n, T, bl):
           f"full {t1 - t0:.3f} s, learned {t2 - t1:.3f} s")
     assert E2 <= E1
     assert jac >= 0.99
+    if lrn.info.get("delegated_to_full_test"):      # out of the model's range: the full test
+        assert np.array_equal(lrn.p_values, full.p_values)
