@@ -24,7 +24,8 @@
 //     exact integers (int32, N < 2^31).
 //   * Epilogue: sixteen warps; warp w reads TMEM lanes 32*(w%4).. (one source
 //     per lane) and a quarter of the 128 target columns with tcgen05.ld, forms
-//     the 8 cells and writes TE(src -> tgt) to out[src, tgt].
+//     the 8 cells and writes TE(src -> tgt) to out[src, tgt], 16 consecutive
+//     targets of a source row as four 16-byte stores.
 //   * Every mbarrier wait is bounded; on expiry the kernel records an error
 //     word, drains the copies it issued (bounded), frees TMEM and returns.
 #include <cuda.h>
@@ -54,6 +55,7 @@ struct B2Params {
   const int32_t* marg;  // (3, n): nf, np, nfp
   float* out;       // (n, n): out[src * ld + tgt]
   int64_t out_ld;
+  int vec_out;      // out and out_ld allow 16-byte row stores
   int* err;         // device error word (1 = a wait expired, 2 = a bin was not 0/1)
 };
 
@@ -422,10 +424,11 @@ __global__ void __launch_bounds__(kB2Threads, 1)
     tmem_ld16(lane_base + 256 + cb, re);
     tmem_wait_ld();
     if (!run || j >= prm.n) continue;
+    const int i0 = m0 + cb;  // first target of the 16 (the same for every lane: broadcast loads)
+    float res[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int i = m0 + cb + q;  // target gene (the same for every lane: broadcast loads)
-      if (i >= prm.n || i == j) continue;
+      const int i = min(i0 + q, prm.n - 1);
       const float nf = (float)prm.marg[i], np_ = (float)prm.marg[prm.n + i];
       const float nfp = (float)prm.marg[2 * prm.n + i];
       const float c1_1 = np_, c1_0 = N - np_;
@@ -443,7 +446,21 @@ __global__ void __launch_bounds__(kB2Threads, 1)
       te += cell_term(np_ - Dv - nfp + C, c1_1, c2a01, c2b10);                  // [0,1,0]
       te += cell_term(nf - E - nfp + C, c1_0, c2a10, c2b00);                    // [1,0,0]
       te += cell_term(N - nf - np_ - npj + nfp + Dv + E - C, c1_0, c2a00, c2b00);  // [0,0,0]
-      prm.out[(int64_t)j * prm.out_ld + i] = (float)((double)te / (double)prm.L);
+      res[q] = (float)((double)te / (double)prm.L);
+    }
+    // row j of the output: 16 consecutive targets, four 16-byte stores when they are
+    // all inside the matrix, off the diagonal and 16-byte aligned; else one by one
+    float* orow = prm.out + (int64_t)j * prm.out_ld;
+    const bool vec = prm.vec_out && i0 + 16 <= prm.n && (j < i0 || j >= i0 + 16);
+    if (vec) {
+#pragma unroll
+      for (int q = 0; q < 16; q += 4)
+        *reinterpret_cast<float4*>(orow + i0 + q) =
+            make_float4(res[q], res[q + 1], res[q + 2], res[q + 3]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (i0 + q < prm.n && i0 + q != j) orow[i0 + q] = res[q];
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -570,6 +587,7 @@ extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int 
   prm.marg = marg;
   prm.out = out;
   prm.out_ld = out_ld;
+  prm.vec_out = (out_ld % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
   prm.err = err;
   const int smem = kStages * kStageBytes + 1024 + 256;
   const unsigned tiles = (unsigned)((n_vars + kTile - 1) / kTile);
