@@ -24,8 +24,9 @@
 //     exact integers (int32, N < 2^31).
 //   * Epilogue: sixteen warps; warp w reads TMEM lanes 32*(w%4).. (one source
 //     per lane) and a quarter of the 128 target columns with tcgen05.ld, forms
-//     the 8 cells and writes TE(src -> tgt) to out[src, tgt], 16 consecutive
-//     targets of a source row as four 16-byte stores.
+//     the 8 cells (target marginals staged in shared memory) and writes
+//     TE(src -> tgt) to out[src, tgt], four consecutive targets of a source row
+//     per 16-byte store.
 //   * Every mbarrier wait is bounded; on expiry the kernel records an error
 //     word, drains the copies it issued (bounded), frees TMEM and returns.
 #include <cuda.h>
@@ -290,6 +291,8 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   uint64_t* accbar = empty + kStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accbar + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  // the tile's target marginals nf, np, nfp as floats (epilogue operands)
+  float* tmarg = reinterpret_cast<float*>(smem + kStages * kStageBytes + 256);
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -407,6 +410,13 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   }
 
   // ---- epilogue: 16 warps; lane quarter warp % 4, column quarter warp / 4 ---
+  // (the warps that neither load nor issue stage the target marginals first)
+  if (tid >= 64) {
+    for (int k = tid - 64; k < 3 * kTile; k += kB2Threads - 64) {
+      const int c = k / kTile, i = m0 + (k - c * kTile);
+      tmarg[k] = i < prm.n ? (float)prm.marg[(int64_t)c * prm.n + i] : 0.f;
+    }
+  }
   bool ok_acc = mbar_wait_sleep(accbar, 0, 200);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -415,6 +425,7 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   const int lq = warp & 3, cq = warp >> 2;
   const int j = n0 + lq * 32 + (tid & 31);  // source gene of this thread's TMEM lane
   const float N = (float)prm.L;
+  const float invL = 1.0f / N;
   const float npj = j < prm.n ? (float)prm.marg[prm.n + j] : 0.f;
   const uint32_t lane_base = tmem + ((uint32_t)(lq * 32) << 16);
   for (int cb = cq * (kTile / 4); cb < (cq + 1) * (kTile / 4); cb += 16) {
@@ -425,42 +436,42 @@ __global__ void __launch_bounds__(kB2Threads, 1)
     tmem_wait_ld();
     if (!run || j >= prm.n) continue;
     const int i0 = m0 + cb;  // first target of the 16 (the same for every lane: broadcast loads)
-    float res[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int i = min(i0 + q, prm.n - 1);
-      const float nf = (float)prm.marg[i], np_ = (float)prm.marg[prm.n + i];
-      const float nfp = (float)prm.marg[2 * prm.n + i];
-      const float c1_1 = np_, c1_0 = N - np_;
-      const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
-      const float C = FP4 ? __uint_as_float(rc[q]) : (float)rc[q];
-      const float Dv = FP4 ? __uint_as_float(rd[q]) : (float)rd[q];
-      const float E = FP4 ? __uint_as_float(re[q]) : (float)re[q];
-      const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
-      float te = 0.f;
-      te += cell_term(C, c1_1, c2a11, c2b11);                                   // [1,1,1]
-      te += cell_term(Dv - C, c1_1, c2a01, c2b11);                              // [0,1,1]
-      te += cell_term(E - C, c1_0, c2a10, c2b01);                               // [1,0,1]
-      te += cell_term(npj - Dv - E + C, c1_0, c2a00, c2b01);                    // [0,0,1]
-      te += cell_term(nfp - C, c1_1, c2a11, c2b10);                             // [1,1,0]
-      te += cell_term(np_ - Dv - nfp + C, c1_1, c2a01, c2b10);                  // [0,1,0]
-      te += cell_term(nf - E - nfp + C, c1_0, c2a10, c2b00);                    // [1,0,0]
-      te += cell_term(N - nf - np_ - npj + nfp + Dv + E - C, c1_0, c2a00, c2b00);  // [0,0,0]
-      res[q] = (float)((double)te / (double)prm.L);
-    }
-    // row j of the output: 16 consecutive targets, four 16-byte stores when they are
-    // all inside the matrix, off the diagonal and 16-byte aligned; else one by one
     float* orow = prm.out + (int64_t)j * prm.out_ld;
-    const bool vec = prm.vec_out && i0 + 16 <= prm.n && (j < i0 || j >= i0 + 16);
-    if (vec) {
 #pragma unroll
-      for (int q = 0; q < 16; q += 4)
-        *reinterpret_cast<float4*>(orow + i0 + q) =
-            make_float4(res[q], res[q + 1], res[q + 2], res[q + 3]);
-    } else {
+    for (int q0 = 0; q0 < 16; q0 += 4) {
+      float res[4];
 #pragma unroll
-      for (int q = 0; q < 16; ++q)
-        if (i0 + q < prm.n && i0 + q != j) orow[i0 + q] = res[q];
+      for (int u = 0; u < 4; ++u) {
+        const int q = q0 + u;
+        const int ti = cb + q;  // target within the tile (marginals 0 beyond n)
+        const float nf = tmarg[ti], np_ = tmarg[kTile + ti], nfp = tmarg[2 * kTile + ti];
+        const float c1_1 = np_, c1_0 = N - np_;
+        const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
+        const float C = FP4 ? __uint_as_float(rc[q]) : (float)rc[q];
+        const float Dv = FP4 ? __uint_as_float(rd[q]) : (float)rd[q];
+        const float E = FP4 ? __uint_as_float(re[q]) : (float)re[q];
+        const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
+        float te = 0.f;
+        te += cell_term(C, c1_1, c2a11, c2b11);                                   // [1,1,1]
+        te += cell_term(Dv - C, c1_1, c2a01, c2b11);                              // [0,1,1]
+        te += cell_term(E - C, c1_0, c2a10, c2b01);                               // [1,0,1]
+        te += cell_term(npj - Dv - E + C, c1_0, c2a00, c2b01);                    // [0,0,1]
+        te += cell_term(nfp - C, c1_1, c2a11, c2b10);                             // [1,1,0]
+        te += cell_term(np_ - Dv - nfp + C, c1_1, c2a01, c2b10);                  // [0,1,0]
+        te += cell_term(nf - E - nfp + C, c1_0, c2a10, c2b00);                    // [1,0,0]
+        te += cell_term(N - nf - np_ - npj + nfp + Dv + E - C, c1_0, c2a00, c2b00);  // [0,0,0]
+        res[u] = te * invL;
+      }
+      // four consecutive targets of row j: one 16-byte store when they are all
+      // inside the matrix, off the diagonal and aligned; else one by one
+      const int ia = i0 + q0;
+      if (prm.vec_out && ia + 4 <= prm.n && (j < ia || j >= ia + 4)) {
+        *reinterpret_cast<float4*>(orow + ia) = make_float4(res[0], res[1], res[2], res[3]);
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (ia + u < prm.n && ia + u != j) orow[ia + u] = res[u];
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -589,7 +600,7 @@ extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int 
   prm.out_ld = out_ld;
   prm.vec_out = (out_ld % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
   prm.err = err;
-  const int smem = kStages * kStageBytes + 1024 + 256;
+  const int smem = kStages * kStageBytes + 1024 + 256 + 3 * kTile * 4;
   const unsigned tiles = (unsigned)((n_vars + kTile - 1) / kTile);
   if (fp4) {
     e = cudaFuncSetAttribute(b2_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,

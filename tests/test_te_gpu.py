@@ -76,6 +76,36 @@ def test_series_longer_than_shared_memory(cuda, threads):
     assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
 
 
+def test_long_series_every_output_mode(cuda):
+    """The sample-tiled staging (series past 65,536 u8 states) behind every output
+    mode: pair-free ids with tau = 2 and K = 2, the matrix, an explicit pair list
+    (the source filter) and the surrogate statistics epilogue, against the oracle."""
+    from tenex_b200.kernels.pair_list import te_pair_list
+    rng = np.random.default_rng(70_001)
+    bins, npv, bmax = _rand_bins(rng, 7, 40_003, 2, 9, K=2)      # row_len 80,006 u8 states
+    te = _gpu_te(bins, npv, bmax, cuda, tau=2).cpu().numpy()
+    assert np.max(np.abs(te - O.te_pairfree(bins, npv, tau=2))) <= TOL
+    db = D.pack_bins(bins, cuda)
+    npv_t = torch.as_tensor(npv, dtype=torch.int32, device=cuda)
+    m = D.te_pairfree(db, npv_t, bmax, tau=1, matrix=True).cpu().numpy()
+    assert np.max(np.abs(m - O.te_matrix(bins, npv))) <= TOL
+    pairs = np.array([[0, 3], [0, 5], [2, 1], [6, 0], [6, 2], [6, 4]], np.int64)
+    got = te_pair_list(db, npv_t, bmax, 1, pairs).cpu().numpy()
+    assert np.max(np.abs(got - O.te_pairs(bins, npv, pairs))) <= TOL
+    # surrogate statistics: one accumulation of the observed bins themselves adds
+    # TE into the sums and counts TE >= observed (all ties)
+    n = 7
+    obs = torch.as_tensor(m, device=cuda)
+    ssum = torch.zeros((n, n), dtype=torch.float64, device=cuda)
+    ssq = torch.zeros_like(ssum)
+    cnt = torch.zeros((n, n), dtype=torch.int32, device=cuda)
+    D.surrogate_accumulate(db, npv_t, bmax, 1, obs, ssum, ssq, cnt)
+    torch.cuda.synchronize()
+    off = ~np.eye(n, dtype=bool)
+    assert np.max(np.abs(ssum.cpu().numpy()[off] - m[off])) <= TOL
+    assert np.all(cnt.cpu().numpy()[off] == 1)
+
+
 def test_series_of_2_pow_24_samples(cuda):
     """N = 2^24 + 40 samples (beyond float32's exact integers): 32-bit counters,
     float64 entropy pass. Counts bit-exact, TE within 1e-6 of the oracle."""
