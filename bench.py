@@ -634,10 +634,34 @@ def binary_leg(dev, reps: int = 5) -> dict:
                                             "time of pack + GEMM; peak = the live %s probe"
                                             % ("tenex_probe_tc_fp4" if form == "fp4"
                                                else "tenex_probe_tc_int8")}}
+    # end to end: pinned host bins -> padded device rows -> matrix -> pinned host matrix
+    # (the reference's compute_te_gemm_b2 is timed the same way, host to host)
+    x_pin = torch.from_numpy(np.ascontiguousarray(x, dtype=np.uint8)).pin_memory()
+    out_pin = torch.empty((n, n), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        d8 = D.empty_bins(n, T, 1, dev)
+        d8.data[:, :T].copy_(x_pin, non_blocking=True)
+        m = te_binary_matrix(d8, 1, check=False)
+        out_pin.copy_(m, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        e2e_step()
+    b.record()
+    torch.cuda.synchronize(dev)
+    e2e_ms = a.elapsed_time(b) / reps
     d = forms["fp4"]
     return {"workload": "cfg2: 2000 genes x 5000 cells, binary Markov bins, GEMM-B2",
             "pairs_per_s": d["pairs_per_s"], "ms": d["ms"], "operands": "fp4 (kind::mxf4)",
-            "roofline": d["roofline"], "int8_form": forms["int8"]}
+            "roofline": d["roofline"], "int8_form": forms["int8"],
+            "e2e": {"value": n * (n - 1) / (e2e_ms / 1e3), "unit": "pairs/s", "ms": e2e_ms,
+                    "h2d_bytes_per_step": int(x.size), "d2h_bytes_per_step": int(n * n * 4),
+                    "path": "pinned host bins -> padded device rows -> te_binary_matrix -> "
+                            "pinned host matrix"}}
 
 
 def fdr_leg(dev, mat, reps: int = 2) -> dict:

@@ -179,8 +179,8 @@ b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int l
 // 0x0; sample 2k in the low nibble of byte k, 2k + 1 in the high one), rows of
 // Lpad / 2 bytes (Lpad a multiple of 256: whole 128-byte TMA boxes), the same
 // per-gene counts and the same 0/1 check. Each lane makes 16 bytes of each
-// operand from 32 samples: two aligned 16-byte loads of P and a 48-byte aligned
-// window of F.
+// operand from 32 samples (two aligned 16-byte loads of P and a 48-byte aligned
+// window of F), two such chunks per pass with all their loads in flight.
 __device__ __forceinline__ uint32_t e2m1_nibbles(uint32_t w) {
   // four 0/1 bytes b0..b3 -> 16 bits: 2*b0 | 2*b1 << 4 | 2*b2 << 8 | 2*b3 << 12
   const uint32_t t = (w | (w >> 4)) & 0x00ff00ffu;
@@ -200,57 +200,75 @@ b2_pack4_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int 
   uint8_t* Pr = ops + (2 * (int64_t)n + g) * rowb;
   int nf = 0, np = 0, nfp = 0;
   uint32_t high = 0;
-  for (int t = lane * 32; t < Lpad; t += 32 * 32) {
-    uint32_t f[8], p[8];
-    const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;
-    if (t + 32 <= L && fa + 48 <= ld) {
-      const uint4 p0 = *reinterpret_cast<const uint4*>(row + t);
-      const uint4 p1 = *reinterpret_cast<const uint4*>(row + t + 16);
-      const uint4 a0 = *reinterpret_cast<const uint4*>(row + fa);
-      const uint4 a1 = *reinterpret_cast<const uint4*>(row + fa + 16);
-      const uint4 a2 = *reinterpret_cast<const uint4*>(row + fa + 32);
-      const uint32_t w[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
-                              a2.x, a2.y, a2.z, a2.w};
-      const uint32_t pw[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-      const int sh = (int)((t + lag) - fa);
+  for (int t0 = lane * 32; t0 < Lpad; t0 += 2 * 32 * 32) {
+    // two 32-sample chunks per pass, all ten loads issued before the first store
+    uint4 pv[2][2], av[2][3];
+    bool fast[2];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const int byte = sh + 4 * k;
-        f[k] = __funnelshift_r(w[byte >> 2], w[(byte >> 2) + 1], (byte & 3) * 8);
-        p[k] = pw[k];
+    for (int u = 0; u < 2; ++u) {
+      const int t = t0 + u * 32 * 32;
+      const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;
+      fast[u] = t + 32 <= L && fa + 48 <= ld;
+      if (fast[u]) {
+        pv[u][0] = *reinterpret_cast<const uint4*>(row + t);
+        pv[u][1] = *reinterpret_cast<const uint4*>(row + t + 16);
+        av[u][0] = *reinterpret_cast<const uint4*>(row + fa);
+        av[u][1] = *reinterpret_cast<const uint4*>(row + fa + 16);
+        av[u][2] = *reinterpret_cast<const uint4*>(row + fa + 32);
       }
-    } else {
+    }
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        uint32_t fk = 0, pk = 0;
-        for (int j = 0; j < 4; ++j) {
-          const int tt = t + 4 * k + j;
-          if (tt < L) {
-            fk |= (uint32_t)row[tt + lag] << (8 * j);
-            pk |= (uint32_t)row[tt] << (8 * j);
-          }
+    for (int u = 0; u < 2; ++u) {
+      const int t = t0 + u * 32 * 32;
+      if (t >= Lpad) break;
+      uint32_t f[8], p[8];
+      if (fast[u]) {
+        const uint32_t w[12] = {av[u][0].x, av[u][0].y, av[u][0].z, av[u][0].w,
+                                av[u][1].x, av[u][1].y, av[u][1].z, av[u][1].w,
+                                av[u][2].x, av[u][2].y, av[u][2].z, av[u][2].w};
+        const uint32_t pw[8] = {pv[u][0].x, pv[u][0].y, pv[u][0].z, pv[u][0].w,
+                                pv[u][1].x, pv[u][1].y, pv[u][1].z, pv[u][1].w};
+        const int sh = (t + lag) & 15;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int byte = sh + 4 * k;
+          f[k] = __funnelshift_r(w[byte >> 2], w[(byte >> 2) + 1], (byte & 3) * 8);
+          p[k] = pw[k];
         }
-        f[k] = fk;
-        p[k] = pk;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          uint32_t fk = 0, pk = 0;
+          for (int j = 0; j < 4; ++j) {
+            const int tt = t + 4 * k + j;
+            if (tt < L) {
+              fk |= (uint32_t)row[tt + lag] << (8 * j);
+              pk |= (uint32_t)row[tt] << (8 * j);
+            }
+          }
+          f[k] = fk;
+          p[k] = pk;
+        }
       }
-    }
-    uint32_t of[4], ofp[4], op[4];
+      uint32_t of[4], ofp[4], op[4];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      high |= (f[k] | p[k]) & 0xfefefefeu;
-      nf += __popc(f[k]);
-      np += __popc(p[k]);
-      nfp += __popc(f[k] & p[k]);
-    }
+      for (int k = 0; k < 8; ++k) {
+        high |= (f[k] | p[k]) & 0xfefefefeu;
+        nf += __popc(f[k]);
+        np += __popc(p[k]);
+        nfp += __popc(f[k] & p[k]);
+      }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      of[k] = e2m1_nibbles(f[2 * k]) | (e2m1_nibbles(f[2 * k + 1]) << 16);
-      ofp[k] = e2m1_nibbles(f[2 * k] & p[2 * k]) | (e2m1_nibbles(f[2 * k + 1] & p[2 * k + 1]) << 16);
-      op[k] = e2m1_nibbles(p[2 * k]) | (e2m1_nibbles(p[2 * k + 1]) << 16);
+      for (int k = 0; k < 4; ++k) {
+        of[k] = e2m1_nibbles(f[2 * k]) | (e2m1_nibbles(f[2 * k + 1]) << 16);
+        ofp[k] = e2m1_nibbles(f[2 * k] & p[2 * k]) |
+                 (e2m1_nibbles(f[2 * k + 1] & p[2 * k + 1]) << 16);
+        op[k] = e2m1_nibbles(p[2 * k]) | (e2m1_nibbles(p[2 * k + 1]) << 16);
+      }
+      *reinterpret_cast<uint4*>(Fr + t / 2) = make_uint4(of[0], of[1], of[2], of[3]);
+      *reinterpret_cast<uint4*>(FPr + t / 2) = make_uint4(ofp[0], ofp[1], ofp[2], ofp[3]);
+      *reinterpret_cast<uint4*>(Pr + t / 2) = make_uint4(op[0], op[1], op[2], op[3]);
     }
-    *reinterpret_cast<uint4*>(Fr + t / 2) = make_uint4(of[0], of[1], of[2], of[3]);
-    *reinterpret_cast<uint4*>(FPr + t / 2) = make_uint4(ofp[0], ofp[1], ofp[2], ofp[3]);
-    *reinterpret_cast<uint4*>(Pr + t / 2) = make_uint4(op[0], op[1], op[2], op[3]);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
