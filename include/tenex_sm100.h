@@ -260,6 +260,13 @@ int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t 
 int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
                                 int64_t lag, float* out, int64_t out_ld, void* workspace,
                                 size_t workspace_bytes, int kind, void* stream);
+/* Same, with the target-tile width of the GEMM chosen by the caller: tile_n =
+ * 0 picks it from n_vars and the SM count (the width whose tiles finish in the
+ * fewest rounds), else one of 128, 112, 96, 80, 64 (TENEX_ERR_BADARG otherwise).
+ * Every width gives bitwise the same matrix. */
+int tenex_te_binary_matrix_ex(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
+                              int64_t lag, float* out, int64_t out_ld, void* workspace,
+                              size_t workspace_bytes, int kind, int tile_n, void* stream);
 /* Error word of the last tenex_te_binary_matrix call on this workspace
  * (synchronises `stream`): TENEX_ERR_BADDATA if a bin was not 0 or 1,
  * TENEX_ERR_TIMEOUT if a pipeline wait expired. */

@@ -6,11 +6,11 @@
 // per-gene marginals, then sum c*log2(c*c1/(c2a*c2b)) / N).
 //
 // B200 design:
-//   * pack kernel: one pass over the bins writes the lag-shifted K-major int8
-//     operand F and FP = F & P (rows padded to a multiple of 128 bytes, zero
-//     filled), the per-gene counts nf, np, nfp, and flags any bin other than
-//     0/1; P is the bins themselves (a tensor map with K extent L, TMA zero-fills
-//     beyond it).
+//   * pack kernel: one pass over the bins (one warp per segment of a row)
+//     writes the lag-shifted K-major int8 operand F and FP = F & P (rows padded
+//     to a multiple of 128 bytes, zero filled), the per-gene counts nf, np, nfp,
+//     and flags any bin other than 0/1; P is the bins themselves (a tensor map
+//     with K extent L, TMA zero-fills beyond it). The 4-bit form packs P too.
 //   * GEMM kernel: one CTA per 128 x 128 (target x source) tile of the matrix.
 //     A producer warp brings, per stage, one 128-byte x 128-row box of FP, P, F
 //     (targets) and P (sources) by TMA (cp.async.bulk.tensor.2d, no multicast),
@@ -33,6 +33,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cstdint>
+#include <iterator>
 #include <mutex>
 
 #include "common.cuh"
@@ -41,13 +44,14 @@
 namespace tenex {
 namespace {
 
-constexpr int kTile = 128;     // M = N = 128
+constexpr int kTile = 128;     // sources per tile (M = 128 TMEM lanes); targets per tile <= 128
 constexpr int kKt = 128;       // bytes of K per pipeline stage (4 MMA K-steps of 32)
 constexpr int kStages = 3;
-constexpr int kOpBytes = kKt * kTile;          // one operand tile per stage (16 KB)
-constexpr int kStageBytes = 4 * kOpBytes;      // FP, P, F (targets) + P (sources)
-constexpr int kTmaBytes = kStageBytes;          // all four by TMA
+// one stage: FP, P, F of TN targets and P of 128 sources, 128 bytes of K each
+// (every box starts on a 1024-byte swizzle atom: TN is a multiple of 16)
+__host__ __device__ constexpr int stage_bytes(int TN) { return (3 * TN + kTile) * kKt; }
 constexpr int kTmemCols = 512;
+constexpr int kTileN[] = {128, 112, 96, 80, 64};  // target-tile widths (MMA N = TN and 2 TN)
 
 struct B2Params {
   int n;            // genes
@@ -60,7 +64,20 @@ struct B2Params {
   int* err;         // device error word (1 = a wait expired, 2 = a bin was not 0/1)
 };
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
       "%14,%15}, [%16];"
@@ -76,190 +93,122 @@ __device__ __forceinline__ void tmem_wait_ld() {
 
 // c * log2(c * c1 / (c2a * c2b)); exactly 0 for an empty cell and where the two
 // products are equal (the reference's ratio is exactly 1 there); otherwise the
-// ratio by approximate division (2 ulp) and lg2.approx, far below the 1e-6 TE budget.
-__device__ __forceinline__ float cell_term(float c, float c1, float c2a, float c2b) {
-  const float num = c * c1, den = c2a * c2b;
-  const float r = (c > 0.f && num != den) ? __fdividef(num, den) : 1.f;
+// ratio as c * (1/c2b) * (c1/c2a), with q = c1/c2a divided once per target state
+// and rb = 1/c2b once per source state (approximate reciprocal, 1 ulp), and
+// lg2.approx: far below the 1e-6 TE budget, and 12 MUFU operations per pair
+// (4 reciprocals, 8 logarithms) instead of a division per cell.
+__device__ __forceinline__ float cell_term(float c, float c1, float c2a, float c2b, float q,
+                                           float rb) {
+  const bool e = c == 0.f || c * c1 == c2a * c2b;
+  const float r = e ? 1.f : c * rb * q;
   return c * __log2f(r);
 }
 
 // Pack: F[g, t] = x[g, t+lag] (the lag-shifted operand TMA cannot address: its
 // copies start on 16-byte boundaries) and FP = F & P for t < L (0 beyond, up to
-// Lpad), plus the per-gene counts nf, np, nfp; P = x[g, t] is read from the bins
-// directly. One warp per gene, kPackWarps genes per CTA, so the counts reduce
-// with shuffles alone (no CTA barrier). Each lane makes 16 bytes of F and FP
-// from two aligned 16-byte loads, two chunks per pass with all six loads issued
-// before the first store; a scalar path covers the row end.
+// Lpad), plus the per-gene counts nf, np, nfp. The int8 form writes F and FP
+// (P is read from the bins directly); the 4-bit form writes F, FP and P as
+// packed E2M1 values (1.0 = 0x2, 0.0 = 0x0; sample 2k in the low nibble of byte
+// k, 2k + 1 in the high one), rows of Lpad / 2 bytes.
+// One warp per segment of a gene's row (32 lanes x one chunk of kChunk samples),
+// so a matrix of a few thousand genes still puts every SM's memory requests in
+// flight at once: a lane issues all its loads (the chunk of P and the aligned
+// window of F around it) before its first store; a scalar path covers the row
+// end. The counts reduce by shuffles and go to `marg` (zeroed by the caller) by
+// one atomic per count and warp.
 // Every bin must be 0 or 1 (the GEMM sums the raw bytes): a larger value sets
 // the error word to 2.
 constexpr int kPackWarps = 4;
 
-__global__ void __launch_bounds__(kPackWarps * 32)
-b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int lag, int Lpad,
-               uint8_t* __restrict__ ops, int32_t* __restrict__ marg, int* __restrict__ err) {
-  const int g = blockIdx.x * kPackWarps + (threadIdx.x >> 5);
-  if (g >= n) return;  // whole warps only: the shuffles below see full warps
-  const int lane = threadIdx.x & 31;
-  const uint8_t* row = bins + (int64_t)g * ld;
-  uint8_t* Fr = ops + (int64_t)g * Lpad;
-  uint8_t* FPr = ops + ((int64_t)n + g) * Lpad;
-  int nf = 0, np = 0, nfp = 0;
-  uint32_t high = 0;  // any bit above bit 0 of a byte: a bin other than 0/1
-  const int sh = lag & 15;
-  for (int t0 = lane * 16; t0 < Lpad; t0 += 2 * 32 * 16) {
-    uint4 pv[2], av[2], bv[2];
-    bool fast[2];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int t = t0 + u * 32 * 16;
-      const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;  // aligned start of F's window
-      fast[u] = t + 16 <= L && fa + 32 <= ld;
-      if (fast[u]) {
-        pv[u] = *reinterpret_cast<const uint4*>(row + t);
-        av[u] = *reinterpret_cast<const uint4*>(row + fa);
-        bv[u] = *reinterpret_cast<const uint4*>(row + fa + 16);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int t = t0 + u * 32 * 16;
-      if (t >= Lpad) break;
-      uint32_t f[4], p[4];
-      if (fast[u]) {
-        const uint32_t w[8] = {av[u].x, av[u].y, av[u].z, av[u].w,
-                               bv[u].x, bv[u].y, bv[u].z, bv[u].w};
-        const uint32_t pw[4] = {pv[u].x, pv[u].y, pv[u].z, pv[u].w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          // bytes sh + 4k .. sh + 4k + 3 of the 32-byte window
-          const int byte = sh + 4 * k;
-          const uint32_t lo = w[byte >> 2], hi = w[(byte >> 2) + 1];
-          f[k] = __funnelshift_r(lo, hi, (byte & 3) * 8);
-          p[k] = pw[k];
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          uint32_t fk = 0, pk = 0;
-          for (int j = 0; j < 4; ++j) {
-            const int tt = t + 4 * k + j;
-            if (tt < L) {
-              fk |= (uint32_t)row[tt + lag] << (8 * j);
-              pk |= (uint32_t)row[tt] << (8 * j);
-            }
-          }
-          f[k] = fk;
-          p[k] = pk;
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) high |= (f[k] | p[k]) & 0xfefefefeu;
-      *reinterpret_cast<uint4*>(Fr + t) = make_uint4(f[0], f[1], f[2], f[3]);
-      *reinterpret_cast<uint4*>(FPr + t) =
-          make_uint4(f[0] & p[0], f[1] & p[1], f[2] & p[2], f[3] & p[3]);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        nf += __popc(f[k]);
-        np += __popc(p[k]);
-        nfp += __popc(f[k] & p[k]);
-      }
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    nf += __shfl_xor_sync(0xffffffffu, nf, o);
-    np += __shfl_xor_sync(0xffffffffu, np, o);
-    nfp += __shfl_xor_sync(0xffffffffu, nfp, o);
-  }
-  if (lane < 3) marg[(int64_t)lane * n + g] = lane == 0 ? nf : (lane == 1 ? np : nfp);
-  if (__any_sync(0xffffffffu, high != 0) && lane == 0) atomicExch(err, 2);
-}
+template <bool FP4>
+struct PackChunk {
+  static constexpr int kSamples = FP4 ? 32 : 16;  // samples per lane
+  static constexpr int kSeg = 32 * kSamples;      // samples per warp
+};
 
-// 4-bit form of the pack: F, FP and P as packed E2M1 values (1.0 = 0x2, 0.0 =
-// 0x0; sample 2k in the low nibble of byte k, 2k + 1 in the high one), rows of
-// Lpad / 2 bytes (Lpad a multiple of 256: whole 128-byte TMA boxes), the same
-// per-gene counts and the same 0/1 check. Each lane makes 16 bytes of each
-// operand from 32 samples (two aligned 16-byte loads of P and a 48-byte aligned
-// window of F), two such chunks per pass with all their loads in flight.
 __device__ __forceinline__ uint32_t e2m1_nibbles(uint32_t w) {
   // four 0/1 bytes b0..b3 -> 16 bits: 2*b0 | 2*b1 << 4 | 2*b2 << 8 | 2*b3 << 12
   const uint32_t t = (w | (w >> 4)) & 0x00ff00ffu;
   return __byte_perm(t, 0, 0x4420) << 1;
 }
 
+template <bool FP4>
 __global__ void __launch_bounds__(kPackWarps * 32)
-b2_pack4_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int lag, int Lpad,
-                uint8_t* __restrict__ ops, int32_t* __restrict__ marg, int* __restrict__ err) {
-  const int g = blockIdx.x * kPackWarps + (threadIdx.x >> 5);
-  if (g >= n) return;  // whole warps only: the shuffles below see full warps
+b2_pack_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int lag, int Lpad,
+               int nseg, uint8_t* __restrict__ ops, int32_t* __restrict__ marg,
+               int* __restrict__ err) {
+  constexpr int S = PackChunk<FP4>::kSamples;
+  constexpr int NW = S / 4;  // 32-bit words of 0/1 bytes per operand and lane
+  const int64_t wid = (int64_t)blockIdx.x * kPackWarps + (threadIdx.x >> 5);
+  if (wid >= (int64_t)n * nseg) return;  // whole warps only: the shuffles below see full warps
+  const int g = (int)(wid / nseg);
+  const int seg = (int)(wid - (int64_t)g * nseg);
   const int lane = threadIdx.x & 31;
-  const int64_t rowb = Lpad / 2;
+  const int t = seg * PackChunk<FP4>::kSeg + lane * S;
   const uint8_t* row = bins + (int64_t)g * ld;
-  uint8_t* Fr = ops + (int64_t)g * rowb;
-  uint8_t* FPr = ops + ((int64_t)n + g) * rowb;
-  uint8_t* Pr = ops + (2 * (int64_t)n + g) * rowb;
   int nf = 0, np = 0, nfp = 0;
-  uint32_t high = 0;
-  for (int t0 = lane * 32; t0 < Lpad; t0 += 2 * 32 * 32) {
-    // two 32-sample chunks per pass, all ten loads issued before the first store
-    uint4 pv[2][2], av[2][3];
-    bool fast[2];
+  uint32_t high = 0;  // any bit above bit 0 of a byte: a bin other than 0/1
+  if (t < Lpad) {
+    uint32_t f[NW], p[NW];
+    const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;  // aligned start of F's window
+    if (t + S <= L && fa + S + 16 <= ld) {
+      uint4 pv[S / 16], av[S / 16 + 1];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int t = t0 + u * 32 * 32;
-      const int64_t fa = (int64_t)(t + lag) & ~(int64_t)15;
-      fast[u] = t + 32 <= L && fa + 48 <= ld;
-      if (fast[u]) {
-        pv[u][0] = *reinterpret_cast<const uint4*>(row + t);
-        pv[u][1] = *reinterpret_cast<const uint4*>(row + t + 16);
-        av[u][0] = *reinterpret_cast<const uint4*>(row + fa);
-        av[u][1] = *reinterpret_cast<const uint4*>(row + fa + 16);
-        av[u][2] = *reinterpret_cast<const uint4*>(row + fa + 32);
+      for (int u = 0; u < S / 16; ++u) pv[u] = *reinterpret_cast<const uint4*>(row + t + 16 * u);
+#pragma unroll
+      for (int u = 0; u < S / 16 + 1; ++u)
+        av[u] = *reinterpret_cast<const uint4*>(row + fa + 16 * u);
+      uint32_t w[NW + 4];
+#pragma unroll
+      for (int u = 0; u < S / 16 + 1; ++u) {
+        w[4 * u] = av[u].x;
+        w[4 * u + 1] = av[u].y;
+        w[4 * u + 2] = av[u].z;
+        w[4 * u + 3] = av[u].w;
+      }
+      // F's words start sh bytes into the window: a whole-word shift by selects
+      // (registers, no local-memory indexing), then a byte funnel shift
+      const int sh = (t + lag) & 15, qw = sh >> 2;
+      uint32_t ws[NW + 1];
+#pragma unroll
+      for (int i = 0; i <= NW; ++i)
+        ws[i] = qw == 0 ? w[i] : qw == 1 ? w[i + 1] : qw == 2 ? w[i + 2] : w[i + 3];
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        f[k] = __funnelshift_r(ws[k], ws[k + 1], (sh & 3) * 8);
+        const uint4 q = pv[k >> 2];
+        p[k] = (k & 3) == 0 ? q.x : (k & 3) == 1 ? q.y : (k & 3) == 2 ? q.z : q.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) {
+        uint32_t fk = 0, pk = 0;
+        for (int j = 0; j < 4; ++j) {
+          const int tt = t + 4 * k + j;
+          if (tt < L) {
+            fk |= (uint32_t)row[tt + lag] << (8 * j);
+            pk |= (uint32_t)row[tt] << (8 * j);
+          }
+        }
+        f[k] = fk;
+        p[k] = pk;
       }
     }
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int t = t0 + u * 32 * 32;
-      if (t >= Lpad) break;
-      uint32_t f[8], p[8];
-      if (fast[u]) {
-        const uint32_t w[12] = {av[u][0].x, av[u][0].y, av[u][0].z, av[u][0].w,
-                                av[u][1].x, av[u][1].y, av[u][1].z, av[u][1].w,
-                                av[u][2].x, av[u][2].y, av[u][2].z, av[u][2].w};
-        const uint32_t pw[8] = {pv[u][0].x, pv[u][0].y, pv[u][0].z, pv[u][0].w,
-                                pv[u][1].x, pv[u][1].y, pv[u][1].z, pv[u][1].w};
-        const int sh = (t + lag) & 15;
+    for (int k = 0; k < NW; ++k) {
+      high |= (f[k] | p[k]) & 0xfefefefeu;
+      nf += __popc(f[k]);
+      np += __popc(p[k]);
+      nfp += __popc(f[k] & p[k]);
+    }
+    if (FP4) {
+      const int64_t rowb = Lpad / 2;
+      uint8_t* Fr = ops + (int64_t)g * rowb;
+      uint8_t* FPr = ops + ((int64_t)n + g) * rowb;
+      uint8_t* Pr = ops + (2 * (int64_t)n + g) * rowb;
+      uint32_t of[NW / 2], ofp[NW / 2], op[NW / 2];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const int byte = sh + 4 * k;
-          f[k] = __funnelshift_r(w[byte >> 2], w[(byte >> 2) + 1], (byte & 3) * 8);
-          p[k] = pw[k];
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          uint32_t fk = 0, pk = 0;
-          for (int j = 0; j < 4; ++j) {
-            const int tt = t + 4 * k + j;
-            if (tt < L) {
-              fk |= (uint32_t)row[tt + lag] << (8 * j);
-              pk |= (uint32_t)row[tt] << (8 * j);
-            }
-          }
-          f[k] = fk;
-          p[k] = pk;
-        }
-      }
-      uint32_t of[4], ofp[4], op[4];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        high |= (f[k] | p[k]) & 0xfefefefeu;
-        nf += __popc(f[k]);
-        np += __popc(p[k]);
-        nfp += __popc(f[k] & p[k]);
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < NW / 2; ++k) {
         of[k] = e2m1_nibbles(f[2 * k]) | (e2m1_nibbles(f[2 * k + 1]) << 16);
         ofp[k] = e2m1_nibbles(f[2 * k] & p[2 * k]) |
                  (e2m1_nibbles(f[2 * k + 1] & p[2 * k + 1]) << 16);
@@ -268,6 +217,12 @@ b2_pack4_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int 
       *reinterpret_cast<uint4*>(Fr + t / 2) = make_uint4(of[0], of[1], of[2], of[3]);
       *reinterpret_cast<uint4*>(FPr + t / 2) = make_uint4(ofp[0], ofp[1], ofp[2], ofp[3]);
       *reinterpret_cast<uint4*>(Pr + t / 2) = make_uint4(op[0], op[1], op[2], op[3]);
+    } else {
+      uint8_t* Fr = ops + (int64_t)g * Lpad;
+      uint8_t* FPr = ops + ((int64_t)n + g) * Lpad;
+      *reinterpret_cast<uint4*>(Fr + t) = make_uint4(f[0], f[1], f[2], f[3]);
+      *reinterpret_cast<uint4*>(FPr + t) =
+          make_uint4(f[0] & p[0], f[1] & p[1], f[2] & p[2], f[3] & p[3]);
     }
   }
 #pragma unroll
@@ -276,15 +231,19 @@ b2_pack4_kernel(const uint8_t* __restrict__ bins, int64_t ld, int n, int L, int 
     np += __shfl_xor_sync(0xffffffffu, np, o);
     nfp += __shfl_xor_sync(0xffffffffu, nfp, o);
   }
-  if (lane < 3) marg[(int64_t)lane * n + g] = lane == 0 ? nf : (lane == 1 ? np : nfp);
+  if (lane < 3) {
+    const int v = lane == 0 ? nf : (lane == 1 ? np : nfp);
+    if (v) atomicAdd(marg + (int64_t)lane * n + g, v);
+  }
   if (__any_sync(0xffffffffu, high != 0) && lane == 0) atomicExch(err, 2);
 }
 
 // Tensor maps of the operands: F and FP (packed, n x Lpad) and P (the bins
 // themselves, n x L with row stride ld; TMA fills columns >= L and rows >= n
 // with zeros). The 4-bit form has all three packed (rows of Lpad / 2 bytes).
+// Target boxes are TN rows high, source boxes 128 (two maps of P).
 struct B2Maps {
-  CUtensorMap F, P, FP;
+  CUtensorMap F, Pt, FP, Ps;
 };
 
 constexpr int kB2Threads = 512;
@@ -293,13 +252,78 @@ constexpr int kB2Threads = 512;
 // up to N = 256) at kSfbCol; 8 columns each hold every layout those take.
 constexpr uint32_t kSfaCol = 384, kSfbCol = 392;
 
+// TE of NC consecutive targets (tile columns cb .. cb + NC - 1) for the source
+// of this thread's TMEM lane: the three sums from TMEM (every lane of the warp
+// loads, as tcgen05.ld requires), the 8 cells from them and the marginals, and
+// row stores of four targets at a time.
+template <bool FP4, int NC>
+__device__ __forceinline__ void b2_cells(const B2Params& prm, uint32_t lane_base, int cb, int TN,
+                                         int m0, int j, bool active, float npj,
+                                         const float* tmarg, const float* tq) {
+  uint32_t rc[NC], rd[NC], re[NC];
+  tmem_ld(lane_base + (uint32_t)cb, rc);
+  tmem_ld(lane_base + (uint32_t)(TN + cb), rd);
+  tmem_ld(lane_base + (uint32_t)(256 + cb), re);
+  tmem_wait_ld();
+  if (!active) return;
+  const float N = (float)prm.L;
+  const float invL = 1.0f / N;
+  const int i0 = m0 + cb;  // first target of the NC (the same for every lane: broadcast loads)
+  float* orow = prm.out + (int64_t)j * prm.out_ld;
+#pragma unroll
+  for (int q0 = 0; q0 < NC; q0 += 4) {
+    float res[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u;
+      const int ti = cb + q;  // target within the tile (marginals 0 beyond n)
+      const float nf = tmarg[ti], np_ = tmarg[kTile + ti], nfp = tmarg[2 * kTile + ti];
+      const float c1_1 = np_, c1_0 = N - np_;
+      const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
+      const float C = FP4 ? __uint_as_float(rc[q]) : (float)rc[q];
+      const float Dv = FP4 ? __uint_as_float(rd[q]) : (float)rd[q];
+      const float E = FP4 ? __uint_as_float(re[q]) : (float)re[q];
+      const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
+      const float q11 = tq[ti], q01 = tq[kTile + ti], q10 = tq[2 * kTile + ti],
+                  q00 = tq[3 * kTile + ti];
+      const float rb11 = __fdividef(1.f, c2b11), rb01 = __fdividef(1.f, c2b01),
+                  rb10 = __fdividef(1.f, c2b10), rb00 = __fdividef(1.f, c2b00);
+      float te = 0.f;
+      te += cell_term(C, c1_1, c2a11, c2b11, q11, rb11);                                // [1,1,1]
+      te += cell_term(Dv - C, c1_1, c2a01, c2b11, q01, rb11);                           // [0,1,1]
+      te += cell_term(E - C, c1_0, c2a10, c2b01, q10, rb01);                            // [1,0,1]
+      te += cell_term(npj - Dv - E + C, c1_0, c2a00, c2b01, q00, rb01);                 // [0,0,1]
+      te += cell_term(nfp - C, c1_1, c2a11, c2b10, q11, rb10);                          // [1,1,0]
+      te += cell_term(np_ - Dv - nfp + C, c1_1, c2a01, c2b10, q01, rb10);               // [0,1,0]
+      te += cell_term(nf - E - nfp + C, c1_0, c2a10, c2b00, q10, rb00);                 // [1,0,0]
+      te += cell_term(N - nf - np_ - npj + nfp + Dv + E - C, c1_0, c2a00, c2b00, q00,
+                      rb00);                                                            // [0,0,0]
+      res[u] = te * invL;
+    }
+    // four consecutive targets of row j: one 16-byte store when they are all
+    // inside the matrix, off the diagonal and aligned; else one by one
+    const int ia = i0 + q0;
+    if (prm.vec_out && ia + 4 <= prm.n && (j < ia || j >= ia + 4)) {
+      *reinterpret_cast<float4*>(orow + ia) = make_float4(res[0], res[1], res[2], res[3]);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (ia + u < prm.n && ia + u != j) orow[ia + u] = res[u];
+    }
+  }
+}
+
 // FP4 = false: kind::i8 MMAs on the int8 operands (K = 32 per MMA), int32 sums.
 // FP4 = true: kind::mxf4 MMAs on the packed E2M1 operands (K = 64 per MMA, two
 // samples per byte: half the shared-memory bytes per multiply), unit block
 // scales, float32 sums (exact integers below 2^24).
-template <bool FP4>
+// TN: targets per tile (a multiple of 16, at most 128): [FP; P] is one MMA of
+// N = 2 TN and F one of N = TN.
+template <bool FP4, int TN>
 __global__ void __launch_bounds__(kB2Threads, 1)
     b2_gemm_kernel(const __grid_constant__ B2Maps maps, B2Params prm) {
+  constexpr int kStageBytes = stage_bytes(TN);
+  constexpr int kTgtBytes = TN * kKt;  // one target operand box per stage
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte align the operand region
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -309,12 +333,14 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   uint64_t* accbar = empty + kStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accbar + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
-  // the tile's target marginals nf, np, nfp as floats (epilogue operands)
+  // the tile's target marginals nf, np, nfp as floats and c1/c2a for the target
+  // states (x1, x0) = 11, 01, 10, 00 (epilogue operands)
   float* tmarg = reinterpret_cast<float*>(smem + kStages * kStageBytes + 256);
+  float* tq = tmarg + 3 * kTile;
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
-  const int m0 = blockIdx.y * kTile;  // targets
+  const int m0 = blockIdx.y * TN;     // targets
   const int n0 = blockIdx.x * kTile;  // sources
   const int nk = (FP4 ? prm.Lpad / 2 : prm.Lpad) / kKt;  // 128-byte K stages
 
@@ -362,13 +388,13 @@ __global__ void __launch_bounds__(kB2Threads, 1)
         break;
       }
       unsigned char* buf = stage_base + s * kStageBytes;
-      mbar_expect_tx(&full[s], kTmaBytes);
+      mbar_expect_tx(&full[s], kStageBytes);
       const int x0 = k * kKt;
-      // one 128-byte x 128-row box per operand, 128-byte swizzled
-      tma_load_2d(buf + 0 * kOpBytes, &maps.FP, x0, m0, &full[s]);
-      tma_load_2d(buf + 1 * kOpBytes, &maps.P, x0, m0, &full[s]);
-      tma_load_2d(buf + 2 * kOpBytes, &maps.F, x0, m0, &full[s]);
-      tma_load_2d(buf + 3 * kOpBytes, &maps.P, x0, n0, &full[s]);
+      // one 128-byte wide box per operand (TN or 128 rows), 128-byte swizzled
+      tma_load_2d(buf + 0 * kTgtBytes, &maps.FP, x0, m0, &full[s]);
+      tma_load_2d(buf + 1 * kTgtBytes, &maps.Pt, x0, m0, &full[s]);
+      tma_load_2d(buf + 2 * kTgtBytes, &maps.F, x0, m0, &full[s]);
+      tma_load_2d(buf + 3 * kTgtBytes, &maps.Ps, x0, n0, &full[s]);
       issued = k + 1;
     }
     if (!ok) {
@@ -385,11 +411,11 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   // back to back. The source tile P_j is the A operand (M = 128 lanes = sources)
   // and the target tiles are B: [FP_i; P_i] (adjacent in the stage, one N = 256
   // MMA) and F_i (N = 128), so a K step reads P_j twice instead of three times
-  // (20 KB of shared memory instead of 24; shared-memory bandwidth bounds the
-  // main loop). TMEM columns 0-127 = C^T, 128-255 = D^T, 256-383 = E^T.
+  // (20 KB of shared memory instead of 24 at TN = 128). TMEM columns 0..TN-1 =
+  // C^T, TN..2TN-1 = D^T, 256..256+TN-1 = E^T.
   if (tid == 32) {
-    const uint32_t idesc256 = FP4 ? idesc_mxf4(kTile, 2 * kTile) : idesc_i8(kTile, 2 * kTile);
-    const uint32_t idesc128 = FP4 ? idesc_mxf4(kTile, kTile) : idesc_i8(kTile, kTile);
+    const uint32_t idesc256 = FP4 ? idesc_mxf4(kTile, 2 * TN) : idesc_i8(kTile, 2 * TN);
+    const uint32_t idesc128 = FP4 ? idesc_mxf4(kTile, TN) : idesc_i8(kTile, TN);
     bool ok = true;
     for (int k = 0; k < nk; ++k) {
       const int s = k % kStages;
@@ -400,9 +426,9 @@ __global__ void __launch_bounds__(kB2Threads, 1)
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       unsigned char* buf = stage_base + s * kStageBytes;
-      const uint32_t bFPP = smem_u32(buf + 0 * kOpBytes);  // FP_i rows, then P_i rows
-      const uint32_t bF = smem_u32(buf + 2 * kOpBytes);
-      const uint32_t aPj = smem_u32(buf + 3 * kOpBytes);
+      const uint32_t bFPP = smem_u32(buf + 0 * kTgtBytes);  // FP_i rows, then P_i rows
+      const uint32_t bF = smem_u32(buf + 2 * kTgtBytes);
+      const uint32_t aPj = smem_u32(buf + 3 * kTgtBytes);
 #pragma unroll
       for (int kk = 0; kk < kKt / 32; ++kk) {
         const uint32_t off = kk * 32;  // 32-byte K step inside the 128-byte swizzle row
@@ -428,11 +454,25 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   }
 
   // ---- epilogue: 16 warps; lane quarter warp % 4, column quarter warp / 4 ---
-  // (the warps that neither load nor issue stage the target marginals first)
+  // (the warps that neither load nor issue stage the target marginals first;
+  // a c2a of 0 gives q = inf or NaN, never read: its cells are empty)
   if (tid >= 64) {
-    for (int k = tid - 64; k < 3 * kTile; k += kB2Threads - 64) {
-      const int c = k / kTile, i = m0 + (k - c * kTile);
-      tmarg[k] = i < prm.n ? (float)prm.marg[(int64_t)c * prm.n + i] : 0.f;
+    for (int k = tid - 64; k < TN; k += kB2Threads - 64) {
+      const int i = m0 + k;
+      float nf = 0.f, np_ = 0.f, nfp = 0.f;
+      if (i < prm.n) {
+        nf = (float)prm.marg[i];
+        np_ = (float)prm.marg[(int64_t)prm.n + i];
+        nfp = (float)prm.marg[2 * (int64_t)prm.n + i];
+      }
+      tmarg[k] = nf;
+      tmarg[kTile + k] = np_;
+      tmarg[2 * kTile + k] = nfp;
+      const float N = (float)prm.L, c1_1 = np_, c1_0 = N - np_;
+      tq[k] = c1_1 / nfp;
+      tq[kTile + k] = c1_1 / (np_ - nfp);
+      tq[2 * kTile + k] = c1_0 / (nf - nfp);
+      tq[3 * kTile + k] = c1_0 / (N - nf - np_ + nfp);
     }
   }
   bool ok_acc = mbar_wait_sleep(accbar, 0, 200);
@@ -442,56 +482,19 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   const bool run = ok_acc && (*(volatile int*)abort_flag == 0);
   const int lq = warp & 3, cq = warp >> 2;
   const int j = n0 + lq * 32 + (tid & 31);  // source gene of this thread's TMEM lane
-  const float N = (float)prm.L;
-  const float invL = 1.0f / N;
   const float npj = j < prm.n ? (float)prm.marg[prm.n + j] : 0.f;
   const uint32_t lane_base = tmem + ((uint32_t)(lq * 32) << 16);
-  for (int cb = cq * (kTile / 4); cb < (cq + 1) * (kTile / 4); cb += 16) {
-    uint32_t rc[16], rd[16], re[16];
-    tmem_ld16(lane_base + 0 + cb, rc);
-    tmem_ld16(lane_base + 128 + cb, rd);
-    tmem_ld16(lane_base + 256 + cb, re);
-    tmem_wait_ld();
-    if (!run || j >= prm.n) continue;
-    const int i0 = m0 + cb;  // first target of the 16 (the same for every lane: broadcast loads)
-    float* orow = prm.out + (int64_t)j * prm.out_ld;
-#pragma unroll
-    for (int q0 = 0; q0 < 16; q0 += 4) {
-      float res[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int q = q0 + u;
-        const int ti = cb + q;  // target within the tile (marginals 0 beyond n)
-        const float nf = tmarg[ti], np_ = tmarg[kTile + ti], nfp = tmarg[2 * kTile + ti];
-        const float c1_1 = np_, c1_0 = N - np_;
-        const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
-        const float C = FP4 ? __uint_as_float(rc[q]) : (float)rc[q];
-        const float Dv = FP4 ? __uint_as_float(rd[q]) : (float)rd[q];
-        const float E = FP4 ? __uint_as_float(re[q]) : (float)re[q];
-        const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
-        float te = 0.f;
-        te += cell_term(C, c1_1, c2a11, c2b11);                                   // [1,1,1]
-        te += cell_term(Dv - C, c1_1, c2a01, c2b11);                              // [0,1,1]
-        te += cell_term(E - C, c1_0, c2a10, c2b01);                               // [1,0,1]
-        te += cell_term(npj - Dv - E + C, c1_0, c2a00, c2b01);                    // [0,0,1]
-        te += cell_term(nfp - C, c1_1, c2a11, c2b10);                             // [1,1,0]
-        te += cell_term(np_ - Dv - nfp + C, c1_1, c2a01, c2b10);                  // [0,1,0]
-        te += cell_term(nf - E - nfp + C, c1_0, c2a10, c2b00);                    // [1,0,0]
-        te += cell_term(N - nf - np_ - npj + nfp + Dv + E - C, c1_0, c2a00, c2b00);  // [0,0,0]
-        res[u] = te * invL;
-      }
-      // four consecutive targets of row j: one 16-byte store when they are all
-      // inside the matrix, off the diagonal and aligned; else one by one
-      const int ia = i0 + q0;
-      if (prm.vec_out && ia + 4 <= prm.n && (j < ia || j >= ia + 4)) {
-        *reinterpret_cast<float4*>(orow + ia) = make_float4(res[0], res[1], res[2], res[3]);
-      } else {
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (ia + u < prm.n && ia + u != j) orow[ia + u] = res[u];
-      }
-    }
+  // TN / 4 target columns per warp, in chunks of 16, 8 and 4 (TN / 4 is a multiple of 4)
+  const bool active = run && j < prm.n;
+  int cb = cq * (TN / 4);
+  const int ce = cb + TN / 4;
+  for (; cb + 16 <= ce; cb += 16)
+    b2_cells<FP4, 16>(prm, lane_base, cb, TN, m0, j, active, npj, tmarg, tq);
+  if (cb + 8 <= ce) {
+    b2_cells<FP4, 8>(prm, lane_base, cb, TN, m0, j, active, npj, tmarg, tq);
+    cb += 8;
   }
+  if (cb + 4 <= ce) b2_cells<FP4, 4>(prm, lane_base, cb, TN, m0, j, active, npj, tmarg, tq);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
@@ -522,12 +525,12 @@ static EncodeTiledFn encode_fn() {
 }
 
 static int make_map(CUtensorMap* map, const uint8_t* base, int rows, int64_t cols,
-                    int64_t stride) {
+                    int64_t stride, int box_rows) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return fail(TENEX_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)stride};
-  const cuuint32_t box[2] = {(cuuint32_t)kKt, (cuuint32_t)kTile};
+  const cuuint32_t box[2] = {(cuuint32_t)kKt, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)base, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -556,10 +559,43 @@ extern "C" size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t 
                   256);
 }
 
-extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int n_vars,
-                                           int64_t row_len, int64_t lag, float* out,
-                                           int64_t out_ld, void* workspace,
-                                           size_t workspace_bytes, int kind, void* stream_) {
+// One GEMM launch of target-tile width TN: ceil(n / 128) x ceil(n / TN) tiles.
+template <bool FP4, int TN>
+static int launch_gemm(const B2Maps& maps, const B2Params& prm, cudaStream_t stream) {
+  const int smem = kStages * stage_bytes(TN) + 1024 + 256 + 7 * kTile * 4;
+  cudaError_t e = cudaFuncSetAttribute(b2_gemm_kernel<FP4, TN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
+  const dim3 grid((unsigned)((prm.n + kTile - 1) / kTile), (unsigned)((prm.n + TN - 1) / TN));
+  b2_gemm_kernel<FP4, TN><<<grid, kB2Threads, smem, stream>>>(maps, prm);
+  return check_launch("b2_gemm_kernel");
+}
+
+// Target-tile width for n genes on `sms` SMs: the one whose tiles (one CTA per
+// SM at a time) finish in the fewest tile-rows, counting each tile's fixed
+// pipeline fill as 16 rows; ties go to the wider tile. n = 2,000 on 148 SMs:
+// TN = 112 (288 tiles, two rounds of 112 rows) against TN = 128 (256 tiles, two
+// rounds of 128 rows).
+static int pick_tile_n(int n, int sms) {
+  const int64_t src_tiles = (n + kTile - 1) / kTile;
+  int best = kTileN[0];
+  int64_t best_cost = INT64_MAX;
+  for (int tn : kTileN) {
+    const int64_t tiles = src_tiles * ((n + tn - 1) / tn);
+    const int64_t rounds = (tiles + sms - 1) / (sms > 0 ? sms : 1);
+    const int64_t cost = rounds * (tn + 16);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = tn;
+    }
+  }
+  return best;
+}
+
+extern "C" int tenex_te_binary_matrix_ex(const uint8_t* bins, int64_t ld, int n_vars,
+                                         int64_t row_len, int64_t lag, float* out,
+                                         int64_t out_ld, void* workspace, size_t workspace_bytes,
+                                         int kind, int tile_n, void* stream_) {
   cudaStream_t stream = as_stream(stream_);
   if (!bins || !out || !workspace) return fail(TENEX_ERR_BADARG, "bins, out, workspace non-NULL");
   if (n_vars < 2) return fail(TENEX_ERR_BADARG, "n_vars must be >= 2");
@@ -571,6 +607,15 @@ extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int 
   if (out_ld < n_vars) return fail(TENEX_ERR_BADARG, "out_ld must be >= n_vars");
   if (kind < 0 || kind > 2)
     return fail(TENEX_ERR_BADARG, "kind must be 0 (default), 1 (int8) or 2 (4-bit)");
+  int tn = tile_n;
+  if (tn == 0) {
+    DevAttr A;
+    const int ast = current_device_attr(&A);
+    if (ast) return ast;
+    tn = pick_tile_n(n_vars, A.sm_count);
+  } else if (std::find(std::begin(kTileN), std::end(kTileN), tn) == std::end(kTileN)) {
+    return fail(TENEX_ERR_BADARG, "tile_n must be 0 (automatic) or one of 128, 112, 96, 80, 64");
+  }
   const bool fp4 = kind != 1;
   const int64_t L = row_len - lag;
   if (L >= ((int64_t)1 << 24))
@@ -586,28 +631,35 @@ extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int 
   const int64_t ob = b2_ops_bytes(n_vars, L);
   int32_t* marg = reinterpret_cast<int32_t*>(ws + ob);
   int* err = reinterpret_cast<int*>(ws + ob + round_up(3 * (int64_t)n_vars * 4, 256));
-  cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), stream);
+  // the per-gene counts (accumulated by the pack) and the error word, in one memset
+  cudaError_t e = cudaMemsetAsync(marg, 0, (size_t)((unsigned char*)err - (unsigned char*)marg) +
+                                               sizeof(int), stream);
   if (e != cudaSuccess) return check_cuda(e, "memset");
-  const int pack_grid = (n_vars + kPackWarps - 1) / kPackWarps;
+  const int seg = fp4 ? PackChunk<true>::kSeg : PackChunk<false>::kSeg;
+  const int nseg = (int)((Lpad + seg - 1) / seg);
+  const int64_t pack_warps = (int64_t)n_vars * nseg;
+  const unsigned pack_grid = (unsigned)((pack_warps + kPackWarps - 1) / kPackWarps);
   if (fp4)
-    b2_pack4_kernel<<<pack_grid, kPackWarps * 32, 0, stream>>>(bins, ld, n_vars, (int)L,
-                                                                (int)lag, (int)Lpad, ops, marg,
-                                                                err);
+    b2_pack_kernel<true><<<pack_grid, kPackWarps * 32, 0, stream>>>(
+        bins, ld, n_vars, (int)L, (int)lag, (int)Lpad, nseg, ops, marg, err);
   else
-    b2_pack_kernel<<<pack_grid, kPackWarps * 32, 0, stream>>>(bins, ld, n_vars, (int)L, (int)lag,
-                                                               (int)Lpad, ops, marg, err);
+    b2_pack_kernel<false><<<pack_grid, kPackWarps * 32, 0, stream>>>(
+        bins, ld, n_vars, (int)L, (int)lag, (int)Lpad, nseg, ops, marg, err);
   int st = check_launch("b2_pack_kernel");
   if (st) return st;
   B2Maps maps;
   if (fp4) {
     const int64_t rb = Lpad / 2;
-    if ((st = make_map(&maps.F, ops, n_vars, rb, rb))) return st;
-    if ((st = make_map(&maps.FP, ops + (int64_t)n_vars * rb, n_vars, rb, rb))) return st;
-    if ((st = make_map(&maps.P, ops + 2 * (int64_t)n_vars * rb, n_vars, rb, rb))) return st;
+    if ((st = make_map(&maps.F, ops, n_vars, rb, rb, tn))) return st;
+    if ((st = make_map(&maps.FP, ops + (int64_t)n_vars * rb, n_vars, rb, rb, tn))) return st;
+    if ((st = make_map(&maps.Pt, ops + 2 * (int64_t)n_vars * rb, n_vars, rb, rb, tn))) return st;
+    if ((st = make_map(&maps.Ps, ops + 2 * (int64_t)n_vars * rb, n_vars, rb, rb, kTile)))
+      return st;
   } else {
-    if ((st = make_map(&maps.F, ops, n_vars, Lpad, Lpad))) return st;
-    if ((st = make_map(&maps.P, bins, n_vars, L, ld))) return st;
-    if ((st = make_map(&maps.FP, ops + (int64_t)n_vars * Lpad, n_vars, Lpad, Lpad))) return st;
+    if ((st = make_map(&maps.F, ops, n_vars, Lpad, Lpad, tn))) return st;
+    if ((st = make_map(&maps.Pt, bins, n_vars, L, ld, tn))) return st;
+    if ((st = make_map(&maps.Ps, bins, n_vars, L, ld, kTile))) return st;
+    if ((st = make_map(&maps.FP, ops + (int64_t)n_vars * Lpad, n_vars, Lpad, Lpad, tn))) return st;
   }
   B2Params prm;
   prm.n = n_vars;
@@ -618,20 +670,26 @@ extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int 
   prm.out_ld = out_ld;
   prm.vec_out = (out_ld % 4 == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) ? 1 : 0;
   prm.err = err;
-  const int smem = kStages * kStageBytes + 1024 + 256 + 3 * kTile * 4;
-  const unsigned tiles = (unsigned)((n_vars + kTile - 1) / kTile);
-  if (fp4) {
-    e = cudaFuncSetAttribute(b2_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             smem);
-    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
-    b2_gemm_kernel<true><<<dim3(tiles, tiles), kB2Threads, smem, stream>>>(maps, prm);
-  } else {
-    e = cudaFuncSetAttribute(b2_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             smem);
-    if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
-    b2_gemm_kernel<false><<<dim3(tiles, tiles), kB2Threads, smem, stream>>>(maps, prm);
+  switch (tn) {
+    case 128: return fp4 ? launch_gemm<true, 128>(maps, prm, stream)
+                         : launch_gemm<false, 128>(maps, prm, stream);
+    case 112: return fp4 ? launch_gemm<true, 112>(maps, prm, stream)
+                         : launch_gemm<false, 112>(maps, prm, stream);
+    case 96: return fp4 ? launch_gemm<true, 96>(maps, prm, stream)
+                        : launch_gemm<false, 96>(maps, prm, stream);
+    case 80: return fp4 ? launch_gemm<true, 80>(maps, prm, stream)
+                        : launch_gemm<false, 80>(maps, prm, stream);
+    default: return fp4 ? launch_gemm<true, 64>(maps, prm, stream)
+                        : launch_gemm<false, 64>(maps, prm, stream);
   }
-  return check_launch("b2_gemm_kernel");
+}
+
+extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int n_vars,
+                                           int64_t row_len, int64_t lag, float* out,
+                                           int64_t out_ld, void* workspace,
+                                           size_t workspace_bytes, int kind, void* stream) {
+  return tenex_te_binary_matrix_ex(bins, ld, n_vars, row_len, lag, out, out_ld, workspace,
+                                   workspace_bytes, kind, 0, stream);
 }
 
 extern "C" int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,

@@ -20,11 +20,19 @@ from tenex_b200.kernels import device as D
 OPERANDS = {"default": 0, "int8": 1, "fp4": 2}
 
 
+TILE_N = (128, 112, 96, 80, 64)
+
+
 def te_binary_matrix(db: D.DeviceBins, tau: int = 1, out: torch.Tensor | None = None,
-                     check: bool = True, operands: str = "default") -> torch.Tensor:
+                     check: bool = True, operands: str = "default",
+                     tile_n: int = 0) -> torch.Tensor:
     """(n, n) float32 device matrix with [src, tgt] = TE(src -> tgt), diagonal 0.
     operands: "int8" (kind::i8 MMAs), "fp4" (the 0/1 values as packed E2M1,
-    kind::mxf4) or "default" (fp4); the counts and TE are the same."""
+    kind::mxf4) or "default" (fp4); the counts and TE are the same.
+    tile_n: targets per GEMM tile, 0 = chosen from n and the SM count, else one
+    of TILE_N (the same matrix bit for bit)."""
+    if tile_n and tile_n not in TILE_N:
+        raise ValueError(f"tile_n={tile_n}: expected 0 or one of {TILE_N}")
     dev = db.data.device
     n = db.n
     lag = tau * db.K
@@ -33,8 +41,8 @@ def te_binary_matrix(db: D.DeviceBins, tau: int = 1, out: torch.Tensor | None = 
     nb = int(native.lib().tenex_b2_workspace_bytes(n, db.row_len, lag))
     ws = torch.empty(nb, dtype=torch.uint8, device=dev)
     s = native.stream_ptr()
-    native.call("tenex_te_binary_matrix_kind", db.ptr(), db.ld, n, db.row_len, lag,
-                out.data_ptr(), n, ws.data_ptr(), nb, OPERANDS[operands], s)
+    native.call("tenex_te_binary_matrix_ex", db.ptr(), db.ld, n, db.row_len, lag,
+                out.data_ptr(), n, ws.data_ptr(), nb, OPERANDS[operands], int(tile_n), s)
     if check:
         native.call("tenex_b2_status", ws.data_ptr(), n, db.row_len, lag, s)
     return out

@@ -85,6 +85,7 @@ _SIGS = {
     "tenex_b2_workspace_bytes": [_I, _L, _L],
     "tenex_te_binary_matrix": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _P],
     "tenex_te_binary_matrix_kind": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _I, _P],
+    "tenex_te_binary_matrix_ex": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _I, _I, _P],
     "tenex_b2_status": [_P, _I, _L, _L, _P],
     "tenex_dpi_trim": [_P, _L, _I, _P, _P, ctypes.c_float, _P, _L, _P],
     "tenex_dpi_trim_sparse": [_P, _P, _P, _I, _P, _P, ctypes.c_float, _P, _P],

@@ -74,3 +74,21 @@ def test_launch_shape_argument_checks():
     assert _status("tenex_te_launch_shape", 100, 1, 0, None, *refs) == bad       # b_max 0
     assert _status("tenex_te_launch_shape", 100, 1, 256, None, *refs) == bad     # b_max 256
     assert _status("tenex_te_launch_shape", 1 << 31, 1, 8, None, *refs) == unsup  # >= 2^31
+
+
+def test_binary_matrix_tile_width_checks():
+    n, T, ld = 4, 64, 64
+    bins = np.zeros(n * ld + 64, np.uint8)
+    out = np.zeros(n * n + 16, np.float32)
+    ws = np.zeros(4096 + 256, np.uint8)
+    bb = _addr(bins) + (-_addr(bins)) % 16
+    wb = _addr(ws) + (-_addr(ws)) % 256
+    bad = native.TENEX_ERR_BADARG
+    for tn in (7, 48, 256, -1):
+        assert _status("tenex_te_binary_matrix_ex", bb, ld, n, T, 1, _addr(out), n, wb, 4096,
+                       0, tn, 0) == bad
+    assert _status("tenex_te_binary_matrix_ex", bb, ld, n, T, 1, _addr(out), n, wb, 4096,
+                   3, 128, 0) == bad                      # unknown operand form
+    from tenex_b200.kernels.gemm_b2 import te_binary_matrix
+    with pytest.raises(ValueError, match="tile_n"):
+        te_binary_matrix(None, 1, tile_n=100)

@@ -6,15 +6,15 @@ import torch
 from oracle import oracle as O
 from tenex_b200 import native, workloads as W
 from tenex_b200.kernels import device as D
-from tenex_b200.kernels.gemm_b2 import te_binary_matrix
+from tenex_b200.kernels.gemm_b2 import TILE_N, te_binary_matrix
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-6
 
 
-def _run(x, cuda, tau=1, operands="default"):
+def _run(x, cuda, tau=1, operands="default", tile_n=0):
     db = D.pack_bins(x, cuda)
-    m = te_binary_matrix(db, tau, operands=operands).cpu().numpy()
+    m = te_binary_matrix(db, tau, operands=operands, tile_n=tile_n).cpu().numpy()
     torch.cuda.synchronize()
     return m
 
@@ -27,6 +27,20 @@ def test_binary_matrix_matches_oracle(cuda, n, T, operands):
     ref = O.te_matrix(x.astype(np.int32), np.full(n, 2, np.int32))
     assert np.all(np.diag(m) == 0)
     assert np.max(np.abs(m - ref)) <= TOL
+
+
+@pytest.mark.parametrize("operands", ["int8", "fp4"])
+@pytest.mark.parametrize("tile_n", TILE_N)
+@pytest.mark.parametrize("n,T", [(130, 300), (257, 1100)])
+def test_every_tile_width_matches_oracle(cuda, n, T, tile_n, operands):
+    # each target-tile width (MMA N = tile_n and 2 tile_n; ragged last tiles at
+    # these n) against the oracle, bitwise equal to the automatic choice
+    x, _ = W.cfg2_binary(n=n, T=T, seed=3 * n + T, n_planted=3)
+    m = _run(x, cuda, operands=operands, tile_n=tile_n)
+    ref = O.te_matrix(x.astype(np.int32), np.full(n, 2, np.int32))
+    assert np.all(np.diag(m) == 0)
+    assert np.max(np.abs(m - ref)) <= TOL
+    assert np.array_equal(m.view(np.uint32), _run(x, cuda, operands=operands).view(np.uint32))
 
 
 @pytest.mark.parametrize("operands", ["int8", "fp4"])
@@ -85,3 +99,6 @@ def test_binary_full_size_sampled_and_deterministic(cuda):
     # the int8 and 4-bit operand forms give the same exact counts, so the same bits
     assert np.array_equal(m.view(np.uint32), _run(x, cuda, operands="int8").view(np.uint32))
     assert np.array_equal(m.view(np.uint32), _run(x, cuda, operands="fp4").view(np.uint32))
+    # and every target-tile width the same bits
+    for tn in TILE_N:
+        assert np.array_equal(m.view(np.uint32), _run(x, cuda, tile_n=tn).view(np.uint32)), tn
