@@ -602,13 +602,14 @@ def binary_leg(dev, reps: int = 5) -> dict:
 
     from tenex_b200 import native, workloads as W
     from tenex_b200.kernels import device as D
-    from tenex_b200.kernels.gemm_b2 import te_binary_matrix
+    from tenex_b200.kernels.gemm_b2 import te_binary_matrix, tile_width
     x, _ = W.cfg2_binary()
     n, T = x.shape
     db = D.pack_bins(x, dev)
     out = torch.zeros((n, n), dtype=torch.float32, device=dev)
     L = T - 1
     tiles = -(-n // 128)
+    tn = tile_width(n)
     forms = {}
     for form, kpad, probe in (("fp4", 256, native.probe_tc_fp4), ("int8", 128, native.probe_tc_int8)):
         for _ in range(3):
@@ -625,6 +626,11 @@ def binary_leg(dev, reps: int = 5) -> dict:
         Lpad = -(-L // kpad) * kpad
         ops = 6.0 * (tiles * 128) ** 2 * Lpad      # 3 GEMMs of (n x Lpad) x (Lpad x n)
         peak = max(probe(100_000) for _ in range(2))
+        # the GEMM's own MMA sequence issued back to back (no copies, no waits): the
+        # instruction-mix bound of its main loop; the work the MMAs execute is
+        # 6 x (sources padded to 128) x (targets padded to the tile width) x L_pad
+        seq = max(native.probe_tc_gemm_b2(form, tn, 2000) for _ in range(2))
+        ops_exec = 6.0 * (tiles * 128) * (-(-n // tn) * tn) * Lpad
         forms[form] = {"ms": ms, "pairs_per_s": n * (n - 1) / (ms / 1e3),
                        "roofline": {"bound": "tensor", "achieved": ops / (ms / 1e3) / 1e12,
                                     "peak": peak / 1e12,
@@ -633,7 +639,13 @@ def binary_leg(dev, reps: int = 5) -> dict:
                                     "note": "achieved = 6*n_pad^2*L_pad ops (C, D, E) / device "
                                             "time of pack + GEMM; peak = the live %s probe"
                                             % ("tenex_probe_tc_fp4" if form == "fp4"
-                                               else "tenex_probe_tc_int8")}}
+                                               else "tenex_probe_tc_int8"),
+                                    "sequence_peak": seq / 1e12,
+                                    "frac_of_sequence": ops_exec / (ms / 1e3) / seq,
+                                    "sequence_note": "the GEMM's own MMA sequence (tile width "
+                                                     "%d) back to back on every SM "
+                                                     "(tenex_probe_tc_gemm_b2), against the "
+                                                     "MMA work executed per call" % tn}}
     # end to end: pinned host bins -> padded device rows -> matrix -> pinned host matrix
     # (the reference's compute_te_gemm_b2 is timed the same way, host to host)
     x_pin = torch.from_numpy(np.ascontiguousarray(x, dtype=np.uint8)).pin_memory()
@@ -657,6 +669,7 @@ def binary_leg(dev, reps: int = 5) -> dict:
     d = forms["fp4"]
     return {"workload": "cfg2: 2000 genes x 5000 cells, binary Markov bins, GEMM-B2",
             "pairs_per_s": d["pairs_per_s"], "ms": d["ms"], "operands": "fp4 (kind::mxf4)",
+            "tile_n": tn,
             "roofline": d["roofline"], "int8_form": forms["int8"],
             "e2e": {"value": n * (n - 1) / (e2e_ms / 1e3), "unit": "pairs/s", "ms": e2e_ms,
                     "h2d_bytes_per_step": int(x.size), "d2h_bytes_per_step": int(n * n * 4),

@@ -260,13 +260,16 @@ int tenex_te_binary_matrix(const uint8_t* bins, int64_t ld, int n_vars, int64_t 
 int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
                                 int64_t lag, float* out, int64_t out_ld, void* workspace,
                                 size_t workspace_bytes, int kind, void* stream);
-/* Same, with the target-tile width of the GEMM chosen by the caller: tile_n =
- * 0 picks it from n_vars and the SM count (the width whose tiles finish in the
- * fewest rounds), else one of 128, 112, 96, 80, 64 (TENEX_ERR_BADARG otherwise).
- * Every width gives bitwise the same matrix. */
+/* Same, with the GEMM's target-tile width chosen by the caller: tile_n = 0
+ * picks it from n_vars and the SM count (the width whose tiles finish in the
+ * fewest rounds, tenex_b2_tile_n), else one of 128, 112, 96, 80, 64
+ * (TENEX_ERR_BADARG otherwise). Every width gives bitwise the same matrix. */
 int tenex_te_binary_matrix_ex(const uint8_t* bins, int64_t ld, int n_vars, int64_t row_len,
                               int64_t lag, float* out, int64_t out_ld, void* workspace,
                               size_t workspace_bytes, int kind, int tile_n, void* stream);
+/* The target-tile width tenex_te_binary_matrix picks on the current device for
+ * n_vars genes. */
+int tenex_b2_tile_n(int n_vars, int* tile_n);
 /* Error word of the last tenex_te_binary_matrix call on this workspace
  * (synchronises `stream`): TENEX_ERR_BADDATA if a bin was not 0 or 1,
  * TENEX_ERR_TIMEOUT if a pipeline wait expired. */
@@ -349,6 +352,14 @@ int tenex_probe_tc_int8(int iters, double* ops, float* ms, void* stream);
  * with unit UE8M0 block scales) tensor-pipe rate, M=128, N=256, K=64 per MMA, the
  * denominator of the 4-bit GEMM-B2 form; same conventions as tenex_probe_tc_int8. */
 int tenex_probe_tc_fp4(int iters, double* ops, float* ms, void* stream);
+/* Roofline probe (no reference counterpart): the GEMM-B2 kernel's own MMA sequence
+ * (per 128-byte K stage four K steps of an N = 2 tile_n and an N = tile_n MMA,
+ * swizzled operands walking three stage buffers) issued back to back on every SM
+ * with no copies and no waits: the rate that bounds the GEMM's main loop for
+ * that instruction mix. kind: 1 = int8, 2 = 4-bit; tile_n in {128, 112, 96, 80,
+ * 64}; `stages` K stages per SM; ops = 6 * 128 * tile_n * K per stage per SM. */
+int tenex_probe_tc_gemm_b2(int kind, int tile_n, int stages, double* ops, float* ms,
+                           void* stream);
 /* Roofline probe (no reference counterpart): FP32 min/max issue rate, the bound of
  * tenex_dpi_trim. Every thread of 2 CTAs x 1024 threads per SM runs `iters` steps
  * of 8 independent chains (two min.f32 and one three-input max.f32 each); returns

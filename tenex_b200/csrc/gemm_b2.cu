@@ -252,10 +252,48 @@ constexpr int kB2Threads = 512;
 // up to N = 256) at kSfbCol; 8 columns each hold every layout those take.
 constexpr uint32_t kSfaCol = 384, kSfbCol = 392;
 
+// TE(src -> target ti of the tile) from the three sums C, D, E of the pair, the
+// target's staged marginals (tmarg: nf, np, nfp; tq: c1/c2a for the target
+// states 11, 01, 10, 00) and the source's np (npj): the 8 cells and their terms.
+__device__ __forceinline__ float b2_pair_te(float C, float Dv, float E, int ti, float npj,
+                                            float N, const float* tmarg, const float* tq) {
+  const float nf = tmarg[ti], np_ = tmarg[kTile + ti], nfp = tmarg[2 * kTile + ti];
+  const float c1_1 = np_, c1_0 = N - np_;
+  const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
+  const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
+  const float q11 = tq[ti], q01 = tq[kTile + ti], q10 = tq[2 * kTile + ti],
+              q00 = tq[3 * kTile + ti];
+  const float rb11 = __fdividef(1.f, c2b11), rb01 = __fdividef(1.f, c2b01),
+              rb10 = __fdividef(1.f, c2b10), rb00 = __fdividef(1.f, c2b00);
+  float te = 0.f;
+  te += cell_term(C, c1_1, c2a11, c2b11, q11, rb11);                                // [1,1,1]
+  te += cell_term(Dv - C, c1_1, c2a01, c2b11, q01, rb11);                           // [0,1,1]
+  te += cell_term(E - C, c1_0, c2a10, c2b01, q10, rb01);                            // [1,0,1]
+  te += cell_term(npj - Dv - E + C, c1_0, c2a00, c2b01, q00, rb01);                 // [0,0,1]
+  te += cell_term(nfp - C, c1_1, c2a11, c2b10, q11, rb10);                          // [1,1,0]
+  te += cell_term(np_ - Dv - nfp + C, c1_1, c2a01, c2b10, q01, rb10);               // [0,1,0]
+  te += cell_term(nf - E - nfp + C, c1_0, c2a10, c2b00, q10, rb00);                 // [1,0,0]
+  te += cell_term(N - nf - np_ - npj + nfp + Dv + E - C, c1_0, c2a00, c2b00, q00,
+                  rb00);                                                            // [0,0,0]
+  return te;
+}
+
+// Four consecutive targets ia .. ia + 3 of source row j: one 16-byte store when
+// they are all inside the matrix, off the diagonal and aligned; else one by one.
+__device__ __forceinline__ void b2_store4(const B2Params& prm, float* orow, int ia, int j,
+                                          const float (&res)[4]) {
+  if (prm.vec_out && ia + 4 <= prm.n && (j < ia || j >= ia + 4)) {
+    *reinterpret_cast<float4*>(orow + ia) = make_float4(res[0], res[1], res[2], res[3]);
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (ia + u < prm.n && ia + u != j) orow[ia + u] = res[u];
+  }
+}
+
 // TE of NC consecutive targets (tile columns cb .. cb + NC - 1) for the source
 // of this thread's TMEM lane: the three sums from TMEM (every lane of the warp
-// loads, as tcgen05.ld requires), the 8 cells from them and the marginals, and
-// row stores of four targets at a time.
+// loads, as tcgen05.ld requires), then b2_pair_te and b2_store4.
 template <bool FP4, int NC>
 __device__ __forceinline__ void b2_cells(const B2Params& prm, uint32_t lane_base, int cb, int TN,
                                          int m0, int j, bool active, float npj,
@@ -268,7 +306,6 @@ __device__ __forceinline__ void b2_cells(const B2Params& prm, uint32_t lane_base
   if (!active) return;
   const float N = (float)prm.L;
   const float invL = 1.0f / N;
-  const int i0 = m0 + cb;  // first target of the NC (the same for every lane: broadcast loads)
   float* orow = prm.out + (int64_t)j * prm.out_ld;
 #pragma unroll
   for (int q0 = 0; q0 < NC; q0 += 4) {
@@ -276,40 +313,12 @@ __device__ __forceinline__ void b2_cells(const B2Params& prm, uint32_t lane_base
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int q = q0 + u;
-      const int ti = cb + q;  // target within the tile (marginals 0 beyond n)
-      const float nf = tmarg[ti], np_ = tmarg[kTile + ti], nfp = tmarg[2 * kTile + ti];
-      const float c1_1 = np_, c1_0 = N - np_;
-      const float c2a11 = nfp, c2a01 = np_ - nfp, c2a10 = nf - nfp, c2a00 = N - nf - np_ + nfp;
       const float C = FP4 ? __uint_as_float(rc[q]) : (float)rc[q];
       const float Dv = FP4 ? __uint_as_float(rd[q]) : (float)rd[q];
       const float E = FP4 ? __uint_as_float(re[q]) : (float)re[q];
-      const float c2b11 = Dv, c2b01 = npj - Dv, c2b10 = np_ - Dv, c2b00 = N - np_ - npj + Dv;
-      const float q11 = tq[ti], q01 = tq[kTile + ti], q10 = tq[2 * kTile + ti],
-                  q00 = tq[3 * kTile + ti];
-      const float rb11 = __fdividef(1.f, c2b11), rb01 = __fdividef(1.f, c2b01),
-                  rb10 = __fdividef(1.f, c2b10), rb00 = __fdividef(1.f, c2b00);
-      float te = 0.f;
-      te += cell_term(C, c1_1, c2a11, c2b11, q11, rb11);                                // [1,1,1]
-      te += cell_term(Dv - C, c1_1, c2a01, c2b11, q01, rb11);                           // [0,1,1]
-      te += cell_term(E - C, c1_0, c2a10, c2b01, q10, rb01);                            // [1,0,1]
-      te += cell_term(npj - Dv - E + C, c1_0, c2a00, c2b01, q00, rb01);                 // [0,0,1]
-      te += cell_term(nfp - C, c1_1, c2a11, c2b10, q11, rb10);                          // [1,1,0]
-      te += cell_term(np_ - Dv - nfp + C, c1_1, c2a01, c2b10, q01, rb10);               // [0,1,0]
-      te += cell_term(nf - E - nfp + C, c1_0, c2a10, c2b00, q10, rb00);                 // [1,0,0]
-      te += cell_term(N - nf - np_ - npj + nfp + Dv + E - C, c1_0, c2a00, c2b00, q00,
-                      rb00);                                                            // [0,0,0]
-      res[u] = te * invL;
+      res[u] = b2_pair_te(C, Dv, E, cb + q, npj, N, tmarg, tq) * invL;
     }
-    // four consecutive targets of row j: one 16-byte store when they are all
-    // inside the matrix, off the diagonal and aligned; else one by one
-    const int ia = i0 + q0;
-    if (prm.vec_out && ia + 4 <= prm.n && (j < ia || j >= ia + 4)) {
-      *reinterpret_cast<float4*>(orow + ia) = make_float4(res[0], res[1], res[2], res[3]);
-    } else {
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (ia + u < prm.n && ia + u != j) orow[ia + u] = res[u];
-    }
+    b2_store4(prm, orow, m0 + cb + q0, j, res);
   }
 }
 
@@ -607,15 +616,12 @@ extern "C" int tenex_te_binary_matrix_ex(const uint8_t* bins, int64_t ld, int n_
   if (out_ld < n_vars) return fail(TENEX_ERR_BADARG, "out_ld must be >= n_vars");
   if (kind < 0 || kind > 2)
     return fail(TENEX_ERR_BADARG, "kind must be 0 (default), 1 (int8) or 2 (4-bit)");
-  int tn = tile_n;
-  if (tn == 0) {
-    DevAttr A;
-    const int ast = current_device_attr(&A);
-    if (ast) return ast;
-    tn = pick_tile_n(n_vars, A.sm_count);
-  } else if (std::find(std::begin(kTileN), std::end(kTileN), tn) == std::end(kTileN)) {
+  if (tile_n != 0 && std::find(std::begin(kTileN), std::end(kTileN), tile_n) == std::end(kTileN))
     return fail(TENEX_ERR_BADARG, "tile_n must be 0 (automatic) or one of 128, 112, 96, 80, 64");
-  }
+  DevAttr A;
+  const int ast = current_device_attr(&A);
+  if (ast) return ast;
+  const int tn = tile_n != 0 ? tile_n : pick_tile_n(n_vars, A.sm_count);
   const bool fp4 = kind != 1;
   const int64_t L = row_len - lag;
   if (L >= ((int64_t)1 << 24))
@@ -682,6 +688,15 @@ extern "C" int tenex_te_binary_matrix_ex(const uint8_t* bins, int64_t ld, int n_
     default: return fp4 ? launch_gemm<true, 64>(maps, prm, stream)
                         : launch_gemm<false, 64>(maps, prm, stream);
   }
+}
+
+extern "C" int tenex_b2_tile_n(int n_vars, int* tile_n) {
+  if (n_vars < 2 || !tile_n) return fail(TENEX_ERR_BADARG, "n_vars >= 2, tile_n non-NULL");
+  DevAttr A;
+  const int st = current_device_attr(&A);
+  if (st) return st;
+  *tile_n = pick_tile_n(n_vars, A.sm_count);
+  return TENEX_OK;
 }
 
 extern "C" int tenex_te_binary_matrix_kind(const uint8_t* bins, int64_t ld, int n_vars,

@@ -12,6 +12,8 @@
 // The entry point times the kernel with CUDA events on `stream` and returns the
 // number of increments and the milliseconds (synchronises the stream).
 //
+// tc_seq_probe: the GEMM-B2 kernel's MMA sequence back to back (below).
+//
 // tc_int8_probe: dense INT8 tensor-pipe throughput, the roofline of the GEMM-B2
 // path. One CTA per SM (its shared-memory request admits one), one thread issues
 // back-to-back tcgen05.mma.cta_group::1.kind::i8 of M = 128, N = 256, K = 32 from
@@ -123,9 +125,136 @@ __global__ void __launch_bounds__(128, 1) tc_probe(int iters, int* err) {
                  : "memory");
 }
 
+// The GEMM-B2 kernel's own MMA sequence issued back to back: per 128-byte K
+// stage, four K steps of two MMAs (the source tile as A against the targets
+// [FP; P] at N = 2 TN into TMEM columns 0.., and F at N = TN into columns 256..),
+// 128-byte swizzled K-major descriptors walking three stage buffers, as the
+// GEMM's main loop issues them, but with no copies and no waits: the rate that
+// bounds the GEMM's main loop for this instruction mix.
+constexpr int kSeqStageMax = (3 * 128 + 128) * 128;  // the widest stage (TN = 128)
+
+template <bool FP4>
+__global__ void __launch_bounds__(128, 1) tc_seq_probe(int tn, int stages, int* err) {
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  unsigned char* sm = (unsigned char*)(((uintptr_t)sm_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 3 * kSeqStageMax);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 3 * kSeqStageMax / 4; i += blockDim.x)
+    reinterpret_cast<uint32_t*>(sm)[i] = 0x22222222u * (uint32_t)(i & 1);  // E2M1 1.0 / int8 34
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (tid < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  constexpr uint32_t kSfa = 384, kSfb = 392;  // the GEMM's scale-factor columns
+  if (FP4) {
+    tmem_st8(tmem + ((uint32_t)(tid & ~31) << 16) + kSfa, 0x7f7f7f7fu);
+    tmem_st8(tmem + ((uint32_t)(tid & ~31) << 16) + kSfb, 0x7f7f7f7fu);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (tid == 0) {
+    const uint32_t i2 = FP4 ? idesc_mxf4(128, 2 * tn) : idesc_i8(128, 2 * tn);
+    const uint32_t i1 = FP4 ? idesc_mxf4(128, tn) : idesc_i8(128, tn);
+    const int stage = (3 * tn + 128) * 128, tgt = tn * 128;
+    for (int k = 0; k < stages; ++k) {
+      unsigned char* buf = sm + (k % 3) * stage;
+      const uint32_t bFPP = smem_u32(buf), bF = smem_u32(buf + 2 * tgt);
+      const uint32_t aP = smem_u32(buf + 3 * tgt);
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const uint32_t off = kk * 32;
+        const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+        const uint64_t ad = smem_desc_sw128(aP + off);
+        if (FP4) {
+          mma_mxf4(tmem, ad, smem_desc_sw128(bFPP + off), i2, acc, tmem + kSfa, tmem + kSfb);
+          mma_mxf4(tmem + 256, ad, smem_desc_sw128(bF + off), i1, acc, tmem + kSfa, tmem + kSfb);
+        } else {
+          mma_i8(tmem, ad, smem_desc_sw128(bFPP + off), i2, acc);
+          mma_i8(tmem + 256, ad, smem_desc_sw128(bF + off), i1, acc);
+        }
+      }
+    }
+    mma_commit(bar);
+    if (!mbar_wait(bar, 0)) atomicExch(err, 1);
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (tid < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512)
+                 : "memory");
+}
+
 }  // namespace tenex
 
 using namespace tenex;
+
+extern "C" int tenex_probe_tc_gemm_b2(int kind, int tile_n, int stages, double* ops, float* ms,
+                                      void* stream_) {
+  if ((kind != 1 && kind != 2) || stages < 1 || !ops || !ms ||
+      !(tile_n == 128 || tile_n == 112 || tile_n == 96 || tile_n == 80 || tile_n == 64))
+    return fail(TENEX_ERR_BADARG,
+                "kind 1 (int8) or 2 (4-bit), tile_n in {128,112,96,80,64}, stages >= 1, outputs "
+                "non-NULL");
+  DevAttr A;
+  int st = current_device_attr(&A);
+  if (st) return st;
+  cudaStream_t s = as_stream(stream_);
+  int* err = nullptr;
+  cudaError_t e = cudaMallocAsync(&err, sizeof(int), s);
+  if (e != cudaSuccess) return check_cuda(e, "cudaMallocAsync");
+  cudaMemsetAsync(err, 0, sizeof(int), s);
+  const int smem = 3 * kSeqStageMax + 2048;
+  const bool fp4 = kind == 2;
+  e = fp4 ? cudaFuncSetAttribute(tc_seq_probe<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem)
+          : cudaFuncSetAttribute(tc_seq_probe<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(err, s);
+    return check_cuda(e, "cudaFuncSetAttribute");
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int rep = 0; rep < 2; ++rep) {  // warm-up launch, then the timed one
+    if (rep == 1) cudaEventRecord(e0, s);
+    const int n = rep == 0 ? (stages < 16 ? stages : 16) : stages;
+    if (fp4)
+      tc_seq_probe<true><<<A.sm_count, 128, smem, s>>>(tile_n, n, err);
+    else
+      tc_seq_probe<false><<<A.sm_count, 128, smem, s>>>(tile_n, n, err);
+  }
+  cudaEventRecord(e1, s);
+  st = check_launch("tc_seq_probe");
+  e = cudaEventSynchronize(e1);
+  if (!st && e != cudaSuccess) st = check_cuda(e, "cudaEventSynchronize");
+  float t = 0.f;
+  cudaEventElapsedTime(&t, e0, e1);
+  int h = 0;
+  cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(err, s);
+  if (st) return st;
+  if (h) return fail(TENEX_ERR_TIMEOUT, "tensor-pipe sequence probe: commit wait expired");
+  *ms = t;
+  *ops = 2.0 * 128 * 3 * tile_n * (fp4 ? 64 : 32) * 4.0 * stages * A.sm_count;
+  return TENEX_OK;
+}
 
 template <bool FP4>
 static int probe_tc(int iters, double* ops, float* ms, void* stream_) {

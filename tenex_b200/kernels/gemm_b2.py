@@ -29,8 +29,8 @@ def te_binary_matrix(db: D.DeviceBins, tau: int = 1, out: torch.Tensor | None = 
     """(n, n) float32 device matrix with [src, tgt] = TE(src -> tgt), diagonal 0.
     operands: "int8" (kind::i8 MMAs), "fp4" (the 0/1 values as packed E2M1,
     kind::mxf4) or "default" (fp4); the counts and TE are the same.
-    tile_n: targets per GEMM tile, 0 = chosen from n and the SM count, else one
-    of TILE_N (the same matrix bit for bit)."""
+    tile_n: targets per GEMM tile, 0 = chosen from n and the SM count
+    (tile_width), else one of TILE_N (the same matrix bit for bit)."""
     if tile_n and tile_n not in TILE_N:
         raise ValueError(f"tile_n={tile_n}: expected 0 or one of {TILE_N}")
     dev = db.data.device
@@ -46,6 +46,15 @@ def te_binary_matrix(db: D.DeviceBins, tau: int = 1, out: torch.Tensor | None = 
     if check:
         native.call("tenex_b2_status", ws.data_ptr(), n, db.row_len, lag, s)
     return out
+
+
+def tile_width(n: int) -> int:
+    """Targets per GEMM tile that te_binary_matrix picks for n genes on the
+    current device."""
+    import ctypes
+    tn = ctypes.c_int()
+    native.call("tenex_b2_tile_n", int(n), ctypes.byref(tn))
+    return tn.value
 
 
 class GEMMB2Kernel(TEKernel):

@@ -86,6 +86,7 @@ _SIGS = {
     "tenex_te_binary_matrix": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _P],
     "tenex_te_binary_matrix_kind": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _I, _P],
     "tenex_te_binary_matrix_ex": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _I, _I, _P],
+    "tenex_b2_tile_n": [_I, ctypes.POINTER(ctypes.c_int)],
     "tenex_b2_status": [_P, _I, _L, _L, _P],
     "tenex_dpi_trim": [_P, _L, _I, _P, _P, ctypes.c_float, _P, _L, _P],
     "tenex_dpi_trim_sparse": [_P, _P, _P, _I, _P, _P, ctypes.c_float, _P, _P],
@@ -106,6 +107,8 @@ _SIGS = {
                             _P],
     "tenex_probe_tc_fp4": [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float),
                            _P],
+    "tenex_probe_tc_gemm_b2": [_I, _I, _I, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_float), _P],
     "tenex_probe_minmax": [_I, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float),
                            _P],
 }
@@ -238,6 +241,17 @@ def probe_tc_fp4(iters: int = 100_000) -> float:
     ops = ctypes.c_double()
     ms = ctypes.c_float()
     call("tenex_probe_tc_fp4", int(iters), ctypes.byref(ops), ctypes.byref(ms), stream_ptr())
+    return ops.value / (ms.value * 1e-3)
+
+
+def probe_tc_gemm_b2(operands: str = "fp4", tile_n: int = 128, stages: int = 2000) -> float:
+    """Measured operations per second of the GEMM-B2 kernel's own MMA sequence
+    (operands "fp4" or "int8", tile_n targets per tile) issued back to back on
+    every SM: the instruction-mix bound of the GEMM's main loop."""
+    ops = ctypes.c_double()
+    ms = ctypes.c_float()
+    call("tenex_probe_tc_gemm_b2", 2 if operands == "fp4" else 1, int(tile_n), int(stages),
+         ctypes.byref(ops), ctypes.byref(ms), stream_ptr())
     return ops.value / (ms.value * 1e-3)
 
 

@@ -84,11 +84,13 @@ def test_binary_matrix_tile_width_checks():
     bb = _addr(bins) + (-_addr(bins)) % 16
     wb = _addr(ws) + (-_addr(ws)) % 256
     bad = native.TENEX_ERR_BADARG
+    def call(kind=0, tn=0):
+        return _status("tenex_te_binary_matrix_ex", bb, ld, n, T, 1, _addr(out), n, wb, 4096,
+                       kind, tn, 0)
+
     for tn in (7, 48, 256, -1):
-        assert _status("tenex_te_binary_matrix_ex", bb, ld, n, T, 1, _addr(out), n, wb, 4096,
-                       0, tn, 0) == bad
-    assert _status("tenex_te_binary_matrix_ex", bb, ld, n, T, 1, _addr(out), n, wb, 4096,
-                   3, 128, 0) == bad                      # unknown operand form
+        assert call(tn=tn) == bad
+    assert call(kind=3, tn=128) == bad                    # unknown operand form
     from tenex_b200.kernels.gemm_b2 import te_binary_matrix
     with pytest.raises(ValueError, match="tile_n"):
         te_binary_matrix(None, 1, tile_n=100)

@@ -43,6 +43,15 @@ def test_every_tile_width_matches_oracle(cuda, n, T, tile_n, operands):
     assert np.array_equal(m.view(np.uint32), _run(x, cuda, operands=operands).view(np.uint32))
 
 
+def test_long_series(cuda):
+    # 70,000 samples per pair (int32 / float32 sums, both forms)
+    x, _ = W.cfg2_binary(n=70, T=70_001, seed=77, n_planted=2)
+    ref = O.te_matrix(x.astype(np.int32), np.full(70, 2, np.int32))
+    m = _run(x, cuda)
+    assert np.max(np.abs(m - ref)) <= TOL
+    assert np.array_equal(m.view(np.uint32), _run(x, cuda, operands="int8").view(np.uint32))
+
+
 @pytest.mark.parametrize("operands", ["int8", "fp4"])
 def test_binary_matches_reference_fixture(cuda, golden, operands):
     g = golden("gemm_b2.npz")
