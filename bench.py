@@ -20,7 +20,8 @@ Side objects of the line:
   surrogate      NetWeaver's surrogate test on cfg5 (full 100-shuffle test and
                  the learned null, wall seconds, edge agreement)
   binary_path    the cfg2 GEMM-B2 matrix, 4-bit and int8 operand forms, each
-                 against its live tensor-pipe probe
+                 against its live tensor-pipe probe and against the GEMM's own
+                 MMA sequence issued back to back (tenex_probe_tc_gemm_b2)
   fdr            NetWeaver's default FDR method on the cfg4 matrix
   cfg3, cfg1     the other TE configs: device time and roofline, end to end,
                  and the CPU oracle on the same workload

@@ -11,22 +11,23 @@
 //     to a multiple of 128 bytes, zero filled), the per-gene counts nf, np, nfp,
 //     and flags any bin other than 0/1; P is the bins themselves (a tensor map
 //     with K extent L, TMA zero-fills beyond it). The 4-bit form packs P too.
-//   * GEMM kernel: one CTA per 128 x 128 (target x source) tile of the matrix.
-//     A producer warp brings, per stage, one 128-byte x 128-row box of FP, P, F
-//     (targets) and P (sources) by TMA (cp.async.bulk.tensor.2d, no multicast),
-//     128-byte swizzled (the K-major SWIZZLE_128B layout the MMA descriptors
-//     name); a separate MMA warp issues, per 32-byte K step, two
-//     tcgen05.mma.kind::i8 with the source tile as A (M = 128 lanes = sources):
-//     B = [FP; P] of the targets as one N = 256 MMA (C^T, D^T) and B = F at
-//     N = 128 (E^T), int32 accumulators in TMEM (384 columns). Shared-memory
-//     bandwidth (operand reads plus TMA writes) bounds the main loop, hence the
-//     source tile read twice per K step rather than three times. The counts are
-//     exact integers (int32, N < 2^31).
+//   * GEMM kernel: one CTA per tile of 128 sources x TN targets (TN from
+//     {128, 112, 96, 80, 64}, picked per matrix so the tiles finish in the
+//     fewest rounds on the SMs). A producer warp brings, per stage, one
+//     128-byte wide box of FP, P, F (TN target rows each) and P (128 source
+//     rows) by TMA (cp.async.bulk.tensor.2d, no multicast), 128-byte swizzled
+//     (the K-major SWIZZLE_128B layout the MMA descriptors name); a separate MMA
+//     warp issues, per 32-byte K step, two tcgen05.mma with the source tile as
+//     A (M = 128 lanes = sources): B = [FP; P] of the targets as one N = 2 TN
+//     MMA (C^T, D^T) and B = F at N = TN (E^T), accumulators in TMEM. The source
+//     tile is read twice per K step rather than three times. kind::i8 on int8
+//     operands (int32 sums, exact) or kind::mxf4 on packed E2M1 operands with
+//     unit block scales (float32 sums, exact below 2^24).
 //   * Epilogue: sixteen warps; warp w reads TMEM lanes 32*(w%4).. (one source
-//     per lane) and a quarter of the 128 target columns with tcgen05.ld, forms
-//     the 8 cells (target marginals staged in shared memory) and writes
-//     TE(src -> tgt) to out[src, tgt], four consecutive targets of a source row
-//     per 16-byte store.
+//     per lane) and a quarter of the TN target columns with tcgen05.ld, forms
+//     the 8 cells (target marginals and c1/c2a staged in shared memory) and
+//     writes TE(src -> tgt) to out[src, tgt], four consecutive targets of a
+//     source row per 16-byte store.
 //   * Every mbarrier wait is bounded; on expiry the kernel records an error
 //     word, drains the copies it issued (bounded), frees TMEM and returns.
 #include <cuda.h>
