@@ -13,7 +13,8 @@
 //     with K extent L, TMA zero-fills beyond it). The 4-bit form packs P too.
 //   * GEMM kernel: one CTA per tile of 128 sources x TN targets (TN from
 //     {128, 112, 96, 80, 64}, picked per matrix so the tiles finish in the
-//     fewest rounds on the SMs). A producer warp brings, per stage, one
+//     fewest rounds on the SMs; widths of 80 and below run two CTAs per SM,
+//     B2Layout). A producer warp brings, per stage, one
 //     128-byte wide box of FP, P, F (TN target rows each) and P (128 source
 //     rows) by TMA (cp.async.bulk.tensor.2d, no multicast), 128-byte swizzled
 //     (the K-major SWIZZLE_128B layout the MMA descriptors name); a separate MMA
@@ -47,12 +48,30 @@ namespace {
 
 constexpr int kTile = 128;     // sources per tile (M = 128 TMEM lanes); targets per tile <= 128
 constexpr int kKt = 128;       // bytes of K per pipeline stage (4 MMA K-steps of 32)
-constexpr int kStages = 3;
 // one stage: FP, P, F of TN targets and P of 128 sources, 128 bytes of K each
 // (every box starts on a 1024-byte swizzle atom: TN is a multiple of 16)
 __host__ __device__ constexpr int stage_bytes(int TN) { return (3 * TN + kTile) * kKt; }
-constexpr int kTmemCols = 512;
 constexpr int kTileN[] = {128, 112, 96, 80, 64};  // target-tile widths (MMA N = TN and 2 TN)
+
+// Per-width layout. TN > 80: one CTA per SM (512 threads, three stages, 512 TMEM
+// columns: C at 0, D at TN, E at 256, 4-bit scale factors at 384 / 392). TN <= 80:
+// the three accumulators and the scale factors fit 256 columns (E at 2 TN rounded
+// up to 32, scale factors at 240 / 248), so two CTAs share an SM (256 threads,
+// two stages each): one CTA's epilogue and stage waits overlap the other's MMAs.
+template <int TN>
+struct B2Layout {
+  static constexpr bool kPair = TN <= 80;
+  static constexpr int kThreads = kPair ? 256 : 512;
+  static constexpr int kCtasPerSm = kPair ? 2 : 1;
+  static constexpr int kStages = kPair ? 2 : 3;
+  static constexpr int kTmemCols = kPair ? 256 : 512;
+  static constexpr uint32_t kECol = kPair ? (uint32_t)((2 * TN + 31) / 32 * 32) : 256u;
+  static constexpr uint32_t kSfaCol = kPair ? 240u : 384u, kSfbCol = kPair ? 248u : 392u;
+  static constexpr int kColGroups = kThreads / 128;  // epilogue warps per TMEM lane quarter
+  static constexpr int kSmem = kStages * stage_bytes(TN) + 1024 + 256 + 7 * kTile * 4;
+  static_assert(!kPair || kECol + TN <= kSfaCol, "accumulators overlap the scale factors");
+  static_assert((TN / kColGroups) % 4 == 0, "epilogue columns per warp: a multiple of 4");
+};
 
 struct B2Params {
   int n;            // genes
@@ -247,11 +266,9 @@ struct B2Maps {
   CUtensorMap F, Pt, FP, Ps;
 };
 
-constexpr int kB2Threads = 512;
-// 4-bit form: TMEM columns of the UE8M0 scale factors (all 1.0), after the
-// three 128-column accumulators: A (sources, M = 128) at kSfaCol, B (targets,
-// up to N = 256) at kSfbCol; 8 columns each hold every layout those take.
-constexpr uint32_t kSfaCol = 384, kSfbCol = 392;
+// 4-bit form: TMEM columns of the UE8M0 scale factors (all 1.0) after the
+// accumulators (B2Layout): A (sources, M = 128) at kSfaCol, B (targets, up to
+// N = 256) at kSfbCol; 8 columns each hold every layout those take.
 
 // TE(src -> target ti of the tile) from the three sums C, D, E of the pair, the
 // target's staged marginals (tmarg: nf, np, nfp; tq: c1/c2a for the target
@@ -297,12 +314,12 @@ __device__ __forceinline__ void b2_store4(const B2Params& prm, float* orow, int 
 // loads, as tcgen05.ld requires), then b2_pair_te and b2_store4.
 template <bool FP4, int NC>
 __device__ __forceinline__ void b2_cells(const B2Params& prm, uint32_t lane_base, int cb, int TN,
-                                         int m0, int j, bool active, float npj,
+                                         uint32_t ecol, int m0, int j, bool active, float npj,
                                          const float* tmarg, const float* tq) {
   uint32_t rc[NC], rd[NC], re[NC];
   tmem_ld(lane_base + (uint32_t)cb, rc);
   tmem_ld(lane_base + (uint32_t)(TN + cb), rd);
-  tmem_ld(lane_base + (uint32_t)(256 + cb), re);
+  tmem_ld(lane_base + ecol + (uint32_t)cb, re);
   tmem_wait_ld();
   if (!active) return;
   const float N = (float)prm.L;
@@ -330,8 +347,11 @@ __device__ __forceinline__ void b2_cells(const B2Params& prm, uint32_t lane_base
 // TN: targets per tile (a multiple of 16, at most 128): [FP; P] is one MMA of
 // N = 2 TN and F one of N = TN.
 template <bool FP4, int TN>
-__global__ void __launch_bounds__(kB2Threads, 1)
+__global__ void __launch_bounds__(B2Layout<TN>::kThreads, B2Layout<TN>::kCtasPerSm)
     b2_gemm_kernel(const __grid_constant__ B2Maps maps, B2Params prm) {
+  using LY = B2Layout<TN>;
+  constexpr int kStages = LY::kStages, kTmemCols = LY::kTmemCols, kB2Threads = LY::kThreads;
+  constexpr uint32_t kSfaCol = LY::kSfaCol, kSfbCol = LY::kSfbCol, kECol = LY::kECol;
   constexpr int kStageBytes = stage_bytes(TN);
   constexpr int kTgtBytes = TN * kKt;  // one target operand box per stage
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -447,11 +467,11 @@ __global__ void __launch_bounds__(kB2Threads, 1)
         if (FP4) {
           mma_mxf4(tmem + 0, ad, smem_desc_sw128(bFPP + off), idesc256, acc, tmem + kSfaCol,
                    tmem + kSfbCol);
-          mma_mxf4(tmem + 256, ad, smem_desc_sw128(bF + off), idesc128, acc, tmem + kSfaCol,
+          mma_mxf4(tmem + kECol, ad, smem_desc_sw128(bF + off), idesc128, acc, tmem + kSfaCol,
                    tmem + kSfbCol);
         } else {
           mma_i8(tmem + 0, ad, smem_desc_sw128(bFPP + off), idesc256, acc);
-          mma_i8(tmem + 256, ad, smem_desc_sw128(bF + off), idesc128, acc);
+          mma_i8(tmem + kECol, ad, smem_desc_sw128(bF + off), idesc128, acc);
         }
       }
       mma_commit(&empty[s]);  // stage s free once these MMAs complete
@@ -463,7 +483,7 @@ __global__ void __launch_bounds__(kB2Threads, 1)
     mma_commit(accbar);  // arrives after every issued MMA, so the epilogue wakes either way
   }
 
-  // ---- epilogue: 16 warps; lane quarter warp % 4, column quarter warp / 4 ---
+  // ---- epilogue: every warp; lane quarter warp % 4, column group warp / 4 -----
   // (the warps that neither load nor issue stage the target marginals first;
   // a c2a of 0 gives q = inf or NaN, never read: its cells are empty)
   if (tid >= 64) {
@@ -494,17 +514,19 @@ __global__ void __launch_bounds__(kB2Threads, 1)
   const int j = n0 + lq * 32 + (tid & 31);  // source gene of this thread's TMEM lane
   const float npj = j < prm.n ? (float)prm.marg[prm.n + j] : 0.f;
   const uint32_t lane_base = tmem + ((uint32_t)(lq * 32) << 16);
-  // TN / 4 target columns per warp, in chunks of 16, 8 and 4 (TN / 4 is a multiple of 4)
+  // TN / kColGroups target columns per warp, in chunks of 16, 8 and 4 (a multiple of 4)
+  constexpr int kCw = TN / LY::kColGroups;
   const bool active = run && j < prm.n;
-  int cb = cq * (TN / 4);
-  const int ce = cb + TN / 4;
+  int cb = cq * kCw;
+  const int ce = cb + kCw;
   for (; cb + 16 <= ce; cb += 16)
-    b2_cells<FP4, 16>(prm, lane_base, cb, TN, m0, j, active, npj, tmarg, tq);
+    b2_cells<FP4, 16>(prm, lane_base, cb, TN, kECol, m0, j, active, npj, tmarg, tq);
   if (cb + 8 <= ce) {
-    b2_cells<FP4, 8>(prm, lane_base, cb, TN, m0, j, active, npj, tmarg, tq);
+    b2_cells<FP4, 8>(prm, lane_base, cb, TN, kECol, m0, j, active, npj, tmarg, tq);
     cb += 8;
   }
-  if (cb + 4 <= ce) b2_cells<FP4, 4>(prm, lane_base, cb, TN, m0, j, active, npj, tmarg, tq);
+  if (cb + 4 <= ce)
+    b2_cells<FP4, 4>(prm, lane_base, cb, TN, kECol, m0, j, active, npj, tmarg, tq);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
@@ -572,12 +594,12 @@ extern "C" size_t tenex_b2_workspace_bytes(int n_vars, int64_t row_len, int64_t 
 // One GEMM launch of target-tile width TN: ceil(n / 128) x ceil(n / TN) tiles.
 template <bool FP4, int TN>
 static int launch_gemm(const B2Maps& maps, const B2Params& prm, cudaStream_t stream) {
-  const int smem = kStages * stage_bytes(TN) + 1024 + 256 + 7 * kTile * 4;
+  const int smem = B2Layout<TN>::kSmem;
   cudaError_t e = cudaFuncSetAttribute(b2_gemm_kernel<FP4, TN>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return check_cuda(e, "cudaFuncSetAttribute");
   const dim3 grid((unsigned)((prm.n + kTile - 1) / kTile), (unsigned)((prm.n + TN - 1) / TN));
-  b2_gemm_kernel<FP4, TN><<<grid, kB2Threads, smem, stream>>>(maps, prm);
+  b2_gemm_kernel<FP4, TN><<<grid, B2Layout<TN>::kThreads, smem, stream>>>(maps, prm);
   return check_launch("b2_gemm_kernel");
 }
 
