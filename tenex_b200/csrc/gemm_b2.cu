@@ -24,8 +24,9 @@
 //     tile is read twice per K step rather than three times. kind::i8 on int8
 //     operands (int32 sums, exact) or kind::mxf4 on packed E2M1 operands with
 //     unit block scales (float32 sums, exact below 2^24).
-//   * Epilogue: sixteen warps; warp w reads TMEM lanes 32*(w%4).. (one source
-//     per lane) and a quarter of the TN target columns with tcgen05.ld, forms
+//   * Epilogue: every warp of the CTA (16, or 8 with two CTAs per SM); warp w
+//     reads TMEM lanes 32*(w%4).. (one source per lane) and its share of the TN
+//     target columns (a quarter, or half) with tcgen05.ld, forms
 //     the 8 cells (target marginals and c1/c2a staged in shared memory) and
 //     writes TE(src -> tgt) to out[src, tgt], four consecutive targets of a
 //     source row per 16-byte store.
