@@ -184,14 +184,26 @@ def call(name: str, *args) -> None:
     check(getattr(lib(), name)(*args), name)
 
 
+_cuda_seen: bool | None = None   # whether this process sees a CUDA device (fixed per process)
+
+
 def stream_ptr(stream: torch.cuda.Stream | None = None) -> int:
-    """The stream handle for the C ABI (the current stream; 0, the legacy default
-    stream, when this process sees no CUDA device, in which case every entry point
-    fails with its own status)."""
-    if stream is None and not torch.cuda.is_available():
+    """The stream handle for the C ABI (the current stream of the current device;
+    0, the legacy default stream, when this process sees no CUDA device, in which
+    case every entry point fails with its own status). The device check runs once
+    per process and the handle comes straight from torch's current-stream table:
+    torch.cuda.current_stream() re-checks device availability on every call
+    (~20 us, a tenth of a small compute() call)."""
+    global _cuda_seen
+    if stream is not None:
+        return int(stream.cuda_stream)
+    if _cuda_seen is None:
+        _cuda_seen = torch.cuda.is_available()
+        if _cuda_seen:
+            torch.cuda.init()
+    if not _cuda_seen:
         return 0
-    s = stream if stream is not None else torch.cuda.current_stream()
-    return int(s.cuda_stream)
+    return int(torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice()))
 
 
 def device_info(device: int | None = None) -> DevInfo:

@@ -89,12 +89,12 @@ def remap_bins(raw, K: int = 1, device=None) -> tuple[D.DeviceBins, torch.Tensor
         native.call("tenex_remap_dense", t.data_ptr(), in_bytes, row, n, row,
                     db.data.data_ptr(), 2 if wide else 1, db.ld, npv.data_ptr(), err.data_ptr(),
                     native.stream_ptr())
-        e = int(err.item())
+        # the error word and b_max come back in one copy (one wait on the stream)
+        e, b_max = (int(v) for v in torch.stack((err[0], npv.max())).cpu())
         if e == 1:
             raise ValueError("a gene's raw bins span more than 8192 values; cannot remap")
         if e == 0:
             break
-    b_max = int(npv.max().item())
     return db, npv, b_max
 
 
