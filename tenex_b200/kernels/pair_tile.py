@@ -32,8 +32,11 @@ _tune_cache: dict[tuple, dict] = {}
 
 
 def _npv_tensor(n_per_var, device) -> torch.Tensor:
-    return torch.as_tensor(np.asarray(n_per_var.cpu() if isinstance(n_per_var, torch.Tensor)
-                                      else n_per_var), dtype=torch.int32).to(device)
+    """int32 n_per_var on `device` (a tensor already there is used as it is: no
+    round trip through the host)."""
+    if isinstance(n_per_var, torch.Tensor):
+        return n_per_var.to(device=device, dtype=torch.int32).contiguous()
+    return torch.as_tensor(np.asarray(n_per_var), dtype=torch.int32).to(device).contiguous()
 
 
 def autotune(db: D.DeviceBins, npv: torch.Tensor, b_max: int, tau: int = 1,
