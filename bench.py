@@ -15,7 +15,8 @@ Profiling options (not the headline run): --genes / --cells shrink the
 workload, --pairs times only the first pair ids, --launch T,C,W fixes the
 launch shape (threads, CTAs per SM, sources per work item) instead of running
 the autotuner, --no-e2e, --no-cpu-baseline, --no-surrogate, --no-fdr,
---no-configs and --no-reference-gpu skip those legs; --only NAME prints one leg.
+--no-configs, --no-next and --no-reference-gpu skip those legs; --only NAME prints
+one leg.
 Side objects of the line:
   surrogate      NetWeaver's surrogate test on cfg5 (full 100-shuffle test and
                  the learned null, wall seconds, edge agreement)
@@ -25,6 +26,10 @@ Side objects of the line:
   fdr            NetWeaver's default FDR method on the cfg4 matrix
   cfg3, cfg1     the other TE configs: device time and roofline, end to end,
                  and the CPU oracle on the same workload
+  next_rows      the hot path's neighbouring rows: the source-filter pair list,
+                 the multi-lag surrogate combine, binarisation and the
+                 coarsening-off overflow launch (device time, roofline, end to end
+                 and the CPU oracle where each applies)
   reference_gpu  the reference's own CUDA wrappers (installed under
                  baseline/_ref) on the same GPU, in a child process that imports
                  nothing of this repository (context, not the reference arm)
@@ -361,6 +366,8 @@ def run_ours(args) -> None:
           if (world == 1 and not args.no_configs) else None)
     c1 = (cfg1_leg(dev, peak_atomic, with_cpu=not args.no_cpu_baseline)
           if (world == 1 and not args.no_configs) else None)
+    nxt = (next_rows_leg(dev, peak_atomic, with_cpu=not args.no_cpu_baseline)
+           if (world == 1 and not args.no_configs and not args.no_next) else None)
     refg = (reference_gpu_leg(dev) if (world == 1 and not args.no_reference_gpu
                                         and total == G * (G - 1)) else None)
     fdrl = fdr_leg(dev, out) if (world == 1 and not args.no_fdr and total == G * (G - 1)) else None
@@ -378,7 +385,7 @@ def run_ours(args) -> None:
             "gpu_launches": 6 * args.steps,  # remap, coarsen x2, prepass, order, TE tile
             "roofline": roofline, "roofline_hbm": roofline_hbm,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "surrogate": sur,
-            "binary_path": binl, "fdr": fdrl, "cfg3": c3, "cfg1": c1,
+            "binary_path": binl, "fdr": fdrl, "cfg3": c3, "cfg1": c1, "next_rows": nxt,
             "reference_gpu": refg}
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -464,6 +471,263 @@ def cfg3_leg(dev, peak: float, with_cpu: bool = True) -> dict:
                     "path": "FullSMEMKernel: pinned host bins -> padded device rows -> "
                             "compute_pairfree_device -> pinned host matrix"},
             "cpu_baseline": cpu_oracle_rate(bins, npv, 5.0, seed=3000) if with_cpu else None}
+
+
+def _median_event_ms(fn, reps: int = 3, warm: int = 2) -> float:
+    """Median device time (CUDA events on the current stream) of fn() after `warm`
+    untimed calls."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(reps)]
+    for a, b in ev:
+        a.record(s)
+        fn()
+        b.record(s)
+    torch.cuda.synchronize()
+    return statistics.median(a.elapsed_time(b) for a, b in ev)
+
+
+def _median_wall_s(fn, reps: int = 3) -> float:
+    """Median wall seconds of fn() (which returns host data) after one warm-up call."""
+    fn()
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts)
+
+
+def _oracle_pairs_rate(bins, npv, pairs: np.ndarray, seconds: float, seed: int,
+                       sample: int = 100_000, tau: int = TAU) -> dict:
+    """The C oracle (every host thread) on seed-fixed samples of `sample` rows of a
+    given [target, source] pair list, one after another for `seconds`."""
+    from oracle import oracle as O
+    b = np.asarray(bins)
+    flat = np.ascontiguousarray(b.reshape(b.shape[0], -1), dtype=np.int32)
+    npv = np.asarray(npv, np.int32)
+    nthreads = os.cpu_count() or 1
+    k = min(sample, pairs.shape[0])
+    done, busy, i = 0, 0.0, 0
+    while i < 1 or busy < seconds:
+        rng = np.random.default_rng(seed + i)
+        smp = pairs[np.sort(rng.choice(pairs.shape[0], k, replace=False))]
+        t0 = time.perf_counter()
+        O.te_pairs(flat, npv, smp, tau, threads=nthreads)
+        busy += time.perf_counter() - t0
+        done += k
+        i += 1
+    return {"value": done / busy, "unit": "pairs/s", "cores": nthreads, "kind": "port",
+            "sample": f"{i} seed-fixed samples of {k} pairs of the list ({busy:.1f} s on "
+                      f"{nthreads} threads; C oracle, exact counts, float64 TE)"}
+
+
+def source_filter_leg(dev, peak: float, with_cpu: bool = True) -> dict:
+    """Source-filter (TF) pair list, the reference's compute_single_gpu with explicit
+    pairs: the cfg3-shaped bins (5,000 genes x 10,000 cells, b ~ U{2..32}) with 500
+    seed-chosen sources, every target against every source (2,499,500 [target,
+    source] pairs): device time of the tenex_te_pairs launch from resident bins and
+    a resident pair list against the shared-memory atomic probe; end to end through
+    the plugin call (host bins and host pairs in, host TE vector out); the C oracle
+    on samples of the same list."""
+    import torch
+
+    from tenex_b200 import native, workloads as W
+    from tenex_b200.kernels import device as D
+    from tenex_b200.kernels.full_smem import FullSMEMKernel
+    from tenex_b200.kernels.pair_list import item_table
+    x, npv = W.cfg3_bins()
+    bins = np.ascontiguousarray(x, dtype=np.uint8)
+    n, T = bins.shape
+    bmax = int(npv.max())
+    rng = np.random.default_rng(3100)
+    srcs = np.sort(rng.choice(n, 500, replace=False)).astype(np.int64)
+    tgt = np.repeat(np.arange(n, dtype=np.int64), srcs.size)
+    src = np.tile(srcs, n)
+    keep = tgt != src
+    pairs = np.ascontiguousarray(np.stack([tgt[keep], src[keep]], axis=1))   # by target
+    P = pairs.shape[0]
+    db = D.pack_bins(bins, dev)
+    npv_t = torch.as_tensor(npv, dtype=torch.int32, device=dev)
+    items = item_table(pairs[:, 0], 128)
+    pairs_d = torch.from_numpy(pairs).to(dev)
+    items_d = torch.from_numpy(items).to(dev)
+    ws = D.workspace(dev, n, db.row_len, bmax)
+    out = torch.empty(P, dtype=torch.float32, device=dev)
+
+    def launch():
+        native.call("tenex_te_pairs", db.ptr(), db.ld, npv_t.data_ptr(), bmax, n, db.row_len,
+                    TAU * db.K, pairs_d.data_ptr(), P, items_d.data_ptr(), items.shape[0] - 1,
+                    out.data_ptr(), ws.data_ptr(), ws.numel(), None, native.stream_ptr())
+
+    ms = _median_event_ms(launch)
+    native.call("tenex_workspace_status", ws.data_ptr(), native.stream_ptr())
+    kern = FullSMEMKernel()
+    e2e_s = _median_wall_s(lambda: kern.compute_single_gpu(bins, pairs, bmax, npv, TAU, None,
+                                                           dev))
+    return {"workload": "source filter: cfg3-shaped bins (5000 genes x 10000 cells, "
+                        "b~U{2..32}), 500 sources, all 5000 targets (2,499,500 pairs)",
+            "pairs_per_s": P / (ms / 1e3), "ms": ms,
+            "roofline": _smem_roofline(P, T - TAU, ms, peak),
+            "e2e": {"value": P / e2e_s, "unit": "pairs/s", "seconds": e2e_s,
+                    "h2d_bytes_per_step": int(bins.nbytes + pairs.nbytes),
+                    "d2h_bytes_per_step": int(P * 4),
+                    "path": "FullSMEMKernel.compute_single_gpu(host bins, host pairs) -> "
+                            "host TE vector"},
+            "cpu_baseline": (_oracle_pairs_rate(bins, npv, pairs, 5.0, seed=3200)
+                             if with_cpu else None)}
+
+
+def multi_lag_leg(dev, with_cpu: bool = True) -> dict:
+    """Multi-lag surrogate combine (Pipeline.infer with taus): 2,000 genes x 5,000
+    cells of expression (the cfg1 generator at cfg5's shape), FSBW-L bins, a TE
+    matrix and the 100-shuffle surrogate test at tau = 1 and at tau = 2, merged per
+    pair by lag_combine="max" with BH-FDR 0.05: wall seconds of the whole call from
+    the host matrix (one timed call after a warm-up call); the CPU figure is the C
+    oracle's estimate of the same two tests (the surrogate leg's routine on these
+    bins, times the number of lags)."""
+    import torch
+
+    from tenex_b200 import Pipeline, TransferEntropyEngine, workloads as W
+    x, _ = W.cfg1_expression(2000, 5000, seed=1006)
+    n = x.shape[0]
+    names = np.array([f"g{i}" for i in range(n)])
+    taus, S = [1, 2], 100
+
+    def call():
+        return Pipeline(TransferEntropyEngine(x, names)).infer(
+            "surrogate_test", taus=taus, lag_combine="max", n_surrogates=S, fdr=0.05,
+            device=str(dev))
+
+    call()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = call()
+    wall = time.perf_counter() - t0
+    cpu = None
+    if with_cpu:
+        te = TransferEntropyEngine(x, names).compute(accelerator="gpu", devices=[dev.index or 0])
+        one = surrogate_cpu_baseline(te.bin_arrs[:, :, 0].astype(np.int32), te.n_per_var, S,
+                                     int(res.block_length), 42, dev)
+        cpu = dict(one, est_full_test_s=one["est_full_test_s"] * len(taus),
+                   note="per-lag estimate of the tau = 1 test, times the number of lags")
+    return {"workload": "multi-lag surrogate test: 2000 genes x 5000 cells expression "
+                        "(FSBW-L), taus [1, 2], 100 block shuffles per lag, lag_combine='max', "
+                        "BH-FDR 0.05",
+            "metric": "Pipeline.infer('surrogate_test', taus=[1, 2]) wall seconds from the host "
+                      "matrix (one call after a warm-up call)",
+            "seconds": wall, "edges": int(len(res.grn)),
+            "pair_surrogate_tes_per_s": n * (n - 1) * (S + 1) * len(taus) / wall,
+            "cpu_baseline": cpu}
+
+
+def binarize_leg(dev, with_cpu: bool = True) -> dict:
+    """Binarisation, the GEMM-B2 path's input step: 10,000 genes x 20,000 cells of
+    float32 expression (half zeros, 800 MB) binarised from a device-resident matrix
+    by 'nonzero', 'mean' and 'median' (device time, median of 3 after 2 warm-ups)
+    against the measured HBM copy rate, algorithmic bytes = the matrix read once
+    plus the uint8 bins written once; end to end for 'median' from the host matrix
+    to host bins; the C / numpy oracle (the reference's arithmetic) on 200 rows,
+    extrapolated to the matrix."""
+    import torch
+
+    from oracle import oracle as O
+    from tenex_b200.binarize import binarize
+    from tenex_b200.kernels import device as D
+    rng = np.random.default_rng(4000)
+    n, T = 10_000, 20_000
+    x = rng.standard_normal((n, T), dtype=np.float32)
+    np.maximum(x, 0.0, out=x)
+    xd = torch.from_numpy(x).to(dev)
+    hbm = measured_peaks().get("hbm_gbs")
+    algo = x.nbytes + n * T
+    out = {"workload": "binarisation: 10000 genes x 20000 cells float32 (half zeros)"}
+    for m in ("nonzero", "mean", "median"):
+        ms = _median_event_ms(lambda m=m: binarize(xd, m, dev))
+        gbs = algo / (ms / 1e3) / 1e9
+        obj = {"ms": ms,
+               "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                            "frac": gbs / hbm if hbm else None,
+                            "note": "matrix read once + uint8 bins written once / device time; "
+                                    "peak = MEASURED_PEAKS.json hbm_gbs (of measured)"}}
+        if with_cpu:
+            t0 = time.perf_counter()
+            O.binarize(x[:200], m)
+            dt = time.perf_counter() - t0
+            obj["cpu_baseline"] = {"value": 200 * T / dt, "unit": "elements/s", "cores": 1,
+                                   "kind": "port", "est_matrix_s": dt * n / 200,
+                                   "sample": "200 rows, numpy (the reference's arithmetic)"}
+        out[m] = obj
+    del xd
+    e2e_s = _median_wall_s(lambda: D.to_host(binarize(x, "median", dev)[0].unpadded()))
+    out["e2e"] = {"method": "median", "seconds": e2e_s, "value": n * T / e2e_s,
+                  "unit": "elements/s", "h2d_bytes_per_step": int(x.nbytes),
+                  "d2h_bytes_per_step": int(n * T),
+                  "path": "host float32 matrix -> binarize -> host uint8 bins"}
+    return out
+
+
+def overflow_leg(dev, with_cpu: bool = True) -> dict:
+    """Coarsening off (the reference's coarsening=False path): 2,000 genes x 20,000
+    cells from the cfg4 generator (5% genes with b in [64, 256], not coarsened),
+    the 1,999 pairs of each of four heavy targets. Pairs whose histogram does not
+    fit shared memory run in the global-memory overflow launch (one b_max^3 slot per
+    CTA); device time of the four launches, and the slot bytes of the overflow pairs
+    (each table written when cleared and read by the entropy pass) against the
+    measured HBM rate; the C oracle on the same pairs."""
+    import torch
+
+    from tenex_b200 import workloads as W
+    from tenex_b200.kernels import device as D
+    from tenex_b200.preprocess import remap_bins
+    x, _ = W.cfg4_bins(2000, 20_000, seed=1007)
+    db, npv_d, bmax = remap_bins(torch.from_numpy(np.ascontiguousarray(x)).to(dev), 1, dev)
+    npv = npv_d.cpu().numpy()
+    bins_h = D.to_host(db.unpadded())            # the dense bins the kernel counts
+    n, T = db.n, db.T
+    heavy = np.where(npv > 38)[0][:4]
+    limit = 38 ** 3                   # cells of the largest table that fits shared memory
+    pairs, big, cells = [], 0, 0
+    for t in heavy:
+        src = np.array([s for s in range(n) if s != t], dtype=np.int64)
+        pairs.append(np.stack([np.full(src.size, t, np.int64), src], axis=1))
+        c = int(npv[t]) ** 2 * npv[src].astype(np.int64)
+        big += int((c > limit).sum())
+        cells += int(c[c > limit].sum())
+    pairs = np.concatenate(pairs)
+
+    def launches():
+        for t in heavy:
+            D.te_pairfree(db, npv_d, bmax, TAU, int(t) * (n - 1), n - 1, check_data=False)
+
+    ms = _median_event_ms(launches)
+    gbs = 2 * 4 * cells / (ms / 1e3) / 1e9
+    hbm = measured_peaks().get("hbm_gbs")
+    return {"workload": "coarsening off: 2000 genes x 20000 cells (cfg4 generator, b up to "
+                        f"{bmax}), all pairs of 4 heavy targets ({pairs.shape[0]} pairs, {big} "
+                        "beyond the shared-memory table)",
+            "pairs_per_s": pairs.shape[0] / (ms / 1e3), "ms": ms,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                         "frac": gbs / hbm if hbm else None,
+                         "note": "8 bytes per cell of the overflow pairs' tables (cleared, then "
+                                 "read by the entropy pass) / device time of the launches; peak "
+                                 "= MEASURED_PEAKS.json hbm_gbs (of measured)"},
+            "cpu_baseline": (_oracle_pairs_rate(bins_h, npv, pairs, 5.0, seed=4100,
+                                                sample=1000) if with_cpu else None)}
+
+
+def next_rows_leg(dev, peak: float, with_cpu: bool = True) -> dict:
+    """The hot path's neighbouring rows, each measured: source-filter pair list,
+    multi-lag surrogate combine, binarisation and the coarsening-off overflow
+    launch."""
+    return {"source_filter": source_filter_leg(dev, peak, with_cpu),
+            "multi_lag": multi_lag_leg(dev, with_cpu),
+            "binarize": binarize_leg(dev, with_cpu),
+            "overflow": overflow_leg(dev, with_cpu)}
 
 
 def cfg1_leg(dev, peak: float, with_cpu: bool = True, reps: int = 5) -> dict:
@@ -885,7 +1149,10 @@ def main():
     ap.add_argument("--no-fdr", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the cfg1 / cfg3 objects of the line")
-    ap.add_argument("--only", choices=["binary", "surrogate", "fdr", "cfg1", "cfg3",
+    ap.add_argument("--no-next", action="store_true",
+                    help="skip the next_rows object (source filter, multi-lag, binarisation, "
+                         "overflow)")
+    ap.add_argument("--only", choices=["binary", "surrogate", "fdr", "cfg1", "cfg3", "next",
                                        "reference_gpu"],
                     default=None,
                     help="run one side leg alone and print its JSON object (profiling)")
@@ -909,13 +1176,13 @@ def main():
     elif args.only == "reference_gpu":
         import torch
         print(json.dumps(reference_gpu_leg(torch.device("cuda", 0))), flush=True)
-    elif args.only in ("cfg1", "cfg3"):
+    elif args.only in ("cfg1", "cfg3", "next"):
         import torch
 
         from tenex_b200 import native
         dev = torch.device("cuda", 0)
         peak = max(native.probe_smem_atomics(0, 8192) for _ in range(3))
-        leg = cfg1_leg if args.only == "cfg1" else cfg3_leg
+        leg = {"cfg1": cfg1_leg, "cfg3": cfg3_leg, "next": next_rows_leg}[args.only]
         print(json.dumps(leg(dev, peak, with_cpu=not args.no_cpu_baseline)), flush=True)
     elif args.only == "surrogate":
         import torch

@@ -70,7 +70,14 @@ struct TeParams {
   int64_t gslot_words;
   int64_t n_items;
   int zbytes;     // bytes per z entry reserved (1 or 2)
-  int bmax;       // max n_per_var (sizes the c2a/c1 region and the marginal rows)
+  int bmax;       // max n_per_var (sizes the c1 row)
+  // largest target b whose marginal tables (c2a, c1/c2a: 12 B x b^2) live in shared
+  // memory; = bmax unless those tables for bmax would crowd out the histograms
+  // (coarsening off, b in the hundreds). Pairs of larger targets run in the
+  // overflow launch with the target's tables in gmarg (per CTA: 3 x bmax^2 words).
+  int mbmax;
+  int32_t* gmarg;
+  int64_t gmarg_words;
   int smem_bytes;
   int out_mode;
   float* out;
@@ -111,15 +118,16 @@ struct SmemLayout {
   int z_off, c2a_off, c1_off, q_off, red_off, misc_off, slot_off;
 };
 
-// ztile: samples staged at a time (the z region holds ztile entries of zbytes).
-__host__ __device__ inline SmemLayout smem_layout(int ztile, int zbytes, int bmax) {
+// ztile: samples staged at a time (the z region holds ztile entries of zbytes);
+// c1 holds bmax entries, the marginal tables mbmax^2.
+__host__ __device__ inline SmemLayout smem_layout(int ztile, int zbytes, int bmax, int mbmax) {
   SmemLayout L;
   int off = 0;
   L.misc_off = off;  off += 64;                               // int misc[16]
   L.red_off = off;   off += kMaxWarps * 8;                    // double red[32]
-  L.c1_off = off;    off += (int)round_up((int64_t)bmax * 4, 16);          // int c1[bt]
-  L.c2a_off = off;   off += (int)round_up((int64_t)bmax * bmax * 4, 16);   // int c2a[bt^2]
-  L.q_off = off;     off += (int)round_up((int64_t)bmax * bmax * 8, 16);   // {c1/c2a, c2a}
+  L.c1_off = off;    off += (int)round_up((int64_t)bmax * 4, 16);            // int c1[bt]
+  L.c2a_off = off;   off += (int)round_up((int64_t)mbmax * mbmax * 4, 16);   // int c2a[bt^2]
+  L.q_off = off;     off += (int)round_up((int64_t)mbmax * mbmax * 8, 16);   // {c1/c2a, c2a}
   L.z_off = off;     off += (int)round_up((int64_t)ztile * zbytes, 16);
   L.slot_off = (int)round_up(off, 128);
   return L;
@@ -245,6 +253,15 @@ __host__ __device__ inline bool slot_fits(int64_t bt, int64_t bs, int N, int64_t
   return N < 65536 && w16 * 4 <= slot_region;
 }
 
+// Whether pair (bt, bs) runs in the shared-memory launch: its histogram fits a
+// slot and the target's marginal tables fit shared memory (bt <= mbmax). Every
+// other pair runs in the overflow launch. Same rule on host and device, and
+// monotone in bs, so sources sorted by b split each target's chunk in one place.
+__host__ __device__ inline bool in_smem(int64_t bt, int64_t bs, int N, int mbmax,
+                                        int64_t slot_region) {
+  return bt <= mbmax && slot_fits(bt, bs, N, slot_region);
+}
+
 // Per-lane part of sum c3 * log2(c3 * c1 / (c2a * c2b)) over the pair's cells.
 // Cell (z = xt1*bt + xt, y) is tab[z * stride + y] (PACK16: the 16-bit half
 // (y & 1) of word z * stride + (y >> 1), stride = hb). Columns (xt, y) are
@@ -359,7 +376,7 @@ __device__ __forceinline__ bool pair_of(const TeParams& P, const ItemCtx& it, in
     p = it.base + (src < it.tgt ? src : src - 1);
     if (src == it.tgt || p < P.p0 || p >= P.p1) return false;
   }
-  if (P.overflow && slot_fits(it.bt, P.npv[src], P.N, it.slot_region) == (MODE == kGmem))
+  if (P.overflow && in_smem(it.bt, P.npv[src], P.N, P.mbmax, it.slot_region) == (MODE == kGmem))
     return false;
   *src_o = src;
   *p_o = p;
@@ -517,12 +534,18 @@ __device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it
 template <bool GMEM>
 __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const SmemLayout SL = smem_layout(P.ztile, P.zbytes, P.bmax);
+  const SmemLayout SL = smem_layout(P.ztile, P.zbytes, P.bmax, P.mbmax);
   int* misc = reinterpret_cast<int*>(smem + SL.misc_off);
   double* red = reinterpret_cast<double*>(smem + SL.red_off);
   int* c1i = reinterpret_cast<int*>(smem + SL.c1_off);
-  int* c2ai = reinterpret_cast<int*>(smem + SL.c2a_off);
-  float2* qa = reinterpret_cast<float2*>(smem + SL.q_off);
+  int* const c2a_sm = reinterpret_cast<int*>(smem + SL.c2a_off);
+  float2* const qa_sm = reinterpret_cast<float2*>(smem + SL.q_off);
+  // a target beyond mbmax (overflow launch only) keeps its tables in this CTA's
+  // global scratch: c2a (bmax^2 ints), then {c1/c2a, c2a} (bmax^2 float2)
+  int* const c2a_gm = GMEM && P.gmarg ? P.gmarg + (int64_t)blockIdx.x * P.gmarg_words : nullptr;
+  float2* const qa_gm =
+      c2a_gm ? reinterpret_cast<float2*>(c2a_gm + 2 * (((int64_t)P.bmax * P.bmax + 1) / 2))
+             : nullptr;
   unsigned char* zsm = smem + SL.z_off;
   uint32_t* slots = reinterpret_cast<uint32_t*>(smem + SL.slot_off);
   const int slot_region = P.smem_bytes - SL.slot_off;
@@ -580,8 +603,8 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
       // sources are sorted by bin count: skip a chunk this launch has no pair of
       if (P.overflow && lo < hi) {
         const int btq = P.npv[tgt];
-        if (!GMEM && !slot_fits(btq, P.npv[P.order[lo]], N, slot_region)) lo = hi;
-        if (GMEM && slot_fits(btq, P.npv[P.order[hi - 1]], N, slot_region)) lo = hi;
+        if (!GMEM && !in_smem(btq, P.npv[P.order[lo]], N, P.mbmax, slot_region)) lo = hi;
+        if (GMEM && in_smem(btq, P.npv[P.order[hi - 1]], N, P.mbmax, slot_region)) lo = hi;
       }
     }
     if (lo >= hi) {
@@ -596,6 +619,10 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     }
     const int bt = P.npv[tgt];
     const int bt2 = bt * bt;
+    // the target's marginal tables: shared memory, or (bt > mbmax: every pair of
+    // this target is an overflow pair) the CTA's global scratch
+    int* const c2ai = bt <= P.mbmax ? c2a_sm : c2a_gm;
+    float2* const qa = bt <= P.mbmax ? qa_sm : qa_gm;
 
     // ---- max b_s over this launch's sources (pair lists: also check indices) --
     unsigned my_max = 1;
@@ -613,7 +640,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
         if (src == tgt || p < P.p0 || p >= P.p1) continue;
       }
       const int bsrc = P.npv[src];
-      if (!bad && P.overflow && slot_fits(bt, bsrc, N, slot_region) == GMEM) continue;
+      if (!bad && P.overflow && in_smem(bt, bsrc, N, P.mbmax, slot_region) == GMEM) continue;
       my_max = max(my_max, (unsigned)bsrc);
       mine = 1;
     }
@@ -808,7 +835,7 @@ static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const D
   if (fixed > A.smem_optin)
     return fail(TENEX_ERR_BADARG, "smem_bytes=%d exceeds the device opt-in %d", fixed,
                 A.smem_optin);
-  const SmemLayout SL = smem_layout(P.ztile, P.zbytes, P.bmax);
+  const SmemLayout SL = smem_layout(P.ztile, P.zbytes, P.bmax, P.mbmax);
   int smem = 0;
   // With shared memory sized automatically, fewer CTAs per SM are used when the
   // largest pair's histogram would not fit (e.g. 38-bin genes need ~110 KB).
@@ -823,27 +850,61 @@ static int plan_te_launch(const TeParams& P, const tenex_te_config* cfg, const D
   if (auto_shape && cps == 1) threads = std::min(1024, A.max_threads_per_sm);
   if ((int64_t)SL.slot_off + 1024 > smem)
     return fail(TENEX_ERR_UNSUPPORTED,
-                "the target block (%d B of shared memory: marginals for b_max = %d and %d "
+                "the target block (%d B of shared memory: marginals for b up to %d and %d "
                 "staged samples) leaves no room for histograms in %d B; coarsen the bins",
-                SL.slot_off, P.bmax, P.ztile, smem);
+                SL.slot_off, P.mbmax, P.ztile, smem);
   L->threads = threads;
   L->smem = smem;
   L->grid = A.sm_count * cps;
   return TENEX_OK;
 }
 
-// Global-memory overflow slots (bytes, 0 if every pair of b_max fits shared
-// memory with N samples at one CTA per SM): one b_max^3 32-bit slot per overflow
-// CTA, as many CTAs as fit 1 GiB (at least one, at most one per SM).
+// Shared memory one CTA per SM can have (the planner's largest choice).
+static int smem_one_cta(const DevAttr& A) {
+  return std::min(A.smem_per_sm - 1024, A.smem_optin) / 16 * 16;
+}
+
+// Largest target b whose marginal tables stay in shared memory: b_max when the
+// target block with tables for b_max leaves at least 1 KB for histograms (the
+// shared-memory kernel's own limit), else the largest b that leaves 64 KB. Targets
+// above it (coarsening off, b in the hundreds) run all their pairs in the overflow
+// launch with the tables in global memory.
+static int marginal_bound(int b_max, int ztile, int zbytes, int smem_max) {
+  if (smem_layout(ztile, zbytes, b_max, b_max).slot_off + 1024 <= smem_max) return b_max;
+  for (int b = b_max - 1; b > 1; --b)
+    if (smem_layout(ztile, zbytes, b_max, b).slot_off + 65536 <= smem_max) return b;
+  return 1;
+}
+
+// Per-CTA global scratch of the overflow launch for a target's marginal tables:
+// c2a (b_max^2 ints, padded to an even count) then {c1/c2a, c2a} (b_max^2 float2).
+static int64_t gmarg_words(int b_max) {
+  const int64_t b2 = (int64_t)b_max * b_max;
+  return round_up(2 * ((b2 + 1) / 2) + 2 * b2, 4);
+}
+
+// Whether some pair needs the overflow launch: the largest pair's histogram does
+// not fit a slot, or the largest target's tables do not fit shared memory.
+static bool needs_overflow(int b_max, int N, int zbytes, int mbmax, int smem) {
+  const SmemLayout SL = smem_layout(z_tile(N, zbytes), zbytes, b_max, mbmax);
+  return b_max > mbmax || !slot_fits(b_max, b_max, N, (int64_t)smem - SL.slot_off);
+}
+
+// Global-memory overflow slots (bytes, 0 if no pair needs the overflow launch): one
+// b_max^3 32-bit slot per overflow CTA, as many CTAs as fit 1 GiB (at least one,
+// at most one per SM), and when targets exceed the marginal bound, each CTA's
+// scratch for their tables.
 static int64_t gmem_slot_count(int b_max, const DevAttr& A) {
   const int64_t words = (int64_t)b_max * b_max * b_max;
   return std::max<int64_t>(1, std::min<int64_t>(A.sm_count, ((int64_t)1 << 30) / (words * 4)));
 }
 static int64_t gmem_bytes(int b_max, int N, int zbytes, const DevAttr& A) {
-  const SmemLayout SL = smem_layout(z_tile(N, zbytes), zbytes, b_max);
-  const int smem = std::min(A.smem_per_sm - 1024, A.smem_optin) / 16 * 16;
-  if (slot_fits(b_max, b_max, N, (int64_t)smem - SL.slot_off)) return 0;
-  return round_up(gmem_slot_count(b_max, A) * (int64_t)b_max * b_max * b_max * 4, 256);
+  const int smem = smem_one_cta(A);
+  const int mb = marginal_bound(b_max, z_tile(N, zbytes), zbytes, smem);
+  if (!needs_overflow(b_max, N, zbytes, mb, smem)) return 0;
+  const int64_t ns = gmem_slot_count(b_max, A);
+  const int64_t marg = mb < b_max ? ns * gmarg_words(b_max) * 4 : 0;
+  return round_up(ns * (int64_t)b_max * b_max * b_max * 4, 256) + round_up(marg, 256);
 }
 
 }  // namespace tenex
@@ -872,6 +933,7 @@ extern "C" int tenex_te_launch_shape(int64_t row_len, int64_t lag, int b_max,
   P.bmax = b_max;
   P.zbytes = b_max <= 16 ? 1 : 2;
   P.ztile = z_tile(P.N, P.zbytes);
+  P.mbmax = marginal_bound(b_max, P.ztile, P.zbytes, smem_one_cta(A));
   const int64_t hb = P.N < 65536 ? (b_max + 1) / 2 : b_max;
   const int64_t worst_slot = round_up((int64_t)b_max * b_max * hb, 4) * 4;
   TeLaunch L{};
@@ -999,6 +1061,7 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   P.bmax = b_max;
   P.zbytes = b_max <= 16 ? 1 : 2;
   P.ztile = z_tile(P.N, P.zbytes);
+  P.mbmax = marginal_bound(b_max, P.ztile, P.zbytes, smem_one_cta(A));
   P.big = P.N >= (1 << 24) ? 1 : 0;
   P.out_mode = out_mode;
   P.out = out;
@@ -1021,21 +1084,28 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
   st = plan_te_launch(P, cfg, A, &L, worst_slot);
   if (st) return st;
   P.smem_bytes = L.smem;
-  // pairs whose histogram does not fit shared memory: global-memory overflow launch
-  const SmemLayout SLh = smem_layout(P.ztile, P.zbytes, P.bmax);
-  const bool overflow = !slot_fits(b_max, b_max, P.N, (int64_t)L.smem - SLh.slot_off);
+  // pairs whose histogram does not fit shared memory, and every pair of a target
+  // beyond the marginal bound: global-memory overflow launch
+  const bool overflow = needs_overflow(b_max, P.N, P.zbytes, P.mbmax, L.smem);
   int64_t n_gslots = 0;
   if (overflow) {
     P.gslot_words = (int64_t)b_max * b_max * b_max;
     n_gslots = gmem_slot_count(b_max, A);
-    const int64_t need = ws_total(n, b_max) + round_up(n_gslots * P.gslot_words * 4, 256);
+    const int64_t slot_bytes = round_up(n_gslots * P.gslot_words * 4, 256);
+    const int64_t marg_bytes =
+        P.mbmax < b_max ? round_up(n_gslots * gmarg_words(b_max) * 4, 256) : 0;
+    const int64_t need = ws_total(n, b_max) + slot_bytes + marg_bytes;
     if ((int64_t)ws_bytes < need)
       return fail(TENEX_ERR_UNSUPPORTED,
                   "pairs with b up to %d do not fit shared memory and need %lld bytes of "
                   "global-memory slots in the workspace (%lld given; size it with "
                   "tenex_te_workspace_bytes)", b_max, (long long)need, (long long)ws_bytes);
-    P.gslots = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(workspace) +
-                                           ws_total(n, b_max));
+    unsigned char* g = reinterpret_cast<unsigned char*>(workspace) + ws_total(n, b_max);
+    P.gslots = reinterpret_cast<uint32_t*>(g);
+    if (marg_bytes) {
+      P.gmarg = reinterpret_cast<int32_t*>(g + slot_bytes);
+      P.gmarg_words = gmarg_words(b_max);
+    }
   }
   P.overflow = overflow ? 1 : 0;
   int64_t grid = L.grid;

@@ -125,11 +125,14 @@ def test_series_of_2_pow_24_samples(cuda):
     assert te[1 * 2 + 0] > 0.01                      # source 0 -> target 1 is coupled
 
 
-@pytest.mark.parametrize("T,b_big", [(900, 90), (70000, 41)])
+@pytest.mark.parametrize("T,b_big", [(900, 90), (70000, 41), (900, 200), (20000, 150)])
 def test_global_memory_overflow_counts(cuda, T, b_big):
     # genes whose b_t^2 * b_s histogram cannot fit shared memory (no coarsening): those
     # pairs run in the global-memory overflow launch, the rest in shared memory. T=70000
-    # makes N >= 65536 (32-bit counters only, so 41 bins already overflow).
+    # makes N >= 65536 (32-bit counters only, so 41 bins already overflow). With b in
+    # the hundreds the target's marginal tables no longer fit shared memory either:
+    # every pair of such a target runs in the overflow launch with the tables in
+    # global memory.
     rng = np.random.default_rng(T + b_big)
     bvals = [3, b_big, 5, b_big - 7, 2]
     n = len(bvals)
