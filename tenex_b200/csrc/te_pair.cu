@@ -68,6 +68,10 @@ struct TeParams {
   int overflow;   // an overflow launch exists: both launches filter pairs by slot_fits
   uint32_t* gslots;
   int64_t gslot_words;
+  // overflow launch, whole series staged: per-CTA c2b counts (gc2b_words each,
+  // zero between pairs) for the entropy from the pair's samples
+  uint32_t* gc2b;
+  int64_t gc2b_words;
   int64_t n_items;
   int zbytes;     // bytes per z entry reserved (1 or 2)
   int bmax;       // max n_per_var (sizes the c1 row)
@@ -383,6 +387,53 @@ __device__ __forceinline__ bool pair_of(const TeParams& P, const ItemCtx& it, in
   return true;
 }
 
+// Overflow launch (whole CTA on one pair, histogram in a global-memory slot),
+// whole series staged: sum c3 * log2(c3 * c1 / (c2a * c2b)) from the pair's N
+// samples instead of its b_t^2 * b_s cells (up to 16.4M at b = 254, with at most N
+// of them nonzero). c2b is counted from the samples into the CTA's c2b scratch;
+// then each sample claims its cell with an exchange against 0, so each nonzero
+// cell is evaluated once (and the slot is left clear for the next pair); the terms
+// (same expression and exact-zero rule as the cell pass) are summed in 2^-32 fixed
+// point, so the total does not depend on which sample claimed a cell or on the
+// order of the additions: bitwise reproducible. Returns the CTA's total.
+__device__ double entropy_samples_gmem(uint32_t* tab, uint32_t* c2b, const unsigned char* zsm,
+                                       bool z8, const uint8_t* srow, int N, int bt, int bs,
+                                       const int* c1i, const float2* qa, int tid, int nthreads,
+                                       double* red) {
+  const uint16_t* z16 = reinterpret_cast<const uint16_t*>(zsm);
+  for (int s = tid; s < N; s += nthreads) {
+    const uint32_t z = z8 ? zsm[s] : z16[s];
+    const uint32_t x0 = z % (uint32_t)bt;
+    atomicAdd(&c2b[x0 * (uint32_t)bs + srow[s]], 1u);
+  }
+  __syncthreads();
+  long long acc = 0;
+  for (int s = tid; s < N; s += nthreads) {
+    const uint32_t z = z8 ? zsm[s] : z16[s];
+    const uint32_t y = srow[s];
+    const uint32_t c = atomicExch(&tab[z * (uint32_t)bs + y], 0u);
+    if (c == 0u) continue;
+    const uint32_t x0 = z % (uint32_t)bt;
+    const float b = (float)c2b[x0 * (uint32_t)bs + y];
+    const float2 q = qa[z];  // {c1/c2a, c2a}
+    const float cf = (float)c;
+    const bool e = cf * (float)c1i[x0] == q.y * b;
+    const float r = e ? 1.f : cf * __frcp_rn(b) * q.x;
+    const float term = cf * __log2f(r);
+    acc += __float2ll_rn(term * 4294967296.0f);  // |term| * 2^32 < 2^63 for N < 2^24
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  long long* red64 = reinterpret_cast<long long*>(red);
+  if ((tid & 31) == 0) red64[tid >> 5] = acc;
+  __syncthreads();
+  long long tot = 0;
+  for (int w = 0; w < (nthreads >> 5); ++w) tot += red64[w];
+  // c2b back to zero for the next pair (b_t * b_s words)
+  for (int i = tid; i < bt * bs; i += nthreads) c2b[i] = 0u;
+  __syncthreads();
+  return (double)tot * (1.0 / 4294967296.0);
+}
+
 // After the histogram of source src (pair id p) is complete in the group's
 // table: optional raw-count export, the entropy pass and the output.
 template <int MODE>
@@ -412,14 +463,20 @@ __device__ __forceinline__ void finish_pair(const TeParams& P, const ItemCtx& it
 
   // -- entropy pass (shared slots are cleared for the next source) ---------
   double tot;
-  if (P.big) {
+  bool cta_total = false;  // tot already holds the whole CTA's sum
+  if (MODE == kGmem && P.gc2b != nullptr && !P.big && P.ztile >= P.N) {
+    tot = entropy_samples_gmem(tab, P.gc2b + (int64_t)blockIdx.x * P.gc2b_words, it.zsm, it.z8,
+                               P.bins + (int64_t)src * P.ld, P.N, bt, bs, it.c1i, it.qa, tid,
+                               G * 32, it.red);
+    cta_total = true;
+  } else if (P.big) {
     tot = dev::warp_sum(entropy_cols_f64<true>(tab, bt, bs, stride, it.c1i, it.c2ai, lane_g,
                                                 gthreads));
   } else {
     tot = dev::warp_sum((double)entropy_cols<PACK16, true>(tab, bt, bs, stride, it.c1i, it.qa,
                                                             lane_g, gthreads));
   }
-  if (G > 1) {
+  if (G > 1 && !cta_total) {
     if ((tid & 31) == 0) it.red[warp] = tot;
     dev::named_bar(1 + g, gthreads);
     if (lane_g == 0) {
@@ -562,6 +619,9 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
   uint32_t* gslot = GMEM ? P.gslots + (int64_t)blockIdx.x * P.gslot_words : nullptr;
   if (GMEM) {
     for (int64_t i = tid; i < P.gslot_words; i += nthreads) gslot[i] = 0u;
+    if (P.gc2b)
+      for (int64_t i = tid; i < P.gc2b_words; i += nthreads)
+        P.gc2b[(int64_t)blockIdx.x * P.gc2b_words + i] = 0u;
     __syncthreads();
   }
 
@@ -883,6 +943,9 @@ static int64_t gmarg_words(int b_max) {
   return round_up(2 * ((b2 + 1) / 2) + 2 * b2, 4);
 }
 
+// Per-CTA c2b scratch of the overflow launch (b_max^2 counts, 16-byte rows of CTAs).
+static int64_t gc2b_words(int b_max) { return round_up((int64_t)b_max * b_max, 4); }
+
 // Whether some pair needs the overflow launch: the largest pair's histogram does
 // not fit a slot, or the largest target's tables do not fit shared memory.
 static bool needs_overflow(int b_max, int N, int zbytes, int mbmax, int smem) {
@@ -891,12 +954,12 @@ static bool needs_overflow(int b_max, int N, int zbytes, int mbmax, int smem) {
 }
 
 // Global-memory overflow slots (bytes, 0 if no pair needs the overflow launch): one
-// b_max^3 32-bit slot per overflow CTA, as many CTAs as fit 1 GiB (at least one,
-// at most one per SM), and when targets exceed the marginal bound, each CTA's
-// scratch for their tables.
+// b_max^3 32-bit slot per overflow CTA, as many CTAs as fit 4 GiB (at least one, at
+// most one per SM: every SM up to b_max = 160, 64 CTAs at b_max = 254), and when
+// targets exceed the marginal bound, each CTA's scratch for their tables.
 static int64_t gmem_slot_count(int b_max, const DevAttr& A) {
   const int64_t words = (int64_t)b_max * b_max * b_max;
-  return std::max<int64_t>(1, std::min<int64_t>(A.sm_count, ((int64_t)1 << 30) / (words * 4)));
+  return std::max<int64_t>(1, std::min<int64_t>(A.sm_count, ((int64_t)4 << 30) / (words * 4)));
 }
 static int64_t gmem_bytes(int b_max, int N, int zbytes, const DevAttr& A) {
   const int smem = smem_one_cta(A);
@@ -904,7 +967,8 @@ static int64_t gmem_bytes(int b_max, int N, int zbytes, const DevAttr& A) {
   if (!needs_overflow(b_max, N, zbytes, mb, smem)) return 0;
   const int64_t ns = gmem_slot_count(b_max, A);
   const int64_t marg = mb < b_max ? ns * gmarg_words(b_max) * 4 : 0;
-  return round_up(ns * (int64_t)b_max * b_max * b_max * 4, 256) + round_up(marg, 256);
+  return round_up(ns * (int64_t)b_max * b_max * b_max * 4, 256) + round_up(marg, 256) +
+         round_up(ns * gc2b_words(b_max) * 4, 256);
 }
 
 }  // namespace tenex
@@ -1094,7 +1158,8 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
     const int64_t slot_bytes = round_up(n_gslots * P.gslot_words * 4, 256);
     const int64_t marg_bytes =
         P.mbmax < b_max ? round_up(n_gslots * gmarg_words(b_max) * 4, 256) : 0;
-    const int64_t need = ws_total(n, b_max) + slot_bytes + marg_bytes;
+    const int64_t c2b_bytes = round_up(n_gslots * gc2b_words(b_max) * 4, 256);
+    const int64_t need = ws_total(n, b_max) + slot_bytes + marg_bytes + c2b_bytes;
     if ((int64_t)ws_bytes < need)
       return fail(TENEX_ERR_UNSUPPORTED,
                   "pairs with b up to %d do not fit shared memory and need %lld bytes of "
@@ -1106,6 +1171,8 @@ static int te_run(const uint8_t* bins, int64_t ld, const int32_t* npv, int b_max
       P.gmarg = reinterpret_cast<int32_t*>(g + slot_bytes);
       P.gmarg_words = gmarg_words(b_max);
     }
+    P.gc2b = reinterpret_cast<uint32_t*>(g + slot_bytes + marg_bytes);
+    P.gc2b_words = gc2b_words(b_max);
   }
   P.overflow = overflow ? 1 : 0;
   int64_t grid = L.grid;

@@ -150,6 +150,9 @@ def test_global_memory_overflow_counts(cuda, T, b_big):
         ref = O.counts(bins, 1, t, s, npv).reshape(-1)
         assert np.array_equal(cnt[p, :ref.size], ref), (p, t, s)
     assert np.max(np.abs(te - O.te_pairfree(bins, npv))) <= TOL
+    # the overflow pairs' entropy from their samples is bitwise reproducible
+    again = _gpu_te(bins, npv, bmax, cuda).cpu().numpy()
+    assert np.array_equal(again.view(np.uint32), te.view(np.uint32))
     # pair-list mode (source filter) takes the same two launches
     pairs = np.array([[1, 0], [1, 3], [0, 1], [4, 3], [3, 1]], np.int64)
     from tenex_b200.kernels.pair_list import te_pair_list
