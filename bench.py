@@ -671,53 +671,44 @@ def binarize_leg(dev, with_cpu: bool = True) -> dict:
     return out
 
 
-def overflow_leg(dev, with_cpu: bool = True) -> dict:
-    """Coarsening off (the reference's coarsening=False path): 2,000 genes x 20,000
-    cells from the cfg4 generator (5% genes with b in [64, 256], not coarsened),
-    the 1,999 pairs of each of four heavy targets. Pairs whose histogram does not
-    fit shared memory run in the global-memory overflow launch (one b_max^3 slot per
-    CTA); device time of the four launches, and the slot bytes of the overflow pairs
-    (each table written when cleared and read by the entropy pass) against the
-    measured HBM rate; the C oracle on the same pairs."""
+def overflow_leg(dev, peak: float, with_cpu: bool = True) -> dict:
+    """Coarsening off (the reference's coarsening=False path): 400 genes x 20,000
+    cells from the cfg4 generator (5% genes with b in [64, 256], not coarsened), all
+    159,600 ordered pairs in one call. Pairs whose histogram does not fit shared
+    memory (every pair with a heavy gene) run in the global-memory overflow launch,
+    the rest in the shared-memory launch; device time of the call, its histogram
+    increments against the shared-memory atomic probe (context: the overflow pairs
+    count with global-memory atomics, three per sample), and the C oracle on
+    samples of the same pairs."""
     import torch
 
     from tenex_b200 import workloads as W
     from tenex_b200.kernels import device as D
     from tenex_b200.preprocess import remap_bins
-    x, _ = W.cfg4_bins(2000, 20_000, seed=1007)
+    x, _ = W.cfg4_bins(400, 20_000, seed=1007)
     db, npv_d, bmax = remap_bins(torch.from_numpy(np.ascontiguousarray(x)).to(dev), 1, dev)
     npv = npv_d.cpu().numpy()
     bins_h = D.to_host(db.unpadded())            # the dense bins the kernel counts
     n, T = db.n, db.T
-    heavy = np.where(npv > 38)[0][:4]
-    limit = 38 ** 3                   # cells of the largest table that fits shared memory
-    pairs, big, cells = [], 0, 0
-    for t in heavy:
-        src = np.array([s for s in range(n) if s != t], dtype=np.int64)
-        pairs.append(np.stack([np.full(src.size, t, np.int64), src], axis=1))
-        c = int(npv[t]) ** 2 * npv[src].astype(np.int64)
-        big += int((c > limit).sum())
-        cells += int(c[c > limit].sum())
-    pairs = np.concatenate(pairs)
-
-    def launches():
-        for t in heavy:
-            D.te_pairfree(db, npv_d, bmax, TAU, int(t) * (n - 1), n - 1, check_data=False)
-
-    ms = _median_event_ms(launches)
-    gbs = 2 * 4 * cells / (ms / 1e3) / 1e9
-    hbm = measured_peaks().get("hbm_gbs")
-    return {"workload": "coarsening off: 2000 genes x 20000 cells (cfg4 generator, b up to "
-                        f"{bmax}), all pairs of 4 heavy targets ({pairs.shape[0]} pairs, {big} "
-                        "beyond the shared-memory table)",
-            "pairs_per_s": pairs.shape[0] / (ms / 1e3), "ms": ms,
-            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
-                         "frac": gbs / hbm if hbm else None,
-                         "note": "8 bytes per cell of the overflow pairs' tables (cleared, then "
-                                 "read by the entropy pass) / device time of the launches; peak "
-                                 "= MEASURED_PEAKS.json hbm_gbs (of measured)"},
-            "cpu_baseline": (_oracle_pairs_rate(bins_h, npv, pairs, 5.0, seed=4100,
-                                                sample=1000) if with_cpu else None)}
+    P = n * (n - 1)
+    heavy = int((npv > 38).sum())
+    out = torch.empty(P, dtype=torch.float32, device=dev)
+    ms = _median_event_ms(lambda: D.te_pairfree(db, npv_d, bmax, TAU, 0, P, out=out,
+                                                check_data=False))
+    rng = np.random.default_rng(4100)
+    ids = np.sort(rng.choice(P, 20_000, replace=False))
+    tg = ids // (n - 1)
+    sl = ids - tg * (n - 1)
+    pairs = np.stack([tg, sl + (sl >= tg)], axis=1)
+    roof = _smem_roofline(P, T - TAU, ms, peak)
+    roof["note"] = ("pairs x (T - tau) histogram increments / device time of the call, against "
+                    "the shared-memory atomic probe for context: the overflow pairs count with "
+                    "global-memory atomics (three per sample), which the probe does not bound")
+    return {"workload": f"coarsening off: 400 genes x 20000 cells (cfg4 generator, {heavy} genes "
+                        f"with b up to {bmax}), all {P} ordered pairs",
+            "pairs_per_s": P / (ms / 1e3), "ms": ms, "roofline": roof,
+            "cpu_baseline": (_oracle_pairs_rate(bins_h, npv, pairs, 5.0, seed=4200,
+                                                sample=2000) if with_cpu else None)}
 
 
 def next_rows_leg(dev, peak: float, with_cpu: bool = True) -> dict:
@@ -727,7 +718,7 @@ def next_rows_leg(dev, peak: float, with_cpu: bool = True) -> dict:
     return {"source_filter": source_filter_leg(dev, peak, with_cpu),
             "multi_lag": multi_lag_leg(dev, with_cpu),
             "binarize": binarize_leg(dev, with_cpu),
-            "overflow": overflow_leg(dev, with_cpu)}
+            "overflow": overflow_leg(dev, peak, with_cpu)}
 
 
 def cfg1_leg(dev, peak: float, with_cpu: bool = True, reps: int = 5) -> dict:
