@@ -243,6 +243,16 @@ int tenex_binarize(const float* x, int64_t ldx, int n_vars, int T, int mode,
                    const float* thresholds, uint8_t* out, int64_t ldo, int32_t* n_per_var,
                    void* stream);
 
+/* Median / quantile binarisation with numpy's thresholds (the reference's
+ * default numpy backend, tenex/binarize.py:126-150: np.median, np.quantile
+ * "linear"; replaces the chunked torch.quantile threshold of
+ * tenex/kernels/binarize_kernel.py:158-183): median != 0 for np.median, else
+ * quantile q in [0, 1]. A row holding a NaN gets numpy's NaN threshold (all
+ * bins 0). Per-row radix selection, no sort; out and n_per_var as
+ * tenex_binarize. */
+int tenex_binarize_select(const float* x, int64_t ldx, int n_vars, int T, int median, double q,
+                          uint8_t* out, int64_t ldo, int32_t* n_per_var, void* stream);
+
 /* Binary (b_max = 2) TE matrix on the tensor cores; replaces compute_te_gemm_b2
  * (tenex/kernels/gemm_b2.py:307-425) and its Triton epilogue (:65-187).
  * bins: uint8 {0,1} padded rows (read in place by TMA: 16-byte aligned rows);

@@ -339,27 +339,14 @@ __global__ void coarsen_narrow_kernel(const uint16_t* __restrict__ in, int64_t l
   }
 }
 
-// Binarisation 1[x > thr_g] into uint8 padded rows, one CTA per gene.
-// mode 0: thr = 0 (nonzero); 1: thr = float32 mean with numpy's pairwise sum and
-// float64 division (np.mean on float32 rows); 2: thr = thr_in[g].
-// n_per_var[g] = max - min + 1 of the binary row (1 if constant, else 2).
-__global__ void binarize_kernel(const float* __restrict__ x, int64_t ldx, int T, int mode,
-                                const float* __restrict__ thr_in, uint8_t* __restrict__ out,
-                                int64_t ldo, int32_t* __restrict__ npv) {
-  __shared__ PairwiseScratch S;
-  __shared__ float sh_thr;
-  const int g = blockIdx.x;
-  const float* row = x + (int64_t)g * ldx;
+// 1[row[t] > thr] into orow[0, T) by all CTA threads; returns (to every thread)
+// bit 0: some sample is 1, bit 1: some sample is 0. A NaN compares false (bin 0).
+// NC: row is global memory read through the non-coherent path; else a generic
+// pointer (a row staged in shared memory).
+template <bool NC = true>
+__device__ int binarize_row(const float* __restrict__ row, uint8_t* __restrict__ orow, int T,
+                            float thr) {
   const int tid = threadIdx.x;
-  if (mode == 1) {
-    const float s = row_pairwise_sum<false>(row, T, 0.f, S);
-    if (tid == 0) sh_thr = __double2float_rn(__ddiv_rn((double)s, (double)T));
-  } else if (tid == 0) {
-    sh_thr = mode == 0 ? 0.f : thr_in[g];
-  }
-  __syncthreads();
-  const float thr = sh_thr;
-  uint8_t* orow = out + (int64_t)g * ldo;
   int any1 = 0, any0 = 0;
   // 16 samples per thread and step when both rows are 16-byte aligned: four
   // 16-byte loads, one 16-byte store of the 0/1 bytes; the same comparison as the
@@ -372,7 +359,7 @@ __global__ void binarize_kernel(const float* __restrict__ x, int64_t ldx, int T,
       uint32_t w[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const float4 a = __ldg(r4 + 4 * v + k);
+        const float4 a = NC ? __ldg(r4 + 4 * v + k) : r4[4 * v + k];
         w[k] = (uint32_t)(a.x > thr) | ((uint32_t)(a.y > thr) << 8) |
                ((uint32_t)(a.z > thr) << 16) | ((uint32_t)(a.w > thr) << 24);
       }
@@ -390,7 +377,345 @@ __global__ void binarize_kernel(const float* __restrict__ x, int64_t ldx, int T,
   }
   any1 = __syncthreads_or(any1);
   any0 = __syncthreads_or(any0);
-  if (tid == 0) npv[g] = (any1 && any0) ? 2 : 1;
+  return (any1 ? 1 : 0) | (any0 ? 2 : 0);
+}
+
+// Binarisation 1[x > thr_g] into uint8 padded rows, one CTA per gene.
+// mode 0: thr = 0 (nonzero); 1: thr = float32 mean with numpy's pairwise sum and
+// float64 division (np.mean on float32 rows; rows longer than one plan, see
+// binarize_mean_kernel); 2: thr = thr_in[g].
+// n_per_var[g] = max - min + 1 of the binary row (1 if constant, else 2).
+__global__ void binarize_kernel(const float* __restrict__ x, int64_t ldx, int T, int mode,
+                                const float* __restrict__ thr_in, uint8_t* __restrict__ out,
+                                int64_t ldo, int32_t* __restrict__ npv) {
+  __shared__ PairwiseScratch S;
+  __shared__ float sh_thr;
+  const int g = blockIdx.x;
+  const float* row = x + (int64_t)g * ldx;
+  const int tid = threadIdx.x;
+  if (mode == 1) {
+    const float s = row_pairwise_sum<false>(row, T, 0.f, S);
+    if (tid == 0) sh_thr = __double2float_rn(__ddiv_rn((double)s, (double)T));
+  } else if (tid == 0) {
+    sh_thr = mode == 0 ? 0.f : thr_in[g];
+  }
+  __syncthreads();
+  const int any = binarize_row(row, out + (int64_t)g * ldo, T, sh_thr);
+  if (tid == 0) npv[g] = any == 3 ? 2 : 1;
+}
+
+// numpy's pairwise_sum tree of one row length (T <= kSuperLen: one level of
+// leaves of <= 128 samples), laid out for a parallel evaluation: the leaves left
+// to right, then the internal nodes sorted by height, so that one pass per height
+// adds the two operands of every node of that height. Value ids: leaves 0..nl-1,
+// internal node at sorted position p: nl + p. The root is the last id.
+constexpr int kMaxPlanHeight = 32;
+struct MeanPlan {
+  int lstart[kMaxLeaves];
+  int16_t llen[kMaxLeaves];
+  uint32_t op[kMaxLeaves];          // sorted internal nodes: left | right << 16
+  float val[2 * kMaxLeaves];        // leaf sums, then internal sums
+  int level[kMaxPlanHeight + 2];    // internal nodes of height h: [level[h], level[h+1])
+  int nl, ni, height;
+};
+
+// Builds the plan (thread 0, serial; once per CTA). val[] is scratch here.
+__device__ void build_mean_plan(int T, MeanPlan& P) {
+  const int nl = enum_nodes(T, 128, P.lstart, reinterpret_cast<int*>(P.val));
+  for (int j = 0; j < nl; ++j) P.llen[j] = (int16_t)reinterpret_cast<int*>(P.val)[j];
+  // post-order walk: internal node m (creation order) gets operands and a height
+  uint32_t* tmp_op = reinterpret_cast<uint32_t*>(P.val);               // [kMaxLeaves)
+  int* tmp_h = reinterpret_cast<int*>(P.val) + kMaxLeaves;              // [kMaxLeaves)
+  int fl[64], fs[64], vid[64], vh[64];
+  int sp = 1, vp = 0, k = 0, ni = 0, H = 0;
+  fl[0] = T;
+  fs[0] = 0;
+  while (sp > 0) {
+    const int l = fl[sp - 1];
+    if (l <= 128) {
+      vid[vp] = k++;
+      vh[vp++] = 0;
+      --sp;
+      continue;
+    }
+    int n2 = l / 2;
+    n2 -= n2 % 8;
+    if (fs[sp - 1] < 2) {
+      fl[sp] = fs[sp - 1] == 0 ? n2 : l - n2;
+      fs[sp - 1] += 1;
+      fs[sp] = 0;
+      ++sp;
+    } else {
+      const int ir = vid[--vp], hr = vh[vp];
+      const int il = vid[--vp], hl = vh[vp];
+      const int h = max(hl, hr) + 1;
+      tmp_op[ni] = (uint32_t)il | ((uint32_t)ir << 16);
+      tmp_h[ni] = h;
+      H = max(H, h);
+      vid[vp] = nl + ni++;
+      vh[vp++] = h;
+      --sp;
+    }
+  }
+  // counting sort by height; children precede parents in post-order, so their
+  // sorted positions are known when a parent is placed
+  int cur[kMaxPlanHeight + 2];
+  for (int h = 0; h <= H + 1; ++h) cur[h] = 0;
+  for (int m = 0; m < ni; ++m) ++cur[tmp_h[m]];
+  int acc = 0;
+  for (int h = 0; h <= H + 1; ++h) {
+    P.level[h] = acc;
+    acc += cur[h];
+    cur[h] = P.level[h];
+  }
+  for (int m = 0; m < ni; ++m) {
+    const int pos = cur[tmp_h[m]]++;
+    uint32_t l = tmp_op[m] & 0xffffu, r = tmp_op[m] >> 16;
+    if ((int)l >= nl) l = nl + tmp_h[l - nl];   // tmp_h[child] already holds its position
+    if ((int)r >= nl) r = nl + tmp_h[r - nl];
+    P.op[pos] = l | (r << 16);
+    tmp_h[m] = pos;
+  }
+  P.nl = nl;
+  P.ni = ni;
+  P.height = H;
+}
+
+// The mean binariser for T <= kSuperLen: a persistent CTA builds the row
+// length's plan once and then, per gene, sums the leaves eight lanes to a leaf
+// (lane k holds numpy's accumulator r[k]: a stride-8 pass over the leaf, so the
+// eight lanes read 32 contiguous bytes per step), folds the eight accumulators
+// with xor shuffles 1, 2, 4 (((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), numpy's order;
+// float addition commutes exactly), adds the tail, then evaluates the internal
+// nodes one height per pass. The row is read again for the comparison (from L2).
+__global__ void __launch_bounds__(256) binarize_mean_kernel(const float* __restrict__ x,
+                                                            int64_t ldx, int T, int n_vars,
+                                                            uint8_t* __restrict__ out,
+                                                            int64_t ldo,
+                                                            int32_t* __restrict__ npv) {
+  __shared__ MeanPlan P;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int n_warps = blockDim.x >> 5;
+  if (tid == 0) build_mean_plan(T, P);
+  __syncthreads();
+  const int nl = P.nl, ni = P.ni, H = P.height;
+  for (int g = blockIdx.x; g < n_vars; g += gridDim.x) {
+    const float* row = x + (int64_t)g * ldx;
+    // leaves: four per warp and step, eight lanes each
+    for (int jb = warp * 4; jb < nl; jb += n_warps * 4) {
+      const int j = jb + (lane >> 3);
+      const int kk = lane & 7;
+      const bool active = j < nl;
+      const int s = active ? P.lstart[j] : 0;
+      const int n = active ? P.llen[j] : 0;
+      const int m8 = n - n % 8;
+      float r = 0.f;
+      if (n >= 8) {
+        const float* a = row + s + kk;
+        r = a[0];
+        for (int i = 8; i < m8; i += 8) r = __fadd_rn(r, a[i]);
+      }
+      r = __fadd_rn(r, __shfl_xor_sync(0xffffffffu, r, 1));
+      r = __fadd_rn(r, __shfl_xor_sync(0xffffffffu, r, 2));
+      r = __fadd_rn(r, __shfl_xor_sync(0xffffffffu, r, 4));
+      if (active && kk == 0) {
+        float res = r;
+        if (n < 8) {
+          res = 0.f;
+          for (int i = 0; i < n; ++i) res = __fadd_rn(res, row[s + i]);
+        } else {
+          for (int i = m8; i < n; ++i) res = __fadd_rn(res, row[s + i]);
+        }
+        P.val[j] = res;
+      }
+    }
+    __syncthreads();
+    for (int h = 1; h <= H; ++h) {
+      for (int p = P.level[h] + tid; p < P.level[h + 1]; p += blockDim.x) {
+        const uint32_t o = P.op[p];
+        P.val[nl + p] = __fadd_rn(P.val[o & 0xffffu], P.val[o >> 16]);
+      }
+      __syncthreads();
+    }
+    const float sum = P.val[ni > 0 ? nl + ni - 1 : 0];
+    const float thr = __double2float_rn(__ddiv_rn((double)sum, (double)T));
+    const int any = binarize_row(row, out + (int64_t)g * ldo, T, thr);
+    if (tid == 0) npv[g] = any == 3 ? 2 : 1;
+    // binarize_row ends in __syncthreads_or: val[] is free for the next gene
+  }
+}
+
+// float32 -> uint32 key with the same order as the values (-inf first, -0 just
+// below +0); selection runs on keys, thresholds come back through select_float.
+__device__ __forceinline__ uint32_t select_key(float v) {
+  const uint32_t u = __float_as_uint(v);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float select_float(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+constexpr int kSelectThreads = 512;
+constexpr int kSelectHead = 2048;     // bytes before the staged row: histogram + misc
+
+// Median / quantile binarisation (the reference's numpy backend: np.median and
+// np.quantile "linear" per row, tenex/binarize.py:126-150). A persistent CTA per
+// group of genes; a row that fits is staged in shared memory (one HBM read),
+// else every pass reads it from global memory (L2). The order statistic of rank
+// k0 is found by four radix passes over 8-bit digits of the order-preserving key
+// (histogram counts aggregated per warp and digit with __match_any_sync, so runs
+// of tied values cost one atomic), the one of rank k0 + 1, where the threshold
+// needs it, is the same key if the tie run goes on, else the smallest key above
+// (one min pass). Any NaN in the row makes numpy's threshold NaN: every bin 0.
+// Thresholds in numpy's arithmetic: median = s[h] (T odd) or float32(
+// double(s[h-1] + s[h] in float32) / 2); quantile: virtual index (T - 1) q in
+// float64, a + (b - a) g for g < 0.5 else b - (b - a)(1 - g), b - a in float32 and
+// the rest in float64; numpy then compares the float32 data with that float64
+// value, which selects the same samples as x > t32 with t32 = the float64 value
+// rounded toward -inf.
+__global__ void __launch_bounds__(kSelectThreads) binarize_select_kernel(
+    const float* __restrict__ x, int64_t ldx, int T, int n_vars, int median, double q,
+    int stage, uint8_t* __restrict__ out, int64_t ldo, int32_t* __restrict__ npv) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  int* hist = reinterpret_cast<int*>(sm);          // [256]
+  int* misc = hist + 256;                          // [8]
+  float* srow = reinterpret_cast<float*>(sm + kSelectHead);
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int n_warps = blockDim.x >> 5;
+  // ranks the threshold reads (same for every gene)
+  int k0;
+  bool need_b;
+  double gam = 0.0;
+  if (median) {
+    k0 = (T & 1) ? T / 2 : T / 2 - 1;
+    need_b = (T & 1) == 0;
+  } else {
+    const double vi = __dmul_rn((double)(T - 1), q);
+    const double lo = floor(vi);
+    gam = __dsub_rn(vi, lo);
+    need_b = vi < (double)(T - 1);
+    k0 = need_b ? (int)lo : T - 1;
+  }
+  for (int g = blockIdx.x; g < n_vars; g += gridDim.x) {
+    const float* grow = x + (int64_t)g * ldx;
+    const float* r = grow;
+    bool nan = false;
+    if (stage) {
+      // 16-byte copies (the host stages only 16-byte aligned rows); the previous
+      // gene's readers of srow finished in binarize_row's closing barrier
+      const int nv = T >> 2;
+      const float4* g4 = reinterpret_cast<const float4*>(grow);
+      float4* s4 = reinterpret_cast<float4*>(srow);
+      for (int v = tid; v < nv; v += blockDim.x) {
+        const float4 a = __ldg(g4 + v);
+        nan |= (a.x != a.x) | (a.y != a.y) | (a.z != a.z) | (a.w != a.w);
+        s4[v] = a;
+      }
+      for (int t = (nv << 2) + tid; t < T; t += blockDim.x) {
+        const float a = __ldg(grow + t);
+        nan |= a != a;
+        srow[t] = a;
+      }
+      r = srow;
+    } else {
+      for (int t = tid; t < T; t += blockDim.x) {
+        const float a = __ldg(grow + t);
+        nan |= a != a;
+      }
+    }
+    nan = __syncthreads_or(nan);
+    float thr = __uint_as_float(0x7fc00000u);    // NaN: every sample compares false
+    if (!nan) {
+      uint32_t prefix = 0u, pmask = 0u;
+      int rank = k0, cnt = 0;
+      for (int shift = 24; shift >= 0; shift -= 8) {
+        if (tid < 256) hist[tid] = 0;
+        __syncthreads();
+        for (int base = warp * 32; base < T; base += n_warps * 32) {
+          const int t = base + lane;
+          int d = 256;                              // 256: not counted
+          if (t < T) {
+            const uint32_t k = select_key(r[t]);
+            if ((k & pmask) == prefix) d = (int)((k >> shift) & 255u);
+          }
+          const unsigned m = __match_any_sync(0xffffffffu, d);
+          if (d < 256 && lane == __ffs(m) - 1) atomicAdd(&hist[d], __popc(m));
+        }
+        __syncthreads();
+        if (warp == 0) {
+          // digit holding rank: lane l scans bins [8l, 8l + 8)
+          int c[8], s = 0;
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            c[i] = hist[lane * 8 + i];
+            s += c[i];
+          }
+          int incl = s;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+          }
+          int before = incl - s;
+          if (rank >= before && rank < incl) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              if (rank >= before && rank < before + c[i]) {
+                misc[0] = lane * 8 + i;
+                misc[1] = rank - before;
+                misc[2] = c[i];
+              }
+              before += c[i];
+            }
+          }
+        }
+        __syncthreads();
+        prefix |= (uint32_t)misc[0] << shift;
+        pmask |= 255u << shift;
+        rank = misc[1];
+        cnt = misc[2];
+      }
+      const float a = select_float(prefix);
+      float b = a;
+      if (need_b && rank + 1 >= cnt) {
+        // the tie run of a ends at rank k0: b = the smallest key above a
+        uint32_t mn = 0xffffffffu;
+        for (int t = tid; t < T; t += blockDim.x) {
+          const uint32_t k = select_key(r[t]);
+          if (k > prefix) mn = min(mn, k);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        if (tid == 0) misc[3] = (int)0xffffffffu;
+        __syncthreads();
+        if (lane == 0) atomicMin(reinterpret_cast<unsigned*>(&misc[3]), mn);
+        __syncthreads();
+        b = select_float((uint32_t)misc[3]);
+      }
+      if (median) {
+        thr = need_b ? __double2float_rn(__dmul_rn((double)__fadd_rn(a, b), 0.5)) : a;
+      } else if (!need_b) {
+        // index at the top: numpy interpolates s[T-1] with itself (b - (b - a)
+        // (1 - gamma)), exact for a finite maximum and NaN (inf - inf) for an
+        // infinite one
+        thr = isinf(a) ? __uint_as_float(0x7fc00000u) : a;
+      } else {
+        const double diff = (double)__fsub_rn(b, a);
+        const double t64 = gam >= 0.5 ? __dsub_rn((double)b, __dmul_rn(diff, __dsub_rn(1.0, gam)))
+                                      : __dadd_rn((double)a, __dmul_rn(diff, gam));
+        thr = __double2float_rn(t64);
+        if ((double)thr > t64) thr = nextafterf(thr, -INFINITY);
+      }
+    }
+    uint8_t* orow = out + (int64_t)g * ldo;
+    const int any = stage ? binarize_row<false>(r, orow, T, thr)
+                          : binarize_row<true>(grow, orow, T, thr);
+    if (tid == 0) npv[g] = any == 3 ? 2 : 1;
+  }
 }
 
 __global__ void coarsen_npv_kernel(int32_t* npv, int n, int limit) {
@@ -500,7 +825,46 @@ extern "C" int tenex_binarize(const float* x, int64_t ldx, int n_vars, int T, in
   if (mode == 2 && !thresholds) return fail(TENEX_ERR_BADARG, "mode 2 needs thresholds");
   if (mode == 1 && (int64_t)T > kMaxPairwiseLen)
     return fail(TENEX_ERR_UNSUPPORTED, "T=%d too long for the mean binariser", T);
+  if (mode == 1 && T <= kSuperLen) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, binarize_mean_kernel, 256, 0);
+    const int grid = (int)std::min<int64_t>(n_vars, (int64_t)std::max(1, sms * per_sm));
+    binarize_mean_kernel<<<grid, 256, 0, as_stream(stream)>>>(x, ldx, T, n_vars, out, ldo,
+                                                              n_per_var);
+    return check_launch("binarize_mean_kernel");
+  }
   binarize_kernel<<<n_vars, 128, 0, as_stream(stream)>>>(x, ldx, T, mode, thresholds, out, ldo,
                                                          n_per_var);
   return check_launch("binarize_kernel");
+}
+
+extern "C" int tenex_binarize_select(const float* x, int64_t ldx, int n_vars, int T, int median,
+                                     double q, uint8_t* out, int64_t ldo, int32_t* n_per_var,
+                                     void* stream) {
+  if (!x || !out || !n_per_var) return fail(TENEX_ERR_BADARG, "x, out, n_per_var non-NULL");
+  if (n_vars < 1 || T < 1) return fail(TENEX_ERR_BADARG, "empty expression matrix");
+  if (ldx < T || ldo < T) return fail(TENEX_ERR_BADARG, "row strides must be >= T");
+  if (!median && !(q >= 0.0 && q <= 1.0))
+    return fail(TENEX_ERR_BADARG, "quantile q must be in [0, 1]");
+  int dev = 0, sms = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  // stage the row in shared memory when it fits and its 16-byte copies are aligned
+  const int64_t staged = (int64_t)kSelectHead + 4 * (int64_t)T;
+  const bool stage = staged <= optin && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
+                     (ldx & 3) == 0;
+  const int smem = stage ? (int)staged : kSelectHead;
+  cudaError_t e = cudaFuncSetAttribute(binarize_select_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return fail(TENEX_ERR_LAUNCH, "binarize_select smem: %s", cudaGetErrorString(e));
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, binarize_select_kernel, kSelectThreads,
+                                                smem);
+  const int grid = (int)std::min<int64_t>(n_vars, (int64_t)std::max(1, sms * per_sm));
+  binarize_select_kernel<<<grid, kSelectThreads, smem, as_stream(stream)>>>(
+      x, ldx, T, n_vars, median ? 1 : 0, q, stage ? 1 : 0, out, ldo, n_per_var);
+  return check_launch("binarize_select_kernel");
 }

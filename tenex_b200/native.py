@@ -82,6 +82,7 @@ _SIGS = {
     "tenex_coarsen": [_P, _L, _I, _L, _P, _I, _P],
     "tenex_coarsen_narrow": [_P, _L, _I, _L, _P, _I, _P, _L, _P],
     "tenex_binarize": [_P, _L, _I, _I, _I, _P, _P, _L, _P, _P],
+    "tenex_binarize_select": [_P, _L, _I, _I, _I, ctypes.c_double, _P, _L, _P, _P],
     "tenex_b2_workspace_bytes": [_I, _L, _L],
     "tenex_te_binary_matrix": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _P],
     "tenex_te_binary_matrix_kind": [_P, _L, _I, _L, _L, _P, _L, _P, _S, _I, _P],

@@ -1,4 +1,6 @@
 """End-to-end engine and preprocessing kernels against the reference goldens / oracle."""
+import warnings
+
 import numpy as np
 import pytest
 import torch
@@ -152,6 +154,64 @@ def test_binarization_routes_to_gemm_b2(cuda, golden, method, q, tag, T):
     assert np.array_equal(b, g[f"{tag}{T}"])
     ref = O.te_matrix(b, np.full(x.shape[0], 2, np.int32))
     assert np.max(np.abs(res.matrix - ref)) <= TOL
+
+
+@pytest.mark.parametrize("n,T", [(3, 1), (3, 7), (5, 8), (5, 9), (40, 128), (40, 129), (40, 1000),
+                                 (2000, 4099), (2000, 20000), (64, 114688), (8, 114689),
+                                 (4, 250000)])
+def test_mean_binarisation_bitexact_vs_numpy(cuda, n, T):
+    """The mean binariser against numpy's float32 np.mean (pairwise sum, float64
+    division) at lengths that reach every leaf shape of the pairwise tree, the
+    persistent plan kernel with more genes than CTAs (n = 2000) and the
+    super-node kernel beyond one plan (T > 114688); NaN / inf rows included."""
+    from tenex_b200.binarize import binarize
+    rng = np.random.default_rng(T)
+    x = (rng.standard_normal((n, T)) * 10.0 ** rng.uniform(-3, 3, (n, 1))).astype(np.float32)
+    x[rng.random((n, T)) < 0.3] = 0
+    x[0] = 1.5                                               # constant row
+    if n > 2:
+        x[1, T // 2] = np.nan
+        x[2, 0] = np.inf
+    db, npv, _, _ = binarize(x, "mean", device=cuda)
+    with np.errstate(invalid="ignore"):
+        ref = (x > np.mean(x, axis=1, keepdims=True)).astype(np.uint8)
+    got = D.to_host(db.unpadded()).reshape(n, T)
+    assert np.array_equal(got, ref)
+    ref_npv = np.where(ref.max(axis=1) != ref.min(axis=1), 2, 1)
+    assert np.array_equal(npv.cpu().numpy(), ref_npv)
+
+
+@pytest.mark.parametrize("n,T", [(4, 1), (4, 2), (6, 7), (40, 400), (40, 401), (2000, 20000),
+                                 (16, 57088), (8, 70000)])
+@pytest.mark.parametrize("method,q", [("median", 0.5), ("quantile", 0.0), ("quantile", 0.25),
+                                      ("quantile", 0.7), ("quantile", 0.999),
+                                      ("quantile", 1.0)])
+def test_select_binarisation_bitexact_vs_numpy(cuda, n, T, method, q):
+    """Median / quantile binarisation against numpy's np.median / np.quantile
+    (the reference's numpy backend): rows staged in shared memory (T a multiple
+    of 4 up to the opt-in size) and read from global memory (odd T, T = 70000),
+    heavy ties (zeros, a few repeated levels), a NaN row (numpy's threshold is
+    NaN: all bins 0), an inf row and a constant row."""
+    from tenex_b200.binarize import binarize
+    rng = np.random.default_rng(T + int(q * 1000))
+    x = (rng.standard_normal((n, T)) * 10.0 ** rng.uniform(-3, 3, (n, 1))).astype(np.float32)
+    x[rng.random((n, T)) < 0.4] = 0
+    x[rng.random((n, T)) < 0.1] = np.float32(2.5)
+    x[0] = -0.0
+    if n > 3:
+        x[1, T // 2] = np.nan
+        x[2, 0] = np.inf
+        x[3, : T // 2] = -np.inf
+    db, npv, _, _ = binarize(x, method, device=cuda, q=q)
+    with np.errstate(invalid="ignore"), warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        thr = (np.median(x, axis=1, keepdims=True) if method == "median"
+               else np.quantile(x, q, axis=1, keepdims=True))
+        ref = (x > thr).astype(np.uint8)
+    got = D.to_host(db.unpadded()).reshape(n, T)
+    assert np.array_equal(got, ref)
+    ref_npv = np.where(ref.max(axis=1) != ref.min(axis=1), 2, 1)
+    assert np.array_equal(npv.cpu().numpy(), ref_npv)
 
 
 def test_source_filter_pair_list(cuda, golden):
