@@ -19,7 +19,11 @@
 //     (G = 1: warp-private histograms for the common small pairs). Counters are
 //     32-bit unless 32-bit slots would need groups of more than 4 warps, then
 //     16-bit halves of a word (N < 65536; two cells per word collide more
-//     often, so packing is the fallback, not the rule). Pairs whose histogram
+//     often, so packing is the fallback, not the rule). Where the item's slots
+//     still fit at that size, table rows get an odd stride in words (b_s | 1,
+//     or the half-word row | 1): rows then start in different banks, so lanes
+//     that share a popular source bin but differ in target state land in
+//     different banks instead of the same one or two. Pairs whose histogram
 //     fits no shared-memory slot (coarsening off) run in a second
 //     instantiation on per-CTA slots in global memory.
 //   * Every sample is one red.shared.add (16 samples per uint4 of source bins).
@@ -268,7 +272,8 @@ __host__ __device__ inline bool in_smem(int64_t bt, int64_t bs, int N, int mbmax
 
 // Per-lane part of sum c3 * log2(c3 * c1 / (c2a * c2b)) over the pair's cells.
 // Cell (z = xt1*bt + xt, y) is tab[z * stride + y] (PACK16: the 16-bit half
-// (y & 1) of word z * stride + (y >> 1), stride = hb). Columns (xt, y) are
+// (y & 1) of word z * stride + (y >> 1)); stride >= the row's words (padding
+// words stay zero). Columns (xt, y) are
 // spread over the group's lanes; CLEAR zeroes every word after reading it.
 // term = c3 * log2(c3 * c1 / (c2a * c2b)), the ratio formed as
 // c3 * (1/c2b) * (c1/c2a) (one reciprocal per column, c1/c2a staged per target)
@@ -280,7 +285,9 @@ __device__ __forceinline__ float entropy_cols(uint32_t* tab, int bt, int bs, int
                                               const int* c1i, const float2* qa, int lane_g,
                                               int gthreads) {
   float acc = 0.f;
-  const int ncy = PACK16 ? stride : bs;
+  // every word of a row, padding included (zero, so skipped by the s == 0 test):
+  // consecutive lanes then read consecutive words, one wavefront per warp
+  const int ncy = stride;
   const int ncols = bt * ncy;
   for (int col = lane_g; col < ncols; col += gthreads) {
     const int j = col / ncy;
@@ -329,10 +336,10 @@ template <bool CLEAR>
 __device__ double entropy_cols_f64(uint32_t* tab, int bt, int bs, int stride, const int* c1i,
                                    const int* c2ai, int lane_g, int gthreads) {
   double acc = 0.0;
-  const int ncols = bt * bs;
+  const int ncols = bt * stride;  // padding words included, as in entropy_cols
   for (int col = lane_g; col < ncols; col += gthreads) {
-    const int j = col / bs;
-    const int y = col - j * bs;
+    const int j = col / stride;
+    const int y = col - j * stride;
     uint64_t s = 0;
     for (int i = 0; i < bt; ++i) s += tab[(i * bt + j) * stride + y];
     if (s == 0u) continue;
@@ -362,7 +369,17 @@ struct ItemCtx {
   const float2* qa;
   double* red;
   int slot_region;    // shared-memory slot region (overflow split rule)
+  bool pad;           // table rows at an odd stride (row words | 1)
 };
+
+// Words per table row: b_s (32-bit counters) or (b_s + 1) / 2 (16-bit halves),
+// made odd when the item's slots were carved at the padded size.
+// The global-memory overflow launch never pads (its slots are sized b_max^3).
+template <int MODE>
+__device__ __forceinline__ uint32_t row_words(uint32_t bs, bool pad) {
+  const uint32_t w = MODE == kSlot16 ? (bs + 1) >> 1 : bs;
+  return (MODE != kGmem && pad) ? (w | 1u) : w;
+}
 
 // Source r of the item for this launch: its id and pair id, or false if the
 // pair is not this launch's (the target itself, outside [p0, p1), or, with an
@@ -445,10 +462,9 @@ __device__ __forceinline__ void finish_pair(const TeParams& P, const ItemCtx& it
   const int bt2 = bt * bt;
   const int bs = P.npv[src];
   constexpr bool PACK16 = MODE == kSlot16;
-  const int hb = PACK16 ? (bs + 1) >> 1 : bs;
   group_sync(G, g, gthreads);
   uint32_t* tab = slot;  // counts read by the entropy pass
-  const int stride = PACK16 ? hb : bs;
+  const int stride = (int)row_words<MODE>((uint32_t)bs, it.pad);
 
   // -- optional raw-count export (parity checks only) --------------------
   if (P.counts_dbg != nullptr) {
@@ -456,7 +472,8 @@ __device__ __forceinline__ void finish_pair(const TeParams& P, const ItemCtx& it
     const int ncell = bt2 * bs;
     for (int c = lane_g; c < ncell; c += gthreads) {
       const int z = c / bs, y = c - z * bs;
-      cd[c] = (int32_t)(PACK16 ? cell_get<true>(tab, z, y, bs, hb) : tab[z * stride + y]);
+      cd[c] = (int32_t)(PACK16 ? cell_get<true>(tab, z, y, stride, stride)
+                               : tab[z * stride + y]);
     }
     group_sync(G, g, gthreads);
   }
@@ -554,10 +571,9 @@ __device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it
       // behind the histogram pass instead of stalling the epilogue
       float obs_m = 0.f;
       if (P.out_mode == kOutStats && lane_g == 0) obs_m = __ldg(P.obs + (int64_t)src * P.n + it.tgt);
-      const uint32_t bs = (uint32_t)P.npv[src];
-      const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
+      const uint32_t rw = row_words<MODE>((uint32_t)P.npv[src], it.pad);
       hist_source<MODE>(slot_addr, it.zsm, it.z8, P.bins + (int64_t)src * P.ld, N, lane_g,
-                        gthreads, bs, hb);
+                        gthreads, rw, rw);
       finish_pair<MODE>(P, it, slot, G, g, lane_g, tid, warp, src, p, obs_m);
     }
     return;
@@ -570,15 +586,14 @@ __device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it
     float obs_m = 0.f;
     if (act && P.out_mode == kOutStats && lane_g == 0)
       obs_m = __ldg(P.obs + (int64_t)src * P.n + it.tgt);
-    const uint32_t bs = act ? (uint32_t)P.npv[src] : 1u;
-    const uint32_t hb = PACK16 ? (bs + 1) >> 1 : bs;
+    const uint32_t rw = row_words<MODE>(act ? (uint32_t)P.npv[src] : 1u, it.pad);
     const uint8_t* srow = P.bins + (int64_t)src * P.ld;
     for (int s0 = 0; s0 < N; s0 += P.ztile) {
       const int n = min(P.ztile, N - s0);
       __syncthreads();  // every group is done with the previous tile
       stage_z<false>(trow, P.lag, it.bt, it.z8, s0, n, zsm, nullptr, tid, nthreads);
       __syncthreads();
-      if (act) hist_source<MODE>(slot_addr, zsm, it.z8, srow + s0, n, lane_g, gthreads, bs, hb);
+      if (act) hist_source<MODE>(slot_addr, zsm, it.z8, srow + s0, n, lane_g, gthreads, rw, rw);
     }
     if (act) finish_pair<MODE>(P, it, slot, G, g, lane_g, tid, warp, src, p, obs_m);
   }
@@ -746,7 +761,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     const int fit16 = GMEM ? 0 : slot_region / (words16 * 4);
     const bool pack16 = !GMEM && (N < 65536) && fit32 * 4 < n_warps && fit16 >= 1;
     const int fit = pack16 ? fit16 : fit32;
-    const int slot_words = pack16 ? words16 : words32;
+    int slot_words = pack16 ? words16 : words32;
     if (fit < 1) {
       if (tid == 0) atomicExch(&P.ws->bad_item, 1);
       __syncthreads();
@@ -756,6 +771,17 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     while (n_warps / G > fit) G <<= 1;
     while (G > 1 && G < n_warps && n_warps / G > 15) G <<= 1;
     const int n_groups = n_warps / G;
+    // odd row stride where the same groups' slots still fit at the padded size
+    // (the group size and the counter width stay as chosen above)
+    bool pad = false;
+    if (!GMEM) {
+      const int64_t rw = pack16 ? ((((int64_t)bsmax + 1) >> 1) | 1) : ((int64_t)bsmax | 1);
+      const int padded = (int)round_up((int64_t)bt2 * rw, 4);
+      if ((int64_t)n_groups * padded * 4 <= slot_region) {
+        slot_words = padded;
+        pad = true;
+      }
+    }
     const int g = warp / G;
     const int lane_g = tid - g * G * 32;
     uint32_t* slot = GMEM ? gslot : slots + (int64_t)g * slot_words;
@@ -781,6 +807,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     it.qa = qa;
     it.red = red;
     it.slot_region = slot_region;
+    it.pad = pad;
     if (GMEM)
       run_sources<kGmem>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
     else if (pack16)
