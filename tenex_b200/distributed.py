@@ -20,7 +20,8 @@ with the single-GPU kernels, and the chunks are assembled by one collective:
     float64 sum / sum of squares and the int32 count_ge.
 
 No kernel here waits on another rank's memory; the only cross-GPU traffic is
-the NCCL broadcast and all-gather.
+the NCCL broadcast and all-gather. Under a gloo process group (CUDA broadcast
+supported, CUDA all-gather not) the all-gather goes through host memory.
 """
 from __future__ import annotations
 
@@ -110,11 +111,15 @@ def gather_pairfree(local: torch.Tensor, n_pairs: int, group=None) -> torch.Tens
     if world == 1:
         return local
     chunk = pair_range(n_pairs, 0, world)[1]
-    send = torch.zeros(chunk, dtype=local.dtype, device=local.device)
+    # NCCL gathers device tensors in place; gloo gathers host tensors only, so
+    # with gloo the chunks go through host memory and the result comes back
+    stage = local.is_cuda and dist.get_backend(group) != "nccl"
+    where = torch.device("cpu") if stage else local.device
+    send = torch.zeros(chunk, dtype=local.dtype, device=where)
     send[:p1 - p0] = local
-    full = torch.empty(chunk * world, dtype=local.dtype, device=local.device)
+    full = torch.empty(chunk * world, dtype=local.dtype, device=where)
     dist.all_gather_into_tensor(full, send, group=group)
-    return full[:n_pairs]
+    return full[:n_pairs].to(local.device) if stage else full[:n_pairs]
 
 
 def assemble_matrices(*mats: torch.Tensor, group=None) -> None:
