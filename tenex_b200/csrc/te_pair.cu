@@ -189,6 +189,38 @@ __device__ __forceinline__ void hist16_z8(uint64_t slot, uint4 yv, uint4 zv, uin
   }
 }
 
+// Same for a group whose target states were sorted at staging (sort_state_groups):
+// zv holds the states in ascending order and pm the sample each came from (nibble
+// j: original position of sorted entry j), so the source's 16 bytes are put in
+// the same order with three byte permutes per four samples. At each step the
+// warp's lanes then hold states of similar rank, whose cells spread over fewer
+// distinct words per bank than cells of unrelated states. The counts do not
+// depend on the order of the samples.
+template <int MODE>
+__device__ __forceinline__ void hist16_z8_sorted(uint64_t slot, uint4 yv, uint4 zv, uint2 pm,
+                                                 uint32_t bs, uint32_t hb) {
+  const uint32_t zs[4] = {zv.x, zv.y, zv.z, zv.w};
+  uint32_t ys[4];
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    const uint32_t nib = ((w < 2 ? pm.x : pm.y) >> (16 * (w & 1))) & 0xffffu;
+    const uint32_t sa = nib & 0x7777u;                   // byte within 8 of the pair
+    const uint32_t sb = 0x3210u | ((nib & 0x8888u) >> 1);  // low (i) or high (i + 4) pair
+    const uint32_t lo = __byte_perm(yv.x, yv.y, sa);
+    const uint32_t hi = __byte_perm(yv.z, yv.w, sa);
+    ys[w] = __byte_perm(lo, hi, sb);
+  }
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const uint32_t y = __byte_perm(ys[w], 0, 0x4440 + b);
+      const uint32_t z = __byte_perm(zs[w], 0, 0x4440 + b);
+      hist_add<MODE>(slot, z, y, bs, hb);
+    }
+  }
+}
+
 template <int MODE>
 __device__ __forceinline__ void hist16_z16(uint64_t slot, uint4 yv, uint4 za, uint4 zb,
                                            uint32_t bs, uint32_t hb) {
@@ -210,14 +242,23 @@ __device__ __forceinline__ void hist16_z16(uint64_t slot, uint4 yv, uint4 za, ui
 // lanes): zsm[i] is the target state of sample i of srow (both 16-byte aligned).
 template <int MODE>
 __device__ __forceinline__ void hist_source(uint64_t slot32, const unsigned char* zsm, bool z8,
-                                            const uint8_t* srow, int n, int lane_g,
-                                            int gthreads, uint32_t bs, uint32_t hb) {
+                                            const uint2* zperm, const uint8_t* srow, int n,
+                                            int lane_g, int gthreads, uint32_t bs, uint32_t hb) {
   const int nvec = n >> 4;
   const uint4* yv = reinterpret_cast<const uint4*>(srow);
   const uint4* zv = reinterpret_cast<const uint4*>(zsm);
   int v = lane_g;
   if (z8) {
-    if (v < nvec) {
+    if (v < nvec && zperm != nullptr) {
+      uint4 ycur = dev::ldg_nc_v4(yv + v);
+      for (; v < nvec; v += gthreads) {
+        const int vn = v + gthreads;
+        uint4 ynext = ycur;
+        if (vn < nvec) ynext = dev::ldg_nc_v4(yv + vn);
+        hist16_z8_sorted<MODE>(slot32, ycur, zv[v], zperm[v], bs, hb);
+        ycur = ynext;
+      }
+    } else if (v < nvec) {
       uint4 ycur = dev::ldg_nc_v4(yv + v);
       for (; v < nvec; v += gthreads) {
         const int vn = v + gthreads;
@@ -370,6 +411,7 @@ struct ItemCtx {
   double* red;
   int slot_region;    // shared-memory slot region (overflow split rule)
   bool pad;           // table rows at an odd stride (row words | 1)
+  const uint2* zperm; // sorted 16-sample groups of 1-byte states, or nullptr
 };
 
 // Words per table row: b_s (32-bit counters) or (b_s + 1) / 2 (16-bit halves),
@@ -531,6 +573,48 @@ __device__ __forceinline__ uint64_t table_addr(uint32_t* slot, int tid) {
 
 // Stages target states of samples [s0, s0 + n) into zsm (all CTA threads);
 // COUNT also adds them to the c2a counts.
+// Sorts every full 16-sample group of 1-byte target states in place (ascending,
+// ties by position) and records in perm[v] where each sorted entry came from
+// (nibble j = original position of entry j). One thread per group: a bitonic
+// network on keys state << 4 | position, in registers.
+__device__ __forceinline__ void sort_state_groups(unsigned char* zsm, uint2* perm, int nvec,
+                                                  int tid, int nthreads) {
+  uint4* zv = reinterpret_cast<uint4*>(zsm);
+  for (int v = tid; v < nvec; v += nthreads) {
+    const uint4 q = zv[v];
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+    uint32_t k[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) k[i] = (((w[i >> 2] >> (8 * (i & 3))) & 0xffu) << 4) | i;
+#pragma unroll
+    for (int size = 2; size <= 16; size <<= 1) {
+#pragma unroll
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int j = i ^ stride;
+          if (j > i) {
+            const uint32_t a = k[i], b = k[j];
+            const uint32_t lo = min(a, b), hi = max(a, b);
+            const bool up = (i & size) == 0;
+            k[i] = up ? lo : hi;
+            k[j] = up ? hi : lo;
+          }
+        }
+      }
+    }
+    uint32_t o[4] = {0u, 0u, 0u, 0u}, p0 = 0u, p1 = 0u;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      o[i >> 2] |= (k[i] >> 4) << (8 * (i & 3));
+      if (i < 8) p0 |= (k[i] & 15u) << (4 * i);
+      else p1 |= (k[i] & 15u) << (4 * (i - 8));
+    }
+    zv[v] = make_uint4(o[0], o[1], o[2], o[3]);
+    perm[v] = make_uint2(p0, p1);
+  }
+}
+
 template <bool COUNT>
 __device__ __forceinline__ void stage_z(const uint8_t* trow, int lag, int bt, bool z8, int s0,
                                         int n, unsigned char* zsm, int* c2ai, int tid,
@@ -560,7 +644,6 @@ __device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it
                                             int lane_g, int tid, int warp, int nthreads) {
   const int gthreads = G * 32;
   const int N = P.N;
-  constexpr bool PACK16 = MODE == kSlot16;
   const uint64_t slot_addr = table_addr<MODE>(slot, tid);
   if (P.ztile >= N) {
     for (int r = g; r < it.n_src; r += n_groups) {
@@ -572,8 +655,8 @@ __device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it
       float obs_m = 0.f;
       if (P.out_mode == kOutStats && lane_g == 0) obs_m = __ldg(P.obs + (int64_t)src * P.n + it.tgt);
       const uint32_t rw = row_words<MODE>((uint32_t)P.npv[src], it.pad);
-      hist_source<MODE>(slot_addr, it.zsm, it.z8, P.bins + (int64_t)src * P.ld, N, lane_g,
-                        gthreads, rw, rw);
+      hist_source<MODE>(slot_addr, it.zsm, it.z8, it.zperm, P.bins + (int64_t)src * P.ld, N,
+                        lane_g, gthreads, rw, rw);
       finish_pair<MODE>(P, it, slot, G, g, lane_g, tid, warp, src, p, obs_m);
     }
     return;
@@ -593,7 +676,8 @@ __device__ __forceinline__ void run_sources(const TeParams& P, const ItemCtx& it
       __syncthreads();  // every group is done with the previous tile
       stage_z<false>(trow, P.lag, it.bt, it.z8, s0, n, zsm, nullptr, tid, nthreads);
       __syncthreads();
-      if (act) hist_source<MODE>(slot_addr, zsm, it.z8, srow + s0, n, lane_g, gthreads, rw, rw);
+      if (act)
+        hist_source<MODE>(slot_addr, zsm, it.z8, nullptr, srow + s0, n, lane_g, gthreads, rw, rw);
     }
     if (act) finish_pair<MODE>(P, it, slot, G, g, lane_g, tid, warp, src, p, obs_m);
   }
@@ -746,6 +830,17 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
         atomicAdd(&c2ai[(uint32_t)trow[s + P.lag] * bt + trow[s]], 1);
     }
     __syncthreads();
+    // 1-byte states of a whole staged series in a region sized for 2-byte ones:
+    // the spare half holds the permutation of each 16-sample group sorted by
+    // state (the shared-memory launch only; the overflow launch's entropy pass
+    // pairs zsm[s] with sample s of the source)
+    const uint2* zperm = nullptr;
+    if (!GMEM && z8 && !tiled && P.zbytes == 2 && N >= 16) {
+      uint2* pm = reinterpret_cast<uint2*>(zsm + round_up((int64_t)N, 16));
+      sort_state_groups(zsm, pm, N >> 4, tid, nthreads);
+      zperm = pm;
+      __syncthreads();
+    }
     const int bsmax = misc[1];
     for (int j = tid; j < bt; j += nthreads) {
       int s = 0;
@@ -808,6 +903,7 @@ __global__ void __launch_bounds__(1024, 1) te_pair_tile_kernel(TeParams P) {
     it.red = red;
     it.slot_region = slot_region;
     it.pad = pad;
+    it.zperm = zperm;
     if (GMEM)
       run_sources<kGmem>(P, it, slot, zsm, G, g, n_groups, lane_g, tid, warp, nthreads);
     else if (pack16)
